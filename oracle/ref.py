@@ -1,0 +1,167 @@
+"""ctypes binding to oracle/_ref/libpigfem_ref.so: the reference PIGFEM's own C++ assembly,
+compiled from its sources against project-written serial shims (oracle/Makefile).
+
+TEST INFRASTRUCTURE ONLY.  Imported by tests/, by __graft_entry__.smoke() and by bench.py's
+CPU-baseline leg, never by the product package.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libpigfem_ref.so")
+
+COH_NONE, COH_BL, COH_BLNU, COH_XN, COH_XNNU, COH_OP, COH_OPNU, COH_OPAUG, COH_OPNUAUG = range(9)
+TRI3, QUAD4, TET4 = 0, 1, 2
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [
+        ("elem_type", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("xmin", ctypes.c_double), ("xmax", ctypes.c_double), ("ymin", ctypes.c_double),
+        ("ymax", ctypes.c_double), ("zmin", ctypes.c_double), ("zmax", ctypes.c_double),
+        ("n_incl", ctypes.c_int), ("incl", ctypes.POINTER(ctypes.c_double)),
+        ("E_matrix", ctypes.c_double), ("nu_matrix", ctypes.c_double),
+        ("E_fiber", ctypes.c_double), ("nu_fiber", ctypes.c_double),
+        ("coh_law", ctypes.c_int), ("coh", ctypes.c_double * 4),
+        ("plane_strain", ctypes.c_int), ("subscale", ctypes.c_int),
+        ("eps_macro", ctypes.c_double * 6), ("app_strain", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(f"oracle library not built: {LIB_PATH} (run `make -C oracle`)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.pgref_create.restype = ctypes.c_void_p
+        L.pgref_create.argtypes = [ctypes.POINTER(_Config)]
+        L.pgref_assemble.restype = ctypes.c_double
+        L.pgref_assemble.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                     ctypes.c_int, ctypes.c_int]
+        L.pgref_time_assemble.restype = ctypes.c_double
+        L.pgref_time_assemble.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.pgref_solve.restype = ctypes.c_int
+        L.pgref_solve.argtypes = [ctypes.c_void_p]
+        L.pgref_set_solver.restype = None
+        L.pgref_set_solver.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 5 + [ctypes.c_int]
+        L.pgref_get.restype = ctypes.c_int
+        L.pgref_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_long),
+                                ctypes.POINTER(ctypes.c_void_p)]
+        L.pgref_destroy.restype = None
+        L.pgref_destroy.argtypes = [ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+@dataclass
+class ProblemSpec:
+    """A problem as the reference's Tests/Main.cpp builds it (structured mesh + inclusions)."""
+    elem_type: int = TRI3
+    n: Sequence[int] = (8, 8)
+    lo: Sequence[float] = (0.0, 0.0)
+    hi: Sequence[float] = (1.0, 1.0)
+    inclusions: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    E_matrix: float = 3.5e3
+    nu_matrix: float = 0.35
+    E_fiber: float = 72e3
+    nu_fiber: float = 0.22
+    coh_law: int = COH_NONE
+    coh: Sequence[float] = (0.0, 0.0, 0.0, 0.0)
+    plane_strain: bool = True
+    subscale: bool = False
+    eps_macro: Sequence[float] = (0.0,) * 6
+    app_strain: float = 0.01
+
+
+class RefProblem:
+    def __init__(self, spec: ProblemSpec):
+        L = lib()
+        self.spec = spec
+        dim = 3 if spec.elem_type == TET4 else 2
+        self.dim = dim
+        self._incl = np.ascontiguousarray(np.asarray(spec.inclusions, dtype=np.float64).reshape(-1, dim + 1))
+        c = _Config()
+        c.elem_type = spec.elem_type
+        n = list(spec.n) + [0] * (3 - len(spec.n))
+        lo = list(spec.lo) + [0.0] * (3 - len(spec.lo))
+        hi = list(spec.hi) + [0.0] * (3 - len(spec.hi))
+        c.nx, c.ny, c.nz = n[:3]
+        c.xmin, c.ymin, c.zmin = lo[:3]
+        c.xmax, c.ymax, c.zmax = hi[:3]
+        c.n_incl = self._incl.shape[0]
+        c.incl = self._incl.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        c.E_matrix, c.nu_matrix, c.E_fiber, c.nu_fiber = spec.E_matrix, spec.nu_matrix, spec.E_fiber, spec.nu_fiber
+        c.coh_law = spec.coh_law
+        for i, v in enumerate(spec.coh):
+            c.coh[i] = v
+        c.plane_strain = int(spec.plane_strain)
+        c.subscale = int(spec.subscale)
+        for i, v in enumerate(spec.eps_macro):
+            c.eps_macro[i] = v
+        c.app_strain = spec.app_strain
+        self._cfg = c
+        self.h = L.pgref_create(ctypes.byref(c))
+        nfc = self.get("n_free_const")
+        self.n_free, self.n_const = int(nfc[0]), int(nfc[1])
+
+    def get(self, name: str) -> np.ndarray:
+        n = ctypes.c_long(0)
+        p = ctypes.c_void_p(0)
+        kind = lib().pgref_get(self.h, name.encode(), ctypes.byref(n), ctypes.byref(p))
+        if kind == 0:
+            raise KeyError(name)
+        if n.value == 0:
+            return np.zeros(0, dtype=np.int32 if kind == 1 else np.float64)
+        ct = ctypes.c_int32 if kind == 1 else ctypes.c_double
+        arr = np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ct)), shape=(n.value,))
+        return arr.copy()
+
+    def csr(self, block: str):
+        rp, ci, v = self.get(f"{block}_rowptr"), self.get(f"{block}_cols"), self.get(f"{block}_vals")
+        shape = tuple(int(s) for s in self.get(f"{block}_shape"))
+        return rp, ci, v, shape
+
+    def assemble(self, U: np.ndarray, isv_committed: np.ndarray | None = None, t_frac: float = 1.0,
+                 func: bool = True, jac: bool = True) -> float:
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        assert U.shape == (self.n_free + self.n_const,)
+        iv = None
+        if isv_committed is not None:
+            isv_committed = np.ascontiguousarray(isv_committed, dtype=np.float64)
+            iv = isv_committed.ctypes.data
+        return lib().pgref_assemble(self.h, U.ctypes.data, iv, t_frac, int(func), int(jac))
+
+    def time_assemble(self, n_rep: int) -> float:
+        return lib().pgref_time_assemble(self.h, n_rep)
+
+    def set_solver(self, rel_tol=1e-8, abs_tol=1e-8, max_dt=1e-2, min_dt=1e-5, T_final=1.0, max_iter=25):
+        lib().pgref_set_solver(self.h, rel_tol, abs_tol, max_dt, min_dt, T_final, max_iter)
+
+    def solve(self) -> str:
+        lib().pgref_solve(self.h)
+        return bytes(self.get("log").astype(np.uint8)).decode(errors="replace")
+
+    def close(self):
+        if self.h:
+            lib().pgref_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
