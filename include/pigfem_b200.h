@@ -1,0 +1,130 @@
+/*
+ * pigfem_b200.h -- C ABI of the B200 finite-element assembly path (libpigfem_b200.so).
+ *
+ * The reference's boundary for this path is
+ *     PetscErrorCode Assembler::assemble(pmatrix& K, pvector& P_int, double delta_t,
+ *                                        std::vector<std::vector<std::vector<double>>>& update_ISVs,
+ *                                        NodalData* solution, bool assembleFunc, bool assembleJac)
+ * (include/Assembler.h:46-48, src/Assembler.cpp:65-146), reached by every solver through a
+ * non-virtual call.  The entry points below are what a host-side Assembler translation unit
+ * forwards to; see INTEGRATION.md for the binding.  Plain pointers and sizes only; every call
+ * returns 0 on success or one of the PG_ERR_* codes (never exits, never traps), with a message
+ * available from pg_last_error().
+ */
+#ifndef PIGFEM_B200_H_
+#define PIGFEM_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PG_OK 0
+#define PG_ERR_INPUT 2        /* invalid description or argument */
+#define PG_ERR_GEOMETRY 3     /* a node on an inclusion surface, a missing intersection, ... */
+#define PG_ERR_UNSUPPORTED 4  /* a cut case outside the tables (the reference stops there too) */
+#define PG_ERR_JACOBIAN 7     /* negative (sub-)element Jacobian */
+#define PG_ERR_DEVICE 10      /* CUDA error or out of device memory */
+#define PG_ERR_NONFINITE 11   /* a NaN/Inf produced in K or R */
+#define PG_ERR_STATE 12       /* call out of order */
+
+/* assembly flags */
+#define PG_FUNC 1   /* assemble the internal-force vector P_int (assembleFunc) */
+#define PG_JAC 2    /* assemble the stiffness K (assembleJac) */
+#define PG_FP32 4   /* FP32-mixed element integration (FP64 accumulation in the scatter) */
+
+/* background element types (Mesh::generate_mesh element types used by the reference drivers) */
+#define PG_TRI3 0
+#define PG_QUAD4 1
+#define PG_TET4 2
+
+/* cohesive laws: bilinear, Xu-Needleman, Ortiz-Pandolfi (plain, no-unloading "NU", augmented "AUG") */
+#define PG_COH_NONE 0
+#define PG_COH_BL 1
+#define PG_COH_BLNU 2
+#define PG_COH_XN 3
+#define PG_COH_XNNU 4
+#define PG_COH_OP 5
+#define PG_COH_OPNU 6
+#define PG_COH_OPAUG 7
+#define PG_COH_OPNUAUG 8
+
+typedef struct pg_ctx pg_ctx;
+
+/* Problem description: the inputs Tests/Main.cpp:150-648 gives Mesh / Problem / BoundaryObject. */
+typedef struct {
+  int32_t elem_type;            /* PG_TRI3, PG_QUAD4 or PG_TET4 */
+  int32_t n[3];                 /* elements per direction (n[2] = 0 in 2D) */
+  double lo[3], hi[3];          /* domain box */
+  int32_t n_incl;               /* number of circles (2D) or spheres (3D) */
+  const double* incl;           /* circles: cx, cy, r; spheres: cx, cy, cz, r */
+  double E_matrix, nu_matrix, E_fiber, nu_fiber;
+  int32_t coh_law;              /* PG_COH_*; applied to every fiber/matrix interface */
+  double coh[4];                /* BL: sigma_c, delta_c1, delta_c2; XN: sigma_c, delta_cn, delta_ct, q; OP: sigma_c, delta_c, beta */
+  int32_t plane_strain;
+  int32_t subscale;             /* 1: periodic mesh, macroscale strain eps_macro, node 0 pinned */
+  double eps_macro[6];          /* Voigt (xx, yy, xy) or (xx, yy, zz, yz, xz, xy), engineering shear */
+  double app_strain;            /* Dirichlet mode: u_x = app_strain * (hi[0]-lo[0]) on the right, 0 on the left, node 0 pinned */
+} pg_problem_desc;
+
+typedef struct {
+  int32_t dim, n_nodes, n_std_nodes, n_enrich_nodes, n_elem, n_cut_elem, n_coh_elem, n_coh_qp;
+  int32_t n_free, n_const, n_isv;
+  int64_t nnz[4];               /* K_ff, K_fp, K_pf, K_pp */
+  int64_t cut_scratch_doubles;  /* element-matrix scratch the cut-element kernel uses */
+} pg_sizes;
+
+/* Set-up: Problem::init + Problem::setup equivalent (src/Problem.cpp:100-339): IGFEM detection,
+ * enrichment, sub-element quadrature, DOF numbering, CSR preallocation; uploads to the device. */
+int pg_create(const pg_problem_desc* desc, pg_ctx** out);
+/* The two halves of pg_create: the host set-up alone (no device needed; pattern, nodes and
+ * set-up tables can be read back) and the upload that makes the context assemble-ready. */
+int pg_create_host(const pg_problem_desc* desc, pg_ctx** out);
+int pg_upload(pg_ctx* ctx);
+/* Read-only view of a set-up table by name (cut-element quadrature, topology); returns 1 for
+ * int32, 2 for float64, 0 for an unknown name.  For tests and tools. */
+int pg_debug_array(const pg_ctx* ctx, const char* name, int64_t* n, const void** ptr);
+void pg_destroy(pg_ctx* ctx);
+const char* pg_last_error(const pg_ctx* ctx);
+int pg_get_sizes(const pg_ctx* ctx, pg_sizes* out);
+
+/* CSR pattern of block b (0 ff, 1 fp, 2 pf, 3 pp): rowptr[nrows+1], cols[nnz]. */
+int pg_get_pattern(const pg_ctx* ctx, int block, int32_t* rowptr, int32_t* cols);
+/* Node coordinates (n_nodes*dim), node-major DOF map (n_nodes*dim), prescribed values of the
+ * constrained DOFs at load fraction 1 (n_const). */
+int pg_get_nodes(const pg_ctx* ctx, double* coords, int32_t* node_dofs, double* dirichlet);
+
+/* Assembler::assemble.  U_node_major: displacement of every node (standard then enrichment),
+ * n_nodes*dim, the reference's NodalData layout, in HOST memory.  t_frac scales eps_macro for
+ * subscale problems (Assembler::assemble_new_load_step).  Outputs (host, may be NULL to skip):
+ * the four K blocks' values in pattern order and P_f (n_free), P_p (n_const).  Internal variables:
+ * trial = committed, updated by the cohesive laws (read with pg_get_isv). */
+int pg_assemble(pg_ctx* ctx, const double* U_node_major, double t_frac, int flags,
+                double* K_ff, double* K_fp, double* K_pf, double* K_pp, double* P_f, double* P_p);
+/* Same, on device-resident data: d_U is a device pointer (n_nodes*dim); results stay in the
+ * context's device buffers (pg_device_outputs). */
+int pg_assemble_device(pg_ctx* ctx, const double* d_U, double t_frac, int flags);
+/* Device pointers of the outputs: K values (4 blocks), P_f, P_p. */
+int pg_device_outputs(pg_ctx* ctx, double** K_vals4, double** P_f, double** P_p);
+/* Stream the context launches on (a cudaStream_t, 0 = legacy default). */
+int pg_set_stream(pg_ctx* ctx, void* stream);
+
+/* Internal variables (InternalVars): committed <- values; read trial or committed; commit
+ * (InternalVars::copy_data_in after a converged load step). */
+int pg_set_isv(pg_ctx* ctx, const double* committed);
+int pg_get_isv(const pg_ctx* ctx, int trial, double* out);
+int pg_commit_isv(pg_ctx* ctx);
+/* Damage zone of every cohesive quadrature point from the last assembly
+ * (0 compression, 1 before the peak, 2 softening, 3 failed). */
+int pg_get_damage_zones(const pg_ctx* ctx, uint8_t* zones);
+
+/* Residual norm ||F_ext,f - P_f||_2 on the device in FP64 with a fixed-order reduction
+ * (SolverNonlinearKSP.cpp:81-84); F_ext is zero for the reference's drivers. */
+int pg_residual_norm(pg_ctx* ctx, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PIGFEM_B200_H_ */

@@ -67,6 +67,8 @@
 #include "InclusionCircle.h"
 #include "InclusionSphere.h"
 #include "Options.h"
+#include "Utilities.h"
+#include "CohesiveElem.h"
 #include "pgshim_objects.h"
 #undef protected
 #undef private
@@ -436,6 +438,35 @@ double pgref_assemble(void* vh, const double* U, const double* isv_committed, do
   export_vec(h, "P_p", s->_P_int.p);
   Export& it = put_d(h, "isv_trial");
   for (auto& e : trial) for (auto& q : e) for (double v : q) it.f64.push_back(v);
+  // Damage zone of every cohesive quadrature point (Material::get_cohesive_damage_zone on the
+  // opening ProblemUtilities::cohesiveDeltaFast forms), in element / cohesive element / qp order.
+  Export& zones = put_i(h, "coh_zone");
+  Mesh* mesh = h->mesh;
+  const id_type nndof = h->prob->get_dofs()->nndof();
+  if (mesh->is_cohesive()) {
+    for (Mesh::element_iterator eit = mesh->active_elements_begin(); eit != mesh->active_elements_end(); ++eit) {
+      Elem* el = *eit;
+      if (!el->is_intersected()) continue;
+      id_type l_elem = mesh->global_to_local_elem(el->get_id());
+      std::vector<double> elem_U;
+      ProblemUtilities::formElementalVector(elem_U, el, h->prob->get_solution());
+      std::vector<std::vector<short_id_type>>& cs = el->getCohesiveElemStructure();
+      id_type curr_qp = mesh->n_volumetric_qps(l_elem);
+      for (id_type ce = 0; ce < el->n_cohesive_elem(); ++ce) {
+        CohesiveElem* coh_el = el->get_cohesive_elem(ce);
+        std::vector<double> cu(coh_el->n_nodes() * nndof);
+        for (id_type n = 0; n < coh_el->n_nodes(); ++n)
+          for (id_type d = 0; d < nndof; ++d) cu[n * nndof + d] = elem_U[cs[ce][n] * nndof + d];
+        Material* mat = el->get_cohesive_material(ce);
+        for (id_type q = 0; q < coh_el->n_q_points(); ++q) {
+          std::vector<double> delta;
+          ProblemUtilities::cohesiveDeltaFast(delta, mesh->get_shape(l_elem, curr_qp), cu, mesh->get_rot_matrix(l_elem, curr_qp));
+          zones.i32.push_back((int)mat->get_cohesive_damage_zone(delta));
+          curr_qp++;
+        }
+      }
+    }
+  }
   return std::chrono::duration<double>(t1 - t0).count();
 }
 

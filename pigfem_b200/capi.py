@@ -1,0 +1,286 @@
+"""ctypes binding of the C ABI in include/pigfem_b200.h (libpigfem_b200.so).
+
+:class:`Problem` is the host-side mirror of the reference's ``Problem`` + ``Assembler`` pair for
+the assembly path: it builds the enriched mesh (``Problem::init`` / ``Problem::setup``), then
+``assemble`` is ``Assembler::assemble`` (src/Assembler.cpp:65-146) with the same argument meaning:
+the nodal displacement field in, the four stiffness blocks K_ff / K_fp / K_pf / K_pp and the two
+internal-force parts P_f / P_p out, with the trial internal variables updated from the committed
+ones.  Errors raise :class:`PigfemError` carrying the library's status code and message (the
+reference prints and exits instead; src/common.h:292-297).
+
+The library is required: there is no CPU fallback.  Loading fails loudly when the CUDA library
+has not been built (``python -c "import __graft_entry__ as g; g.build()"``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libpigfem_b200.so")
+
+TRI3, QUAD4, TET4 = 0, 1, 2
+COH_NONE, COH_BL, COH_BLNU, COH_XN, COH_XNNU, COH_OP, COH_OPNU, COH_OPAUG, COH_OPNUAUG = range(9)
+FUNC, JAC, FP32 = 1, 2, 4
+ERRORS = {2: "PG_ERR_INPUT", 3: "PG_ERR_GEOMETRY", 4: "PG_ERR_UNSUPPORTED", 7: "PG_ERR_JACOBIAN",
+          10: "PG_ERR_DEVICE", 11: "PG_ERR_NONFINITE", 12: "PG_ERR_STATE"}
+
+# Every symbol include/pigfem_b200.h declares.
+EXPORTED = [
+    "pg_create", "pg_create_host", "pg_upload", "pg_debug_array", "pg_destroy", "pg_last_error",
+    "pg_get_sizes", "pg_get_pattern", "pg_get_nodes", "pg_assemble", "pg_assemble_device",
+    "pg_device_outputs", "pg_set_stream", "pg_set_isv", "pg_get_isv", "pg_commit_isv",
+    "pg_get_damage_zones", "pg_residual_norm",
+]
+
+
+class PigfemError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class _Desc(ctypes.Structure):
+    _fields_ = [
+        ("elem_type", ctypes.c_int32), ("n", ctypes.c_int32 * 3), ("lo", ctypes.c_double * 3),
+        ("hi", ctypes.c_double * 3), ("n_incl", ctypes.c_int32), ("incl", ctypes.POINTER(ctypes.c_double)),
+        ("E_matrix", ctypes.c_double), ("nu_matrix", ctypes.c_double), ("E_fiber", ctypes.c_double),
+        ("nu_fiber", ctypes.c_double), ("coh_law", ctypes.c_int32), ("coh", ctypes.c_double * 4),
+        ("plane_strain", ctypes.c_int32), ("subscale", ctypes.c_int32), ("eps_macro", ctypes.c_double * 6),
+        ("app_strain", ctypes.c_double),
+    ]
+
+
+class _Sizes(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int32) for k in ("dim", "n_nodes", "n_std_nodes", "n_enrich_nodes", "n_elem",
+                                              "n_cut_elem", "n_coh_elem", "n_coh_qp", "n_free", "n_const", "n_isv")] + \
+               [("nnz", ctypes.c_int64 * 4), ("cut_scratch_doubles", ctypes.c_int64)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libpigfem_b200.so and declare its signatures; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it first (make -C pigfem_b200/csrc)")
+    L = ctypes.CDLL(path)
+    vp, i32, dbl, p = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+    sig = {
+        "pg_create": (i32, [ctypes.POINTER(_Desc), ctypes.POINTER(vp)]),
+        "pg_create_host": (i32, [ctypes.POINTER(_Desc), ctypes.POINTER(vp)]),
+        "pg_upload": (i32, [vp]),
+        "pg_debug_array": (i32, [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(vp)]),
+        "pg_destroy": (None, [vp]),
+        "pg_last_error": (ctypes.c_char_p, [vp]),
+        "pg_get_sizes": (i32, [vp, ctypes.POINTER(_Sizes)]),
+        "pg_get_pattern": (i32, [vp, i32, p, p]),
+        "pg_get_nodes": (i32, [vp, p, p, p]),
+        "pg_assemble": (i32, [vp, p, dbl, i32, p, p, p, p, p, p]),
+        "pg_assemble_device": (i32, [vp, p, dbl, i32]),
+        "pg_device_outputs": (i32, [vp, p, p, p]),
+        "pg_set_stream": (i32, [vp, vp]),
+        "pg_set_isv": (i32, [vp, p]),
+        "pg_get_isv": (i32, [vp, i32, p]),
+        "pg_commit_isv": (i32, [vp]),
+        "pg_get_damage_zones": (i32, [vp, p]),
+        "pg_residual_norm": (i32, [vp, ctypes.POINTER(dbl)]),
+    }
+    for name, (rt, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = rt
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data
+
+
+@dataclass
+class ProblemDesc:
+    """Problem inputs, as the reference's Tests/Main.cpp assembles them."""
+    elem_type: int = TRI3
+    n: Sequence[int] = (8, 8)
+    lo: Sequence[float] = (0.0, 0.0)
+    hi: Sequence[float] = (1.0, 1.0)
+    inclusions: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    E_matrix: float = 3.5e3
+    nu_matrix: float = 0.35
+    E_fiber: float = 72e3
+    nu_fiber: float = 0.22
+    coh_law: int = COH_NONE
+    coh: Sequence[float] = (0.0, 0.0, 0.0, 0.0)
+    plane_strain: bool = True
+    subscale: bool = False
+    eps_macro: Sequence[float] = (0.0,) * 6
+    app_strain: float = 0.01
+
+    @property
+    def dim(self) -> int:
+        return 3 if self.elem_type == TET4 else 2
+
+
+class Problem:
+    """One enriched mesh resident on the GPU (a ``pg_ctx``)."""
+
+    def __init__(self, desc: ProblemDesc, device: bool = True):
+        L = load_library()
+        self.desc = desc
+        dim = desc.dim
+        self._incl = np.ascontiguousarray(np.asarray(desc.inclusions, dtype=np.float64).reshape(-1, dim + 1))
+        d = _Desc()
+        d.elem_type = desc.elem_type
+        n = list(desc.n) + [0] * 3
+        lo = list(desc.lo) + [0.0] * 3
+        hi = list(desc.hi) + [0.0] * 3
+        for i in range(3):
+            d.n[i], d.lo[i], d.hi[i] = n[i], lo[i], hi[i]
+        d.n_incl = self._incl.shape[0]
+        d.incl = self._incl.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        d.E_matrix, d.nu_matrix, d.E_fiber, d.nu_fiber = desc.E_matrix, desc.nu_matrix, desc.E_fiber, desc.nu_fiber
+        d.coh_law = desc.coh_law
+        for i, v in enumerate(desc.coh):
+            d.coh[i] = v
+        d.plane_strain, d.subscale = int(desc.plane_strain), int(desc.subscale)
+        for i, v in enumerate(desc.eps_macro):
+            d.eps_macro[i] = v
+        d.app_strain = desc.app_strain
+        self._d = d
+        h = ctypes.c_void_p(0)
+        rc = L.pg_create_host(ctypes.byref(d), ctypes.byref(h))
+        self.h = h
+        if rc:
+            msg = L.pg_last_error(h).decode() if h.value else "invalid description"
+            self.close()
+            raise PigfemError(rc, msg)
+        self.device = False
+        self._sizes()
+        if device:
+            self.upload()
+
+    # ------------------------------------------------------------------ set-up
+    def upload(self):
+        self._check(load_library().pg_upload(self.h))
+        self.device = True
+        self._sizes()
+
+    def _check(self, rc: int):
+        if rc:
+            raise PigfemError(rc, load_library().pg_last_error(self.h).decode())
+
+    def _sizes(self):
+        s = _Sizes()
+        self._check(load_library().pg_get_sizes(self.h, ctypes.byref(s)))
+        self.sizes = {k: getattr(s, k) for k, _ in _Sizes._fields_ if k != "nnz"}
+        self.sizes["nnz"] = [int(v) for v in s.nnz]
+        self.dim = s.dim
+        self.n_nodes, self.n_free, self.n_const, self.n_isv = s.n_nodes, s.n_free, s.n_const, s.n_isv
+        self.nnz = self.sizes["nnz"]
+
+    def pattern(self, block: int):
+        nrows = [self.n_free, self.n_free, self.n_const, self.n_const][block]
+        ncols = [self.n_free, self.n_const, self.n_free, self.n_const][block]
+        rp = np.zeros(nrows + 1, np.int32)
+        ci = np.zeros(max(self.nnz[block], 1), np.int32)
+        self._check(load_library().pg_get_pattern(self.h, block, _ptr(rp), _ptr(ci)))
+        return rp, ci[: self.nnz[block]], (nrows, ncols)
+
+    def nodes(self):
+        X = np.zeros(self.n_nodes * self.dim)
+        dofs = np.zeros(self.n_nodes * self.dim, np.int32)
+        dir_ = np.zeros(max(self.n_const, 1))
+        self._check(load_library().pg_get_nodes(self.h, _ptr(X), _ptr(dofs), _ptr(dir_)))
+        return X.reshape(-1, self.dim), dofs.reshape(-1, self.dim), dir_[: self.n_const]
+
+    def debug(self, name: str) -> np.ndarray:
+        n = ctypes.c_int64(0)
+        p = ctypes.c_void_p(0)
+        kind = load_library().pg_debug_array(self.h, name.encode(), ctypes.byref(n), ctypes.byref(p))
+        if kind == 0:
+            raise KeyError(name)
+        if n.value == 0:
+            return np.zeros(0, np.int32 if kind == 1 else np.float64)
+        ct = ctypes.c_int32 if kind == 1 else ctypes.c_double
+        return np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ct)), shape=(n.value,)).copy()
+
+    # ------------------------------------------------------------------ assembly
+    def node_major(self, U_dof: np.ndarray) -> np.ndarray:
+        """Scatter a DOF vector (free then constrained) to the node-major NodalData layout."""
+        _, dofs, _ = self.nodes()
+        return np.ascontiguousarray(np.asarray(U_dof, np.float64)[dofs.reshape(-1)])
+
+    def assemble(self, U_node: np.ndarray, t_frac: float = 1.0, flags: int = FUNC | JAC,
+                 out: Optional[dict] = None) -> dict:
+        """Assembler::assemble on host buffers; returns {'K_ff','K_fp','K_pf','K_pp','P_f','P_p'}."""
+        if not self.device:
+            raise PigfemError(12, "context has no device residency (constructed with device=False)")
+        U_node = np.ascontiguousarray(U_node, dtype=np.float64)
+        if U_node.size != self.n_nodes * self.dim:
+            raise PigfemError(2, f"U has {U_node.size} entries, expected {self.n_nodes * self.dim}")
+        if out is None:
+            out = {f"K_{b}": np.zeros(max(self.nnz[i], 1)) for i, b in enumerate(("ff", "fp", "pf", "pp"))}
+            out["P_f"] = np.zeros(max(self.n_free, 1))
+            out["P_p"] = np.zeros(max(self.n_const, 1))
+        self._check(load_library().pg_assemble(self.h, _ptr(U_node), float(t_frac), int(flags),
+                                               _ptr(out["K_ff"]), _ptr(out["K_fp"]), _ptr(out["K_pf"]),
+                                               _ptr(out["K_pp"]), _ptr(out["P_f"]), _ptr(out["P_p"])))
+        res = {f"K_{b}": out[f"K_{b}"][: self.nnz[i]] for i, b in enumerate(("ff", "fp", "pf", "pp"))}
+        res["P_f"] = out["P_f"][: self.n_free]
+        res["P_p"] = out["P_p"][: self.n_const]
+        return res
+
+    def assemble_device(self, d_U: int, t_frac: float = 1.0, flags: int = FUNC | JAC):
+        self._check(load_library().pg_assemble_device(self.h, ctypes.c_void_p(d_U), float(t_frac), int(flags)))
+
+    def device_outputs(self):
+        K = (ctypes.c_void_p * 4)()
+        pf, pp = ctypes.c_void_p(0), ctypes.c_void_p(0)
+        self._check(load_library().pg_device_outputs(self.h, K, ctypes.byref(pf), ctypes.byref(pp)))
+        return [K[i] for i in range(4)], pf.value, pp.value
+
+    def set_stream(self, stream_handle: int):
+        self._check(load_library().pg_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+    def set_isv(self, committed: np.ndarray):
+        committed = np.ascontiguousarray(committed, np.float64)
+        if committed.size != self.n_isv:
+            raise PigfemError(2, f"{committed.size} internal variables given, {self.n_isv} expected")
+        self._check(load_library().pg_set_isv(self.h, _ptr(committed)))
+
+    def get_isv(self, trial: bool = True) -> np.ndarray:
+        v = np.zeros(max(self.n_isv, 1))
+        self._check(load_library().pg_get_isv(self.h, int(trial), _ptr(v)))
+        return v[: self.n_isv]
+
+    def commit_isv(self):
+        self._check(load_library().pg_commit_isv(self.h))
+
+    def damage_zones(self) -> np.ndarray:
+        z = np.zeros(max(self.sizes["n_coh_qp"], 1), np.uint8)
+        self._check(load_library().pg_get_damage_zones(self.h, _ptr(z)))
+        return z[: self.sizes["n_coh_qp"]]
+
+    def residual_norm(self) -> float:
+        v = ctypes.c_double(0.0)
+        self._check(load_library().pg_residual_norm(self.h, ctypes.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            load_library().pg_destroy(self.h)
+            self.h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

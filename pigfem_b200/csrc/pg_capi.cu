@@ -1,0 +1,429 @@
+// pg_capi.cu -- the C ABI (include/pigfem_b200.h): set-up, device residency, launches.
+//
+// A pg_ctx owns every device buffer of one problem: geometry, topology, the cut-element
+// quadrature tables, the CSR structure and values of the four blocks, the residual, the
+// committed and trial internal variables and the cut-element scratch.  The caller owns its
+// host arrays; pointers are never retained across calls.
+#include "pg_kernels.cuh"
+#include "pg_setup.h"
+#include "../../include/pigfem_b200.h"
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+struct pg_ctx {
+  pg::Setup s;
+  std::string err;
+  cudaStream_t stream = 0;
+  std::vector<void*> allocs;
+  pgd::DevProblem P{};
+  double* d_U = nullptr;
+  double* d_isv_committed = nullptr;
+  double* d_isv_trial = nullptr;
+  uint8_t* d_zone = nullptr;
+  int* d_err = nullptr;
+  double* d_red = nullptr;  // residual-norm partials
+  long long cut_scratch = 0;
+  int max_nd = 0;
+  int maxnb_fast = 0;
+  int n_coh_qp = 0;
+  bool assembled = false;
+};
+
+namespace {
+
+int set_err(pg_ctx* c, int code, const std::string& m) {
+  if (c) c->err = m;
+  return code;
+}
+
+template <typename T>
+int upload(pg_ctx* c, const std::vector<T>& h, const T** out) {
+  *out = nullptr;
+  if (h.empty()) return 0;
+  void* p = nullptr;
+  if (cudaMalloc(&p, h.size() * sizeof(T)) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "cudaMalloc failed");
+  c->allocs.push_back(p);
+  if (cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    return set_err(c, PG_ERR_DEVICE, "cudaMemcpy failed");
+  *out = (const T*)p;
+  return 0;
+}
+
+template <typename T>
+int dalloc(pg_ctx* c, size_t n, T** out) {
+  *out = nullptr;
+  if (n == 0) n = 1;
+  void* p = nullptr;
+  if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "cudaMalloc failed");
+  c->allocs.push_back(p);
+  cudaMemset(p, 0, n * sizeof(T));
+  *out = (T*)p;
+  return 0;
+}
+
+#define PG_TRY(x) do { int _e = (x); if (_e) return _e; } while (0)
+
+// Fixed-order sum of squares: each block reduces a contiguous chunk in a fixed tree order.
+__global__ void k_sumsq_partial(const double* x, int n, double* part) {
+  __shared__ double sh[256];
+  const int chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int b0 = blockIdx.x * chunk, b1 = min(n, b0 + chunk);
+  double s = 0.0;
+  for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) s += x[i] * x[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+__global__ void k_sum_final(const double* part, int n, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s += part[i];
+    out[0] = s;
+  }
+}
+
+int launch(pg_ctx* c, double t_frac, int flags) {
+  pgd::DevProblem P = c->P;
+  P.U = c->d_U;
+  P.flags = flags;
+  for (int v = 0; v < 6; ++v) P.eps_macro[v] = c->s.desc.eps_macro[v] * t_frac;
+  if (c->s.ncut > 0) {
+    const int wpb = 4;
+    const int nv = c->s.dim == 2 ? 3 : 6;
+    const size_t smem = (size_t)wpb * pgd::cut_smem_per_warp(c->max_nd, nv) * sizeof(double);
+    const int grid = (c->s.ncut + wpb - 1) / wpb;
+    if (c->s.dim == 2) {
+      cudaFuncSetAttribute(pgd::k_cut_elements<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      pgd::k_cut_elements<2><<<grid, 32 * wpb, smem, c->stream>>>(P, c->max_nd);
+    } else {
+      cudaFuncSetAttribute(pgd::k_cut_elements<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      pgd::k_cut_elements<3><<<grid, 32 * wpb, smem, c->stream>>>(P, c->max_nd);
+    }
+  }
+  const int tpb = 128;
+  if (P.n_fast_rows > 0) {
+    const int grid = (P.n_fast_rows + tpb - 1) / tpb;
+    const bool fp32 = (flags & PG_FP32) != 0;
+    if (c->s.dim == 2) {
+      if (fp32) pgd::k_rows_fast<2, 9, float><<<grid, tpb, 0, c->stream>>>(P);
+      else pgd::k_rows_fast<2, 9, double><<<grid, tpb, 0, c->stream>>>(P);
+    } else {
+      if (fp32) pgd::k_rows_fast<3, 15, float><<<grid, tpb, 0, c->stream>>>(P);
+      else pgd::k_rows_fast<3, 15, double><<<grid, tpb, 0, c->stream>>>(P);
+    }
+  }
+  if (P.n_slow_rows > 0) {
+    const int grid = (P.n_slow_rows + tpb - 1) / tpb;
+    if (c->s.dim == 2) pgd::k_rows_slow<2><<<grid, tpb, 0, c->stream>>>(P);
+    else pgd::k_rows_slow<3><<<grid, tpb, 0, c->stream>>>(P);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(c, PG_ERR_DEVICE, std::string("launch failed: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pg_create_host(const pg_problem_desc* d, pg_ctx** out) {
+  if (!d || !out) return PG_ERR_INPUT;
+  *out = nullptr;
+  pg_ctx* c = new pg_ctx;
+  pg::ProblemDesc pd;
+  pd.elem_type = d->elem_type;
+  for (int i = 0; i < 3; ++i) { pd.n[i] = d->n[i]; pd.lo[i] = d->lo[i]; pd.hi[i] = d->hi[i]; }
+  const int dim = (d->elem_type == PG_TET4) ? 3 : 2;
+  if (d->n_incl < 0 || (d->n_incl > 0 && !d->incl)) { delete c; return PG_ERR_INPUT; }
+  pd.incl.assign(d->incl, d->incl + (size_t)d->n_incl * (dim + 1));
+  pd.E_matrix = d->E_matrix; pd.nu_matrix = d->nu_matrix; pd.E_fiber = d->E_fiber; pd.nu_fiber = d->nu_fiber;
+  pd.coh_law = d->coh_law;
+  for (int i = 0; i < 4; ++i) pd.coh[i] = d->coh[i];
+  pd.plane_strain = d->plane_strain; pd.subscale = d->subscale;
+  for (int i = 0; i < 6; ++i) pd.eps_macro[i] = d->eps_macro[i];
+  pd.app_strain = d->app_strain;
+  if (d->elem_type == PG_QUAD4) { c->err = "quad4 background elements are not on the device path"; *out = c; return PG_ERR_UNSUPPORTED; }
+  int rc = pg::build_setup(pd, c->s);
+  if (rc) { c->err = c->s.error; *out = c; return rc == 2 ? PG_ERR_INPUT : (rc == 4 ? PG_ERR_UNSUPPORTED : (rc == 7 ? PG_ERR_JACOBIAN : PG_ERR_GEOMETRY)); }
+  c->n_coh_qp = (int)c->s.cqp_wgt.size();
+  *out = c;
+  return 0;
+}
+
+int pg_upload(pg_ctx* c) {
+  if (!c) return PG_ERR_INPUT;
+  pg::Setup& s = c->s;
+  const int dim = s.dim;
+
+  // ---- derived row-ownership tables
+  const int n_nodes = s.n_std + s.n_enr;
+  std::vector<uint8_t> mask(s.n_dn, 0);
+  for (int a = 0; a < s.n_dn; ++a) {
+    const int na = s.dn_node[a];
+    for (int q = 0; q < dim; ++q) if (s.node_dof[(size_t)na * dim + q] < s.n_free) mask[a] |= (uint8_t)(1 << q);
+  }
+  std::vector<int> pf(s.dn_nbr.size()), pc(s.dn_nbr.size());
+  for (int a = 0; a < s.n_dn; ++a) {
+    int f = 0, p = 0;
+    for (int k = s.dn_nbr_off[a]; k < s.dn_nbr_off[a + 1]; ++k) {
+      pf[k] = f; pc[k] = p;
+      const int m = mask[s.dn_nbr[k]];
+      for (int q = 0; q < dim; ++q) { if (m & (1 << q)) f++; else p++; }
+    }
+  }
+  const int maxnb = (dim == 2) ? 9 : 15;
+  std::vector<int> fast, slow;
+  for (int a = 0; a < s.n_dn; ++a) {
+    bool ok = (s.dn_nbr_off[a + 1] - s.dn_nbr_off[a]) <= maxnb;
+    for (int k = s.dn_adj_off[a]; k < s.dn_adj_off[a + 1] && ok; ++k) ok = s.cut_of[s.dn_adj[k] >> 5] < 0;
+    for (int q = 0; q < dim; ++q) (ok ? fast : slow).push_back(a * dim + q);
+  }
+  // cut-element scratch layout
+  std::vector<long long> ke_off(s.ncut + 1, 0);
+  std::vector<int> re_off(s.ncut + 1, 0);
+  for (int cc = 0; cc < s.ncut; ++cc) {
+    const int nd = (s.cut_node_off[cc + 1] - s.cut_node_off[cc]) * dim;
+    c->max_nd = std::max(c->max_nd, nd);
+    ke_off[cc + 1] = ke_off[cc] + (long long)nd * nd;
+    re_off[cc + 1] = re_off[cc] + nd;
+  }
+  c->cut_scratch = ke_off[s.ncut] + re_off[s.ncut];
+  c->n_coh_qp = (int)s.cqp_wgt.size();
+
+  // ---- device residency
+  pgd::DevProblem& P = c->P;
+  P.dim = dim; P.npe = s.npe; P.nvoigt = s.nvoigt;
+  P.n_nodes = n_nodes; P.ne = s.ne; P.ncut = s.ncut; P.n_dn = s.n_dn;
+  P.n_free = s.n_free; P.n_const = s.n_const; P.subscale = s.desc.subscale;
+  for (int m = 0; m < 2; ++m) for (int i = 0; i < 36; ++i) { P.D[m][i] = s.D[m][i]; P.Df[m][i] = (float)s.D[m][i]; }
+  P.coh.law = s.coh.law; P.coh.nvar = s.coh.nvar; P.coh.sigma_c = s.coh.sigma_c; P.coh.delta_c1 = s.coh.delta_c1;
+  P.coh.delta_c2 = s.coh.delta_c2; P.coh.delta_cn = s.coh.delta_cn; P.coh.delta_ct = s.coh.delta_ct; P.coh.q = s.coh.q;
+  P.coh.delta_c = s.coh.delta_c; P.coh.beta2 = s.coh.beta2; P.coh.alpha = s.coh.alpha;
+  std::vector<float> Xf(s.X.begin(), s.X.end());
+  PG_TRY(upload(c, s.X, &P.X));
+  PG_TRY(upload(c, Xf, &P.Xf));
+  PG_TRY(upload(c, s.conn, &P.conn));
+  PG_TRY(upload(c, s.elem_mat, &P.emat));
+  PG_TRY(upload(c, s.cut_of, &P.cut_of));
+  PG_TRY(upload(c, s.node_dof, &P.node_dof));
+  PG_TRY(upload(c, s.node_dn, &P.node_dn));
+  PG_TRY(upload(c, s.cut_node_off, &P.cut_node_off));
+  PG_TRY(upload(c, s.cut_nodes, &P.cut_nodes));
+  PG_TRY(upload(c, s.cut_qp_off, &P.cut_qp_off));
+  PG_TRY(upload(c, s.qp_wgt, &P.qp_wgt));
+  PG_TRY(upload(c, s.qp_mat, &P.qp_mat));
+  PG_TRY(upload(c, s.qp_grad_off, &P.qp_grad_off));
+  PG_TRY(upload(c, s.qp_grad, &P.qp_grad));
+  PG_TRY(upload(c, s.cut_coh_off, &P.cut_coh_off));
+  PG_TRY(upload(c, s.coh_nh, &P.coh_nh));
+  PG_TRY(upload(c, s.coh_local_off, &P.coh_local_off));
+  PG_TRY(upload(c, s.coh_local, &P.coh_local));
+  PG_TRY(upload(c, s.coh_qp_off, &P.coh_qp_off));
+  PG_TRY(upload(c, s.cqp_N, &P.cqp_N));
+  PG_TRY(upload(c, s.cqp_R, &P.cqp_R));
+  PG_TRY(upload(c, s.cqp_wgt, &P.cqp_wgt));
+  PG_TRY(upload(c, s.cqp_isv, &P.cqp_isv));
+  PG_TRY(upload(c, ke_off, &P.ke_off));
+  PG_TRY(upload(c, re_off, &P.re_off));
+  double* dke; double* dre;
+  PG_TRY(dalloc(c, (size_t)ke_off[s.ncut], &dke));
+  PG_TRY(dalloc(c, (size_t)re_off[s.ncut], &dre));
+  P.ke = dke; P.re = dre;
+  PG_TRY(dalloc(c, (size_t)s.n_isv, &c->d_isv_committed));
+  PG_TRY(dalloc(c, (size_t)s.n_isv, &c->d_isv_trial));
+  P.isv_committed = c->d_isv_committed; P.isv_trial = c->d_isv_trial;
+  PG_TRY(dalloc(c, (size_t)c->n_coh_qp, &c->d_zone));
+  P.zone = c->d_zone;
+  PG_TRY(upload(c, s.dn_node, &P.dn_node));
+  PG_TRY(upload(c, s.dn_nbr_off, &P.dn_nbr_off));
+  PG_TRY(upload(c, s.dn_nbr, &P.dn_nbr));
+  PG_TRY(upload(c, pf, &P.dn_nbr_pf));
+  PG_TRY(upload(c, pc, &P.dn_nbr_pc));
+  PG_TRY(upload(c, s.dn_adj_off, &P.dn_adj_off));
+  PG_TRY(upload(c, s.dn_adj, &P.dn_adj));
+  PG_TRY(upload(c, mask, &P.dn_mask));
+  PG_TRY(upload(c, fast, &P.fast_rows));
+  PG_TRY(upload(c, slow, &P.slow_rows));
+  P.n_fast_rows = (int)fast.size(); P.n_slow_rows = (int)slow.size();
+  for (int b = 0; b < 4; ++b) {
+    PG_TRY(upload(c, s.rp[b], &P.rp[b]));
+    PG_TRY(dalloc(c, s.ci[b].size(), &P.val[b]));
+  }
+  PG_TRY(dalloc(c, (size_t)s.n_free, &P.Pf));
+  PG_TRY(dalloc(c, (size_t)s.n_const, &P.Pp));
+  PG_TRY(dalloc(c, (size_t)n_nodes * dim, &c->d_U));
+  PG_TRY(dalloc(c, 1, &c->d_err));
+  P.err = c->d_err;
+  PG_TRY(dalloc(c, 1024, &c->d_red));
+  return 0;
+}
+
+int pg_create(const pg_problem_desc* d, pg_ctx** out) {
+  int rc = pg_create_host(d, out);
+  if (rc) return rc;
+  return pg_upload(*out);
+}
+
+int pg_debug_array(const pg_ctx* c, const char* name, int64_t* n, const void** ptr) {
+  if (!c || !name || !n || !ptr) return 0;
+  const pg::Setup& s = c->s;
+  struct { const char* k; const void* p; size_t n; int kind; } tab[] = {
+      {"cut_elem", s.cut_elem.data(), s.cut_elem.size(), 1}, {"cut_node_off", s.cut_node_off.data(), s.cut_node_off.size(), 1},
+      {"cut_nodes", s.cut_nodes.data(), s.cut_nodes.size(), 1}, {"cut_qp_off", s.cut_qp_off.data(), s.cut_qp_off.size(), 1},
+      {"qp_wgt", s.qp_wgt.data(), s.qp_wgt.size(), 2}, {"qp_mat", s.qp_mat.data(), s.qp_mat.size(), 1},
+      {"qp_grad_off", s.qp_grad_off.data(), s.qp_grad_off.size(), 1}, {"qp_grad", s.qp_grad.data(), s.qp_grad.size(), 2},
+      {"cut_coh_off", s.cut_coh_off.data(), s.cut_coh_off.size(), 1}, {"coh_nh", s.coh_nh.data(), s.coh_nh.size(), 1},
+      {"coh_local_off", s.coh_local_off.data(), s.coh_local_off.size(), 1}, {"coh_local", s.coh_local.data(), s.coh_local.size(), 1},
+      {"coh_qp_off", s.coh_qp_off.data(), s.coh_qp_off.size(), 1}, {"cqp_N", s.cqp_N.data(), s.cqp_N.size(), 2},
+      {"cqp_R", s.cqp_R.data(), s.cqp_R.size(), 2}, {"cqp_wgt", s.cqp_wgt.data(), s.cqp_wgt.size(), 2},
+      {"cqp_isv", s.cqp_isv.data(), s.cqp_isv.size(), 1}, {"conn", s.conn.data(), s.conn.size(), 1},
+      {"elem_mat", s.elem_mat.data(), s.elem_mat.size(), 1}, {"cut_of", s.cut_of.data(), s.cut_of.size(), 1},
+      {"node_detect", s.node_detect.data(), s.node_detect.size(), 1}, {"enr_edge", s.enr_edge.data(), s.enr_edge.size(), 1},
+      {"enr_incl", s.enr_incl.data(), s.enr_incl.size(), 1}, {"sub_type", s.sub_type.data(), s.sub_type.size(), 1},
+      {"cut_sub_off", s.cut_sub_off.data(), s.cut_sub_off.size(), 1}, {"sub_mat", s.sub_mat.data(), s.sub_mat.size(), 1},
+  };
+  for (auto& t : tab)
+    if (std::strcmp(t.k, name) == 0) { *n = (int64_t)t.n; *ptr = t.p; return t.kind; }
+  *n = 0; *ptr = nullptr;
+  return 0;
+}
+
+void pg_destroy(pg_ctx* c) {
+  if (!c) return;
+  for (void* p : c->allocs) cudaFree(p);
+  delete c;
+}
+
+const char* pg_last_error(const pg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int pg_get_sizes(const pg_ctx* c, pg_sizes* o) {
+  if (!c || !o) return PG_ERR_INPUT;
+  const pg::Setup& s = c->s;
+  o->dim = s.dim; o->n_nodes = s.n_std + s.n_enr; o->n_std_nodes = s.n_std; o->n_enrich_nodes = s.n_enr;
+  o->n_elem = s.ne; o->n_cut_elem = s.ncut; o->n_coh_elem = (int)s.coh_nh.size(); o->n_coh_qp = c->n_coh_qp;
+  o->n_free = s.n_free; o->n_const = s.n_const; o->n_isv = s.n_isv;
+  for (int b = 0; b < 4; ++b) o->nnz[b] = (int64_t)s.ci[b].size();
+  o->cut_scratch_doubles = c->cut_scratch;
+  return 0;
+}
+
+int pg_get_pattern(const pg_ctx* c, int b, int32_t* rowptr, int32_t* cols) {
+  if (!c || b < 0 || b > 3) return PG_ERR_INPUT;
+  if (rowptr) std::memcpy(rowptr, c->s.rp[b].data(), c->s.rp[b].size() * sizeof(int32_t));
+  if (cols && !c->s.ci[b].empty()) std::memcpy(cols, c->s.ci[b].data(), c->s.ci[b].size() * sizeof(int32_t));
+  return 0;
+}
+
+int pg_get_nodes(const pg_ctx* c, double* coords, int32_t* node_dofs, double* dirichlet) {
+  if (!c) return PG_ERR_INPUT;
+  if (coords) std::memcpy(coords, c->s.X.data(), c->s.X.size() * sizeof(double));
+  if (node_dofs) std::memcpy(node_dofs, c->s.node_dof.data(), c->s.node_dof.size() * sizeof(int32_t));
+  if (dirichlet && !c->s.dirichlet.empty()) std::memcpy(dirichlet, c->s.dirichlet.data(), c->s.dirichlet.size() * sizeof(double));
+  return 0;
+}
+
+int pg_set_stream(pg_ctx* c, void* stream) {
+  if (!c) return PG_ERR_INPUT;
+  c->stream = (cudaStream_t)stream;
+  return 0;
+}
+
+int pg_assemble_device(pg_ctx* c, const double* d_U, double t_frac, int flags) {
+  if (!c || !d_U) return PG_ERR_INPUT;
+  if (!(flags & (PG_FUNC | PG_JAC))) return 0;
+  double* keep = c->d_U;
+  c->d_U = const_cast<double*>(d_U);
+  int rc = launch(c, t_frac, flags);
+  c->d_U = keep;
+  c->assembled = (rc == 0);
+  return rc;
+}
+
+int pg_assemble(pg_ctx* c, const double* U, double t_frac, int flags, double* Kff, double* Kfp, double* Kpf, double* Kpp,
+                double* Pf, double* Pp) {
+  if (!c || !U) return PG_ERR_INPUT;
+  if (!(flags & (PG_FUNC | PG_JAC))) return 0;
+  const pg::Setup& s = c->s;
+  const size_t nU = (size_t)(s.n_std + s.n_enr) * s.dim;
+  if (cudaMemcpyAsync(c->d_U, U, nU * sizeof(double), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+    return set_err(c, PG_ERR_DEVICE, "copy of U failed");
+  cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
+  PG_TRY(launch(c, t_frac, flags));
+  double* outs[4] = {Kff, Kfp, Kpf, Kpp};
+  if (flags & PG_JAC)
+    for (int b = 0; b < 4; ++b)
+      if (outs[b] && !s.ci[b].empty())
+        cudaMemcpyAsync(outs[b], c->P.val[b], s.ci[b].size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (flags & PG_FUNC) {
+    if (Pf && s.n_free) cudaMemcpyAsync(Pf, c->P.Pf, (size_t)s.n_free * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (Pp && s.n_const) cudaMemcpyAsync(Pp, c->P.Pp, (size_t)s.n_const * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  }
+  int herr = 0;
+  cudaMemcpyAsync(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return set_err(c, PG_ERR_DEVICE, std::string("assembly failed: ") + cudaGetErrorString(e));
+  c->assembled = true;
+  if (herr & pgd::ERR_NONFINITE) return set_err(c, PG_ERR_NONFINITE, "non-finite value in a cut-element matrix or vector");
+  if (herr) return set_err(c, PG_ERR_DEVICE, "scatter map inconsistency detected on the device");
+  return 0;
+}
+
+int pg_device_outputs(pg_ctx* c, double** K, double** Pf, double** Pp) {
+  if (!c) return PG_ERR_INPUT;
+  if (K) for (int b = 0; b < 4; ++b) K[b] = c->P.val[b];
+  if (Pf) *Pf = c->P.Pf;
+  if (Pp) *Pp = c->P.Pp;
+  return 0;
+}
+
+int pg_set_isv(pg_ctx* c, const double* v) {
+  if (!c || (!v && c->s.n_isv)) return PG_ERR_INPUT;
+  if (c->s.n_isv == 0) return 0;
+  if (cudaMemcpy(c->d_isv_committed, v, (size_t)c->s.n_isv * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+    return set_err(c, PG_ERR_DEVICE, "copy of internal variables failed");
+  return 0;
+}
+
+int pg_get_isv(const pg_ctx* c, int trial, double* out) {
+  if (!c || (!out && c->s.n_isv)) return PG_ERR_INPUT;
+  if (c->s.n_isv == 0) return 0;
+  cudaStreamSynchronize(c->stream);
+  cudaMemcpy(out, trial ? c->d_isv_trial : c->d_isv_committed, (size_t)c->s.n_isv * sizeof(double), cudaMemcpyDeviceToHost);
+  return 0;
+}
+
+int pg_commit_isv(pg_ctx* c) {
+  if (!c) return PG_ERR_INPUT;
+  if (c->s.n_isv == 0) return 0;
+  cudaMemcpyAsync(c->d_isv_committed, c->d_isv_trial, (size_t)c->s.n_isv * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+  return cudaStreamSynchronize(c->stream) == cudaSuccess ? 0 : PG_ERR_DEVICE;
+}
+
+int pg_get_damage_zones(const pg_ctx* c, uint8_t* z) {
+  if (!c || (!z && c->n_coh_qp)) return PG_ERR_INPUT;
+  if (!c->n_coh_qp) return 0;
+  cudaStreamSynchronize(c->stream);
+  cudaMemcpy(z, c->d_zone, (size_t)c->n_coh_qp, cudaMemcpyDeviceToHost);
+  return 0;
+}
+
+int pg_residual_norm(pg_ctx* c, double* out) {
+  if (!c || !out) return PG_ERR_INPUT;
+  const int nb = 256;
+  k_sumsq_partial<<<nb, 256, 0, c->stream>>>(c->P.Pf, c->s.n_free, c->d_red);
+  k_sum_final<<<1, 32, 0, c->stream>>>(c->d_red, nb, c->d_red + nb);
+  double v = 0.0;
+  cudaMemcpyAsync(&v, c->d_red + nb, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "residual norm failed");
+  *out = sqrt(v);
+  return 0;
+}
+
+}  // extern "C"

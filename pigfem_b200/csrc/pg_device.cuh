@@ -1,0 +1,250 @@
+// pg_device.cuh -- device-side data layout and element physics of the B200 assembly path.
+//
+// Physics restated from the reference (paths relative to the PIGFEM source tree):
+//   small-strain kernel ........ src/AssemblerSmallStrainStructural.cpp:23-50 (eps = B U [+ eps_macro],
+//                                K = B^T D B, P = B^T sigma), B in Voigt order xx, yy, (zz), (yz, xz,) xy
+//                                with engineering shear (src/Utilities.cpp:68-127)
+//   linear elastic stress ...... src/material_lei.cpp:232-299 (sigma = D eps)
+//   cohesive kernel ............ src/AssemblerSmallStrainStructural.cpp:86-104, src/Utilities.cpp:528-594
+//   cohesive laws .............. src/Material_BilinearCohesive{,NU}.cpp, src/Material_XNCohesive{,NU}.cpp,
+//                                src/Material_OPCohesive{,NU,Aug,NUAug}.cpp
+//   damage zones ............... src/Material_BilinearCohesiveNU.cpp:255-266, src/Material_OPCohesiveNU.cpp:217-234,
+//                                src/Material_XNCohesiveNU.cpp:264-287
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pgd {
+
+constexpr int kMaxNodesCut = 32;  // element-local node slots (parent + enrichment); matches the set-up encoding
+
+enum { COH_NONE = 0, COH_BL = 1, COH_BLNU = 2, COH_XN = 3, COH_XNNU = 4, COH_OP = 5, COH_OPNU = 6, COH_OPAUG = 7, COH_OPNUAUG = 8 };
+enum { FLAG_FUNC = 1, FLAG_JAC = 2, FLAG_FP32 = 4 };
+enum { ERR_NONFINITE = 1, ERR_CUT_OVERFLOW = 2, ERR_BAD_SLOT = 4 };
+
+struct CohConst {
+  int law, nvar;
+  double sigma_c, delta_c1, delta_c2, delta_cn, delta_ct, q, delta_c, beta2, alpha;
+};
+
+// Everything one assembly launch reads or writes, as device pointers.
+struct DevProblem {
+  int dim, npe, nvoigt;
+  int n_nodes, ne, ncut, n_dn;
+  int n_free, n_const;
+  int subscale;
+  double D[2][36];
+  float Df[2][36];
+  CohConst coh;
+  // geometry / state
+  const double* X;    // n_nodes * dim
+  const float* Xf;    // n_nodes * dim (FP32 copy for the mixed path)
+  const double* U;    // n_nodes * dim, node-major (the reference's NodalData layout)
+  const int* conn;    // ne * npe
+  const int* emat;    // ne
+  const int* cut_of;  // ne
+  const int* node_dof;  // n_nodes * dim
+  const int* node_dn;   // n_nodes
+  // cut elements
+  const int* cut_node_off; const int* cut_nodes;
+  const int* cut_qp_off; const double* qp_wgt; const int* qp_mat; const int* qp_grad_off; const double* qp_grad;
+  const int* cut_coh_off; const int* coh_nh; const int* coh_local_off; const int* coh_local;
+  const int* coh_qp_off; const double* cqp_N; const double* cqp_R; const double* cqp_wgt; const int* cqp_isv;
+  const long long* ke_off;  // per cut element: offset of its element matrix in the scratch
+  const int* re_off;        // per cut element: offset of its element vector in the scratch
+  double* ke;               // scratch: element matrices of the cut elements
+  double* re;               // scratch: element vectors of the cut elements
+  const double* isv_committed;
+  double* isv_trial;
+  uint8_t* zone;            // per cohesive qp: damage zone (0 compression, 1 loading, 2 softening, 3 failed)
+  // row ownership
+  const int* dn_node; const int* dn_nbr_off; const int* dn_nbr; const int* dn_nbr_pf; const int* dn_nbr_pc;
+  const int* dn_adj_off; const int* dn_adj; const uint8_t* dn_mask;
+  const int* fast_rows; int n_fast_rows;   // (dnode * dim + q) rows whose elements are all uncut
+  const int* slow_rows; int n_slow_rows;   // the remaining rows
+  // outputs: CSR values of the four blocks and the two residual parts
+  const int* rp[4];
+  double* val[4];
+  double* Pf; double* Pp;
+  // per-call
+  double eps_macro[6];
+  int flags;
+  int* err;
+};
+
+// ---------------------------------------------------------------- cohesive laws (FP64)
+// delta (dim entries, tangential first, normal last) may be overwritten by the 1e-20 clamp, as the
+// reference's getDeltaEff / getDnDt do.  T gets the traction, Dm the dim x dim tangent (row-major),
+// isv the trial internal variables of this quadrature point (updated in place), zone the damage zone.
+__device__ inline void coh_law(const CohConst& c, int dim, double* delta, double* T, double* Dm, double* isv, uint8_t* zone) {
+  double nrm = 0.0;
+  for (int i = 0; i < dim; ++i) nrm += delta[i] * delta[i];
+  if (nrm < 1e-40)
+    for (int i = 0; i < dim; ++i) delta[i] = 1e-20;
+  const int law = c.law;
+  if (law == COH_XN || law == COH_XNNU) {
+    const double Dn = delta[dim - 1];
+    const double Dt = (dim == 2) ? delta[0] : sqrt(pow(delta[0], 2) + pow(delta[1], 2));
+    const double phi_n = c.sigma_c * c.delta_cn * exp(1.0);
+    double Tn, dTndDn, Tt, dTtdDt;
+    const double dTndDt = 0.0, dTtdDn = 0.0;
+    if (law == COH_XNNU) {
+      const double shear_rat = Dt / c.delta_ct;
+      const double shear_rat_exp = exp(-pow(shear_rat, 2));
+      const double norm_rat = Dn / c.delta_cn;
+      const double norm_rat_exp = exp(-1.0 * norm_rat);
+      Tn = (phi_n / c.delta_cn) * norm_rat_exp * norm_rat;
+      Tt = (2.0 * phi_n * Dt / pow(c.delta_ct, 2)) * c.q * shear_rat_exp;
+      dTndDn = (phi_n / c.delta_cn) * norm_rat_exp * ((1 - norm_rat) / c.delta_cn);
+      dTtdDt = (2.0 * phi_n / pow(c.delta_ct, 2)) * c.q * (1 - 2.0 * pow(shear_rat, 2)) * shear_rat_exp;
+    } else {
+      double& Dn_max = isv[0];
+      double& Dt_max = isv[1];
+      if (Dn >= Dn_max || Dn <= 0) {
+        const double norm_rat = Dn / c.delta_cn;
+        const double norm_rat_exp = exp(-1.0 * norm_rat);
+        Tn = (phi_n / c.delta_cn) * norm_rat_exp * norm_rat;
+        dTndDn = (phi_n / c.delta_cn) * norm_rat_exp * ((1 - norm_rat) / c.delta_cn);
+        Dn_max = Dn;
+      } else {
+        const double norm_rat_max = Dn_max / c.delta_cn;
+        const double norm_rat_exp_max = exp(-1.0 * norm_rat_max);
+        const double Tn_max = (phi_n / c.delta_cn) * norm_rat_exp_max * norm_rat_max;
+        Tn = (Dn / Dn_max) * Tn_max;
+        dTndDn = Tn_max / Dn_max;
+      }
+      if (fabs(Dt) >= Dt_max) {
+        const double shear_rat = Dt / c.delta_ct;
+        const double shear_rat_exp = exp(-pow(shear_rat, 2));
+        Tt = (2.0 * phi_n * c.q / c.delta_ct) * shear_rat_exp * shear_rat;
+        dTtdDt = (2.0 * phi_n / pow(c.delta_ct, 2)) * c.q * (1 - 2.0 * pow(shear_rat, 2)) * shear_rat_exp;
+        Dt_max = fabs(Dt);
+      } else {
+        const double shear_rat_max = Dt_max / c.delta_ct;
+        const double shear_rat_exp_max = exp(-pow(shear_rat_max, 2));
+        const double Tt_max = (2.0 * phi_n * c.q / c.delta_ct) * shear_rat_exp_max * shear_rat_max;
+        Tt = (Dt / Dt_max) * Tt_max;
+        dTtdDt = Tt_max / Dt_max;
+      }
+    }
+    T[dim - 1] = Tn;
+    if (dim == 2) {
+      T[0] = Tt;
+      Dm[0] = dTtdDt; Dm[1] = dTtdDn; Dm[2] = dTndDt; Dm[3] = dTndDn;
+    } else {
+      T[0] = Tt * (delta[0] / Dt);
+      T[1] = Tt * (delta[1] / Dt);
+      Dm[0] = dTtdDt * pow(delta[0] / Dt, 2) + (Tt / Dt) * (1 - pow(delta[0] / Dt, 2));
+      Dm[1] = (dTtdDt - Tt / Dt) * (delta[0] * delta[1] / (Dt * Dt));
+      Dm[2] = dTtdDn * (delta[0] / Dt);
+      Dm[3] = (dTtdDt - Tt / Dt) * (delta[0] * delta[1] / (Dt * Dt));
+      Dm[4] = dTtdDt * pow(delta[1] / Dt, 2) + (Tt / Dt) * (1 - pow(delta[1] / Dt, 2));
+      Dm[5] = dTtdDn * (delta[1] / Dt);
+      Dm[6] = dTndDt * (delta[0] / Dt);
+      Dm[7] = dTndDt * (delta[1] / Dt);
+      Dm[8] = dTndDn;
+    }
+    // zone from the larger of the normalised openings
+    const double a = Dn / c.delta_cn, b = Dt / c.delta_ct;
+    const double nf = (a > b) ? a : b;
+    *zone = (nf <= 0) ? 0 : (nf <= 1 ? 1 : (nf <= 5.0 ? 2 : 3));
+    return;
+  }
+  // bilinear and Ortiz-Pandolfi share the effective-opening form
+  double deff = pow(delta[dim - 1], 2);
+  for (int i = 0; i < dim - 1; ++i) deff += c.beta2 * pow(delta[i], 2);
+  deff = sqrt(deff);
+  double trac = 0.0, dtrac = 0.0;
+  double dmax_copy = 0.0;
+  if (law == COH_BL || law == COH_BLNU) {
+    // BilinearCohesiveMaterial never writes delta_max, so both variants follow the loading curve.
+    const double delta_max = (law == COH_BL) ? isv[0] : 0.0;
+    if (law == COH_BLNU || deff >= delta_max || deff < 0.0) {
+      if (deff >= 0 && deff < c.delta_c1) { trac = deff * (c.sigma_c / c.delta_c1); dtrac = (c.sigma_c / c.delta_c1); }
+      else if (deff >= c.delta_c1 && deff < c.delta_c2) {
+        trac = c.sigma_c * (1 - (deff - c.delta_c1) / (c.delta_c2 - c.delta_c1));
+        dtrac = -1.0 * (c.sigma_c / (c.delta_c2 - c.delta_c1));
+      } else { trac = 0; dtrac = 0; }
+    } else {
+      double max_traction;
+      if (delta_max >= 0 && delta_max < c.delta_c1) max_traction = delta_max * (c.sigma_c / c.delta_c1);
+      else if (delta_max >= c.delta_c1 && delta_max < c.delta_c2) max_traction = c.sigma_c * (1 - (delta_max - c.delta_c1) / (c.delta_c2 - c.delta_c1));
+      else max_traction = 0;
+      trac = max_traction * (deff / delta_max);
+      dtrac = max_traction / delta_max;
+    }
+  } else {
+    const bool unloading_law = (law == COH_OP || law == COH_OPAUG);
+    if (unloading_law) {
+      double& delta_max = isv[0];
+      dmax_copy = delta_max;
+      if (deff >= delta_max || deff < 0.0) {
+        trac = c.sigma_c * (deff / c.delta_c) * exp(1.0 - deff / c.delta_c);
+        dtrac = (c.sigma_c / c.delta_c) * (1.0 - deff / c.delta_c) * exp(1.0 - deff / c.delta_c);
+        delta_max = deff;
+      } else {
+        const double max_traction = c.sigma_c * (delta_max / c.delta_c) * exp(1.0 - delta_max / c.delta_c);
+        trac = max_traction * (deff / delta_max);
+        dtrac = max_traction / delta_max;
+      }
+    } else {
+      trac = c.sigma_c * (deff / c.delta_c) * exp(1.0 - deff / c.delta_c);
+      dtrac = (c.sigma_c / c.delta_c) * (1.0 - deff / c.delta_c) * exp(1.0 - deff / c.delta_c);
+    }
+  }
+  double br[3], dd[3];
+  for (int i = 0; i < dim; ++i) br[i] = c.beta2 * delta[i];
+  br[dim - 1] += (1.0 - c.beta2) * delta[dim - 1];
+  for (int i = 0; i < dim; ++i) T[i] = (trac / deff) * br[i];
+  const bool compress = delta[dim - 1] < 0;
+  if (compress) {
+    if (law == COH_OPAUG) T[dim - 1] = (c.sigma_c / c.alpha) * exp(1.0 - dmax_copy / c.delta_c) * sinh(c.alpha * delta[dim - 1] / c.delta_c);
+    else if (law == COH_OPNUAUG) T[dim - 1] = (c.sigma_c * exp(1.0) / c.alpha) * sinh(c.alpha * delta[dim - 1] / c.delta_c);
+  }
+  dd[dim - 1] = delta[dim - 1] / deff;
+  for (int i = 0; i < dim - 1; ++i) dd[i] = c.beta2 * delta[i] / deff;
+  for (int i = 0; i < dim; ++i)
+    for (int k = 0; k < dim; ++k)
+      Dm[i * dim + k] = br[i] * (dtrac * deff - trac) * (dd[k] / pow(deff, 2)) +
+                        (trac / deff) * (c.beta2 * (i == k ? 1.0 : 0.0) + (1.0 - c.beta2) * (i == dim - 1 ? 1.0 : 0.0) * (k == dim - 1 ? 1.0 : 0.0));
+  if (compress) {
+    if (law == COH_BL || law == COH_BLNU) {
+      T[dim - 1] = (c.sigma_c / c.alpha) * sinh(c.alpha * delta[dim - 1] / c.delta_c1);
+      for (int i = 0; i < dim - 1; ++i) Dm[(dim - 1) * dim + i] = 0.0;
+      Dm[(dim - 1) * dim + dim - 1] = (c.sigma_c / c.delta_c1) * cosh(c.alpha * delta[dim - 1] / c.delta_c1);
+    } else if (law == COH_OPAUG) {
+      for (int i = 0; i < dim - 1; ++i) Dm[(dim - 1) * dim + i] = 0.0;
+      Dm[(dim - 1) * dim + dim - 1] = (c.sigma_c / c.delta_c) * exp(1.0 - dmax_copy / c.delta_c) * cosh(c.alpha * delta[dim - 1] / c.delta_c);
+    } else if (law == COH_OPNUAUG) {
+      for (int i = 0; i < dim - 1; ++i) Dm[(dim - 1) * dim + i] = 0.0;
+      Dm[(dim - 1) * dim + dim - 1] = (c.sigma_c * exp(1.0) / c.delta_c) * cosh(c.alpha * delta[dim - 1] / c.delta_c);
+    }
+  }
+  if (law == COH_BL || law == COH_BLNU) {
+    *zone = compress ? 0 : (deff <= c.delta_c1 ? 1 : (deff <= c.delta_c2 ? 2 : 3));
+  } else {
+    const double nf = deff / c.delta_c;
+    *zone = (nf <= 0) ? 0 : (nf <= 1 ? 1 : (nf <= 5.0 ? 2 : 3));
+  }
+}
+
+// Voigt B-matrix entry B(r, k*dim + q) for a node with gradient g (dim entries).
+template <typename T>
+__device__ inline T bmat(int dim, int r, int q, const T* g) {
+  if (dim == 2) {
+    if (r == 0) return q == 0 ? g[0] : T(0);
+    if (r == 1) return q == 1 ? g[1] : T(0);
+    return q == 0 ? g[1] : g[0];
+  }
+  switch (r) {
+    case 0: return q == 0 ? g[0] : T(0);
+    case 1: return q == 1 ? g[1] : T(0);
+    case 2: return q == 2 ? g[2] : T(0);
+    case 3: return q == 0 ? T(0) : (q == 1 ? g[2] : g[1]);
+    case 4: return q == 1 ? T(0) : (q == 0 ? g[2] : g[0]);
+    default: return q == 2 ? T(0) : (q == 0 ? g[1] : g[0]);
+  }
+}
+
+}  // namespace pgd

@@ -1,0 +1,793 @@
+// pg_setup.cpp -- host-side IGFEM set-up (see pg_setup.h).
+//
+// Reference steps restated here (paths relative to the PIGFEM source tree):
+//   structured mesh ............ src/Mesh.cpp:236-647 (Mesh::generate_mesh), periodic sets 649-760
+//   node detection ............. src/Mesh.cpp:2883-2929, src/InclusionCircle.cpp:142-163,
+//                                src/InclusionSphere.cpp:156-178
+//   cut-case tables ............ src/tri3.cpp:287-441 (Tri3::detection), src/tet4.cpp (Tet4::detection)
+//   enrichment nodes ........... src/Mesh.cpp:3103-3252 (Mesh::add_enrichments, serial),
+//                                src/Mesh.cpp:3661-3720 (add_enrich_node_to_elem), src/Inclusion.cpp:32-121
+//   sub-elements ............... src/elem.cpp:428-558 (generate_integration_elem, transformDetectionCohToReg)
+//   quadrature data ............ src/Mesh.cpp:1475-1643 (Mesh::store_shape_functions),
+//                                src/elem.cpp:115-139, src/Utilities.cpp:1017-1072 (det / inverse),
+//                                src/tri3.cpp:93-208, src/quad4.cpp:65-150, src/Polygon.cpp:51-228,
+//                                src/CohEdge2.cpp:55-200, src/CohesiveElem.cpp:140-238
+//   DOF numbering .............. src/DofObject.cpp:241-535
+//   CSR pattern ................ src/Assembler.cpp:659-679 (every element DOF pair is inserted)
+//   linear elastic D ........... src/material_lei.cpp:52-97
+#include "pg_setup.h"
+#include "pg_roots.h"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <set>
+#include <sstream>
+#include <tuple>
+#include <utility>
+
+namespace pg {
+namespace {
+
+const double kPI = 3.14159265358979323846264338327950;
+
+// ------------------------------------------------------------------ small dense helpers
+// det / inverse exactly as the reference's Utilities::det / Utilities::inverse compute them.
+double det2(const double J[2][2]) { return J[0][0] * J[1][1] - J[0][1] * J[1][0]; }
+double det3(const double J[3][3]) {
+  return J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+         J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+}
+void inv2(const double J[2][2], double R[2][2]) {
+  double d = det2(J);
+  double s = 1.0 / d;
+  R[0][0] = J[1][1] * s; R[1][1] = J[0][0] * s; R[0][1] = (-1.0 * J[0][1]) * s; R[1][0] = (-1.0 * J[1][0]) * s;
+}
+void inv3(const double J[3][3], double R[3][3]) {
+  R[0][0] = J[1][1] * J[2][2] - J[2][1] * J[1][2];
+  R[0][1] = -1.0 * (J[0][1] * J[2][2] - J[2][1] * J[0][2]);
+  R[0][2] = J[0][1] * J[1][2] - J[1][1] * J[0][2];
+  R[1][0] = -1.0 * (J[1][0] * J[2][2] - J[2][0] * J[1][2]);
+  R[1][1] = J[0][0] * J[2][2] - J[2][0] * J[0][2];
+  R[1][2] = -1.0 * (J[0][0] * J[1][2] - J[1][0] * J[0][2]);
+  R[2][0] = J[1][0] * J[2][1] - J[2][0] * J[1][1];
+  R[2][1] = -1.0 * (J[0][0] * J[2][1] - J[2][0] * J[0][1]);
+  R[2][2] = J[0][0] * J[1][1] - J[1][0] * J[0][1];
+  double s = 1.0 / det3(J);
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) R[i][j] *= s;
+}
+
+// Maps reference-coordinate gradients dNdr (n x dim) through the element geometry (node
+// coordinates xs, n x dim) to physical gradients dNdx and the Jacobian determinant
+// (Elem::transform_gradients).
+void transform_gradients(int dim, int n, const double* dNdr, const double* xs, double* dNdx, double* J) {
+  if (dim == 2) {
+    double Jac[2][2] = {{0, 0}, {0, 0}};
+    for (int a = 0; a < 2; ++a) for (int i = 0; i < 2; ++i) for (int k = 0; k < n; ++k) Jac[a][i] += dNdr[k * 2 + a] * xs[k * 2 + i];
+    *J = det2(Jac);
+    double R[2][2]; inv2(Jac, R);
+    for (int k = 0; k < n; ++k)
+      for (int i = 0; i < 2; ++i) dNdx[k * 2 + i] = R[i][0] * dNdr[k * 2 + 0] + R[i][1] * dNdr[k * 2 + 1];
+  } else {
+    double Jac[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int a = 0; a < 3; ++a) for (int i = 0; i < 3; ++i) for (int k = 0; k < n; ++k) Jac[a][i] += dNdr[k * 3 + a] * xs[k * 3 + i];
+    *J = det3(Jac);
+    double R[3][3]; inv3(Jac, R);
+    for (int k = 0; k < n; ++k)
+      for (int i = 0; i < 3; ++i)
+        dNdx[k * 3 + i] = R[i][0] * dNdr[k * 3 + 0] + R[i][1] * dNdr[k * 3 + 1] + R[i][2] * dNdr[k * 3 + 2];
+  }
+}
+
+// ------------------------------------------------------------------ quadrature rules
+// Tri3 order 3 (src/tri3.cpp:111-118): the 4-point rule with a negative centroid weight.
+const double kTri4[4][3] = {
+    {0.333333333333333333333333333333333, 0.333333333333333333333333333333333, -0.281250000000000000000000000000000},
+    {0.200000000000000000000000000000000, 0.200000000000000000000000000000000, 0.260416666666666666666666666666665},
+    {0.200000000000000000000000000000000, 0.600000000000000000000000000000000, 0.260416666666666666666666666666665},
+    {0.600000000000000000000000000000000, 0.200000000000000000000000000000000, 0.260416666666666666666666666666665}};
+// Tri3 order 5 (src/tri3.cpp:131-141), used by Polygon sub-elements (default order 5).
+const double kTri7[7][3] = {
+    {0.33333333333333, 0.33333333333333, 0.112500000000000}, {0.47014206410511, 0.47014206410511, 0.066197076394255},
+    {0.47014206410511, 0.05971587178977, 0.066197076394255}, {0.05971587178977, 0.47014206410511, 0.066197076394255},
+    {0.10128650732346, 0.10128650732346, 0.062969590272415}, {0.10128650732346, 0.79742698535309, 0.062969590272415},
+    {0.79742698535309, 0.10128650732346, 0.062969590272415}};
+// Gauss-Legendre 2-point (edge order 3).
+const double kGauss2 = 0.57735026918962576450914878050196;
+
+void tri3_shape(double r, double s, double* N, double* dN) {
+  N[0] = 1.0 - r - s; N[1] = r; N[2] = s;
+  dN[0] = -1.0; dN[1] = -1.0; dN[2] = 1.0; dN[3] = 0.0; dN[4] = 0.0; dN[5] = 1.0;
+}
+void quad4_shape(double r, double s, double* N, double* dN) {
+  N[0] = 0.25 * (1.0 - r) * (1.0 - s); N[1] = 0.25 * (1.0 + r) * (1.0 - s);
+  N[2] = 0.25 * (1.0 + r) * (1.0 + s); N[3] = 0.25 * (1.0 - r) * (1.0 + s);
+  dN[0] = -0.25 * (1.0 - s); dN[1] = -0.25 * (1.0 - r);
+  dN[2] = 0.25 * (1.0 - s);  dN[3] = -0.25 * (1.0 + r);
+  dN[4] = 0.25 * (1.0 + s);  dN[5] = 0.25 * (1.0 + r);
+  dN[6] = -0.25 * (1.0 + s); dN[7] = 0.25 * (1.0 - r);
+}
+// Quad4 order 3: tensor product of the 2-point edge rule, qp -> (qp % 2, qp / 2) (src/quad4.cpp:108-127).
+void quad4_qp(int qp, double* r, double* s, double* w) {
+  const double g[2] = {-kGauss2, kGauss2};
+  *r = g[qp % 2]; *s = g[qp / 2]; *w = 1.0 * 1.0;
+}
+
+// Polygon (Wachspress over the regular reference polygon), src/Polygon.cpp:51-228.
+void poly_points(int nn, double px[], double py[]) {
+  for (int n = 0; n < nn; ++n) {
+    px[n] = std::cos(2.0 * kPI * (n + 1) / nn);
+    py[n] = std::sin(2.0 * kPI * (n + 1) / nn);
+  }
+}
+void poly_tri(int nn, int t, int tri[3]) { tri[0] = nn; tri[1] = t; tri[2] = (t == nn - 1) ? 0 : t + 1; }
+void poly_qp(int nn, int qp, double* r, double* s, double* w) {
+  double px[32], py[32];
+  poly_points(nn, px, py);
+  px[nn] = 0.0; py[nn] = 0.0;
+  const int t = qp / 7, q = qp % 7;
+  double tN[3], tdN[6];
+  tri3_shape(kTri7[q][0], kTri7[q][1], tN, tdN);
+  int tri[3]; poly_tri(nn, t, tri);
+  double J0[2][2] = {{0, 0}, {0, 0}};
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j)
+      for (int n = 0; n < 3; ++n) J0[i][j] += (i == 0 ? px[tri[n]] : py[tri[n]]) * tdN[n * 2 + j];
+  double dJ = J0[0][0] * J0[1][1] - J0[0][1] * J0[1][0];
+  *w = dJ * kTri7[q][2];
+  double cx = 0.0, cy = 0.0;
+  for (int n = 0; n < 3; ++n) { cx += tN[n] * px[tri[n]]; cy += tN[n] * py[tri[n]]; }
+  *r = cx; *s = cy;
+}
+void poly_shape(int nn, double r, double s, double* N, double* dN) {
+  double px[33], py[33];
+  poly_points(nn, px, py);
+  px[nn] = r; py[nn] = s;
+  double A[33], dA[33][2], alpha[32], dal[32][2];
+  for (int n = 0; n < nn; ++n) {
+    int tri[3]; poly_tri(nn, n, tri);
+    const double x0 = px[tri[0]], y0 = py[tri[0]], x1 = px[tri[1]], y1 = py[tri[1]], x2 = px[tri[2]], y2 = py[tri[2]];
+    A[n + 1] = 0.5 * ((x1 * y2 - y1 * x2) - (x0 * y2 - y0 * x2) + (x0 * y1 - y0 * x1));
+    dA[n + 1][0] = 0.5 * (y2 - y1);
+    dA[n + 1][1] = 0.5 * (x1 - x2);
+  }
+  A[0] = A[nn]; dA[0][0] = dA[nn][0]; dA[0][1] = dA[nn][1];
+  double sa = 0.0, sd0 = 0.0, sd1 = 0.0;
+  for (int n = 0; n < nn; ++n) {
+    alpha[n] = 1.0 / (A[n] * A[n + 1]);
+    dal[n][0] = -1.0 * alpha[n] * (dA[n][0] / A[n] + dA[n + 1][0] / A[n + 1]);
+    dal[n][1] = -1.0 * alpha[n] * (dA[n][1] / A[n] + dA[n + 1][1] / A[n + 1]);
+    sa += alpha[n]; sd0 += dal[n][0]; sd1 += dal[n][1];
+  }
+  for (int n = 0; n < nn; ++n) {
+    if (N) N[n] = alpha[n] / sa;
+    double Nn = alpha[n] / sa;
+    dN[n * 2 + 0] = (dal[n][0] - Nn * sd0) / sa;
+    dN[n * 2 + 1] = (dal[n][1] - Nn * sd1) / sa;
+  }
+}
+
+// Tet4 order 3 (src/tet4.cpp:87-160): 5 points, weights summing to 1 (6x the tet volume).
+const double kTet5[5][4] = {{0.25, 0.25, 0.25, -0.8},
+                            {0.5, 0.166666666666666666666666666666667, 0.166666666666666666666666666666667, 0.45},
+                            {0.166666666666666666666666666666667, 0.5, 0.166666666666666666666666666666667, 0.45},
+                            {0.166666666666666666666666666666667, 0.166666666666666666666666666666667, 0.5, 0.45},
+                            {0.166666666666666666666666666666667, 0.166666666666666666666666666666667, 0.166666666666666666666666666666667, 0.45}};
+void tet4_shape(double r, double s, double t, double* N, double* dN) {
+  N[0] = 1.0 - r - s - t; N[1] = r; N[2] = s; N[3] = t;
+  const double g[12] = {-1, -1, -1, 1, 0, 0, 0, 1, 0, 0, 0, 1};
+  for (int i = 0; i < 12; ++i) dN[i] = g[i];
+}
+
+// ------------------------------------------------------------------ inclusions
+struct Inclusion {
+  int dim;
+  double c[3], r;
+  // Bounding box used by Mesh::detect_node before the exact test.  The sphere's upper z bound is
+  // the centre's y coordinate plus r, as the reference writes it (src/InclusionSphere.cpp:158).
+  bool in_box(const double* x) const {
+    if (dim == 2) return (c[0] - r <= x[0]) && (c[1] - r <= x[1]) && (x[0] <= c[0] + r) && (x[1] <= c[1] + r);
+    return (c[0] - r <= x[0]) && (c[1] - r <= x[1]) && (c[2] - r <= x[2]) && (x[0] <= c[0] + r) && (x[1] <= c[1] + r) &&
+           (x[2] <= c[1] + r);
+  }
+  // 0 outside, 1 on the surface (within 1e-12), 2 inside.
+  int detect(const double* x) const {
+    double val;
+    if (dim == 2) {
+      double dx = x[0] - c[0], dy = x[1] - c[1];
+      val = (std::sqrt(dx * dx + dy * dy) - r) / r;
+    } else {
+      double gx = x[0] - c[0], gy = x[1] - c[1], gz = x[2] - c[2];
+      val = std::pow(gx / r, 2) + std::pow(gy / r, 2) + std::pow(gz / r, 2) - 1.0;
+    }
+    if (val > 1e-12) return 0;
+    if (val < -1e-12) return 2;
+    return 1;
+  }
+  // level set along the edge p0 -> p1 and its derivative (InclusionCircle::int_fdf / InclusionSphere)
+  void fdf(const double* p0, const double* p1, double a, double* f, double* df) const {
+    if (dim == 2) {
+      double g0 = p0[0] + a * (p1[0] - p0[0]) - c[0];
+      double g1 = p0[1] + a * (p1[1] - p0[1]) - c[1];
+      double d0 = p1[0] - p0[0], d1 = p1[1] - p0[1];
+      *f = std::pow(g0 / r, 2) + std::pow(g1 / r, 2) - 1;
+      *df = (1 / (r * r)) * 2.0 * (g0 * d0 + g1 * d1);
+    } else {
+      double g0 = p0[0] + a * (p1[0] - p0[0]) - c[0];
+      double g1 = p0[1] + a * (p1[1] - p0[1]) - c[1];
+      double g2 = p0[2] + a * (p1[2] - p0[2]) - c[2];
+      double d0 = p1[0] - p0[0], d1 = p1[1] - p0[1], d2 = p1[2] - p0[2];
+      *f = std::pow(g0 / r, 2) + std::pow(g1 / r, 2) + std::pow(g2 / r, 2) - 1.0;
+      *df = (2.0 / (r * r)) * (g0 * d0 + g1 * d1 + g2 * d2);
+    }
+  }
+};
+
+struct EdgeFn {
+  const Inclusion* inc;
+  const double* p0;
+  const double* p1;
+  void eval(double a, double* f, double* df) const { inc->fdf(p0, p1, a, f, df); }
+};
+
+// ------------------------------------------------------------------ cut-case tables
+struct CutCase {
+  std::vector<int> cut_edge;   // local edge of each enrichment node
+  std::vector<int> incl;       // inclusion of each enrichment node
+  std::vector<std::vector<int>> sub;   // sub-element local node lists (parent 0..npe-1, enrichment npe.., mirrors after)
+  std::vector<int> sub_mat;    // -1 = the element's own material, k >= 0 = inclusion k's material
+  std::vector<std::vector<int>> coh;   // cohesive element local node lists
+};
+
+// Tri3::detection (src/tri3.cpp:287-441): node detection values -> cut case (cohesive numbering).
+bool tri3_case(const int nd[3], CutCase& cc) {
+  const int n0 = nd[0], n1 = nd[1], n2 = nd[2];
+  const bool n0e1 = n0 == n1, n0e2 = n0 == n2, n1e2 = n1 == n2;
+  std::vector<int> v = {n0, n1, n2};
+  std::sort(v.begin(), v.end());
+  v.erase(std::unique(v.begin(), v.end()), v.end());
+  const int nu = (int)v.size();
+  if (nu == 1) return false;
+  auto M = [](int k) { return k; };  // inclusion index as material selector (-1 = element material)
+  if (nu == 2) {
+    if (v[0] < 0) {
+      if (n1e2) {
+        cc.cut_edge = {2, 0}; cc.sub_mat = {M(n0), M(n1)};
+        if (n0 < n1) { cc.sub = {{0, 4, 3}, {1, 2, 5, 6}}; cc.coh = {{3, 4, 5, 6}}; }
+        else { cc.sub = {{0, 6, 5}, {1, 2, 3, 4}}; cc.coh = {{4, 3, 6, 5}}; }
+      } else if (n0e2) {
+        cc.cut_edge = {0, 1}; cc.sub_mat = {M(n1), M(n0)};
+        if (n1 < n0) { cc.sub = {{1, 4, 3}, {2, 0, 5, 6}}; cc.coh = {{3, 4, 5, 6}}; }
+        else { cc.sub = {{1, 6, 5}, {2, 0, 3, 4}}; cc.coh = {{4, 3, 6, 5}}; }
+      } else {
+        cc.cut_edge = {1, 2}; cc.sub_mat = {M(n2), M(n0)};
+        if (n2 < n0) { cc.sub = {{2, 4, 3}, {0, 1, 5, 6}}; cc.coh = {{3, 4, 5, 6}}; }
+        else { cc.sub = {{2, 6, 5}, {0, 1, 3, 4}}; cc.coh = {{4, 3, 6, 5}}; }
+      }
+      cc.incl.assign(cc.cut_edge.size(), v[1]);
+    } else {
+      if (n1e2) {
+        cc.cut_edge = {2, 0, 2, 0}; cc.incl = {n0, n0, n1, n1};
+        cc.sub_mat = {M(n0), -1, M(n1)}; cc.sub = {{0, 8, 7}, {4, 6, 5, 3}, {1, 2, 9, 10}};
+      } else if (n0e2) {
+        cc.cut_edge = {0, 1, 0, 1}; cc.incl = {n1, n1, n2, n2};
+        cc.sub_mat = {M(n1), -1, M(n2)}; cc.sub = {{1, 8, 7}, {4, 6, 5, 3}, {2, 0, 9, 10}};
+      } else {
+        cc.cut_edge = {1, 2, 1, 2}; cc.incl = {n2, n2, n0, n0};
+        cc.sub_mat = {M(n2), -1, M(n0)}; cc.sub = {{2, 8, 7}, {4, 6, 5, 3}, {0, 1, 9, 10}};
+      }
+      cc.coh = {{4, 3, 8, 7}, {5, 6, 9, 10}};
+    }
+  } else {
+    if (v[0] < 0) {
+      if (n0 < 0) {
+        cc.cut_edge = {1, 0, 2, 1}; cc.incl = {n1, n1, n2, n2};
+        cc.sub_mat = {M(n1), -1, M(n2)}; cc.sub = {{1, 7, 8}, {0, 4, 3, 6, 5}, {2, 9, 10}};
+      } else if (n1 < 0) {
+        cc.cut_edge = {2, 1, 0, 2}; cc.incl = {n2, n2, n0, n0};
+        cc.sub_mat = {M(n2), -1, M(n0)}; cc.sub = {{2, 7, 8}, {1, 4, 3, 6, 5}, {0, 9, 10}};
+      } else {
+        cc.cut_edge = {0, 2, 1, 0}; cc.incl = {n0, n0, n1, n1};
+        cc.sub_mat = {M(n0), -1, M(n1)}; cc.sub = {{0, 7, 8}, {2, 4, 3, 6, 5}, {1, 9, 10}};
+      }
+      cc.coh = {{3, 4, 7, 8}, {5, 6, 9, 10}};
+    } else {
+      cc.cut_edge = {0, 2, 2, 1, 1, 0}; cc.incl = {n0, n0, n2, n2, n1, n1};
+      cc.sub_mat = {M(n0), M(n2), M(n1), -1};
+      cc.sub = {{0, 9, 10}, {2, 11, 12}, {1, 13, 14}, {8, 7, 6, 5, 4, 3}};
+      cc.coh = {{3, 4, 9, 10}, {5, 6, 11, 12}, {7, 8, 13, 14}};
+    }
+  }
+  return true;
+}
+
+const int kTriEdge[3][2] = {{0, 1}, {1, 2}, {2, 0}};
+const int kQuadEdge[4][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}};
+const int kTetEdge[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+
+}  // namespace
+
+int build_setup(const ProblemDesc& d, Setup& s) {
+  s = Setup();
+  s.desc = d;
+  s.etype = d.elem_type;
+  s.dim = (d.elem_type == TET4) ? 3 : 2;
+  s.npe = (d.elem_type == TRI3) ? 3 : 4;
+  s.cohesive = d.coh_law != COH_NONE;
+  const int dim = s.dim;
+  if (d.elem_type == QUAD4 && !d.incl.empty()) {
+    s.error = "cut quad4 parents are not supported; use tri3 or tet4 background elements with inclusions";
+    return 2;
+  }
+
+  // ---------------- materials (material_lei.cpp:52-97); D is latched per material by dimension
+  s.nvoigt = (dim == 2) ? 3 : 6;
+  const double Es[2] = {d.E_matrix, d.E_fiber}, nus[2] = {d.nu_matrix, d.nu_fiber};
+  for (int m = 0; m < 2; ++m) {
+    double* D = s.D[m];
+    for (int i = 0; i < 36; ++i) D[i] = 0.0;
+    const double E = Es[m], nu = nus[m];
+    if (dim == 2) {
+      if (d.plane_strain) {
+        double coef = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
+        D[0] = coef * (1.0 - nu); D[1] = coef * nu; D[3] = coef * nu; D[4] = coef * (1.0 - nu);
+        D[8] = coef * (1.0 - 2.0 * nu) / 2.0;
+      } else {
+        double coef = E / (1.0 - nu * nu);
+        D[0] = coef; D[1] = coef * nu; D[3] = coef * nu; D[4] = coef; D[8] = coef * (1.0 - nu) / 2.0;
+      }
+    } else {
+      double coef = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
+      for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) D[i * 6 + j] = coef * (i == j ? (1.0 - nu) : nu);
+      for (int i = 3; i < 6; ++i) D[i * 6 + i] = coef * (1.0 - 2.0 * nu) / 2;
+    }
+  }
+
+  // ---------------- cohesive law constants
+  s.coh.law = d.coh_law;
+  switch (d.coh_law) {
+    case COH_BL: case COH_BLNU:
+      s.coh.sigma_c = d.coh[0]; s.coh.delta_c1 = d.coh[1]; s.coh.delta_c2 = d.coh[2];
+      s.coh.nvar = (d.coh_law == COH_BL) ? 1 : 0; break;
+    case COH_XN: case COH_XNNU:
+      s.coh.sigma_c = d.coh[0]; s.coh.delta_cn = d.coh[1]; s.coh.delta_ct = d.coh[2]; s.coh.q = d.coh[3];
+      s.coh.nvar = (d.coh_law == COH_XN) ? 2 : 0; break;
+    case COH_OP: case COH_OPNU: case COH_OPAUG: case COH_OPNUAUG:
+      s.coh.sigma_c = d.coh[0]; s.coh.delta_c = d.coh[1]; s.coh.beta2 = d.coh[2] * d.coh[2];
+      s.coh.nvar = (d.coh_law == COH_OP || d.coh_law == COH_OPAUG) ? 1 : 0; break;
+    default: break;
+  }
+
+  // ---------------- structured mesh (Mesh::generate_mesh)
+  const int Nx = d.n[0], Ny = d.n[1], Nz = (dim == 3) ? d.n[2] : 0;
+  if (Nx <= 0 || Ny <= 0 || (dim == 3 && Nz <= 0)) { s.error = "grid counts must be positive"; return 2; }
+  const double hx = (d.hi[0] - d.lo[0]) / Nx, hy = (d.hi[1] - d.lo[1]) / Ny;
+  const double hz = (dim == 3) ? (d.hi[2] - d.lo[2]) / Nz : 0.0;
+  const long long nstd_ll = (long long)(Nx + 1) * (Ny + 1) * (Nz + 1);
+  if (nstd_ll > 400000000LL) { s.error = "mesh too large"; return 2; }
+  s.n_std = (int)nstd_ll;
+  std::vector<double> X3((size_t)s.n_std * 3);  // 3-component copy used by the geometric tests
+  for (int k = 0; k <= Nz; ++k)
+    for (int j = 0; j <= Ny; ++j)
+      for (int i = 0; i <= Nx; ++i) {
+        size_t id = (size_t)i + (size_t)j * (Nx + 1) + (size_t)k * (Nx + 1) * (Ny + 1);
+        X3[id * 3 + 0] = d.lo[0] + i * hx;
+        X3[id * 3 + 1] = d.lo[1] + j * hy;
+        X3[id * 3 + 2] = (dim == 3 ? d.lo[2] : 0.0) + k * hz;
+      }
+  auto nid = [&](int i, int j, int k) { return i + j * (Nx + 1) + k * (Nx + 1) * (Ny + 1); };
+  if (d.elem_type == TRI3) {
+    s.ne = 2 * Nx * Ny;
+    s.conn.resize((size_t)s.ne * 3);
+    size_t e = 0;
+    for (int j = 0; j < Ny; ++j)
+      for (int i = 0; i < Nx; ++i) {
+        int c[6];
+        if ((i + j) % 2 == 0) {
+          c[0] = nid(i, j, 0); c[1] = nid(i + 1, j, 0); c[2] = nid(i + 1, j + 1, 0);
+          c[3] = nid(i, j, 0); c[4] = nid(i + 1, j + 1, 0); c[5] = nid(i, j + 1, 0);
+        } else {
+          c[0] = nid(i, j, 0); c[1] = nid(i + 1, j, 0); c[2] = nid(i, j + 1, 0);
+          c[3] = nid(i + 1, j, 0); c[4] = nid(i + 1, j + 1, 0); c[5] = nid(i, j + 1, 0);
+        }
+        for (int t = 0; t < 6; ++t) s.conn[e * 3 + t] = c[t];
+        e += 2;
+      }
+  } else if (d.elem_type == QUAD4) {
+    s.ne = Nx * Ny;
+    s.conn.resize((size_t)s.ne * 4);
+    size_t e = 0;
+    for (int j = 0; j < Ny; ++j)
+      for (int i = 0; i < Nx; ++i, ++e) {
+        s.conn[e * 4 + 0] = nid(i, j, 0); s.conn[e * 4 + 1] = nid(i + 1, j, 0);
+        s.conn[e * 4 + 2] = nid(i + 1, j + 1, 0); s.conn[e * 4 + 3] = nid(i, j + 1, 0);
+      }
+  } else {
+    s.ne = 6 * Nx * Ny * Nz;
+    s.conn.resize((size_t)s.ne * 4);
+    size_t e = 0;
+    for (int k = 0; k < Nz; ++k)
+      for (int j = 0; j < Ny; ++j)
+        for (int i = 0; i < Nx; ++i) {
+          const int n0 = nid(i, j, k), n1 = nid(i + 1, j, k), n2 = nid(i + 1, j + 1, k), n3 = nid(i, j + 1, k);
+          const int n4 = nid(i, j, k + 1), n5 = nid(i + 1, j, k + 1), n6 = nid(i + 1, j + 1, k + 1), n7 = nid(i, j + 1, k + 1);
+          const int tets[6][4] = {{n0, n2, n3, n6}, {n0, n3, n7, n6}, {n0, n7, n4, n6},
+                                  {n0, n5, n6, n4}, {n1, n5, n6, n0}, {n1, n6, n2, n0}};
+          for (int t = 0; t < 6; ++t, ++e)
+            for (int q = 0; q < 4; ++q) s.conn[e * 4 + q] = tets[t][q];
+        }
+  }
+  s.elem_mat.assign(s.ne, 0);
+  s.cut_of.assign(s.ne, -1);
+
+  // periodic DOF owners (Mesh::build_periodic_nodesets: the primary is the lowest id of a set)
+  s.dnode.resize(s.n_std);
+  for (int k = 0; k <= Nz; ++k)
+    for (int j = 0; j <= Ny; ++j)
+      for (int i = 0; i <= Nx; ++i) {
+        int id = nid(i, j, k);
+        s.dnode[id] = d.subscale ? nid(i % Nx, j % Ny, (dim == 3) ? (k % Nz) : 0) : id;
+      }
+
+  // ---------------- inclusions and node detection (Mesh::detect_node)
+  std::vector<Inclusion> incs;
+  const int stride = dim + 1;
+  for (size_t i = 0; i + stride <= d.incl.size(); i += stride) {
+    Inclusion in;
+    in.dim = dim;
+    in.c[0] = d.incl[i]; in.c[1] = d.incl[i + 1]; in.c[2] = (dim == 3) ? d.incl[i + 2] : 0.0;
+    in.r = d.incl[i + dim];
+    incs.push_back(in);
+  }
+  const int ninc = (int)incs.size();
+  s.node_detect.assign(s.n_std, -1);
+  for (int n = 0; n < s.n_std; ++n) {
+    const double* x = &X3[(size_t)n * 3];
+    int res = -1;
+    for (int j = ninc - 1; j >= 0; --j) {
+      if (!incs[j].in_box(x)) continue;
+      int r = incs[j].detect(x);
+      if (r == 0) continue;
+      if (r == 1) {
+        std::ostringstream os;
+        os << "node " << n << " lies on the surface of inclusion " << j
+           << " (the reference stops here: src/Mesh.cpp:2904-2911)";
+        s.error = os.str();
+        return 3;
+      }
+      res = j;
+      break;
+    }
+    s.node_detect[n] = res;
+  }
+
+  // ---------------- element detection (Tri3::detection / Tet4::detection)
+  std::vector<CutCase> cases;
+  std::vector<int> cut_elems;
+  for (int e = 0; e < s.ne; ++e) {
+    int nd[4];
+    for (int q = 0; q < s.npe; ++q) nd[q] = s.node_detect[s.conn[(size_t)e * s.npe + q]];
+    bool all_same = true;
+    for (int q = 1; q < s.npe; ++q) all_same &= (nd[q] == nd[0]);
+    if (all_same) {
+      if (nd[0] != -1) s.elem_mat[e] = 1;  // entirely inside a fiber
+      continue;
+    }
+    CutCase cc;
+    bool cut = false;
+    if (d.elem_type == TRI3) cut = tri3_case(nd, cc);
+    else { s.error = "element type has no cut-case table here"; return 4; }
+    if (!cut) continue;
+    s.cut_of[e] = (int)cut_elems.size();
+    cut_elems.push_back(e);
+    cases.push_back(cc);
+  }
+  s.ncut = (int)cut_elems.size();
+  s.cut_elem = cut_elems;
+
+  // ---------------- enrichment nodes (Mesh::add_enrichments, serial)
+  const int (*emap)[2] = (d.elem_type == TRI3) ? kTriEdge : (d.elem_type == QUAD4 ? kQuadEdge : kTetEdge);
+  std::set<std::tuple<int, int, int>> cut_edges;  // (min node, max node, inclusion), ordered as std::set<pair<vector,id>>
+  for (int c = 0; c < s.ncut; ++c) {
+    const int e = cut_elems[c];
+    const CutCase& cc = cases[c];
+    for (size_t i = 0; i < cc.cut_edge.size(); ++i) {
+      int a = s.conn[(size_t)e * s.npe + emap[cc.cut_edge[i]][0]], b = s.conn[(size_t)e * s.npe + emap[cc.cut_edge[i]][1]];
+      if (a > b) std::swap(a, b);
+      cut_edges.insert(std::make_tuple(a, b, cc.incl[i]));
+    }
+  }
+  const int n_init = (int)cut_edges.size();
+  s.n_enr_initial = n_init;
+  s.n_enr = s.cohesive ? 2 * n_init : n_init;
+  std::map<std::tuple<int, int, int>, int> edge_index;
+  std::vector<double> XE((size_t)s.n_enr * 3);
+  s.enr_edge.resize((size_t)s.n_enr * 2);
+  s.enr_incl.resize(s.n_enr);
+  {
+    int k = 0;
+    for (const auto& t : cut_edges) {
+      const int a = std::get<0>(t), b = std::get<1>(t), inc = std::get<2>(t);
+      const double* p0 = &X3[(size_t)a * 3];
+      const double* p1 = &X3[(size_t)b * 3];
+      double fa, fb, dfa;
+      incs[inc].fdf(p0, p1, 0.0, &fa, &dfa);
+      incs[inc].fdf(p0, p1, 1.0, &fb, &dfa);
+      if (fa * fb >= 0) {
+        std::ostringstream os;
+        os << "no sign change of inclusion " << inc << " on edge " << a << "-" << b << " (src/Inclusion.cpp:38-39)";
+        s.error = os.str();
+        return 5;
+      }
+      EdgeFn fn{&incs[inc], p0, p1};
+      double alpha = steffensen_then_brent(fn);
+      for (int q = 0; q < 3; ++q) XE[(size_t)k * 3 + q] = p0[q] + alpha * (p1[q] - p0[q]);
+      s.enr_edge[(size_t)k * 2] = a; s.enr_edge[(size_t)k * 2 + 1] = b; s.enr_incl[k] = inc;
+      edge_index[t] = k;
+      ++k;
+    }
+    if (s.cohesive)
+      for (int m = 0; m < n_init; ++m) {
+        for (int q = 0; q < 3; ++q) XE[(size_t)(m + n_init) * 3 + q] = XE[(size_t)m * 3 + q];
+        s.enr_edge[(size_t)(m + n_init) * 2] = s.enr_edge[(size_t)m * 2];
+        s.enr_edge[(size_t)(m + n_init) * 2 + 1] = s.enr_edge[(size_t)m * 2 + 1];
+        s.enr_incl[m + n_init] = s.enr_incl[m];
+      }
+  }
+  const int n_nodes = s.n_std + s.n_enr;
+  s.X.resize((size_t)n_nodes * dim);
+  for (int n = 0; n < s.n_std; ++n) for (int q = 0; q < dim; ++q) s.X[(size_t)n * dim + q] = X3[(size_t)n * 3 + q];
+  for (int n = 0; n < s.n_enr; ++n) for (int q = 0; q < dim; ++q) s.X[(size_t)(s.n_std + n) * dim + q] = XE[(size_t)n * 3 + q];
+  for (int n = 0; n < s.n_enr; ++n) s.dnode.push_back(s.n_std + n);
+  auto X3of = [&](int node) -> const double* {
+    return node < s.n_std ? &X3[(size_t)node * 3] : &XE[(size_t)(node - s.n_std) * 3];
+  };
+
+  // ---------------- per cut element: nodes, sub-elements, quadrature data
+  s.cut_node_off.push_back(0);
+  s.cut_sub_off.push_back(0);
+  s.sub_node_off.push_back(0);
+  s.cut_qp_off.push_back(0);
+  s.qp_grad_off.push_back(0);
+  s.cut_coh_off.push_back(0);
+  s.coh_local_off.push_back(0);
+  s.coh_qp_off.push_back(0);
+  for (int c = 0; c < s.ncut; ++c) {
+    const int e = cut_elems[c];
+    CutCase cc = cases[c];
+    const int ncut_e = (int)cc.cut_edge.size();
+    const int n_en = s.cohesive ? 2 * ncut_e : ncut_e;
+    // transformDetectionCohToReg: fold mirror indices back when the mesh is not cohesive
+    if (!s.cohesive) {
+      for (auto& sub : cc.sub)
+        for (int& v : sub)
+          if (v >= s.npe + ncut_e) v -= ncut_e;
+      cc.coh.clear();
+    }
+    // enrichment node of each slot (add_enrich_node_to_elem)
+    std::vector<int> slot(n_en, -1);
+    for (int i = 0; i < ncut_e; ++i) {
+      int a = s.conn[(size_t)e * s.npe + emap[cc.cut_edge[i]][0]], b = s.conn[(size_t)e * s.npe + emap[cc.cut_edge[i]][1]];
+      if (a > b) std::swap(a, b);
+      auto it = edge_index.find(std::make_tuple(a, b, cc.incl[i]));
+      if (it == edge_index.end()) { s.error = "internal: cut edge without enrichment node"; return 6; }
+      // first cut-edge entry with this (edge, inclusion) takes the node
+      int first = i;
+      for (int i2 = 0; i2 < i; ++i2) {
+        int a2 = s.conn[(size_t)e * s.npe + emap[cc.cut_edge[i2]][0]], b2 = s.conn[(size_t)e * s.npe + emap[cc.cut_edge[i2]][1]];
+        if (a2 > b2) std::swap(a2, b2);
+        if (a2 == a && b2 == b && cc.incl[i2] == cc.incl[i]) { first = i2; break; }
+      }
+      if (first != i) { s.error = "internal: repeated (edge, inclusion) in one element"; return 6; }
+      slot[i] = s.n_std + it->second;
+      if (s.cohesive) slot[i + ncut_e] = s.n_std + it->second + n_init;
+    }
+    // element node list: parent nodes then enrichment slots
+    std::vector<int> enodes;
+    for (int q = 0; q < s.npe; ++q) enodes.push_back(s.conn[(size_t)e * s.npe + q]);
+    for (int q = 0; q < n_en; ++q) enodes.push_back(slot[q]);
+    const int nall = (int)enodes.size();
+    for (int v : enodes) s.cut_nodes.push_back(v);
+    s.cut_node_off.push_back((int)s.cut_nodes.size());
+
+    // parent gradients (constant for the affine tri3 / tet4 parents)
+    double pxs[4 * 3], pdNdr[4 * 3], pdNdx[4 * 3], pN[4], pJ;
+    for (int q = 0; q < s.npe; ++q) for (int k = 0; k < dim; ++k) pxs[q * dim + k] = X3of(enodes[q])[k];
+    if (dim == 2) tri3_shape(0.0, 0.0, pN, pdNdr);
+    else tet4_shape(0.0, 0.0, 0.0, pN, pdNdr);
+    transform_gradients(dim, s.npe, pdNdr, pxs, pdNdx, &pJ);
+
+    for (size_t ie = 0; ie < cc.sub.size(); ++ie) {
+      const std::vector<int>& sub = cc.sub[ie];
+      const int nsn = (int)sub.size();
+      int stype;
+      if (dim == 2) stype = (nsn == 3) ? SUB_TRI3 : (nsn == 4 ? SUB_QUAD4 : SUB_POLYGON);
+      else stype = (nsn == 4) ? SUB_TET4 : (nsn == 6 ? SUB_PRISM6 : SUB_HEX8);
+      const int mat = (cc.sub_mat[ie] < 0) ? s.elem_mat[e] : 1;
+      s.sub_type.push_back(stype);
+      s.sub_mat.push_back(mat);
+      std::vector<int> gsub(nsn);
+      double sx[32 * 3];
+      for (int q = 0; q < nsn; ++q) {
+        gsub[q] = enodes[sub[q]];
+        s.sub_nodes.push_back(gsub[q]);
+        for (int k = 0; k < dim; ++k) sx[q * dim + k] = X3of(gsub[q])[k];
+      }
+      s.sub_node_off.push_back((int)s.sub_nodes.size());
+      int nqp = 0;
+      if (stype == SUB_TRI3) nqp = 4;
+      else if (stype == SUB_QUAD4) nqp = 4;
+      else if (stype == SUB_POLYGON) nqp = 7 * nsn;
+      else { s.error = "3D sub-elements are not supported here"; return 4; }
+      for (int qp = 0; qp < nqp; ++qp) {
+        double r, t, w, cN[32], cdN[64], cdNdx[64], cJ;
+        if (stype == SUB_TRI3) { r = kTri4[qp][0]; t = kTri4[qp][1]; w = kTri4[qp][2]; tri3_shape(r, t, cN, cdN); }
+        else if (stype == SUB_QUAD4) { quad4_qp(qp, &r, &t, &w); quad4_shape(r, t, cN, cdN); }
+        else { poly_qp(nsn, qp, &r, &t, &w); poly_shape(nsn, r, t, cN, cdN); }
+        transform_gradients(2, nsn, cdN, sx, cdNdx, &cJ);
+        if (cJ < 0.0) { s.error = "negative sub-element Jacobian (src/Mesh.cpp:1561)"; return 7; }
+        s.qp_wgt.push_back(cJ * w);
+        s.qp_mat.push_back(mat);
+        // gradients over the element's nodes: parent gradients, then the child gradient of the
+        // sub-element node that is each enrichment node (zero when the sub-element lacks it)
+        for (int q = 0; q < s.npe; ++q) for (int k = 0; k < dim; ++k) s.qp_grad.push_back(pdNdx[q * dim + k]);
+        for (int en = 0; en < n_en; ++en) {
+          const int id = enodes[s.npe + en];
+          int found = -1;
+          for (int q = 0; q < nsn; ++q) if (gsub[q] == id) { found = q; break; }
+          for (int k = 0; k < dim; ++k) s.qp_grad.push_back(found >= 0 ? 1.0 * cdNdx[found * dim + k] : 0.0);
+        }
+        s.qp_grad_off.push_back((int)s.qp_grad.size());
+      }
+    }
+    s.cut_sub_off.push_back((int)s.sub_type.size());
+    s.cut_qp_off.push_back((int)s.qp_wgt.size());
+
+    // cohesive elements (CohEdge2, 2-point Gauss; rotation from the '-' side nodes)
+    for (size_t ce = 0; ce < cc.coh.size(); ++ce) {
+      const std::vector<int>& cl = cc.coh[ce];
+      const int nh = (int)cl.size() / 2;
+      s.coh_nh.push_back(nh);
+      for (int v : cl) s.coh_local.push_back(v);
+      s.coh_local_off.push_back((int)s.coh_local.size());
+      if (dim != 2) { s.error = "3D cohesive elements are not supported here"; return 4; }
+      for (int qp = 0; qp < 2; ++qp) {
+        const double xi = (qp == 0) ? -kGauss2 : kGauss2;
+        const double w = 1.0;
+        const double N0 = 0.5 * (1.0 - xi), N1 = 0.5 * (1 + xi);
+        const double* x0 = X3of(enodes[cl[0]]);
+        const double* x1 = X3of(enodes[cl[1]]);
+        double Jac[2] = {0.0, 0.0};
+        for (int i = 0; i < 2; ++i) { Jac[i] += -0.5 * x0[i]; Jac[i] += 0.5 * x1[i]; }
+        const double nrm[2] = {-Jac[1], Jac[0]};
+        const double mag = std::sqrt(Jac[0] * Jac[0] + Jac[1] * Jac[1]);
+        const double dA = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1]);
+        s.cqp_N.push_back(N0 * 1.0);
+        s.cqp_N.push_back(N1 * 1.0);
+        s.cqp_R.push_back(Jac[0] / mag); s.cqp_R.push_back(Jac[1] / mag);
+        s.cqp_R.push_back(nrm[0] / dA);  s.cqp_R.push_back(nrm[1] / dA);
+        s.cqp_wgt.push_back(dA * w);
+        s.cqp_isv.push_back(s.n_isv);
+        s.n_isv += s.coh.nvar;
+      }
+      s.coh_qp_off.push_back((int)s.cqp_wgt.size());
+    }
+    s.cut_coh_off.push_back((int)s.coh_nh.size());
+  }
+
+  // ---------------- DOF numbering (DofObject::set_local_owned_normal_dofs / _enrich_dofs)
+  // Dirichlet conditions as Tests/Main.cpp:549-581 applies them.
+  std::vector<std::vector<std::pair<bool, double>>> bc(s.n_std, std::vector<std::pair<bool, double>>(dim, {false, 0.0}));
+  if (d.subscale) {
+    for (int q = 0; q < dim; ++q) bc[0][q] = {true, 0.0};
+  } else {
+    const double app = (d.hi[0] - d.lo[0]) * d.app_strain;
+    for (int k = 0; k <= Nz; ++k)
+      for (int j = 0; j <= Ny; ++j) {
+        bc[nid(Nx, j, k)][0] = {true, app};
+        bc[nid(0, j, k)][0] = {true, 0.0};
+      }
+    for (int q = 0; q < dim; ++q) bc[0][q] = {true, 0.0};
+  }
+  int nfree = 0, nconst_ = 0;
+  for (int n = 0; n < s.n_std; ++n)
+    if (s.dnode[n] == n) for (int q = 0; q < dim; ++q) { if (bc[n][q].first) nconst_++; else nfree++; }
+  nfree += s.n_enr * dim;
+  s.n_free = nfree; s.n_const = nconst_;
+  s.node_dof.assign((size_t)n_nodes * dim, -1);
+  s.dirichlet.assign(nconst_, 0.0);
+  {
+    int f = 0, p = 0;
+    for (int n = 0; n < s.n_std; ++n) {
+      if (s.dnode[n] != n) continue;
+      for (int q = 0; q < dim; ++q) {
+        if (bc[n][q].first) { s.node_dof[(size_t)n * dim + q] = nfree + p; s.dirichlet[p] = bc[n][q].second; ++p; }
+        else s.node_dof[(size_t)n * dim + q] = f++;
+      }
+    }
+    for (int n = 0; n < s.n_enr; ++n)
+      for (int q = 0; q < dim; ++q) s.node_dof[(size_t)(s.n_std + n) * dim + q] = f++;
+    for (int n = 0; n < s.n_std; ++n)
+      if (s.dnode[n] != n)
+        for (int q = 0; q < dim; ++q) s.node_dof[(size_t)n * dim + q] = s.node_dof[(size_t)s.dnode[n] * dim + q];
+  }
+
+  // ---------------- DOF nodes, adjacency and the CSR pattern
+  s.node_dn.assign(n_nodes, -1);
+  for (int n = 0; n < n_nodes; ++n)
+    if (s.dnode[n] == n) { s.node_dn[n] = s.n_dn++; s.dn_node.push_back(n); }
+  for (int n = 0; n < n_nodes; ++n) s.node_dn[n] = s.node_dn[s.dnode[n]];
+  std::vector<std::vector<int>> adj(s.n_dn);
+  std::vector<std::vector<int>> nb(s.n_dn);
+  auto elem_nodes = [&](int e, std::vector<int>& out) {
+    out.clear();
+    if (s.cut_of[e] < 0) for (int q = 0; q < s.npe; ++q) out.push_back(s.conn[(size_t)e * s.npe + q]);
+    else {
+      const int c = s.cut_of[e];
+      for (int k = s.cut_node_off[c]; k < s.cut_node_off[c + 1]; ++k) out.push_back(s.cut_nodes[k]);
+    }
+  };
+  std::vector<int> en;
+  for (int e = 0; e < s.ne; ++e) {
+    elem_nodes(e, en);
+    if ((int)en.size() > 32) { s.error = "element with more than 32 nodes"; return 8; }
+    for (size_t a = 0; a < en.size(); ++a) {
+      const int da = s.node_dn[en[a]];
+      adj[da].push_back(e * 32 + (int)a);
+      for (size_t b = 0; b < en.size(); ++b) nb[da].push_back(s.node_dn[en[b]]);
+    }
+  }
+  s.dn_adj_off.assign(1, 0);
+  s.dn_nbr_off.assign(1, 0);
+  for (int a = 0; a < s.n_dn; ++a) {
+    std::sort(nb[a].begin(), nb[a].end());
+    nb[a].erase(std::unique(nb[a].begin(), nb[a].end()), nb[a].end());
+    for (int v : adj[a]) s.dn_adj.push_back(v);
+    s.dn_adj_off.push_back((int)s.dn_adj.size());
+    for (int v : nb[a]) s.dn_nbr.push_back(v);
+    s.dn_nbr_off.push_back((int)s.dn_nbr.size());
+  }
+  // CSR of the four blocks; rows in DOF order follow DOF-node order.
+  s.nrows[0] = s.n_free; s.ncols[0] = s.n_free;
+  s.nrows[1] = s.n_free; s.ncols[1] = s.n_const;
+  s.nrows[2] = s.n_const; s.ncols[2] = s.n_free;
+  s.nrows[3] = s.n_const; s.ncols[3] = s.n_const;
+  for (int b = 0; b < 4; ++b) { s.rp[b].assign(s.nrows[b] + 1, 0); s.ci[b].clear(); }
+  // row lengths
+  for (int a = 0; a < s.n_dn; ++a) {
+    const int na = s.dn_node[a];
+    int cf = 0, cp = 0;
+    for (int k = s.dn_nbr_off[a]; k < s.dn_nbr_off[a + 1]; ++k) {
+      const int nbn = s.dn_node[s.dn_nbr[k]];
+      for (int q = 0; q < dim; ++q) { if (s.node_dof[(size_t)nbn * dim + q] < s.n_free) cf++; else cp++; }
+    }
+    for (int q = 0; q < dim; ++q) {
+      const int g = s.node_dof[(size_t)na * dim + q];
+      if (g < s.n_free) { s.rp[0][g + 1] = cf; s.rp[1][g + 1] = cp; }
+      else { s.rp[2][g - s.n_free + 1] = cf; s.rp[3][g - s.n_free + 1] = cp; }
+    }
+  }
+  for (int b = 0; b < 4; ++b) for (int r = 0; r < s.nrows[b]; ++r) s.rp[b][r + 1] += s.rp[b][r];
+  for (int b = 0; b < 4; ++b) s.ci[b].assign(s.rp[b][s.nrows[b]], -1);
+  for (int a = 0; a < s.n_dn; ++a) {
+    const int na = s.dn_node[a];
+    for (int q = 0; q < dim; ++q) {
+      const int g = s.node_dof[(size_t)na * dim + q];
+      const bool rf = g < s.n_free;
+      int pf = rf ? s.rp[0][g] : s.rp[2][g - s.n_free];
+      int pp = rf ? s.rp[1][g] : s.rp[3][g - s.n_free];
+      int* cif = rf ? s.ci[0].data() : s.ci[2].data();
+      int* cip = rf ? s.ci[1].data() : s.ci[3].data();
+      for (int k = s.dn_nbr_off[a]; k < s.dn_nbr_off[a + 1]; ++k) {
+        const int nbn = s.dn_node[s.dn_nbr[k]];
+        for (int q2 = 0; q2 < dim; ++q2) {
+          const int g2 = s.node_dof[(size_t)nbn * dim + q2];
+          if (g2 < s.n_free) cif[pf++] = g2; else cip[pp++] = g2 - s.n_free;
+        }
+      }
+    }
+  }
+  return 0;
+}
+
+}  // namespace pg

@@ -1,0 +1,61 @@
+"""Problem cases shared by the golden-fixture generator and the parity tests.
+
+Each case is a structured background mesh with circular (2D) or spherical (3D) inclusions, the
+benchmark materials and, where named, a cohesive law on every fiber/matrix interface; a seeded
+displacement field (DOF vector, free then constrained) and seeded committed internal variables
+drive one assembly.  Sizes are small enough for the reference's CPU assembly to finish in well
+under a second.
+"""
+import numpy as np
+
+E_M, NU_M, E_F, NU_F = 3.5e3, 0.35, 72e3, 0.22
+BL = (50.0, 5e-7, 5e-3, 0.0)
+XN = (50.0, 2e-4, 3e-4, 1.0)
+OP = (50.0, 2e-4, 1.0, 0.0)
+
+CASES = {
+    # name: dict(elem_type, n, incl, coh_law, coh, subscale, eps_macro, u_scale, isv_scale, seed)
+    "lin_tri3_one_fiber": dict(elem_type=0, n=(8, 8), incl=[[0.5, 0.5, 0.23]], coh_law=0, coh=(0, 0, 0, 0),
+                               subscale=0, u_scale=1e-3, isv_scale=0.0, seed=1),
+    "lin_tri3_three_fibers": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13], [0.45, 0.78, 0.1]],
+                                  coh_law=0, coh=(0, 0, 0, 0), subscale=0, u_scale=1e-3, isv_scale=0.0, seed=2),
+    "lin_tri3_two_fibers_one_element": dict(elem_type=0, n=(8, 8), incl=[[0.3817, 0.5123, 0.1031], [0.6022, 0.4871, 0.1017]],
+                                            coh_law=0, coh=(0, 0, 0, 0), subscale=0, u_scale=1e-3, isv_scale=0.0, seed=3),
+    "lin_tri3_subscale": dict(elem_type=0, n=(12, 12), incl=[[0.41, 0.47, 0.2]], coh_law=0, coh=(0, 0, 0, 0),
+                              subscale=1, eps_macro=(0.01, -0.004, 0.002), u_scale=1e-3, isv_scale=0.0, seed=4),
+    "coh_bl": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=1, coh=BL,
+                   subscale=0, u_scale=2e-4, isv_scale=0.0, seed=5),
+    "coh_blnu": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=2, coh=BL,
+                     subscale=0, u_scale=2e-4, isv_scale=0.0, seed=6),
+    "coh_xn": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=3, coh=XN,
+                   subscale=0, u_scale=2e-4, isv_scale=2e-4, seed=7),
+    "coh_xnnu": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=4, coh=XN,
+                     subscale=0, u_scale=2e-4, isv_scale=0.0, seed=8),
+    "coh_op": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=5, coh=OP,
+                   subscale=0, u_scale=2e-4, isv_scale=3e-4, seed=9),
+    "coh_opnu": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=6, coh=OP,
+                     subscale=0, u_scale=2e-4, isv_scale=0.0, seed=10),
+    "coh_opaug": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=7, coh=OP,
+                      subscale=0, u_scale=2e-4, isv_scale=3e-4, seed=11),
+    "coh_opnuaug": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=8, coh=OP,
+                        subscale=0, u_scale=2e-4, isv_scale=0.0, seed=12),
+    "coh_bl_two_fibers_one_element": dict(elem_type=0, n=(8, 8), incl=[[0.3817, 0.5123, 0.1031], [0.6022, 0.4871, 0.1017]],
+                                          coh_law=1, coh=BL, subscale=0, u_scale=2e-4, isv_scale=0.0, seed=13),
+}
+
+
+def case_arrays(c, n_free, n_const, n_isv):
+    """Seeded DOF vector and committed internal variables of a case."""
+    rng = np.random.default_rng(c["seed"])
+    U = rng.uniform(-c["u_scale"], c["u_scale"], n_free + n_const)
+    isv = rng.uniform(0.0, c["isv_scale"], n_isv) if c["isv_scale"] > 0 else np.zeros(n_isv)
+    return U, isv
+
+
+def spec_kwargs(c):
+    dim = 3 if c["elem_type"] == 2 else 2
+    em = tuple(c.get("eps_macro", ())) + (0.0,) * (6 - len(c.get("eps_macro", ())))
+    return dict(elem_type=c["elem_type"], n=c["n"], lo=(0.0,) * dim, hi=(1.0,) * dim,
+                inclusions=np.array(c["incl"], dtype=np.float64), E_matrix=E_M, nu_matrix=NU_M, E_fiber=E_F,
+                nu_fiber=NU_F, coh_law=c["coh_law"], coh=c["coh"], plane_strain=True, subscale=bool(c["subscale"]),
+                eps_macro=em, app_strain=0.01)

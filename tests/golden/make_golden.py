@@ -1,0 +1,40 @@
+"""Generates the golden fixtures tests/golden/<case>.npz by running the reference's own CPU
+assembly (oracle/_ref, built from the reference sources by oracle/Makefile) on the cases of
+tests/golden/cases.py.  Run from the repository root:  python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+from cases import CASES, case_arrays, spec_kwargs  # noqa: E402
+from oracle import ref  # noqa: E402
+
+
+def main(names=None):
+    for name, c in CASES.items():
+        if names and name not in names:
+            continue
+        R = ref.RefProblem(ref.ProblemSpec(**spec_kwargs(c)))
+        n_isv = int(R.get("isv_off")[-1])
+        U, isv = case_arrays(c, R.n_free, R.n_const, n_isv)
+        R.assemble(U, isv, 1.0)
+        out = dict(U_dof=U, isv_committed=isv, node_dofs=R.get("node_dofs"), isv_off=R.get("isv_off"),
+                   isv_elem_qp_off=R.get("isv_elem_qp_off"), P_f=R.get("P_f"), P_p=R.get("P_p"),
+                   isv_trial=R.get("isv_trial"), coh_zone=R.get("coh_zone"),
+                   node_coords=R.get("node_coords"), enrich_coords=R.get("enrich_coords"))
+        for b in ("K_ff", "K_fp", "K_pf", "K_pp"):
+            rp, ci, v, sh = R.csr(b)
+            out[b + "_rowptr"], out[b + "_cols"], out[b + "_vals"] = rp, ci, v
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        print(name, "free", R.n_free, "const", R.n_const, "nnz_ff", len(out["K_ff_vals"]), "isv", n_isv)
+        R.close()
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])
