@@ -326,6 +326,7 @@ void* pgref_create(const pgref_config* cfg) {
   else h->prob = new ProblemLinearElasticity;
   writeToScreen = false;
   logFile = h->log_path;
+  h->prob->getOptions()->setBoolOption("-WRITE_VTK", "false");
   h->prob->set_parameter("plane_strain", cfg->plane_strain ? 1.0 : 0.0);
   h->prob->attach_mesh(&mesh);
   writeToScreen = false;

@@ -3,8 +3,13 @@
 Each case is a structured background mesh with circular (2D) or spherical (3D) inclusions, the
 benchmark materials and, where named, a cohesive law on every fiber/matrix interface; a seeded
 displacement field (DOF vector, free then constrained) and seeded committed internal variables
-drive one assembly.  Sizes are small enough for the reference's CPU assembly to finish in well
-under a second.
+drive one assembly.  In cohesive cases the '+' (mirror) enrichment nodes are displaced from their
+'-' partners along the interface normal by a seeded opening drawn from `open` (log-uniform
+between the two bounds, negative bounds give compression), so every law is driven through its
+loading, softening, failed and (for the memory laws, with committed maxima drawn around the
+current opening) unloading branches at physically sized openings; `compress` cases exercise the
+compression penalty at openings where it stays finite.  Sizes are small enough for the reference's
+CPU assembly to finish in well under a second.
 """
 import numpy as np
 
@@ -24,38 +29,75 @@ CASES = {
     "lin_tri3_subscale": dict(elem_type=0, n=(12, 12), incl=[[0.41, 0.47, 0.2]], coh_law=0, coh=(0, 0, 0, 0),
                               subscale=1, eps_macro=(0.01, -0.004, 0.002), u_scale=1e-3, isv_scale=0.0, seed=4),
     "coh_bl": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=1, coh=BL,
-                   subscale=0, u_scale=2e-4, isv_scale=0.0, seed=5),
+                   subscale=0, u_scale=1e-6, isv_scale=0.0, seed=5, open=(1e-7, 1.2e-2)),
     "coh_blnu": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=2, coh=BL,
-                     subscale=0, u_scale=2e-4, isv_scale=0.0, seed=6),
+                     subscale=0, u_scale=1e-6, isv_scale=0.0, seed=6, open=(1e-7, 1.2e-2)),
     "coh_xn": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=3, coh=XN,
-                   subscale=0, u_scale=2e-4, isv_scale=2e-4, seed=7),
+                   subscale=0, u_scale=1e-6, isv_scale=1.0, seed=7, open=(1e-6, 1e-3)),
     "coh_xnnu": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=4, coh=XN,
-                     subscale=0, u_scale=2e-4, isv_scale=0.0, seed=8),
+                     subscale=0, u_scale=1e-6, isv_scale=0.0, seed=8, open=(1e-6, 1e-3)),
     "coh_op": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=5, coh=OP,
-                   subscale=0, u_scale=2e-4, isv_scale=3e-4, seed=9),
+                   subscale=0, u_scale=1e-6, isv_scale=1.0, seed=9, open=(1e-6, 1e-3)),
     "coh_opnu": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=6, coh=OP,
-                     subscale=0, u_scale=2e-4, isv_scale=0.0, seed=10),
+                     subscale=0, u_scale=1e-6, isv_scale=0.0, seed=10, open=(1e-6, 1e-3)),
     "coh_opaug": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=7, coh=OP,
-                      subscale=0, u_scale=2e-4, isv_scale=3e-4, seed=11),
+                      subscale=0, u_scale=1e-6, isv_scale=1.0, seed=11, open=(1e-6, 1e-3)),
     "coh_opnuaug": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=8, coh=OP,
-                        subscale=0, u_scale=2e-4, isv_scale=0.0, seed=12),
+                        subscale=0, u_scale=1e-6, isv_scale=0.0, seed=12, open=(1e-6, 1e-3)),
+    "coh_bl_compression": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=1, coh=BL,
+                               subscale=0, u_scale=1e-9, isv_scale=0.0, seed=14, open=(-2e-8, -1e-9)),
+    "coh_opaug_compression": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=7, coh=OP,
+                                  subscale=0, u_scale=1e-9, isv_scale=1.0, seed=15, open=(-4e-6, -1e-7)),
+    "coh_opnuaug_compression": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=8, coh=OP,
+                                    subscale=0, u_scale=1e-9, isv_scale=0.0, seed=16, open=(-4e-6, -1e-7)),
     "coh_bl_two_fibers_one_element": dict(elem_type=0, n=(8, 8), incl=[[0.3817, 0.5123, 0.1031], [0.6022, 0.4871, 0.1017]],
-                                          coh_law=1, coh=BL, subscale=0, u_scale=2e-4, isv_scale=0.0, seed=13),
+                                          coh_law=1, coh=BL, subscale=0, u_scale=1e-6, isv_scale=0.0, seed=13,
+                                          open=(1e-7, 1.2e-2)),
 }
 
 
 def case_arrays(c, n_free, n_const, n_isv):
-    """Seeded DOF vector and committed internal variables of a case."""
+    """Seeded DOF vector and committed internal variables of a bulk-only case."""
     rng = np.random.default_rng(c["seed"])
     U = rng.uniform(-c["u_scale"], c["u_scale"], n_free + n_const)
     isv = rng.uniform(0.0, c["isv_scale"], n_isv) if c["isv_scale"] > 0 else np.zeros(n_isv)
     return U, isv
 
 
+def cohesive_state(c, node_dofs, n_free, n_const, elem_node_off, elem_nodes, elem_cut, elem_coh_off,
+                   coh_struct, coh_struct_off, coh_qp_off, coh_R):
+    """DOF vector of a cohesive case (see the module docstring).
+
+    The topology arguments are the enriched-mesh tables (element node lists with enrichment nodes
+    after the parent nodes, cohesive local node lists, per-qp rotation matrices whose last row is
+    the interface normal)."""
+    rng = np.random.default_rng(c["seed"])
+    dim = 3 if c["elem_type"] == 2 else 2
+    U = rng.uniform(-c["u_scale"], c["u_scale"], n_free + n_const)
+    nd = node_dofs.reshape(-1, dim)
+    lo, hi = c["open"]
+    sign = 1.0 if lo > 0 else -1.0
+    a, b = np.log(abs(lo)), np.log(abs(hi))
+    for e in np.nonzero(elem_cut)[0]:
+        nodes = elem_nodes[elem_node_off[e]:elem_node_off[e + 1]]
+        for ce in range(elem_coh_off[e], elem_coh_off[e + 1]):
+            cl = coh_struct[coh_struct_off[ce]:coh_struct_off[ce + 1]]
+            nh = len(cl) // 2
+            q0, q1 = coh_qp_off[ce], coh_qp_off[ce + 1]
+            R = coh_R[q0 * dim * dim:q1 * dim * dim].reshape(-1, dim, dim).mean(axis=0)
+            for k in range(nh):
+                d_n = sign * np.exp(rng.uniform(min(a, b), max(a, b)))
+                d_t = rng.uniform(-0.3, 0.3) * abs(d_n)
+                jump = d_n * R[dim - 1] + d_t * R[0]
+                U[nd[nodes[cl[k + nh]]]] = U[nd[nodes[cl[k]]]] + jump
+    return U
+
+
 def spec_kwargs(c):
     dim = 3 if c["elem_type"] == 2 else 2
     em = tuple(c.get("eps_macro", ())) + (0.0,) * (6 - len(c.get("eps_macro", ())))
+    app = c["solve"][1] if "solve" in c else 0.01
     return dict(elem_type=c["elem_type"], n=c["n"], lo=(0.0,) * dim, hi=(1.0,) * dim,
                 inclusions=np.array(c["incl"], dtype=np.float64), E_matrix=E_M, nu_matrix=NU_M, E_fiber=E_F,
                 nu_fiber=NU_F, coh_law=c["coh_law"], coh=c["coh"], plane_strain=True, subscale=bool(c["subscale"]),
-                eps_macro=em, app_strain=0.01)
+                eps_macro=em, app_strain=app)

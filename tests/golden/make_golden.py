@@ -12,7 +12,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
-from cases import CASES, case_arrays, spec_kwargs  # noqa: E402
+from cases import CASES, case_arrays, cohesive_state, spec_kwargs  # noqa: E402
 from oracle import ref  # noqa: E402
 
 
@@ -22,9 +22,21 @@ def main(names=None):
             continue
         R = ref.RefProblem(ref.ProblemSpec(**spec_kwargs(c)))
         n_isv = int(R.get("isv_off")[-1])
-        U, isv = case_arrays(c, R.n_free, R.n_const, n_isv)
-        R.assemble(U, isv, 1.0)
-        out = dict(U_dof=U, isv_committed=isv, node_dofs=R.get("node_dofs"), isv_off=R.get("isv_off"),
+        if c["coh_law"]:
+            U = cohesive_state(c, R.get("node_dofs"), R.n_free, R.n_const, R.get("elem_node_off"), R.get("elem_nodes"),
+                               R.get("elem_cut"), R.get("elem_coh_off"), R.get("coh_struct"), R.get("coh_struct_off"),
+                               R.get("coh_qp_off"), R.get("coh_qp_R"))
+            isv = np.zeros(n_isv)
+            if c["isv_scale"] > 0 and n_isv:
+                # committed maxima around the current openings: about half the points unload
+                R.assemble(U, isv, 1.0)
+                rng = np.random.default_rng(c["seed"] + 1000)
+                isv = R.get("isv_trial") * rng.uniform(0.5, 1.5, n_isv)
+        else:
+            U, isv = case_arrays(c, R.n_free, R.n_const, n_isv)
+        t_frac = 1.0
+        R.assemble(U, isv, t_frac)
+        out = dict(U_dof=U, isv_committed=isv, t_frac=np.array([t_frac]), node_dofs=R.get("node_dofs"), isv_off=R.get("isv_off"),
                    isv_elem_qp_off=R.get("isv_elem_qp_off"), P_f=R.get("P_f"), P_p=R.get("P_p"),
                    isv_trial=R.get("isv_trial"), coh_zone=R.get("coh_zone"),
                    node_coords=R.get("node_coords"), enrich_coords=R.get("enrich_coords"))
