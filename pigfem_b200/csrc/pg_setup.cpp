@@ -346,11 +346,16 @@ int build_setup(const ProblemDesc& d, Setup& s) {
   // ---------------- cohesive law constants
   s.coh.law = d.coh_law;
   switch (d.coh_law) {
+    // Mesh::add_material stores a copy made by each law's copy(); the bilinear copy passes ALPHA as
+    // sqrt(alpha) (src/Material_BilinearCohesiveNU.cpp:37 with set_alpha storing its argument,
+    // :493-499), so the mesh's bilinear laws use alpha = sqrt(50); the Xu-Needleman copy passes Q
+    // as sqrt(q) (src/Material_XNCohesiveNU.cpp:35, set_q :384-390).
     case COH_BL: case COH_BLNU:
       s.coh.sigma_c = d.coh[0]; s.coh.delta_c1 = d.coh[1]; s.coh.delta_c2 = d.coh[2];
+      s.coh.alpha = std::sqrt(50.0);
       s.coh.nvar = (d.coh_law == COH_BL) ? 1 : 0; break;
     case COH_XN: case COH_XNNU:
-      s.coh.sigma_c = d.coh[0]; s.coh.delta_cn = d.coh[1]; s.coh.delta_ct = d.coh[2]; s.coh.q = d.coh[3];
+      s.coh.sigma_c = d.coh[0]; s.coh.delta_cn = d.coh[1]; s.coh.delta_ct = d.coh[2]; s.coh.q = std::sqrt(d.coh[3]);
       s.coh.nvar = (d.coh_law == COH_XN) ? 2 : 0; break;
     case COH_OP: case COH_OPNU: case COH_OPAUG: case COH_OPNUAUG:
       s.coh.sigma_c = d.coh[0]; s.coh.delta_c = d.coh[1]; s.coh.beta2 = d.coh[2] * d.coh[2];

@@ -15,7 +15,7 @@ import numpy as np
 
 E_M, NU_M, E_F, NU_F = 3.5e3, 0.35, 72e3, 0.22
 BL = (50.0, 5e-7, 5e-3, 0.0)
-XN = (50.0, 2e-4, 3e-4, 1.0)
+XN = (50.0, 2e-4, 3e-4, 1.7)
 OP = (50.0, 2e-4, 1.0, 0.0)
 
 CASES = {
