@@ -110,6 +110,11 @@ int pg_device_outputs(pg_ctx* ctx, double** K_vals4, double** P_f, double** P_p)
 /* Stream the context launches on (a cudaStream_t, 0 = legacy default). */
 int pg_set_stream(pg_ctx* ctx, void* stream);
 
+/* Per-kernel device timing of the following assemblies (CUDA events on the context's stream):
+ * ms[0] cut-element kernel, ms[1] fast row kernel, ms[2] general row kernel, of the last call. */
+int pg_set_timing(pg_ctx* ctx, int on);
+int pg_kernel_times(pg_ctx* ctx, float* ms);
+
 /* Internal variables (InternalVars): committed <- values; read trial or committed; commit
  * (InternalVars::copy_data_in after a converged load step). */
 int pg_set_isv(pg_ctx* ctx, const double* committed);

@@ -34,7 +34,7 @@ EXPORTED = [
     "pg_create", "pg_create_host", "pg_upload", "pg_debug_array", "pg_destroy", "pg_last_error",
     "pg_get_sizes", "pg_get_pattern", "pg_get_nodes", "pg_assemble", "pg_assemble_device",
     "pg_device_outputs", "pg_set_stream", "pg_set_isv", "pg_get_isv", "pg_commit_isv",
-    "pg_get_damage_zones", "pg_residual_norm",
+    "pg_get_damage_zones", "pg_residual_norm", "pg_set_timing", "pg_kernel_times",
 ]
 
 
@@ -92,6 +92,8 @@ def load_library(path: str = LIB_PATH):
         "pg_commit_isv": (i32, [vp]),
         "pg_get_damage_zones": (i32, [vp, p]),
         "pg_residual_norm": (i32, [vp, ctypes.POINTER(dbl)]),
+        "pg_set_timing": (i32, [vp, i32]),
+        "pg_kernel_times": (i32, [vp, p]),
     }
     for name, (rt, args) in sig.items():
         f = getattr(L, name)
@@ -273,6 +275,15 @@ class Problem:
         v = ctypes.c_double(0.0)
         self._check(load_library().pg_residual_norm(self.h, ctypes.byref(v)))
         return v.value
+
+    def set_timing(self, on: bool = True):
+        self._check(load_library().pg_set_timing(self.h, int(on)))
+
+    def kernel_times(self) -> np.ndarray:
+        """Device milliseconds of [cut-element, fast-row, general-row] kernels of the last assembly."""
+        ms = np.zeros(3, np.float32)
+        self._check(load_library().pg_kernel_times(self.h, _ptr(ms)))
+        return ms
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

@@ -30,6 +30,9 @@ struct pg_ctx {
   int maxnb_fast = 0;
   int n_coh_qp = 0;
   bool assembled = false;
+  std::vector<int> fast_rows, slow_rows;
+  bool timing = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace {
@@ -90,6 +93,9 @@ __global__ void k_sum_final(const double* part, int n, double* out) {
 }
 
 int launch(pg_ctx* c, double t_frac, int flags) {
+  if (c->timing && !c->ev[0])
+    for (int i = 0; i < 4; ++i) cudaEventCreate(&c->ev[i]);
+  if (c->timing) cudaEventRecord(c->ev[0], c->stream);
   pgd::DevProblem P = c->P;
   P.U = c->d_U;
   P.flags = flags;
@@ -107,6 +113,7 @@ int launch(pg_ctx* c, double t_frac, int flags) {
       pgd::k_cut_elements<3><<<grid, 32 * wpb, smem, c->stream>>>(P, c->max_nd);
     }
   }
+  if (c->timing) cudaEventRecord(c->ev[1], c->stream);
   const int tpb = 128;
   if (P.n_fast_rows > 0) {
     const int grid = (P.n_fast_rows + tpb - 1) / tpb;
@@ -119,11 +126,13 @@ int launch(pg_ctx* c, double t_frac, int flags) {
       else pgd::k_rows_fast<3, 15, double><<<grid, tpb, 0, c->stream>>>(P);
     }
   }
+  if (c->timing) cudaEventRecord(c->ev[2], c->stream);
   if (P.n_slow_rows > 0) {
     const int grid = (P.n_slow_rows + tpb - 1) / tpb;
     if (c->s.dim == 2) pgd::k_rows_slow<2><<<grid, tpb, 0, c->stream>>>(P);
     else pgd::k_rows_slow<3><<<grid, tpb, 0, c->stream>>>(P);
   }
+  if (c->timing) cudaEventRecord(c->ev[3], c->stream);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(c, PG_ERR_DEVICE, std::string("launch failed: ") + cudaGetErrorString(e));
   return 0;
@@ -251,6 +260,8 @@ int pg_upload(pg_ctx* c) {
   PG_TRY(upload(c, mask, &P.dn_mask));
   PG_TRY(upload(c, fast, &P.fast_rows));
   PG_TRY(upload(c, slow, &P.slow_rows));
+  c->fast_rows = fast;
+  c->slow_rows = slow;
   P.n_fast_rows = (int)fast.size(); P.n_slow_rows = (int)slow.size();
   for (int b = 0; b < 4; ++b) {
     PG_TRY(upload(c, s.rp[b], &P.rp[b]));
@@ -288,6 +299,8 @@ int pg_debug_array(const pg_ctx* c, const char* name, int64_t* n, const void** p
       {"node_detect", s.node_detect.data(), s.node_detect.size(), 1}, {"enr_edge", s.enr_edge.data(), s.enr_edge.size(), 1},
       {"enr_incl", s.enr_incl.data(), s.enr_incl.size(), 1}, {"sub_type", s.sub_type.data(), s.sub_type.size(), 1},
       {"cut_sub_off", s.cut_sub_off.data(), s.cut_sub_off.size(), 1}, {"sub_mat", s.sub_mat.data(), s.sub_mat.size(), 1},
+      {"fast_rows", c->fast_rows.data(), c->fast_rows.size(), 1}, {"slow_rows", c->slow_rows.data(), c->slow_rows.size(), 1},
+      {"dn_node", s.dn_node.data(), s.dn_node.size(), 1},
   };
   for (auto& t : tab)
     if (std::strcmp(t.k, name) == 0) { *n = (int64_t)t.n; *ptr = t.p; return t.kind; }
@@ -295,8 +308,22 @@ int pg_debug_array(const pg_ctx* c, const char* name, int64_t* n, const void** p
   return 0;
 }
 
+int pg_set_timing(pg_ctx* c, int on) {
+  if (!c) return PG_ERR_INPUT;
+  c->timing = on != 0;
+  return 0;
+}
+
+int pg_kernel_times(pg_ctx* c, float* ms) {
+  if (!c || !ms || !c->timing || !c->ev[0]) return set_err(c, PG_ERR_STATE, "timing is off or nothing was launched");
+  if (cudaEventSynchronize(c->ev[3]) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "event wait failed");
+  for (int i = 0; i < 3; ++i) cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]);
+  return 0;
+}
+
 void pg_destroy(pg_ctx* c) {
   if (!c) return;
+  for (int i = 0; i < 4; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   for (void* p : c->allocs) cudaFree(p);
   delete c;
 }

@@ -1,0 +1,127 @@
+"""Seeded synthetic fiber-composite RVEs (the benchmark workloads).
+
+The reference reads fiber layouts from CSV files (Tests/Main.cpp:744-860) and publishes no data
+set; the workloads here are seeded synthetic layouts with the sizes and distributions of the
+benchmark configurations:
+
+* ``cohesive_2d``: unit square, N x N quads split into 2 N^2 tri3 (Mesh::generate_mesh), fibers
+  placed by rejection sampling with radius ~ U[r_lo, r_hi], centre ~ U[r, 1-r]^2 and a minimum
+  surface gap; bilinear cohesive law on every interface.
+* ``linear_3d``: unit cube, N^3 hexes split into 6 tet4, spheres placed the same way.
+
+Layouts are drawn from a counter-based Philox generator keyed by (workload, seed, request), so
+the same key always gives the same RVE.  Layouts the reference cannot process are rejected:
+a mesh node closer than 1e-9 r to a fiber surface (src/Mesh.cpp:2904-2911 stops the run), and in
+3D any tet whose nodes see two different spheres (src/tet4.cpp:259-264).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from .capi import COH_BL, TET4, TRI3, ProblemDesc
+
+E_MATRIX, NU_MATRIX = 3.5e3, 0.35   # MPa
+E_FIBER, NU_FIBER = 72e3, 0.22
+# Bilinear interface: sigma_c = 50 MPa, delta_c2 = 5e-3 L, initial stiffness sigma_c / delta_c1
+# with delta_c1 = delta_c2 / 1e4.
+BL_PARAMS = (50.0, 5e-7, 5e-3, 0.0)
+
+
+def philox(workload: int, seed: int, request: int = 0) -> np.random.Generator:
+    return np.random.Generator(np.random.Philox(key=np.array([workload, seed], dtype=np.uint64),
+                                                counter=np.array([request, 0, 0, 0], dtype=np.uint64)))
+
+
+def place_fibers(rng: np.random.Generator, n_fibers: int, r_lo: float, r_hi: float, gap: float, dim: int,
+                 max_attempts: int = 200000, radius_scale: float = 1.0) -> np.ndarray:
+    """Rejection sampling: returns an (n, dim+1) array of (centre, r); stops early if the
+    attempt budget is spent (the achieved count is the array length)."""
+    out = []
+    attempts = 0
+    while len(out) < n_fibers and attempts < max_attempts:
+        attempts += 1
+        r = rng.uniform(r_lo, r_hi) * radius_scale
+        c = rng.uniform(r, 1.0 - r, dim)
+        ok = True
+        for f in out:
+            if np.linalg.norm(c - f[:dim]) < r + f[dim] + gap:
+                ok = False
+                break
+        if ok:
+            out.append(np.concatenate([c, [r]]))
+    return np.array(out).reshape(-1, dim + 1)
+
+
+def surface_clearance_ok(fibers: np.ndarray, n: int, dim: int, tol_rel: float = 1e-9) -> bool:
+    """No structured-grid node within tol_rel * r of any fiber surface."""
+    h = 1.0 / n
+    for f in fibers:
+        c, r = f[:dim], f[dim]
+        lo = np.maximum(np.floor((c - r) / h).astype(int) - 1, 0)
+        hi = np.minimum(np.ceil((c + r) / h).astype(int) + 1, n)
+        axes = [np.arange(lo[d], hi[d] + 1) * h for d in range(dim)]
+        grid = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, dim)
+        d = np.sqrt(((grid - c) ** 2).sum(1))
+        if np.any(np.abs(d - r) <= tol_rel * r):
+            return False
+    return True
+
+
+@dataclass
+class RVE:
+    desc: ProblemDesc
+    fibers: np.ndarray
+    volume_fraction: float
+
+
+def cohesive_2d(n: int = 512, n_fibers: int = 200, r_lo: float = 0.008, r_hi: float = 0.015, gap: float = 0.002,
+                seed: int = 1, request: int = 0, workload: int = 1, app_strain: float = 0.02,
+                coh_law: int = COH_BL, coh=BL_PARAMS, target_vf: Optional[float] = None) -> RVE:
+    rng = philox(workload, seed, request)
+    scale = 1.0
+    if target_vf is not None:
+        # radii scaled so the expected fiber area matches the target volume fraction
+        mean_r2 = (r_hi ** 3 - r_lo ** 3) / (3 * (r_hi - r_lo))
+        scale = math.sqrt(target_vf / (n_fibers * math.pi * mean_r2))
+    for _ in range(20):
+        fib = place_fibers(rng, n_fibers, r_lo, r_hi, gap, 2, radius_scale=scale)
+        if surface_clearance_ok(fib, n, 2):
+            break
+    vf = float(np.sum(np.pi * fib[:, 2] ** 2))
+    desc = ProblemDesc(elem_type=TRI3, n=(n, n), lo=(0.0, 0.0), hi=(1.0, 1.0), inclusions=fib,
+                       E_matrix=E_MATRIX, nu_matrix=NU_MATRIX, E_fiber=E_FIBER, nu_fiber=NU_FIBER,
+                       coh_law=coh_law, coh=coh, plane_strain=True, subscale=False, app_strain=app_strain)
+    return RVE(desc, fib, vf)
+
+
+def interface_state(problem, seed: int = 0, open_lo: float = 1e-7, open_hi: float = 6e-3, u_scale: float = 1e-6):
+    """A displacement field (node-major) with seeded tensile openings at every cohesive interface:
+    each '+' enrichment node is displaced from its '-' partner along the interface normal by a
+    log-uniform opening in [open_lo, open_hi], so the bilinear law runs through its loading,
+    softening and failed branches.  Bulk displacements are small random values."""
+    rng = np.random.default_rng(seed)
+    dim = problem.dim
+    X, dofs, _ = problem.nodes()
+    U = rng.uniform(-u_scale, u_scale, X.shape[0] * dim).reshape(-1, dim)
+    cut_node_off = problem.debug("cut_node_off")
+    cut_nodes = problem.debug("cut_nodes")
+    cut_coh_off = problem.debug("cut_coh_off")
+    coh_local_off = problem.debug("coh_local_off")
+    coh_local = problem.debug("coh_local")
+    coh_qp_off = problem.debug("coh_qp_off")
+    R = problem.debug("cqp_R").reshape(-1, dim, dim)
+    a, b = math.log(open_lo), math.log(open_hi)
+    for c in range(len(cut_node_off) - 1):
+        nodes = cut_nodes[cut_node_off[c]:cut_node_off[c + 1]]
+        for ce in range(cut_coh_off[c], cut_coh_off[c + 1]):
+            cl = coh_local[coh_local_off[ce]:coh_local_off[ce + 1]]
+            nh = len(cl) // 2
+            Rm = R[coh_qp_off[ce]:coh_qp_off[ce + 1]].mean(axis=0)
+            for k in range(nh):
+                dn = math.exp(rng.uniform(a, b))
+                U[nodes[cl[k + nh]]] = U[nodes[cl[k]]] + dn * Rm[dim - 1] + rng.uniform(-0.3, 0.3) * dn * Rm[0]
+    return np.ascontiguousarray(U.reshape(-1))
