@@ -110,8 +110,10 @@ int pg_device_outputs(pg_ctx* ctx, double** K_vals4, double** P_f, double** P_p)
 /* Stream the context launches on (a cudaStream_t, 0 = legacy default). */
 int pg_set_stream(pg_ctx* ctx, void* stream);
 
-/* Per-kernel device timing of the following assemblies (CUDA events on the context's stream):
- * ms[0] cut-element kernel, ms[1] fast row kernel, ms[2] general row kernel, of the last call. */
+/* Device timing of the last assembly from CUDA events the context records on its streams:
+ * ms[0] cohesive points + cut-element blocks, ms[1] fast rows (side stream, concurrent with ms[0]),
+ * ms[2] general rows, ms[3] the whole assembly (fork to join).  pg_set_timing is kept for callers
+ * that toggle it; the events are always recorded. */
 int pg_set_timing(pg_ctx* ctx, int on);
 int pg_kernel_times(pg_ctx* ctx, float* ms);
 

@@ -280,8 +280,9 @@ class Problem:
         self._check(load_library().pg_set_timing(self.h, int(on)))
 
     def kernel_times(self) -> np.ndarray:
-        """Device milliseconds of [cut-element, fast-row, general-row] kernels of the last assembly."""
-        ms = np.zeros(3, np.float32)
+        """Device milliseconds of the last assembly: [cohesive points + cut blocks, fast rows
+        (concurrent), general rows, whole assembly]."""
+        ms = np.zeros(4, np.float32)
         self._check(load_library().pg_kernel_times(self.h, _ptr(ms)))
         return ms
 

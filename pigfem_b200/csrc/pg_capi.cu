@@ -30,9 +30,10 @@ struct pg_ctx {
   int maxnb_fast = 0;
   int n_coh_qp = 0;
   bool assembled = false;
-  std::vector<int> fast_rows, slow_rows;
+  std::vector<int> fast_dn, slow_dn;
   bool timing = false;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 namespace {
@@ -93,46 +94,64 @@ __global__ void k_sum_final(const double* part, int n, double* out) {
 }
 
 int launch(pg_ctx* c, double t_frac, int flags) {
-  if (c->timing && !c->ev[0])
-    for (int i = 0; i < 4; ++i) cudaEventCreate(&c->ev[i]);
-  if (c->timing) cudaEventRecord(c->ev[0], c->stream);
+  if (!c->ev[0])
+    for (int i = 0; i < 6; ++i) cudaEventCreateWithFlags(&c->ev[i], cudaEventDefault);
   pgd::DevProblem P = c->P;
   P.U = c->d_U;
   P.flags = flags;
   for (int v = 0; v < 6; ++v) P.eps_macro[v] = c->s.desc.eps_macro[v] * t_frac;
-  if (c->s.ncut > 0) {
-    const int wpb = 4;
-    const int nv = c->s.dim == 2 ? 3 : 6;
-    const size_t smem = (size_t)wpb * pgd::cut_smem_per_warp(c->max_nd, nv) * sizeof(double);
-    const int grid = (c->s.ncut + wpb - 1) / wpb;
-    if (c->s.dim == 2) {
-      cudaFuncSetAttribute(pgd::k_cut_elements<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      pgd::k_cut_elements<2><<<grid, 32 * wpb, smem, c->stream>>>(P, c->max_nd);
+  const int dim = c->s.dim;
+  const bool fp32 = (flags & PG_FP32) != 0;
+  // fork: the fast rows (uncut elements only) run on the side stream, concurrently with the
+  // cut-element kernels and the general rows on the main stream
+  cudaEventRecord(c->ev[0], c->stream);
+  cudaStreamWaitEvent(c->side, c->ev[0], 0);
+  if (P.n_fast_dn > 0) {
+    const int tpb = 128;
+    const int grid = (P.n_fast_dn + tpb - 1) / tpb;
+    const int maxnb = (dim == 2) ? 9 : 15;
+    const size_t smem = (size_t)tpb * maxnb * dim * dim * sizeof(double);
+    if (dim == 2) {
+      if (fp32) { cudaFuncSetAttribute(pgd::k_rows_fast<2, 9, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                  pgd::k_rows_fast<2, 9, float><<<grid, tpb, smem, c->side>>>(P); }
+      else { cudaFuncSetAttribute(pgd::k_rows_fast<2, 9, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+             pgd::k_rows_fast<2, 9, double><<<grid, tpb, smem, c->side>>>(P); }
     } else {
-      cudaFuncSetAttribute(pgd::k_cut_elements<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      pgd::k_cut_elements<3><<<grid, 32 * wpb, smem, c->stream>>>(P, c->max_nd);
+      const int tpb3 = 64;
+      const int grid3 = (P.n_fast_dn + tpb3 - 1) / tpb3;
+      const size_t smem3 = (size_t)tpb3 * maxnb * dim * dim * sizeof(double);
+      if (fp32) { cudaFuncSetAttribute(pgd::k_rows_fast<3, 15, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
+                  pgd::k_rows_fast<3, 15, float><<<grid3, tpb3, smem3, c->side>>>(P); }
+      else { cudaFuncSetAttribute(pgd::k_rows_fast<3, 15, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
+             pgd::k_rows_fast<3, 15, double><<<grid3, tpb3, smem3, c->side>>>(P); }
     }
   }
-  if (c->timing) cudaEventRecord(c->ev[1], c->stream);
-  const int tpb = 128;
-  if (P.n_fast_rows > 0) {
-    const int grid = (P.n_fast_rows + tpb - 1) / tpb;
-    const bool fp32 = (flags & PG_FP32) != 0;
-    if (c->s.dim == 2) {
-      if (fp32) pgd::k_rows_fast<2, 9, float><<<grid, tpb, 0, c->stream>>>(P);
-      else pgd::k_rows_fast<2, 9, double><<<grid, tpb, 0, c->stream>>>(P);
-    } else {
-      if (fp32) pgd::k_rows_fast<3, 15, float><<<grid, tpb, 0, c->stream>>>(P);
-      else pgd::k_rows_fast<3, 15, double><<<grid, tpb, 0, c->stream>>>(P);
-    }
+  cudaEventRecord(c->ev[1], c->side);
+  if (P.n_coh_qp > 0) {
+    const int tpb = 128;
+    const int grid = (P.n_coh_qp + tpb - 1) / tpb;
+    if (dim == 2) pgd::k_coh_points<2><<<grid, tpb, 0, c->stream>>>(P);
+    else pgd::k_coh_points<3><<<grid, tpb, 0, c->stream>>>(P);
   }
-  if (c->timing) cudaEventRecord(c->ev[2], c->stream);
-  if (P.n_slow_rows > 0) {
-    const int grid = (P.n_slow_rows + tpb - 1) / tpb;
-    if (c->s.dim == 2) pgd::k_rows_slow<2><<<grid, tpb, 0, c->stream>>>(P);
-    else pgd::k_rows_slow<3><<<grid, tpb, 0, c->stream>>>(P);
+  cudaEventRecord(c->ev[2], c->stream);
+  if (P.ncut > 0) {
+    if (dim == 2) pgd::k_cut_blocks<2><<<P.ncut, 64, 0, c->stream>>>(P);
+    else pgd::k_cut_blocks<3><<<P.ncut, 64, 0, c->stream>>>(P);
   }
-  if (c->timing) cudaEventRecord(c->ev[3], c->stream);
+  cudaEventRecord(c->ev[3], c->stream);
+  if (P.n_slow_dn > 0) {
+    const int tpb = 32;
+    const int grid = (P.n_slow_dn + tpb - 1) / tpb;
+    const size_t smem = (size_t)tpb * P.maxnb_general * dim * dim * sizeof(double);
+    if (dim == 2) { cudaFuncSetAttribute(pgd::k_rows_general<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                    pgd::k_rows_general<2><<<grid, tpb, smem, c->stream>>>(P); }
+    else { cudaFuncSetAttribute(pgd::k_rows_general<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+           pgd::k_rows_general<3><<<grid, tpb, smem, c->stream>>>(P); }
+  }
+  cudaEventRecord(c->ev[4], c->stream);
+  // join
+  cudaStreamWaitEvent(c->stream, c->ev[1], 0);
+  cudaEventRecord(c->ev[5], c->stream);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(c, PG_ERR_DEVICE, std::string("launch failed: ") + cudaGetErrorString(e));
   return 0;
@@ -178,22 +197,42 @@ int pg_upload(pg_ctx* c) {
     const int na = s.dn_node[a];
     for (int q = 0; q < dim; ++q) if (s.node_dof[(size_t)na * dim + q] < s.n_free) mask[a] |= (uint8_t)(1 << q);
   }
-  std::vector<int> pf(s.dn_nbr.size()), pc(s.dn_nbr.size());
-  for (int a = 0; a < s.n_dn; ++a) {
-    int f = 0, p = 0;
-    for (int k = s.dn_nbr_off[a]; k < s.dn_nbr_off[a + 1]; ++k) {
-      pf[k] = f; pc[k] = p;
-      const int m = mask[s.dn_nbr[k]];
-      for (int q = 0; q < dim; ++q) { if (m & (1 << q)) f++; else p++; }
-    }
-  }
+  // neighbour masks, adjacency slots, fast/general split
+  std::vector<uint8_t> nbr_mask(s.dn_nbr.size());
+  for (size_t k = 0; k < s.dn_nbr.size(); ++k) nbr_mask[k] = mask[s.dn_nbr[k]];
+  std::vector<int> slot32(s.dn_adj.size(), 0), slot_off(s.dn_adj.size() + 1, 0);
+  std::vector<uint8_t> slots;
   const int maxnb = (dim == 2) ? 9 : 15;
   std::vector<int> fast, slow;
+  int maxnb_general = 1;
   for (int a = 0; a < s.n_dn; ++a) {
-    bool ok = (s.dn_nbr_off[a + 1] - s.dn_nbr_off[a]) <= maxnb;
-    for (int k = s.dn_adj_off[a]; k < s.dn_adj_off[a + 1] && ok; ++k) ok = s.cut_of[s.dn_adj[k] >> 5] < 0;
-    for (int q = 0; q < dim; ++q) (ok ? fast : slow).push_back(a * dim + q);
+    const int* nb = s.dn_nbr.data() + s.dn_nbr_off[a];
+    const int nn = s.dn_nbr_off[a + 1] - s.dn_nbr_off[a];
+    if (nn > 255) return set_err(c, PG_ERR_UNSUPPORTED, "a DOF node with more than 255 neighbours");
+    bool ok = nn <= maxnb;
+    for (int k = s.dn_adj_off[a]; k < s.dn_adj_off[a + 1]; ++k) {
+      const int e = s.dn_adj[k] >> 5;
+      std::vector<int> en;
+      if (s.cut_of[e] < 0) { ok = ok && true; for (int q = 0; q < s.npe; ++q) en.push_back(s.conn[(size_t)e * s.npe + q]); }
+      else {
+        ok = false;
+        const int cc = s.cut_of[e];
+        for (int q = s.cut_node_off[cc]; q < s.cut_node_off[cc + 1]; ++q) en.push_back(s.cut_nodes[q]);
+      }
+      slot_off[k] = (int)slots.size();
+      for (size_t lb = 0; lb < en.size(); ++lb) {
+        const int db = s.node_dn[en[lb]];
+        const int pos = (int)(std::lower_bound(nb, nb + nn, db) - nb);
+        if (pos >= nn || nb[pos] != db) return set_err(c, PG_ERR_STATE, "internal: adjacency without neighbour slot");
+        slots.push_back((uint8_t)pos);
+        if (s.cut_of[e] < 0) slot32[k] |= pos << (8 * lb);
+      }
+    }
+    slot_off[s.dn_adj.size()] = (int)slots.size();
+    if (ok) fast.push_back(a);
+    else { slow.push_back(a); maxnb_general = std::max(maxnb_general, nn); }
   }
+  slot_off[s.dn_adj.size()] = (int)slots.size();
   // cut-element scratch layout
   std::vector<long long> ke_off(s.ncut + 1, 0);
   std::vector<int> re_off(s.ncut + 1, 0);
@@ -252,17 +291,33 @@ int pg_upload(pg_ctx* c) {
   P.zone = c->d_zone;
   PG_TRY(upload(c, s.dn_node, &P.dn_node));
   PG_TRY(upload(c, s.dn_nbr_off, &P.dn_nbr_off));
-  PG_TRY(upload(c, s.dn_nbr, &P.dn_nbr));
-  PG_TRY(upload(c, pf, &P.dn_nbr_pf));
-  PG_TRY(upload(c, pc, &P.dn_nbr_pc));
+  PG_TRY(upload(c, nbr_mask, &P.dn_nbr_mask));
   PG_TRY(upload(c, s.dn_adj_off, &P.dn_adj_off));
   PG_TRY(upload(c, s.dn_adj, &P.dn_adj));
-  PG_TRY(upload(c, mask, &P.dn_mask));
-  PG_TRY(upload(c, fast, &P.fast_rows));
-  PG_TRY(upload(c, slow, &P.slow_rows));
-  c->fast_rows = fast;
-  c->slow_rows = slow;
-  P.n_fast_rows = (int)fast.size(); P.n_slow_rows = (int)slow.size();
+  PG_TRY(upload(c, slot32, &P.adj_slot32));
+  PG_TRY(upload(c, slot_off, &P.adj_slot_off));
+  PG_TRY(upload(c, slots, &P.adj_slots));
+  PG_TRY(upload(c, fast, &P.fast_dn));
+  PG_TRY(upload(c, slow, &P.slow_dn));
+  c->fast_dn = fast;
+  c->slow_dn = slow;
+  P.n_fast_dn = (int)fast.size(); P.n_slow_dn = (int)slow.size();
+  P.maxnb_general = maxnb_general;
+  // cohesive points: owning cut element and cohesive element
+  {
+    std::vector<int> cqp_cut(c->n_coh_qp), cqp_ce(c->n_coh_qp);
+    for (int cc = 0; cc < s.ncut; ++cc)
+      for (int ce = s.cut_coh_off[cc]; ce < s.cut_coh_off[cc + 1]; ++ce)
+        for (int q = s.coh_qp_off[ce]; q < s.coh_qp_off[ce + 1]; ++q) { cqp_cut[q] = cc; cqp_ce[q] = ce; }
+    PG_TRY(upload(c, cqp_cut, &P.cqp_cut));
+    PG_TRY(upload(c, cqp_ce, &P.cqp_ce));
+    double* dcpt;
+    PG_TRY(dalloc(c, (size_t)c->n_coh_qp * (dim * dim + dim), &dcpt));
+    P.cpt = dcpt;
+    P.n_coh_qp = c->n_coh_qp;
+  }
+  if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess)
+    return set_err(c, PG_ERR_DEVICE, "stream creation failed");
   for (int b = 0; b < 4; ++b) {
     PG_TRY(upload(c, s.rp[b], &P.rp[b]));
     PG_TRY(dalloc(c, s.ci[b].size(), &P.val[b]));
@@ -299,7 +354,7 @@ int pg_debug_array(const pg_ctx* c, const char* name, int64_t* n, const void** p
       {"node_detect", s.node_detect.data(), s.node_detect.size(), 1}, {"enr_edge", s.enr_edge.data(), s.enr_edge.size(), 1},
       {"enr_incl", s.enr_incl.data(), s.enr_incl.size(), 1}, {"sub_type", s.sub_type.data(), s.sub_type.size(), 1},
       {"cut_sub_off", s.cut_sub_off.data(), s.cut_sub_off.size(), 1}, {"sub_mat", s.sub_mat.data(), s.sub_mat.size(), 1},
-      {"fast_rows", c->fast_rows.data(), c->fast_rows.size(), 1}, {"slow_rows", c->slow_rows.data(), c->slow_rows.size(), 1},
+      {"fast_dn", c->fast_dn.data(), c->fast_dn.size(), 1}, {"slow_dn", c->slow_dn.data(), c->slow_dn.size(), 1},
       {"dn_node", s.dn_node.data(), s.dn_node.size(), 1},
   };
   for (auto& t : tab)
@@ -315,15 +370,24 @@ int pg_set_timing(pg_ctx* c, int on) {
 }
 
 int pg_kernel_times(pg_ctx* c, float* ms) {
-  if (!c || !ms || !c->timing || !c->ev[0]) return set_err(c, PG_ERR_STATE, "timing is off or nothing was launched");
-  if (cudaEventSynchronize(c->ev[3]) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "event wait failed");
-  for (int i = 0; i < 3; ++i) cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]);
+  if (!c || !ms || !c->ev[0]) return set_err(c, PG_ERR_STATE, "nothing was launched");
+  if (cudaEventSynchronize(c->ev[5]) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "event wait failed");
+  // [0] cohesive points + cut blocks, [1] fast rows (side stream), [2] general rows, [3] whole assembly
+  float a = 0, b = 0;
+  cudaEventElapsedTime(&a, c->ev[1], c->ev[3]);
+  (void)a;
+  cudaEventElapsedTime(&ms[0], c->ev[0], c->ev[3]);
+  cudaEventElapsedTime(&ms[1], c->ev[0], c->ev[1]);
+  cudaEventElapsedTime(&ms[2], c->ev[3], c->ev[4]);
+  cudaEventElapsedTime(&b, c->ev[0], c->ev[5]);
+  ms[3] = b;
   return 0;
 }
 
 void pg_destroy(pg_ctx* c) {
   if (!c) return;
-  for (int i = 0; i < 4; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  for (int i = 0; i < 6; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+  if (c->side) cudaStreamDestroy(c->side);
   for (void* p : c->allocs) cudaFree(p);
   delete c;
 }

@@ -59,10 +59,17 @@ struct DevProblem {
   double* isv_trial;
   uint8_t* zone;            // per cohesive qp: damage zone (0 compression, 1 loading, 2 softening, 3 failed)
   // row ownership
-  const int* dn_node; const int* dn_nbr_off; const int* dn_nbr; const int* dn_nbr_pf; const int* dn_nbr_pc;
-  const int* dn_adj_off; const int* dn_adj; const uint8_t* dn_mask;
-  const int* fast_rows; int n_fast_rows;   // (dnode * dim + q) rows whose elements are all uncut
-  const int* slow_rows; int n_slow_rows;   // the remaining rows
+  const int* dn_node; const int* dn_nbr_off; const uint8_t* dn_nbr_mask;  // free-DOF bits of each neighbour
+  const int* dn_adj_off; const int* dn_adj;      // adjacent (element << 5 | local node)
+  const int* adj_slot32;                         // uncut elements: neighbour slot of each element node, 8 bits each
+  const int* adj_slot_off; const uint8_t* adj_slots;  // all elements: neighbour slot of each element node
+  const int* fast_dn; int n_fast_dn;             // DOF nodes whose elements are all uncut
+  const int* slow_dn; int n_slow_dn;             // the remaining DOF nodes
+  int maxnb_general;                             // slab slots per thread in k_rows_general
+  // cohesive points
+  int n_coh_qp;
+  const int* cqp_cut; const int* cqp_ce;
+  double* cpt;                                   // per cohesive point: w R^T D R, w R^T T
   // outputs: CSR values of the four blocks and the two residual parts
   const int* rp[4];
   double* val[4];
