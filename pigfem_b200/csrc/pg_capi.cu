@@ -4,10 +4,11 @@
 // quadrature tables, the CSR structure and values of the four blocks, the residual, the
 // committed and trial internal variables and the cut-element scratch.  The caller owns its
 // host arrays; pointers are never retained across calls.
-#include "pg_kernels.cuh"
+#include "pg_stencil.cuh"
 #include "pg_setup.h"
 #include "../../include/pigfem_b200.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -31,6 +32,11 @@ struct pg_ctx {
   int n_coh_qp = 0;
   bool assembled = false;
   std::vector<int> fast_dn, slow_dn;
+  int tile_nodes = 128;
+  int max_cut_qp = 1, max_cut_nodes = 1;
+  const int4* stencil = nullptr;
+  int n_stencil = 0;
+  pgd::GridInfo grid{0, 0, 0};
   bool timing = false;
   cudaStream_t side = nullptr;
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -106,27 +112,6 @@ int launch(pg_ctx* c, double t_frac, int flags) {
   // cut-element kernels and the general rows on the main stream
   cudaEventRecord(c->ev[0], c->stream);
   cudaStreamWaitEvent(c->side, c->ev[0], 0);
-  if (P.n_fast_dn > 0) {
-    const int tpb = 128;
-    const int grid = (P.n_fast_dn + tpb - 1) / tpb;
-    const int maxnb = (dim == 2) ? 9 : 15;
-    const size_t smem = (size_t)tpb * maxnb * dim * dim * sizeof(double);
-    if (dim == 2) {
-      if (fp32) { cudaFuncSetAttribute(pgd::k_rows_fast<2, 9, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                  pgd::k_rows_fast<2, 9, float><<<grid, tpb, smem, c->side>>>(P); }
-      else { cudaFuncSetAttribute(pgd::k_rows_fast<2, 9, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-             pgd::k_rows_fast<2, 9, double><<<grid, tpb, smem, c->side>>>(P); }
-    } else {
-      const int tpb3 = 64;
-      const int grid3 = (P.n_fast_dn + tpb3 - 1) / tpb3;
-      const size_t smem3 = (size_t)tpb3 * maxnb * dim * dim * sizeof(double);
-      if (fp32) { cudaFuncSetAttribute(pgd::k_rows_fast<3, 15, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
-                  pgd::k_rows_fast<3, 15, float><<<grid3, tpb3, smem3, c->side>>>(P); }
-      else { cudaFuncSetAttribute(pgd::k_rows_fast<3, 15, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
-             pgd::k_rows_fast<3, 15, double><<<grid3, tpb3, smem3, c->side>>>(P); }
-    }
-  }
-  cudaEventRecord(c->ev[1], c->side);
   if (P.n_coh_qp > 0) {
     const int tpb = 128;
     const int grid = (P.n_coh_qp + tpb - 1) / tpb;
@@ -135,18 +120,42 @@ int launch(pg_ctx* c, double t_frac, int flags) {
   }
   cudaEventRecord(c->ev[2], c->stream);
   if (P.ncut > 0) {
-    if (dim == 2) pgd::k_cut_blocks<2><<<P.ncut, 64, 0, c->stream>>>(P);
-    else pgd::k_cut_blocks<3><<<P.ncut, 64, 0, c->stream>>>(P);
+    const size_t smem = (size_t)pgd::cut_smem_doubles(c->max_cut_qp, c->max_cut_nodes, dim) * sizeof(double);
+    if (dim == 2) { cudaFuncSetAttribute(pgd::k_cut_blocks<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                    pgd::k_cut_blocks<2><<<P.ncut, 64, smem, c->stream>>>(P); }
+    else { cudaFuncSetAttribute(pgd::k_cut_blocks<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+           pgd::k_cut_blocks<3><<<P.ncut, 64, smem, c->stream>>>(P); }
   }
+  // the stencil rows are issued after the (small) cut-element grids so both are resident together
+  if (c->n_stencil > 0) {
+    const int tpb = 128;
+    const int nthreads = (dim == 2) ? c->n_stencil : 3 * c->n_stencil;
+    const int grid = (nthreads + tpb - 1) / tpb;
+    if (dim == 2) {
+      if (fp32) pgd::k_rows_stencil<2, float><<<grid, tpb, 0, c->side>>>(P, c->grid, c->stencil, c->n_stencil);
+      else pgd::k_rows_stencil<2, double><<<grid, tpb, 0, c->side>>>(P, c->grid, c->stencil, c->n_stencil);
+    } else {
+      if (fp32) pgd::k_rows_stencil<3, float><<<grid, tpb, 0, c->side>>>(P, c->grid, c->stencil, c->n_stencil);
+      else pgd::k_rows_stencil<3, double><<<grid, tpb, 0, c->side>>>(P, c->grid, c->stencil, c->n_stencil);
+    }
+  }
+  cudaEventRecord(c->ev[1], c->side);
   cudaEventRecord(c->ev[3], c->stream);
   if (P.n_slow_dn > 0) {
-    const int tpb = 32;
-    const int grid = (P.n_slow_dn + tpb - 1) / tpb;
-    const size_t smem = (size_t)tpb * P.maxnb_general * dim * dim * sizeof(double);
-    if (dim == 2) { cudaFuncSetAttribute(pgd::k_rows_general<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                    pgd::k_rows_general<2><<<grid, tpb, smem, c->stream>>>(P); }
-    else { cudaFuncSetAttribute(pgd::k_rows_general<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-           pgd::k_rows_general<3><<<grid, tpb, smem, c->stream>>>(P); }
+    const int slots = P.maxnb_general;
+    if (dim == 2) {
+      constexpr int G = 8;
+      const int grid = (P.n_slow_dn + (128 / G) - 1) / (128 / G);
+      const size_t smem = (size_t)(128 / G) * slots * 4 * sizeof(double);
+      cudaFuncSetAttribute(pgd::k_rows<2, G, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      pgd::k_rows<2, G, double, true><<<grid, 128, smem, c->stream>>>(P, P.slow_dn, P.n_slow_dn, slots);
+    } else {
+      constexpr int G = 32;
+      const int grid = (P.n_slow_dn + (128 / G) - 1) / (128 / G);
+      const size_t smem = (size_t)(128 / G) * slots * 9 * sizeof(double);
+      cudaFuncSetAttribute(pgd::k_rows<3, G, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      pgd::k_rows<3, G, double, true><<<grid, 128, smem, c->stream>>>(P, P.slow_dn, P.n_slow_dn, slots);
+    }
   }
   cudaEventRecord(c->ev[4], c->stream);
   // join
@@ -229,10 +238,73 @@ int pg_upload(pg_ctx* c) {
       }
     }
     slot_off[s.dn_adj.size()] = (int)slots.size();
-    if (ok) fast.push_back(a);
-    else { slow.push_back(a); maxnb_general = std::max(maxnb_general, nn); }
+    (void)ok;
+    slow.push_back(a);
+    maxnb_general = std::max(maxnb_general, nn);
   }
   slot_off[s.dn_adj.size()] = (int)slots.size();
+  // Structured-grid stencil nodes (pg_stencil.cuh): interior DOF nodes two cells from the domain
+  // boundary whose adjacency, neighbours and row layout match their class table exactly, whose
+  // elements are all uncut and whose neighbour DOFs are all free.  Everything else is general.
+  std::vector<int4> stencil;
+  {
+    const int Nx = s.desc.n[0], Ny = s.desc.n[1], Nz = (dim == 3) ? s.desc.n[2] : 0;
+    const int sx = Nx + 1, sxy = sx * (Ny + 1);
+    const bool grid_ok = (s.etype == pg::TRI3 || s.etype == pg::TET4);
+    std::vector<char> in_stencil(s.n_dn, 0);
+    std::vector<std::vector<int4>> by_class(2);
+    for (int a = 0; a < s.n_dn && grid_ok; ++a) {
+      const int nid = s.dn_node[a];
+      if (nid >= s.n_std) continue;
+      const int i = nid % sx, j = (nid / sx) % (Ny + 1), k = nid / sxy;
+      if (i < 2 || i > Nx - 2 || j < 2 || j > Ny - 2) continue;
+      if (dim == 3 && (k < 2 || k > Nz - 2)) continue;
+      const int cls = (dim == 2) ? ((i + j) % 2) : 0;
+      const int NN = (dim == 2) ? (cls == 0 ? pgd::Tri3Stencil0::NN : pgd::Tri3Stencil1::NN) : pgd::Tet4Stencil0::NN;
+      const int NADJ = (dim == 2) ? (cls == 0 ? pgd::Tri3Stencil0::NADJ : pgd::Tri3Stencil1::NADJ) : pgd::Tet4Stencil0::NADJ;
+      auto off = [&](int q, int d) {
+        return (dim == 2) ? (cls == 0 ? pgd::Tri3Stencil0::off(q, d) : pgd::Tri3Stencil1::off(q, d)) : pgd::Tet4Stencil0::off(q, d);
+      };
+      auto entv = [&](int q, int cidx) {
+        return (dim == 2) ? (cls == 0 ? pgd::Tri3Stencil0::ent(q, cidx) : pgd::Tri3Stencil1::ent(q, cidx)) : pgd::Tet4Stencil0::ent(q, cidx);
+      };
+      bool ok = (s.dn_nbr_off[a + 1] - s.dn_nbr_off[a]) == NN && (s.dn_adj_off[a + 1] - s.dn_adj_off[a]) == NADJ;
+      for (int q = 0; ok && q < NN; ++q) {
+        const int nb = s.dn_node[s.dn_nbr[s.dn_nbr_off[a] + q]];
+        ok = nb == nid + off(q, 0) + off(q, 1) * sx + off(q, 2) * sxy && mask[s.dn_nbr[s.dn_nbr_off[a] + q]] == (1 << dim) - 1;
+      }
+      for (int q = 0; ok && q < NADJ; ++q) {
+        const int ci = i + entv(q, 0), cj = j + entv(q, 1), ck = k + entv(q, 2);
+        const int e = (dim == 2) ? 2 * (cj * Nx + ci) + entv(q, 3) : 6 * ((ck * Ny + cj) * Nx + ci) + entv(q, 3);
+        const int entry = s.dn_adj[s.dn_adj_off[a] + q];
+        ok = (entry >> 5) == e && (entry & 31) == entv(q, 4) && s.cut_of[e] < 0;
+        for (int n = 0; ok && n <= dim; ++n) {
+          const int sl = entv(q, 5 + n);
+          ok = s.conn[(size_t)e * (dim + 1) + n] == nid + off(sl, 0) + off(sl, 1) * sx + off(sl, 2) * sxy;
+        }
+      }
+      if (!ok) continue;
+      const int g0 = s.node_dof[(size_t)nid * dim];
+      for (int q = 0; ok && q < dim; ++q) ok = s.node_dof[(size_t)nid * dim + q] == g0 + q && g0 + q < s.n_free;
+      if (!ok) continue;
+      const int row0 = s.rp[0][g0];
+      for (int q = 0; ok && q < dim; ++q)
+        ok = s.rp[0][g0 + q] == row0 + q * NN * dim && s.rp[0][g0 + q + 1] - s.rp[0][g0 + q] == NN * dim &&
+             s.rp[1][g0 + q + 1] == s.rp[1][g0 + q];
+      if (!ok) continue;
+      by_class[cls].push_back(make_int4(nid, g0, row0, cls));
+      in_stencil[a] = 1;
+    }
+    for (auto& v : by_class) stencil.insert(stencil.end(), v.begin(), v.end());
+    std::vector<int> rest;
+    maxnb_general = 1;
+    for (int a = 0; a < s.n_dn; ++a)
+      if (!in_stencil[a]) { rest.push_back(a); maxnb_general = std::max(maxnb_general, s.dn_nbr_off[a + 1] - s.dn_nbr_off[a]); }
+    slow.swap(rest);
+    fast.clear();
+    for (auto& v : stencil) fast.push_back(s.node_dn[v.x]);
+    c->grid = pgd::GridInfo{Nx, Ny, Nz};
+  }
   // cut-element scratch layout
   std::vector<long long> ke_off(s.ncut + 1, 0);
   std::vector<int> re_off(s.ncut + 1, 0);
@@ -254,6 +326,13 @@ int pg_upload(pg_ctx* c) {
   P.coh.law = s.coh.law; P.coh.nvar = s.coh.nvar; P.coh.sigma_c = s.coh.sigma_c; P.coh.delta_c1 = s.coh.delta_c1;
   P.coh.delta_c2 = s.coh.delta_c2; P.coh.delta_cn = s.coh.delta_cn; P.coh.delta_ct = s.coh.delta_ct; P.coh.q = s.coh.q;
   P.coh.delta_c = s.coh.delta_c; P.coh.beta2 = s.coh.beta2; P.coh.alpha = s.coh.alpha;
+  {
+    std::vector<double> Dh(72);
+    std::vector<float> Dfh(72);
+    for (int m = 0; m < 2; ++m) for (int i = 0; i < 36; ++i) { Dh[m * 36 + i] = s.D[m][i]; Dfh[m * 36 + i] = (float)s.D[m][i]; }
+    PG_TRY(upload(c, Dh, &P.Dd));
+    PG_TRY(upload(c, Dfh, &P.Dfd));
+  }
   std::vector<float> Xf(s.X.begin(), s.X.end());
   PG_TRY(upload(c, s.X, &P.X));
   PG_TRY(upload(c, Xf, &P.Xf));
@@ -264,11 +343,54 @@ int pg_upload(pg_ctx* c) {
   PG_TRY(upload(c, s.node_dn, &P.node_dn));
   PG_TRY(upload(c, s.cut_node_off, &P.cut_node_off));
   PG_TRY(upload(c, s.cut_nodes, &P.cut_nodes));
-  PG_TRY(upload(c, s.cut_qp_off, &P.cut_qp_off));
-  PG_TRY(upload(c, s.qp_wgt, &P.qp_wgt));
-  PG_TRY(upload(c, s.qp_mat, &P.qp_mat));
-  PG_TRY(upload(c, s.qp_grad_off, &P.qp_grad_off));
-  PG_TRY(upload(c, s.qp_grad, &P.qp_grad));
+  // Device quadrature tables: the quadrature points of an affine (tri3 / tet4) sub-element of an
+  // affine parent share one gradient set, so they are merged into one point carrying the sum of
+  // their weights (w_0 + w_1 + ... in rule order).  K and R change only by rounding.
+  {
+    std::vector<int> dq_off(1, 0), dq_mat, dg_off(1, 0);
+    std::vector<double> dq_w, dg;
+    for (int cc = 0; cc < s.ncut; ++cc) {
+      int qp = s.cut_qp_off[cc];
+      for (int sb = s.cut_sub_off[cc]; sb < s.cut_sub_off[cc + 1]; ++sb) {
+        const int st = s.sub_type[sb];
+        const int nsn = s.sub_node_off[sb + 1] - s.sub_node_off[sb];
+        int nq = 0;
+        if (st == pg::SUB_TRI3 || st == pg::SUB_QUAD4) nq = 4;
+        else if (st == pg::SUB_POLYGON) nq = 7 * nsn;
+        else if (st == pg::SUB_TET4) nq = 5;
+        else if (st == pg::SUB_PRISM6) nq = 8;
+        else nq = 8;
+        const bool affine = (st == pg::SUB_TRI3 || st == pg::SUB_TET4);
+        if (affine) {
+          double w = 0.0;
+          for (int q = 0; q < nq; ++q) w += s.qp_wgt[qp + q];
+          dq_w.push_back(w);
+          dq_mat.push_back(s.qp_mat[qp]);
+          dg.insert(dg.end(), s.qp_grad.begin() + s.qp_grad_off[qp], s.qp_grad.begin() + s.qp_grad_off[qp + 1]);
+          dg_off.push_back((int)dg.size());
+        } else {
+          for (int q = 0; q < nq; ++q) {
+            dq_w.push_back(s.qp_wgt[qp + q]);
+            dq_mat.push_back(s.qp_mat[qp + q]);
+            dg.insert(dg.end(), s.qp_grad.begin() + s.qp_grad_off[qp + q], s.qp_grad.begin() + s.qp_grad_off[qp + q + 1]);
+            dg_off.push_back((int)dg.size());
+          }
+        }
+        qp += nq;
+      }
+      if (qp != s.cut_qp_off[cc + 1]) return set_err(c, PG_ERR_STATE, "internal: quadrature count mismatch");
+      dq_off.push_back((int)dq_w.size());
+    }
+    for (int cc = 0; cc < s.ncut; ++cc) {
+      c->max_cut_qp = std::max(c->max_cut_qp, dq_off[cc + 1] - dq_off[cc]);
+      c->max_cut_nodes = std::max(c->max_cut_nodes, s.cut_node_off[cc + 1] - s.cut_node_off[cc]);
+    }
+    PG_TRY(upload(c, dq_off, &P.cut_qp_off));
+    PG_TRY(upload(c, dq_w, &P.qp_wgt));
+    PG_TRY(upload(c, dq_mat, &P.qp_mat));
+    PG_TRY(upload(c, dg_off, &P.qp_grad_off));
+    PG_TRY(upload(c, dg, &P.qp_grad));
+  }
   PG_TRY(upload(c, s.cut_coh_off, &P.cut_coh_off));
   PG_TRY(upload(c, s.coh_nh, &P.coh_nh));
   PG_TRY(upload(c, s.coh_local_off, &P.coh_local_off));
@@ -299,8 +421,15 @@ int pg_upload(pg_ctx* c) {
   PG_TRY(upload(c, slots, &P.adj_slots));
   PG_TRY(upload(c, fast, &P.fast_dn));
   PG_TRY(upload(c, slow, &P.slow_dn));
+  {
+    const int4* dst = nullptr;
+    PG_TRY(upload(c, stencil, &dst));
+    c->stencil = dst;
+    c->n_stencil = (int)stencil.size();
+  }
   c->fast_dn = fast;
   c->slow_dn = slow;
+
   P.n_fast_dn = (int)fast.size(); P.n_slow_dn = (int)slow.size();
   P.maxnb_general = maxnb_general;
   // cohesive points: owning cut element and cohesive element
@@ -355,7 +484,9 @@ int pg_debug_array(const pg_ctx* c, const char* name, int64_t* n, const void** p
       {"enr_incl", s.enr_incl.data(), s.enr_incl.size(), 1}, {"sub_type", s.sub_type.data(), s.sub_type.size(), 1},
       {"cut_sub_off", s.cut_sub_off.data(), s.cut_sub_off.size(), 1}, {"sub_mat", s.sub_mat.data(), s.sub_mat.size(), 1},
       {"fast_dn", c->fast_dn.data(), c->fast_dn.size(), 1}, {"slow_dn", c->slow_dn.data(), c->slow_dn.size(), 1},
-      {"dn_node", s.dn_node.data(), s.dn_node.size(), 1},
+      {"dn_node", s.dn_node.data(), s.dn_node.size(), 1}, {"dn_nbr", s.dn_nbr.data(), s.dn_nbr.size(), 1},
+      {"dn_nbr_off", s.dn_nbr_off.data(), s.dn_nbr_off.size(), 1}, {"dn_adj", s.dn_adj.data(), s.dn_adj.size(), 1},
+      {"dn_adj_off", s.dn_adj_off.data(), s.dn_adj_off.size(), 1},
   };
   for (auto& t : tab)
     if (std::strcmp(t.k, name) == 0) { *n = (int64_t)t.n; *ptr = t.p; return t.kind; }

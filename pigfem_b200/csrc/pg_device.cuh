@@ -36,6 +36,8 @@ struct DevProblem {
   int subscale;
   double D[2][36];
   float Df[2][36];
+  const double* Dd;   // D of the two bulk materials in device memory (2 x 36), read through the L1
+  const float* Dfd;
   CohConst coh;
   // geometry / state
   const double* X;    // n_nodes * dim
@@ -64,6 +66,8 @@ struct DevProblem {
   const int* adj_slot32;                         // uncut elements: neighbour slot of each element node, 8 bits each
   const int* adj_slot_off; const uint8_t* adj_slots;  // all elements: neighbour slot of each element node
   const int* fast_dn; int n_fast_dn;             // DOF nodes whose elements are all uncut
+  const int* tile_elem_off; const int* tile_elems; int tile_max_elems;  // elements each tile of fast nodes touches
+  const uint16_t* adj_local;                     // tile-local index of each adjacency entry's element
   const int* slow_dn; int n_slow_dn;             // the remaining DOF nodes
   int maxnb_general;                             // slab slots per thread in k_rows_general
   // cohesive points

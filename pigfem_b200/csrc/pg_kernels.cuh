@@ -10,13 +10,11 @@
 //                    cohesive blocks (src/Assembler.cpp:278-365); one thread per node for the
 //                    element vector.  Blocks go to a scratch area in (i, j) block order so a block
 //                    row is contiguous.  FP64.
-//   k_rows_fast      one thread per DOF node whose elements are all uncut simplices: recomputes the
-//                    geometry of each adjacent element from node coordinates, accumulates its block
-//                    row in a per-thread shared-memory slab (one dim x dim block per neighbour node,
-//                    slots precomputed), then writes every CSR value of its dim rows exactly once,
-//                    plus the residual entries.  Runs concurrently with the cut-element kernels.
-//   k_rows_general   the same ownership for the remaining DOF nodes (nodes of cut elements,
-//                    enrichment nodes), taking cut-element block rows from the scratch.
+//   k_rows           one lane group per DOF node (row owner).  Instantiated twice: for the DOF nodes
+//                    whose elements are all uncut simplices (geometry recomputed from node
+//                    coordinates; runs concurrently with the cut-element kernels) and for the rest
+//                    (nodes of cut elements, enrichment nodes), which also take cut-element block
+//                    rows from the scratch.  Every CSR value of the node's rows is written once.
 // No atomics anywhere: every row has one owner and sums in a fixed order, so results are
 // bit-reproducible from run to run.
 #pragma once
@@ -185,11 +183,100 @@ __device__ __forceinline__ void simplex_block_row(const DevProblem& P, int e, in
   }
 }
 
-// Writes the dim rows of DOF node a from the slab acc (slot-major, dim x dim per slot).
-template <int DIM>
-__device__ __forceinline__ void write_rows(const DevProblem& P, int a, int nn, const double* acc, int stride, const double* r) {
+// Row assembly, one lane group of G threads per DOF node.  Each lane takes one adjacent element
+// (uncut: geometry recomputed from the node coordinates; cut: its block row from the scratch),
+// the lanes add their block rows into the node's shared-memory slab one after another in
+// adjacency order (deterministic, no atomics), the residual is reduced with a fixed shuffle tree,
+// and the group writes every CSR value of the node's dim rows exactly once.  All loads of the
+// group's elements are in flight together.
+template <int DIM, int G, typename T, bool GENERAL>
+__global__ void __launch_bounds__(128) k_rows(DevProblem P, const int* __restrict__ dn_list, int n_list, int slab_slots) {
+  constexpr int NPE = DIM + 1;
+  constexpr int NV = (DIM == 2) ? 3 : 6;
+  constexpr int NB = 128 / G;
+  extern __shared__ double smem[];
+  const int grp = threadIdx.x / G, g = threadIdx.x % G;
+  const int node = blockIdx.x * NB + grp;
+  const bool valid = node < n_list;
+  const int lane = threadIdx.x & 31;
+  double* slab = smem + (size_t)grp * slab_slots * DIM * DIM;
+  int a = 0, nn = 0, ad0 = 0, nadj = 0;
+  if (valid) {
+    a = __ldg(&dn_list[node]);
+    const int nb0 = __ldg(&P.dn_nbr_off[a]);
+    nn = __ldg(&P.dn_nbr_off[a + 1]) - nb0;
+    ad0 = __ldg(&P.dn_adj_off[a]);
+    nadj = __ldg(&P.dn_adj_off[a + 1]) - ad0;
+    for (int i = g; i < nn * DIM * DIM; i += G) slab[i] = 0.0;
+  }
+  // passes over the adjacency, uniform across the warp
+  int passes = (nadj + G - 1) / G;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) passes = max(passes, __shfl_xor_sync(0xffffffffu, passes, o));
+  __syncwarp();
+  double r[DIM];
+#pragma unroll
+  for (int q = 0; q < DIM; ++q) r[q] = 0.0;
+  for (int pass = 0; pass < passes; ++pass) {
+    const int idx = pass * G + g;
+    const bool have = valid && idx < nadj;
+    const int s = ad0 + idx;
+    T kv[NPE][DIM][DIM];
+    unsigned slots = 0;
+    int cut = -1, la = 0;
+    if (have) {
+      const int ent = __ldg(&P.dn_adj[s]);
+      const int e = ent >> 5;
+      la = ent & 31;
+      if (GENERAL) cut = __ldg(&P.cut_of[e]);
+      if (cut < 0) {
+        slots = (unsigned)__ldg(&P.adj_slot32[s]);
+        const int m = __ldg(&P.emat[e]);
+        T D[NV * NV];
+#pragma unroll
+        for (int i = 0; i < NV * NV; ++i) D[i] = (sizeof(T) == 4) ? (T)__ldg(&P.Dfd[m * 36 + i]) : (T)__ldg(&P.Dd[m * 36 + i]);
+        T rv[DIM];
+        simplex_block_row<DIM, T>(P, e, la, D, kv, rv);
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) r[q] += (double)rv[q];
+      } else {
+        const double* rb = P.re + __ldg(&P.re_off[cut]) + la * DIM;
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) r[q] += rb[q];
+      }
+    }
+    for (int t = 0; t < G; ++t) {
+      if (have && g == t) {
+        if (cut < 0) {
+#pragma unroll
+          for (int lb = 0; lb < NPE; ++lb) {
+            double* ak = slab + ((slots >> (8 * lb)) & 255) * DIM * DIM;
+#pragma unroll
+            for (int i = 0; i < DIM * DIM; ++i) ak[i] += (double)kv[lb][i / DIM][i % DIM];
+          }
+        } else {
+          const int mn = __ldg(&P.cut_node_off[cut + 1]) - __ldg(&P.cut_node_off[cut]);
+          const double* kb = P.ke + __ldg(&P.ke_off[cut]) + (size_t)la * mn * DIM * DIM;
+          const int so = __ldg(&P.adj_slot_off[s]);
+          for (int lb = 0; lb < mn; ++lb) {
+            double* ak = slab + __ldg(&P.adj_slots[so + lb]) * DIM * DIM;
+#pragma unroll
+            for (int i = 0; i < DIM * DIM; ++i) ak[i] += kb[lb * DIM * DIM + i];
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+  // residual: fixed-order tree over the group's lanes
+#pragma unroll
+  for (int q = 0; q < DIM; ++q)
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) r[q] += __shfl_down_sync(0xffffffffu, r[q], o, G);
+  if (!valid) return;
   const int na = __ldg(&P.dn_node[a]);
   const int nb0 = __ldg(&P.dn_nbr_off[a]);
+  const uint8_t* masks = P.dn_nbr_mask + nb0;
 #pragma unroll
   for (int q = 0; q < DIM; ++q) {
     const int gdof = __ldg(&P.node_dof[(size_t)na * DIM + q]);
@@ -199,118 +286,23 @@ __device__ __forceinline__ void write_rows(const DevProblem& P, int a, int nn, c
       const int bF = rf ? 0 : 2, bC = rf ? 1 : 3;
       double* vF = P.val[bF] + __ldg(&P.rp[bF][rr]);
       double* vC = P.val[bC] + __ldg(&P.rp[bC][rr]);
-      for (int k = 0; k < nn; ++k) {
-        const int mask = __ldg(&P.dn_nbr_mask[nb0 + k]);
+      for (int k = g; k < nn; k += G) {
+        int pf = 0;
+        for (int k2 = 0; k2 < k; ++k2) pf += __popc(__ldg(&masks[k2]));
+        int pc = k * DIM - pf;
+        const int mk = __ldg(&masks[k]);
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
-          const double v = acc[((k * DIM + q) * DIM + d) * stride];
-          if (mask & (1 << d)) *vF++ = v; else *vC++ = v;
+          const double v = slab[(k * DIM + q) * DIM + d];
+          if (mk & (1 << d)) vF[pf++] = v; else vC[pc++] = v;
         }
       }
     }
-    if (P.flags & FLAG_FUNC) {
+    if ((P.flags & FLAG_FUNC) && g == 0) {
       if (rf) P.Pf[rr] = r[q]; else P.Pp[rr] = r[q];
     }
   }
-}
-
-// DOF nodes whose adjacent elements are all uncut simplices.  acc: MAXNB x dim x dim doubles per
-// thread in shared memory, thread-interleaved (stride = blockDim.x) so lanes hit distinct banks.
-template <int DIM, int MAXNB, typename T>
-__global__ void __launch_bounds__(128) k_rows_fast(DevProblem P) {
-  constexpr int NPE = DIM + 1;
-  constexpr int NV = (DIM == 2) ? 3 : 6;
-  extern __shared__ double slab[];
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= P.n_fast_dn) return;
-  const int stride = blockDim.x;
-  double* acc = slab + threadIdx.x;
-  const int a = __ldg(&P.fast_dn[t]);
-  const int nn = __ldg(&P.dn_nbr_off[a + 1]) - __ldg(&P.dn_nbr_off[a]);
-  for (int i = 0; i < nn * DIM * DIM; ++i) acc[i * stride] = 0.0;
-  T D[2][NV * NV];
-#pragma unroll
-  for (int m = 0; m < 2; ++m)
-#pragma unroll
-    for (int i = 0; i < NV * NV; ++i) D[m][i] = (sizeof(T) == 4) ? (T)P.Df[m][i] : (T)P.D[m][i];
-  double r[DIM];
-#pragma unroll
-  for (int q = 0; q < DIM; ++q) r[q] = 0.0;
-  const int ad0 = __ldg(&P.dn_adj_off[a]), ad1 = __ldg(&P.dn_adj_off[a + 1]);
-  for (int s = ad0; s < ad1; ++s) {
-    const int ent = __ldg(&P.dn_adj[s]);
-    const unsigned slots = (unsigned)__ldg(&P.adj_slot32[s]);
-    const int e = ent >> 5, la = ent & 31;
-    const int m = __ldg(&P.emat[e]);
-    T kv[NPE][DIM][DIM], rv[DIM];
-    simplex_block_row<DIM, T>(P, e, la, m ? D[1] : D[0], kv, rv);
-#pragma unroll
-    for (int q = 0; q < DIM; ++q) r[q] += (double)rv[q];
-#pragma unroll
-    for (int lb = 0; lb < NPE; ++lb) {
-      const int k = (slots >> (8 * lb)) & 255;
-      double* ak = acc + (size_t)k * DIM * DIM * stride;
-#pragma unroll
-      for (int q = 0; q < DIM; ++q)
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) ak[(q * DIM + d) * stride] += (double)kv[lb][q][d];
-    }
-  }
-  write_rows<DIM>(P, a, nn, acc, stride, r);
-}
-
-// Remaining DOF nodes; the slab holds P.maxnb_general slots per thread.
-template <int DIM>
-__global__ void __launch_bounds__(64) k_rows_general(DevProblem P) {
-  constexpr int NPE = DIM + 1;
-  extern __shared__ double slab[];
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= P.n_slow_dn) return;
-  const int stride = blockDim.x;
-  double* acc = slab + threadIdx.x;
-  const int a = __ldg(&P.slow_dn[t]);
-  const int nn = __ldg(&P.dn_nbr_off[a + 1]) - __ldg(&P.dn_nbr_off[a]);
-  for (int i = 0; i < nn * DIM * DIM; ++i) acc[i * stride] = 0.0;
-  double r[DIM];
-#pragma unroll
-  for (int q = 0; q < DIM; ++q) r[q] = 0.0;
-  const int ad0 = __ldg(&P.dn_adj_off[a]), ad1 = __ldg(&P.dn_adj_off[a + 1]);
-  for (int s = ad0; s < ad1; ++s) {
-    const int ent = __ldg(&P.dn_adj[s]);
-    const int e = ent >> 5, la = ent & 31;
-    const int c = __ldg(&P.cut_of[e]);
-    if (c < 0) {
-      const unsigned slots = (unsigned)__ldg(&P.adj_slot32[s]);
-      const int m = __ldg(&P.emat[e]);
-      double kv[NPE][DIM][DIM], rv[DIM];
-      simplex_block_row<DIM, double>(P, e, la, P.D[m], kv, rv);
-#pragma unroll
-      for (int q = 0; q < DIM; ++q) r[q] += rv[q];
-#pragma unroll
-      for (int lb = 0; lb < NPE; ++lb) {
-        const int k = (slots >> (8 * lb)) & 255;
-        double* ak = acc + (size_t)k * DIM * DIM * stride;
-#pragma unroll
-        for (int q = 0; q < DIM; ++q)
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) ak[(q * DIM + d) * stride] += kv[lb][q][d];
-      }
-    } else {
-      const int mn = __ldg(&P.cut_node_off[c + 1]) - __ldg(&P.cut_node_off[c]);
-      const double* kb = P.ke + __ldg(&P.ke_off[c]) + (size_t)la * mn * DIM * DIM;
-      const double* rb = P.re + __ldg(&P.re_off[c]) + la * DIM;
-#pragma unroll
-      for (int q = 0; q < DIM; ++q) r[q] += rb[q];
-      const int so = __ldg(&P.adj_slot_off[s]);
-      for (int lb = 0; lb < mn; ++lb) {
-        const int k = __ldg(&P.adj_slots[so + lb]);
-        double* ak = acc + (size_t)k * DIM * DIM * stride;
-#pragma unroll
-        for (int i = 0; i < DIM * DIM; ++i) ak[i * stride] += kb[lb * DIM * DIM + i];
-      }
-    }
-  }
-  write_rows<DIM>(P, a, nn, acc, stride, r);
+  (void)lane;
 }
 
 // Cohesive law at every cohesive quadrature point.  Output per point: w R^T D R (dim x dim) then
@@ -384,32 +376,70 @@ __global__ void __launch_bounds__(128) k_coh_points(DevProblem P) {
   if (bad) atomicOr(P.err, ERR_NONFINITE);
 }
 
-// Element blocks of the cut elements (see the file comment).
+// Element blocks of the cut elements (see the file comment).  The element's quadrature data
+// (gradients over all its nodes, weights, materials), its nodal displacements and the stress at
+// every quadrature point are staged in shared memory first; the dynamic shared size is
+// cut_smem_doubles(max points, max nodes).
+__host__ __device__ inline int cut_smem_doubles(int nq, int mn, int dim) {
+  const int nv = (dim == 2) ? 3 : 6;
+  return nq * mn * dim + 2 * nq + nq * nv + mn * dim + 8;
+}
 template <int DIM>
 __global__ void __launch_bounds__(64) k_cut_blocks(DevProblem P) {
   constexpr int NV = (DIM == 2) ? 3 : 6;
+  extern __shared__ double sm[];
   const int c = blockIdx.x;
   if (c >= P.ncut) return;
   const int o0 = __ldg(&P.cut_node_off[c]);
   const int mn = __ldg(&P.cut_node_off[c + 1]) - o0;
   const int q0 = __ldg(&P.cut_qp_off[c]), q1 = __ldg(&P.cut_qp_off[c + 1]);
+  const int nq = q1 - q0;
   const int ce0 = __ldg(&P.cut_coh_off[c]), ce1 = __ldg(&P.cut_coh_off[c + 1]);
+  double* sg = sm;                          // nq x mn x DIM
+  double* sw = sg + (size_t)nq * mn * DIM;  // nq weights
+  double* smat = sw + nq;                   // nq materials (as doubles)
+  double* ssig = smat + nq;                 // nq x NV stresses
+  double* su = ssig + (size_t)nq * NV;      // mn x DIM displacements
+  const int* nodes = P.cut_nodes + o0;
+  const int gbase = __ldg(&P.qp_grad_off[q0]);
+  for (int i = threadIdx.x; i < nq * mn * DIM; i += blockDim.x) sg[i] = __ldg(&P.qp_grad[gbase + i]);
+  for (int i = threadIdx.x; i < nq; i += blockDim.x) { sw[i] = __ldg(&P.qp_wgt[q0 + i]); smat[i] = (double)__ldg(&P.qp_mat[q0 + i]); }
+  for (int i = threadIdx.x; i < mn * DIM; i += blockDim.x) su[i] = P.U[(size_t)__ldg(&nodes[i / DIM]) * DIM + (i % DIM)];
+  __syncthreads();
+  for (int qq = threadIdx.x; qq < nq; qq += blockDim.x) {
+    const double* g = sg + (size_t)qq * mn * DIM;
+    double eps[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) eps[v] = 0.0;
+    for (int n = 0; n < mn; ++n) add_strain<DIM, double>(g + n * DIM, su + n * DIM, eps);
+    if (P.subscale) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) eps[v] += P.eps_macro[v];
+    }
+    double D[NV * NV];
+    const int m = (int)smat[qq];
+#pragma unroll
+    for (int i = 0; i < NV * NV; ++i) D[i] = __ldg(&P.Dd[m * 36 + i]);
+    lei_stress<DIM, double>(D, eps, ssig + (size_t)qq * NV);
+  }
+  __syncthreads();
   double* kout = P.ke + __ldg(&P.ke_off[c]);
   bool bad = false;
   for (int p = threadIdx.x; p < mn * mn; p += blockDim.x) {
     const int i = p / mn, j = p - i * mn;
     double kb[DIM][DIM];
 #pragma unroll
-    for (int a = 0; a < DIM; ++a)
+    for (int x = 0; x < DIM; ++x)
 #pragma unroll
-      for (int b = 0; b < DIM; ++b) kb[a][b] = 0.0;
-    for (int qp = q0; qp < q1; ++qp) {
-      const double w = __ldg(&P.qp_wgt[qp]);
-      const double* D = P.D[__ldg(&P.qp_mat[qp])];
-      const double* g = P.qp_grad + __ldg(&P.qp_grad_off[qp]);
-      double gi[DIM], gj[DIM];
+      for (int y = 0; y < DIM; ++y) kb[x][y] = 0.0;
+    for (int qq = 0; qq < nq; ++qq) {
+      const double w = sw[qq];
+      const int m = (int)smat[qq];
+      double D[NV * NV];
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) { gi[d] = __ldg(&g[i * DIM + d]); gj[d] = __ldg(&g[j * DIM + d]); }
+      for (int x = 0; x < NV * NV; ++x) D[x] = __ldg(&P.Dd[m * 36 + x]);
+      const double* gi = sg + ((size_t)qq * mn + i) * DIM;
+      const double* gj = sg + ((size_t)qq * mn + j) * DIM;
 #pragma unroll
       for (int q = 0; q < DIM; ++q) {
         double part[NV];
@@ -436,48 +466,25 @@ __global__ void __launch_bounds__(64) k_cut_blocks(DevProblem P) {
         const double* wr = P.cpt + (size_t)cq * (DIM * DIM + DIM);
         const double nn = N[a1] * N[a2];
 #pragma unroll
-        for (int a = 0; a < DIM; ++a)
+        for (int x = 0; x < DIM; ++x)
 #pragma unroll
-          for (int b = 0; b < DIM; ++b) kb[a][b] += sgn * (nn * wr[a * DIM + b]);
+          for (int y = 0; y < DIM; ++y) kb[x][y] += sgn * (nn * wr[x * DIM + y]);
       }
     }
     double* o = kout + (size_t)p * DIM * DIM;
 #pragma unroll
-    for (int a = 0; a < DIM; ++a)
+    for (int x = 0; x < DIM; ++x)
 #pragma unroll
-      for (int b = 0; b < DIM; ++b) { o[a * DIM + b] = kb[a][b]; bad |= !isfinite(kb[a][b]); }
+      for (int y = 0; y < DIM; ++y) { o[x * DIM + y] = kb[x][y]; bad |= !isfinite(kb[x][y]); }
   }
-  // element vector: one thread per node
-  const int* nodes = P.cut_nodes + o0;
   for (int i = threadIdx.x; i < mn; i += blockDim.x) {
     double r[DIM];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) r[d] = 0.0;
-    for (int qp = q0; qp < q1; ++qp) {
-      const double w = __ldg(&P.qp_wgt[qp]);
-      const double* D = P.D[__ldg(&P.qp_mat[qp])];
-      const double* g = P.qp_grad + __ldg(&P.qp_grad_off[qp]);
-      double eps[NV];
+    for (int qq = 0; qq < nq; ++qq) {
+      const double* gi = sg + ((size_t)qq * mn + i) * DIM;
 #pragma unroll
-      for (int v = 0; v < NV; ++v) eps[v] = 0.0;
-      for (int n = 0; n < mn; ++n) {
-        const int nd = __ldg(&nodes[n]);
-        double gn[DIM], un[DIM];
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) { gn[d] = __ldg(&g[n * DIM + d]); un[d] = P.U[(size_t)nd * DIM + d]; }
-        add_strain<DIM, double>(gn, un, eps);
-      }
-      if (P.subscale) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) eps[v] += P.eps_macro[v];
-      }
-      double sig[NV];
-      lei_stress<DIM, double>(D, eps, sig);
-      double gi[DIM];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) gi[d] = __ldg(&g[i * DIM + d]);
-#pragma unroll
-      for (int q = 0; q < DIM; ++q) r[q] += w * bt_sig<DIM, double>(gi, sig, q);
+      for (int q = 0; q < DIM; ++q) r[q] += sw[qq] * bt_sig<DIM, double>(gi, ssig + (size_t)qq * NV, q);
     }
     for (int ce = ce0; ce < ce1; ++ce) {
       const int nh = __ldg(&P.coh_nh[ce]);

@@ -1,0 +1,213 @@
+// pg_stencil.cuh -- structured-grid fast path of the row assembly.
+//
+// The background meshes are the reference's structured grids (Mesh::generate_mesh,
+// src/Mesh.cpp:386-604): quads split into two tri3 with the union-jack alternation, hexes split
+// into six tet4.  Away from the domain boundary and from cut elements every DOF node of such a
+// grid has the same neighbourhood up to its class (the parity of i + j for tri3, a single class
+// for tet4).  The tables below give, for each class, the neighbour offsets in row order and, for
+// each adjacent element, its cell offset, its index within the cell, the row node's local index
+// and the neighbour slot of each of its nodes.  They restate the reference's cell-splitting
+// tables in row-owner form; the set-up checks every node it sends here against them and sends
+// any node that does not match to the general kernel.  With the slots known at compile time the
+// whole block row lives in registers, node and element ids come from grid arithmetic (no
+// adjacency or connectivity reads) and each row is written with contiguous stores.
+#pragma once
+
+#include "pg_kernels.cuh"
+
+namespace pgd {
+
+struct Tri3Stencil0 {
+  static constexpr int NN = 9, NADJ = 8;
+  // neighbour offsets (di, dj, dk) in row (node id) order
+  __host__ __device__ static constexpr int off(int s, int d) {
+    constexpr int t[NN][3] = {{-1, -1, 0}, {0, -1, 0}, {1, -1, 0}, {-1, 0, 0}, {0, 0, 0}, {1, 0, 0}, {-1, 1, 0}, {0, 1, 0}, {1, 1, 0}};
+    return t[s][d];
+  }
+  // adjacent elements: cell offset (di, dj, dk), element within the cell, local index of the
+  // row node, neighbour slot of each element node in connectivity order
+  __host__ __device__ static constexpr int ent(int a, int c) {
+    constexpr int t[NADJ][8] = {{-1, -1, 0, 0, 2, 0, 1, 4}, {-1, -1, 0, 1, 1, 0, 4, 3}, {0, -1, 0, 0, 2, 1, 2, 4}, {0, -1, 0, 1, 2, 2, 5, 4}, {-1, 0, 0, 0, 1, 3, 4, 6}, {-1, 0, 0, 1, 0, 4, 7, 6}, {0, 0, 0, 0, 0, 4, 5, 8}, {0, 0, 0, 1, 0, 4, 8, 7}};
+    return t[a][c];
+  }
+};
+struct Tri3Stencil1 {
+  static constexpr int NN = 5, NADJ = 4;
+  // neighbour offsets (di, dj, dk) in row (node id) order
+  __host__ __device__ static constexpr int off(int s, int d) {
+    constexpr int t[NN][3] = {{0, -1, 0}, {-1, 0, 0}, {0, 0, 0}, {1, 0, 0}, {0, 1, 0}};
+    return t[s][d];
+  }
+  // adjacent elements: cell offset (di, dj, dk), element within the cell, local index of the
+  // row node, neighbour slot of each element node in connectivity order
+  __host__ __device__ static constexpr int ent(int a, int c) {
+    constexpr int t[NADJ][8] = {{-1, -1, 0, 1, 1, 0, 2, 1}, {0, -1, 0, 1, 2, 0, 3, 2}, {-1, 0, 0, 0, 1, 1, 2, 4}, {0, 0, 0, 0, 0, 2, 3, 4}};
+    return t[a][c];
+  }
+};
+struct Tet4Stencil0 {
+  static constexpr int NN = 15, NADJ = 24;
+  // neighbour offsets (di, dj, dk) in row (node id) order
+  __host__ __device__ static constexpr int off(int s, int d) {
+    constexpr int t[NN][3] = {{-1, -1, -1}, {0, -1, -1}, {-1, 0, -1}, {0, 0, -1}, {-1, -1, 0}, {0, -1, 0}, {-1, 0, 0}, {0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0}, {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+    return t[s][d];
+  }
+  // adjacent elements: cell offset (di, dj, dk), element within the cell, local index of the
+  // row node, neighbour slot of each element node in connectivity order
+  __host__ __device__ static constexpr int ent(int a, int c) {
+    constexpr int t[NADJ][9] = {{-1, -1, -1, 0, 3, 0, 3, 2, 7}, {-1, -1, -1, 1, 3, 0, 2, 6, 7}, {-1, -1, -1, 2, 3, 0, 6, 4, 7}, {-1, -1, -1, 3, 2, 0, 5, 7, 4}, {-1, -1, -1, 4, 2, 1, 5, 7, 0}, {-1, -1, -1, 5, 1, 1, 7, 3, 0}, {0, -1, -1, 1, 2, 1, 3, 7, 8}, {0, -1, -1, 2, 1, 1, 7, 5, 8}, {-1, 0, -1, 3, 1, 2, 7, 9, 6}, {-1, 0, -1, 4, 1, 3, 7, 9, 2}, {0, 0, -1, 2, 2, 3, 9, 7, 10}, {0, 0, -1, 3, 3, 3, 8, 10, 7}, {-1, -1, 0, 0, 1, 4, 7, 6, 11}, {-1, -1, 0, 5, 2, 5, 11, 7, 4}, {0, -1, 0, 0, 2, 5, 8, 7, 12}, {0, -1, 0, 1, 1, 5, 7, 11, 12}, {-1, 0, 0, 4, 0, 7, 11, 13, 6}, {-1, 0, 0, 5, 0, 7, 13, 9, 6}, {0, 0, 0, 0, 0, 7, 10, 9, 14}, {0, 0, 0, 1, 0, 7, 9, 13, 14}, {0, 0, 0, 2, 0, 7, 13, 11, 14}, {0, 0, 0, 3, 0, 7, 12, 14, 11}, {0, 0, 0, 4, 3, 8, 12, 14, 7}, {0, 0, 0, 5, 3, 8, 14, 10, 7}};
+    return t[a][c];
+  }
+};
+
+
+struct GridInfo {
+  int nx, ny, nz;
+};
+
+// sigma = D eps for the isotropic linear-elastic D (only its nonzero entries)
+template <int DIM, typename T>
+__device__ __forceinline__ void lei_stress_iso(const T* d, const T* e, T* s) {
+  // d: 2D {D00, D01, D10, D11, D22}; 3D {D00, D01, D02, D10, D11, D12, D20, D21, D22, D33, D44, D55}
+  if (DIM == 2) { s[0] = d[0] * e[0] + d[1] * e[1]; s[1] = d[2] * e[0] + d[3] * e[1]; s[2] = d[4] * e[2]; }
+  else {
+    s[0] = d[0] * e[0] + d[1] * e[1] + d[2] * e[2];
+    s[1] = d[3] * e[0] + d[4] * e[1] + d[5] * e[2];
+    s[2] = d[6] * e[0] + d[7] * e[1] + d[8] * e[2];
+    s[3] = d[9] * e[3]; s[4] = d[10] * e[4]; s[5] = d[11] * e[5];
+  }
+}
+// part = (B_a(:, q))^T D using only the nonzero entries of the isotropic D (the zero terms of the
+// reference's SmallStrainKFast contribute exact zeros).
+template <int DIM, typename T>
+__device__ __forceinline__ void part_iso(const T* d, const T* ga, int q, T* part) {
+  if (DIM == 2) {
+    if (q == 0) { part[0] = ga[0] * d[0]; part[1] = ga[0] * d[1]; part[2] = ga[1] * d[4]; }
+    else        { part[0] = ga[1] * d[2]; part[1] = ga[1] * d[3]; part[2] = ga[0] * d[4]; }
+  } else {
+    if (q == 0) { part[0] = ga[0] * d[0]; part[1] = ga[0] * d[1]; part[2] = ga[0] * d[2]; part[3] = T(0); part[4] = ga[2] * d[10]; part[5] = ga[1] * d[11]; }
+    else if (q == 1) { part[0] = ga[1] * d[3]; part[1] = ga[1] * d[4]; part[2] = ga[1] * d[5]; part[3] = ga[2] * d[9]; part[4] = T(0); part[5] = ga[0] * d[11]; }
+    else { part[0] = ga[2] * d[6]; part[1] = ga[2] * d[7]; part[2] = ga[2] * d[8]; part[3] = ga[1] * d[9]; part[4] = ga[0] * d[10]; part[5] = T(0); }
+  }
+}
+
+template <int DIM, typename T>
+__device__ __forceinline__ void iso_d(const DevProblem& P, int m, T* d) {
+  const int* idx;
+  constexpr int n = (DIM == 2) ? 5 : 12;
+  const int i2[5] = {0, 1, 3, 4, 8};
+  const int i3[12] = {0, 1, 2, 6, 7, 8, 12, 13, 14, 21, 28, 35};
+#pragma unroll
+  for (int k = 0; k < n; ++k) {
+    const int o = (DIM == 2) ? i2[k] : i3[k];
+    d[k] = (sizeof(T) == 4) ? (T)__ldg(&P.Dfd[m * 36 + o]) : (T)__ldg(&P.Dd[m * 36 + o]);
+  }
+  (void)idx;
+}
+
+// Rows of one stencil node.  Q < 0: all dim rows in one thread; Q >= 0: row Q only.
+template <class S, int DIM, typename T, int Q>
+__device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo& gi, int nid, int g0, int row0) {
+  constexpr int NPE = DIM + 1;
+  constexpr int NV = (DIM == 2) ? 3 : 6;
+  constexpr int ND = (DIM == 2) ? 5 : 12;
+  constexpr int QB = (Q < 0) ? 0 : Q, QE = (Q < 0) ? DIM : Q + 1;
+  const int sx = gi.nx + 1, sxy = sx * (gi.ny + 1);
+  const int i = nid % sx, j = (nid / sx) % (gi.ny + 1), k = nid / sxy;
+  T dm[2][ND];
+  iso_d<DIM, T>(P, 0, dm[0]);
+  iso_d<DIM, T>(P, 1, dm[1]);
+  double acc[S::NN][QE - QB][DIM];
+#pragma unroll
+  for (int s = 0; s < S::NN; ++s)
+#pragma unroll
+    for (int q = 0; q < QE - QB; ++q)
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) acc[s][q][d] = 0.0;
+  double r[QE - QB];
+#pragma unroll
+  for (int q = 0; q < QE - QB; ++q) r[q] = 0.0;
+#pragma unroll
+  for (int a = 0; a < S::NADJ; ++a) {
+    const int ci = i + S::ent(a, 0), cj = j + S::ent(a, 1), ck = k + S::ent(a, 2);
+    const int e = (DIM == 2) ? 2 * (cj * gi.nx + ci) + S::ent(a, 3) : 6 * ((ck * gi.ny + cj) * gi.nx + ci) + S::ent(a, 3);
+    const int m = __ldg(&P.emat[e]);
+    T x[NPE][DIM], u[NPE][DIM], g[NPE][DIM], J;
+#pragma unroll
+    for (int n = 0; n < NPE; ++n) {
+      const int sl = S::ent(a, 5 + n);
+      const int id = nid + S::off(sl, 0) + S::off(sl, 1) * sx + S::off(sl, 2) * sxy;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        if (sizeof(T) == 4) x[n][d] = (T)__ldg(&P.Xf[(size_t)id * DIM + d]);
+        else x[n][d] = (T)__ldg(&P.X[(size_t)id * DIM + d]);
+        u[n][d] = (T)__ldg(&P.U[(size_t)id * DIM + d]);
+      }
+    }
+    simplex_geom<DIM, T>(x, g, &J);
+    const T w = J * (T)((DIM == 2) ? tri4_wsum() : tet5_wsum());
+    T eps[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) eps[v] = 0;
+#pragma unroll
+    for (int n = 0; n < NPE; ++n) add_strain<DIM, T>(g[n], u[n], eps);
+    if (P.subscale) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) eps[v] += (T)P.eps_macro[v];
+    }
+    const T* d = m ? dm[1] : dm[0];
+    T sig[NV];
+    lei_stress_iso<DIM, T>(d, eps, sig);
+    const int la = S::ent(a, 4);
+#pragma unroll
+    for (int q = QB; q < QE; ++q) {
+      T part[NV];
+      part_iso<DIM, T>(d, g[la], q, part);
+      r[q - QB] += (double)(w * bt_sig<DIM, T>(g[la], sig, q));
+#pragma unroll
+      for (int lb = 0; lb < NPE; ++lb)
+#pragma unroll
+        for (int q2 = 0; q2 < DIM; ++q2) acc[S::ent(a, 5 + lb)][q - QB][q2] += (double)(w * part_b<DIM, T>(part, g[lb], q2));
+    }
+  }
+#pragma unroll
+  for (int q = QB; q < QE; ++q) {
+    if (P.flags & FLAG_JAC) {
+      double* v = P.val[0] + row0 + (size_t)q * S::NN * DIM;
+#pragma unroll
+      for (int s = 0; s < S::NN; ++s)
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) v[s * DIM + d] = acc[s][q - QB][d];
+    }
+    if (P.flags & FLAG_FUNC) P.Pf[g0 + q] = r[q - QB];
+  }
+}
+
+// One thread per stencil node (2D) or per (stencil node, row) (3D).  st: {node id, first free
+// DOF, first CSR slot of its first row, class} per node, class-sorted.
+template <int DIM, typename T>
+__global__ void __launch_bounds__(128) k_rows_stencil(DevProblem P, GridInfo gi, const int4* __restrict__ st, int n) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (DIM == 2) {
+    if (t >= n) return;
+    const int4 v = __ldg(&st[t]);
+    if (v.w == 0) stencil_rows<Tri3Stencil0, 2, T, -1>(P, gi, v.x, v.y, v.z);
+    else stencil_rows<Tri3Stencil1, 2, T, -1>(P, gi, v.x, v.y, v.z);
+  } else {
+    if (t >= 3 * n) return;
+    const int node = t / 3, q = t - node * 3;
+    const int4 v = __ldg(&st[node]);
+    if (q == 0) stencil_rows<Tet4Stencil0, 3, T, 0>(P, gi, v.x, v.y, v.z);
+    else if (q == 1) stencil_rows<Tet4Stencil0, 3, T, 1>(P, gi, v.x, v.y, v.z);
+    else stencil_rows<Tet4Stencil0, 3, T, 2>(P, gi, v.x, v.y, v.z);
+  }
+}
+
+// Host-side copies of the tables for the set-up's check.
+struct StencilView {
+  int nn, nadj, npe;
+  const int (*off)[3];
+  const int* ent;  // nadj x (5 + npe)
+};
+
+}  // namespace pgd
