@@ -34,6 +34,9 @@ struct pg_ctx {
   std::vector<int> fast_dn, slow_dn;
   int tile_nodes = 128;
   int max_cut_qp = 1, max_cut_nodes = 1;
+  const int* cut_list[2] = {nullptr, nullptr};
+  int n_cut_list[2] = {0, 0};
+  int cut_cls_qp[2] = {1, 1}, cut_cls_nodes[2] = {1, 1};
   const int4* stencil = nullptr;
   int n_stencil = 0;
   pgd::GridInfo grid{0, 0, 0};
@@ -118,15 +121,7 @@ int launch(pg_ctx* c, double t_frac, int flags) {
     if (dim == 2) pgd::k_coh_points<2><<<grid, tpb, 0, c->stream>>>(P);
     else pgd::k_coh_points<3><<<grid, tpb, 0, c->stream>>>(P);
   }
-  cudaEventRecord(c->ev[2], c->stream);
-  if (P.ncut > 0) {
-    const size_t smem = (size_t)pgd::cut_smem_doubles(c->max_cut_qp, c->max_cut_nodes, dim) * sizeof(double);
-    if (dim == 2) { cudaFuncSetAttribute(pgd::k_cut_blocks<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                    pgd::k_cut_blocks<2><<<P.ncut, 64, smem, c->stream>>>(P); }
-    else { cudaFuncSetAttribute(pgd::k_cut_blocks<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-           pgd::k_cut_blocks<3><<<P.ncut, 64, smem, c->stream>>>(P); }
-  }
-  // the stencil rows are issued after the (small) cut-element grids so both are resident together
+  // the stencil rows run on the side stream, concurrently with the cohesive points and general rows
   if (c->n_stencil > 0) {
     const int tpb = 128;
     const int nthreads = (dim == 2) ? c->n_stencil : 3 * c->n_stencil;
@@ -144,17 +139,17 @@ int launch(pg_ctx* c, double t_frac, int flags) {
   if (P.n_slow_dn > 0) {
     const int slots = P.maxnb_general;
     if (dim == 2) {
-      constexpr int G = 8;
+      constexpr int G = 4;
       const int grid = (P.n_slow_dn + (128 / G) - 1) / (128 / G);
       const size_t smem = (size_t)(128 / G) * slots * 4 * sizeof(double);
-      cudaFuncSetAttribute(pgd::k_rows<2, G, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      pgd::k_rows<2, G, double, true><<<grid, 128, smem, c->stream>>>(P, P.slow_dn, P.n_slow_dn, slots);
+      cudaFuncSetAttribute(pgd::k_rows_general<2, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      pgd::k_rows_general<2, G><<<grid, 128, smem, c->stream>>>(P, slots);
     } else {
       constexpr int G = 32;
       const int grid = (P.n_slow_dn + (128 / G) - 1) / (128 / G);
       const size_t smem = (size_t)(128 / G) * slots * 9 * sizeof(double);
-      cudaFuncSetAttribute(pgd::k_rows<3, G, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      pgd::k_rows<3, G, double, true><<<grid, 128, smem, c->stream>>>(P, P.slow_dn, P.n_slow_dn, slots);
+      cudaFuncSetAttribute(pgd::k_rows_general<3, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      pgd::k_rows_general<3, G><<<grid, 128, smem, c->stream>>>(P, slots);
     }
   }
   cudaEventRecord(c->ev[4], c->stream);
@@ -317,6 +312,39 @@ int pg_upload(pg_ctx* c) {
   c->cut_scratch = ke_off[s.ncut] + re_off[s.ncut];
   c->n_coh_qp = (int)s.cqp_wgt.size();
 
+  // descriptors of the general rows (k_rows_general)
+  std::vector<int4> gdesc, adesc;
+  std::vector<int> growd, aresd;
+  for (int a : slow) {
+    const int na = s.dn_node[a];
+    gdesc.push_back(make_int4((int)adesc.size(), s.dn_adj_off[a + 1] - s.dn_adj_off[a], s.dn_nbr_off[a],
+                              s.dn_nbr_off[a + 1] - s.dn_nbr_off[a]));
+    int rows[3][3];
+    for (int q = 0; q < dim; ++q) {
+      const int gq = s.node_dof[(size_t)na * dim + q];
+      const bool rf = gq < s.n_free;
+      const int rr = rf ? gq : gq - s.n_free;
+      rows[0][q] = gq;
+      rows[1][q] = rf ? s.rp[0][rr] : s.rp[2][rr];
+      rows[2][q] = rf ? s.rp[1][rr] : s.rp[3][rr];
+    }
+    for (int t = 0; t < 3; ++t) for (int q = 0; q < dim; ++q) growd.push_back(rows[t][q]);
+    for (int k = s.dn_adj_off[a]; k < s.dn_adj_off[a + 1]; ++k) {
+      const int e = s.dn_adj[k] >> 5, la = s.dn_adj[k] & 31;
+      const int cc = s.cut_of[e];
+      if (cc < 0) {
+        adesc.push_back(make_int4(e, la, slot32[k], s.elem_mat[e]));
+        aresd.push_back(0);
+      } else {
+        const int mn = s.cut_node_off[cc + 1] - s.cut_node_off[cc];
+        const long long kro = ke_off[cc] + (long long)la * mn * dim * dim;
+        if (kro > 2147483647LL) return set_err(c, PG_ERR_UNSUPPORTED, "cut-element scratch beyond 2^31 doubles");
+        adesc.push_back(make_int4(e, la | (mn << 8), slot_off[k], (int)kro));
+        aresd.push_back(cc);
+      }
+    }
+  }
+
   // ---- device residency
   pgd::DevProblem& P = c->P;
   P.dim = dim; P.npe = s.npe; P.nvoigt = s.nvoigt;
@@ -385,6 +413,21 @@ int pg_upload(pg_ctx* c) {
       c->max_cut_qp = std::max(c->max_cut_qp, dq_off[cc + 1] - dq_off[cc]);
       c->max_cut_nodes = std::max(c->max_cut_nodes, s.cut_node_off[cc + 1] - s.cut_node_off[cc]);
     }
+    {
+      // size classes: at most 8 points and 8 nodes (one fiber: tri3 + quad4 sub-elements), the rest
+      std::vector<int> lists[2];
+      for (int cc = 0; cc < s.ncut; ++cc) {
+        const int nq = dq_off[cc + 1] - dq_off[cc], mn = s.cut_node_off[cc + 1] - s.cut_node_off[cc];
+        const int cls = (nq <= 8 && mn <= 8) ? 0 : 1;
+        lists[cls].push_back(cc);
+        c->cut_cls_qp[cls] = std::max(c->cut_cls_qp[cls], nq);
+        c->cut_cls_nodes[cls] = std::max(c->cut_cls_nodes[cls], mn);
+      }
+      for (int cls = 0; cls < 2; ++cls) {
+        PG_TRY(upload(c, lists[cls], &c->cut_list[cls]));
+        c->n_cut_list[cls] = (int)lists[cls].size();
+      }
+    }
     PG_TRY(upload(c, dq_off, &P.cut_qp_off));
     PG_TRY(upload(c, dq_w, &P.qp_wgt));
     PG_TRY(upload(c, dq_mat, &P.qp_mat));
@@ -432,6 +475,10 @@ int pg_upload(pg_ctx* c) {
 
   P.n_fast_dn = (int)fast.size(); P.n_slow_dn = (int)slow.size();
   P.maxnb_general = maxnb_general;
+  PG_TRY(upload(c, gdesc, &P.gdesc));
+  PG_TRY(upload(c, growd, &P.growd));
+  PG_TRY(upload(c, adesc, &P.adesc));
+  PG_TRY(upload(c, aresd, &P.aresd));
   // cohesive points: owning cut element and cohesive element
   {
     std::vector<int> cqp_cut(c->n_coh_qp), cqp_ce(c->n_coh_qp);
@@ -457,6 +504,25 @@ int pg_upload(pg_ctx* c) {
   PG_TRY(dalloc(c, 1, &c->d_err));
   P.err = c->d_err;
   PG_TRY(dalloc(c, 1024, &c->d_red));
+  // state-independent volumetric blocks of the cut elements, once
+  if (s.ncut > 0) {
+    double* dg;
+    PG_TRY(dalloc(c, (size_t)re_off[s.ncut] / dim * dim * (dim == 2 ? 3 : 6), &dg));
+    P.gmac = dg;
+    for (int cls = 0; cls < 2; ++cls) {
+      const int n = c->n_cut_list[cls];
+      if (n == 0) continue;
+      const size_t smem = (size_t)pgd::cut_smem_doubles(c->cut_cls_qp[cls], c->cut_cls_nodes[cls], dim) * sizeof(double);
+      if (dim == 2) { cudaFuncSetAttribute(pgd::k_cut_volumetric<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                      pgd::k_cut_volumetric<2><<<n, 64, smem>>>(P, c->cut_list[cls], n, dg); }
+      else { cudaFuncSetAttribute(pgd::k_cut_volumetric<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+             pgd::k_cut_volumetric<3><<<n, 64, smem>>>(P, c->cut_list[cls], n, dg); }
+    }
+    int herr = 0;
+    if (cudaDeviceSynchronize() != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "cut-element set-up kernel failed");
+    cudaMemcpy(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (herr) return set_err(c, PG_ERR_NONFINITE, "non-finite cut-element stiffness at set-up");
+  }
   return 0;
 }
 

@@ -55,7 +55,8 @@ struct DevProblem {
   const int* coh_qp_off; const double* cqp_N; const double* cqp_R; const double* cqp_wgt; const int* cqp_isv;
   const long long* ke_off;  // per cut element: offset of its element matrix in the scratch
   const int* re_off;        // per cut element: offset of its element vector in the scratch
-  double* ke;               // scratch: element matrices of the cut elements
+  double* ke;               // cache: volumetric element matrices of the cut elements (set-up)
+  const double* gmac;       // cache: macroscale-strain response of the cut elements (set-up)
   double* re;               // scratch: element vectors of the cut elements
   const double* isv_committed;
   double* isv_trial;
@@ -69,7 +70,8 @@ struct DevProblem {
   const int* tile_elem_off; const int* tile_elems; int tile_max_elems;  // elements each tile of fast nodes touches
   const uint16_t* adj_local;                     // tile-local index of each adjacency entry's element
   const int* slow_dn; int n_slow_dn;             // the remaining DOF nodes
-  int maxnb_general;                             // slab slots per thread in k_rows_general
+  int maxnb_general;                             // slab slots per node in k_rows_general
+  const int4* gdesc; const int* growd; const int4* adesc; const int* aresd;  // k_rows_general descriptors
   // cohesive points
   int n_coh_qp;
   const int* cqp_cut; const int* cqp_ce;
@@ -85,6 +87,8 @@ struct DevProblem {
 };
 
 // ---------------------------------------------------------------- cohesive laws (FP64)
+// x^2 as one correctly rounded product (what pow(x, 2) returns on the reference's host).
+__device__ __forceinline__ double sq(double x) { return x * x; }
 // delta (dim entries, tangential first, normal last) may be overwritten by the 1e-20 clamp, as the
 // reference's getDeltaEff / getDnDt do.  T gets the traction, Dm the dim x dim tangent (row-major),
 // isv the trial internal variables of this quadrature point (updated in place), zone the damage zone.
@@ -96,19 +100,19 @@ __device__ inline void coh_law(const CohConst& c, int dim, double* delta, double
   const int law = c.law;
   if (law == COH_XN || law == COH_XNNU) {
     const double Dn = delta[dim - 1];
-    const double Dt = (dim == 2) ? delta[0] : sqrt(pow(delta[0], 2) + pow(delta[1], 2));
+    const double Dt = (dim == 2) ? delta[0] : sqrt(sq(delta[0]) + sq(delta[1]));
     const double phi_n = c.sigma_c * c.delta_cn * exp(1.0);
     double Tn, dTndDn, Tt, dTtdDt;
     const double dTndDt = 0.0, dTtdDn = 0.0;
     if (law == COH_XNNU) {
       const double shear_rat = Dt / c.delta_ct;
-      const double shear_rat_exp = exp(-pow(shear_rat, 2));
+      const double shear_rat_exp = exp(-sq(shear_rat));
       const double norm_rat = Dn / c.delta_cn;
       const double norm_rat_exp = exp(-1.0 * norm_rat);
       Tn = (phi_n / c.delta_cn) * norm_rat_exp * norm_rat;
-      Tt = (2.0 * phi_n * Dt / pow(c.delta_ct, 2)) * c.q * shear_rat_exp;
+      Tt = (2.0 * phi_n * Dt / sq(c.delta_ct)) * c.q * shear_rat_exp;
       dTndDn = (phi_n / c.delta_cn) * norm_rat_exp * ((1 - norm_rat) / c.delta_cn);
-      dTtdDt = (2.0 * phi_n / pow(c.delta_ct, 2)) * c.q * (1 - 2.0 * pow(shear_rat, 2)) * shear_rat_exp;
+      dTtdDt = (2.0 * phi_n / sq(c.delta_ct)) * c.q * (1 - 2.0 * sq(shear_rat)) * shear_rat_exp;
     } else {
       double& Dn_max = isv[0];
       double& Dt_max = isv[1];
@@ -127,13 +131,13 @@ __device__ inline void coh_law(const CohConst& c, int dim, double* delta, double
       }
       if (fabs(Dt) >= Dt_max) {
         const double shear_rat = Dt / c.delta_ct;
-        const double shear_rat_exp = exp(-pow(shear_rat, 2));
+        const double shear_rat_exp = exp(-sq(shear_rat));
         Tt = (2.0 * phi_n * c.q / c.delta_ct) * shear_rat_exp * shear_rat;
-        dTtdDt = (2.0 * phi_n / pow(c.delta_ct, 2)) * c.q * (1 - 2.0 * pow(shear_rat, 2)) * shear_rat_exp;
+        dTtdDt = (2.0 * phi_n / sq(c.delta_ct)) * c.q * (1 - 2.0 * sq(shear_rat)) * shear_rat_exp;
         Dt_max = fabs(Dt);
       } else {
         const double shear_rat_max = Dt_max / c.delta_ct;
-        const double shear_rat_exp_max = exp(-pow(shear_rat_max, 2));
+        const double shear_rat_exp_max = exp(-sq(shear_rat_max));
         const double Tt_max = (2.0 * phi_n * c.q / c.delta_ct) * shear_rat_exp_max * shear_rat_max;
         Tt = (Dt / Dt_max) * Tt_max;
         dTtdDt = Tt_max / Dt_max;
@@ -146,11 +150,11 @@ __device__ inline void coh_law(const CohConst& c, int dim, double* delta, double
     } else {
       T[0] = Tt * (delta[0] / Dt);
       T[1] = Tt * (delta[1] / Dt);
-      Dm[0] = dTtdDt * pow(delta[0] / Dt, 2) + (Tt / Dt) * (1 - pow(delta[0] / Dt, 2));
+      Dm[0] = dTtdDt * sq(delta[0] / Dt) + (Tt / Dt) * (1 - sq(delta[0] / Dt));
       Dm[1] = (dTtdDt - Tt / Dt) * (delta[0] * delta[1] / (Dt * Dt));
       Dm[2] = dTtdDn * (delta[0] / Dt);
       Dm[3] = (dTtdDt - Tt / Dt) * (delta[0] * delta[1] / (Dt * Dt));
-      Dm[4] = dTtdDt * pow(delta[1] / Dt, 2) + (Tt / Dt) * (1 - pow(delta[1] / Dt, 2));
+      Dm[4] = dTtdDt * sq(delta[1] / Dt) + (Tt / Dt) * (1 - sq(delta[1] / Dt));
       Dm[5] = dTtdDn * (delta[1] / Dt);
       Dm[6] = dTndDt * (delta[0] / Dt);
       Dm[7] = dTndDt * (delta[1] / Dt);
@@ -163,8 +167,8 @@ __device__ inline void coh_law(const CohConst& c, int dim, double* delta, double
     return;
   }
   // bilinear and Ortiz-Pandolfi share the effective-opening form
-  double deff = pow(delta[dim - 1], 2);
-  for (int i = 0; i < dim - 1; ++i) deff += c.beta2 * pow(delta[i], 2);
+  double deff = sq(delta[dim - 1]);
+  for (int i = 0; i < dim - 1; ++i) deff += c.beta2 * sq(delta[i]);
   deff = sqrt(deff);
   double trac = 0.0, dtrac = 0.0;
   double dmax_copy = 0.0;
@@ -217,7 +221,7 @@ __device__ inline void coh_law(const CohConst& c, int dim, double* delta, double
   for (int i = 0; i < dim - 1; ++i) dd[i] = c.beta2 * delta[i] / deff;
   for (int i = 0; i < dim; ++i)
     for (int k = 0; k < dim; ++k)
-      Dm[i * dim + k] = br[i] * (dtrac * deff - trac) * (dd[k] / pow(deff, 2)) +
+      Dm[i * dim + k] = br[i] * (dtrac * deff - trac) * (dd[k] / sq(deff)) +
                         (trac / deff) * (c.beta2 * (i == k ? 1.0 : 0.0) + (1.0 - c.beta2) * (i == dim - 1 ? 1.0 : 0.0) * (k == dim - 1 ? 1.0 : 0.0));
   if (compress) {
     if (law == COH_BL || law == COH_BLNU) {

@@ -1,20 +1,17 @@
 // pg_kernels.cuh -- the assembly kernels.
 //
-//   k_coh_points     one thread per cohesive quadrature point: opening delta = R sum_n N_n (U+ - U-)
-//                    (src/Utilities.cpp:528-540), the traction-separation law with its internal-
-//                    variable update and damage zone, and the weighted R^T D R / R^T T the element
-//                    blocks need (src/Utilities.cpp:543-594).  FP64.
-//   k_cut_blocks     one block per cut element, one thread per node pair (i, j): the dim x dim
-//                    block of the element matrix, sum over sub-element quadrature points of
-//                    w B_i^T D B_j with enriched gradients (src/Assembler.cpp:223-274) plus the
-//                    cohesive blocks (src/Assembler.cpp:278-365); one thread per node for the
-//                    element vector.  Blocks go to a scratch area in (i, j) block order so a block
-//                    row is contiguous.  FP64.
-//   k_rows           one lane group per DOF node (row owner).  Instantiated twice: for the DOF nodes
-//                    whose elements are all uncut simplices (geometry recomputed from node
-//                    coordinates; runs concurrently with the cut-element kernels) and for the rest
-//                    (nodes of cut elements, enrichment nodes), which also take cut-element block
-//                    rows from the scratch.  Every CSR value of the node's rows is written once.
+//   k_coh_points     one thread per cohesive quadrature point: opening delta = R sum_n N_n (U+ - U-),
+//                    the traction-separation law with its internal-variable update and damage
+//                    zone, and the weighted R^T D R / R^T T (src/Utilities.cpp:528-594).  FP64.
+//   k_cut_volumetric run once at set-up: the cut elements' volumetric (linear, state-independent)
+//                    element matrices from sub-element quadrature with enriched B-matrices
+//                    (src/Assembler.cpp:223-274), cached for every later assembly.  FP64.
+//   k_rows_general   one lane group per DOF node (row owner) for every node the structured stencil
+//                    path (pg_stencil.cuh) does not take: boundary rows, nodes of cut elements and
+//                    enrichment nodes; uncut elements are recomputed from node coordinates; for cut
+//                    elements the cached volumetric block row is combined with the nodal
+//                    displacements and the cohesive points' blocks (src/Assembler.cpp:278-365).
+//                    Every CSR value is written once.
 // No atomics anywhere: every row has one owner and sums in a fixed order, so results are
 // bit-reproducible from run to run.
 #pragma once
@@ -183,34 +180,35 @@ __device__ __forceinline__ void simplex_block_row(const DevProblem& P, int e, in
   }
 }
 
-// Row assembly, one lane group of G threads per DOF node.  Each lane takes one adjacent element
-// (uncut: geometry recomputed from the node coordinates; cut: its block row from the scratch),
-// the lanes add their block rows into the node's shared-memory slab one after another in
-// adjacency order (deterministic, no atomics), the residual is reduced with a fixed shuffle tree,
-// and the group writes every CSR value of the node's dim rows exactly once.  All loads of the
-// group's elements are in flight together.
-template <int DIM, int G, typename T, bool GENERAL>
-__global__ void __launch_bounds__(128) k_rows(DevProblem P, const int* __restrict__ dn_list, int n_list, int slab_slots) {
+// Row assembly for the DOF nodes the stencil path does not take (boundary rows, nodes of cut
+// elements, enrichment nodes): one lane group of G threads per DOF node.  Each lane takes one
+// adjacent element (uncut: geometry recomputed from the node coordinates; cut: its block row from
+// the scratch), the lanes add their block rows into the node's shared-memory slab one after
+// another in adjacency order (deterministic, no atomics), the residual is reduced with a fixed
+// shuffle tree, and the group writes every CSR value of the node's rows exactly once.
+// Everything a node or an adjacency entry needs is packed into descriptors so the dependent
+// loads are: node descriptor -> adjacency descriptors -> element data.
+//   gdesc[node]      int4 {adjacency begin, adjacency count, neighbour begin, neighbour count}
+//   growd[node]      3*DIM ints: global DOF of each row, first slot in the row's F block, in its C block
+//   adesc[entry]     int4 {element, local node | nodes of a cut element << 8, slots (uncut: 8 bits per
+//                    node; cut: offset into adj_slots), material (uncut) / block-row offset (cut)}
+//   aresd[entry]     element-vector offset of the cut element's row (cut entries)
+template <int DIM, int G>
+__global__ void __launch_bounds__(128) k_rows_general(DevProblem P, int slab_slots) {
   constexpr int NPE = DIM + 1;
   constexpr int NV = (DIM == 2) ? 3 : 6;
   constexpr int NB = 128 / G;
   extern __shared__ double smem[];
   const int grp = threadIdx.x / G, g = threadIdx.x % G;
   const int node = blockIdx.x * NB + grp;
-  const bool valid = node < n_list;
-  const int lane = threadIdx.x & 31;
+  const bool valid = node < P.n_slow_dn;
   double* slab = smem + (size_t)grp * slab_slots * DIM * DIM;
-  int a = 0, nn = 0, ad0 = 0, nadj = 0;
+  int4 gd = make_int4(0, 0, 0, 0);
   if (valid) {
-    a = __ldg(&dn_list[node]);
-    const int nb0 = __ldg(&P.dn_nbr_off[a]);
-    nn = __ldg(&P.dn_nbr_off[a + 1]) - nb0;
-    ad0 = __ldg(&P.dn_adj_off[a]);
-    nadj = __ldg(&P.dn_adj_off[a + 1]) - ad0;
-    for (int i = g; i < nn * DIM * DIM; i += G) slab[i] = 0.0;
+    gd = __ldg(&P.gdesc[node]);
+    for (int i = g; i < gd.w * DIM * DIM; i += G) slab[i] = 0.0;
   }
-  // passes over the adjacency, uniform across the warp
-  int passes = (nadj + G - 1) / G;
+  int passes = (gd.y + G - 1) / G;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) passes = max(passes, __shfl_xor_sync(0xffffffffu, passes, o));
   __syncwarp();
@@ -219,73 +217,130 @@ __global__ void __launch_bounds__(128) k_rows(DevProblem P, const int* __restric
   for (int q = 0; q < DIM; ++q) r[q] = 0.0;
   for (int pass = 0; pass < passes; ++pass) {
     const int idx = pass * G + g;
-    const bool have = valid && idx < nadj;
-    const int s = ad0 + idx;
-    T kv[NPE][DIM][DIM];
-    unsigned slots = 0;
-    int cut = -1, la = 0;
+    const bool have = valid && idx < gd.y;
+    int4 ad = make_int4(0, 0, 0, 0);
+    double kv[NPE][DIM][DIM];
     if (have) {
-      const int ent = __ldg(&P.dn_adj[s]);
-      const int e = ent >> 5;
-      la = ent & 31;
-      if (GENERAL) cut = __ldg(&P.cut_of[e]);
-      if (cut < 0) {
-        slots = (unsigned)__ldg(&P.adj_slot32[s]);
-        const int m = __ldg(&P.emat[e]);
-        T D[NV * NV];
+      ad = __ldg(&P.adesc[gd.x + idx]);
+      const int la = ad.y & 255, mn = ad.y >> 8;
+      if (mn == 0) {
+        double D[NV * NV];
 #pragma unroll
-        for (int i = 0; i < NV * NV; ++i) D[i] = (sizeof(T) == 4) ? (T)__ldg(&P.Dfd[m * 36 + i]) : (T)__ldg(&P.Dd[m * 36 + i]);
-        T rv[DIM];
-        simplex_block_row<DIM, T>(P, e, la, D, kv, rv);
+        for (int i = 0; i < NV * NV; ++i) D[i] = __ldg(&P.Dd[ad.w * 36 + i]);
+        double rv[DIM];
+        simplex_block_row<DIM, double>(P, ad.x, la, D, kv, rv);
 #pragma unroll
-        for (int q = 0; q < DIM; ++q) r[q] += (double)rv[q];
+        for (int q = 0; q < DIM; ++q) r[q] += rv[q];
       } else {
-        const double* rb = P.re + __ldg(&P.re_off[cut]) + la * DIM;
+        // cut element: K_vol (state independent, cached at set-up) times the element's nodal
+        // displacements, the macroscale-strain response, and the cohesive internal forces
+        const int cc = __ldg(&P.aresd[gd.x + idx]);
+        const double* kb = P.ke + ad.w;
+        const int* cn = P.cut_nodes + __ldg(&P.cut_node_off[cc]);
+        for (int lb = 0; lb < mn; ++lb) {
+          const int nd = __ldg(&cn[lb]);
+          double u[DIM];
 #pragma unroll
-        for (int q = 0; q < DIM; ++q) r[q] += rb[q];
+          for (int d = 0; d < DIM; ++d) u[d] = P.U[(size_t)nd * DIM + d];
+#pragma unroll
+          for (int q = 0; q < DIM; ++q)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) r[q] += kb[lb * DIM * DIM + q * DIM + d] * u[d];
+        }
+        if (P.subscale) {
+          const double* gm = P.gmac + __ldg(&P.re_off[cc]) / DIM * DIM * NV + (size_t)la * DIM * NV;
+#pragma unroll
+          for (int q = 0; q < DIM; ++q)
+#pragma unroll
+            for (int v = 0; v < NV; ++v) r[q] += gm[q * NV + v] * P.eps_macro[v];
+        }
+        const int ce0 = __ldg(&P.cut_coh_off[cc]), ce1 = __ldg(&P.cut_coh_off[cc + 1]);
+        for (int ce = ce0; ce < ce1; ++ce) {
+          const int nh = __ldg(&P.coh_nh[ce]);
+          const int* cl = P.coh_local + __ldg(&P.coh_local_off[ce]);
+          int n1 = -1;
+          for (int k = 0; k < 2 * nh; ++k) if (__ldg(&cl[k]) == la) n1 = k;
+          if (n1 < 0) continue;
+          const double sgn = (n1 >= nh) ? 1.0 : -1.0;
+          double pc[DIM];
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) pc[d] = 0.0;
+          for (int cq = __ldg(&P.coh_qp_off[ce]); cq < __ldg(&P.coh_qp_off[ce + 1]); ++cq) {
+            const double nv = __ldg(&P.cqp_N[(size_t)cq * nh + n1 % nh]);
+            const double* wt = P.cpt + (size_t)cq * (DIM * DIM + DIM) + DIM * DIM;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) pc[d] += sgn * (nv * wt[d]);
+          }
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) r[d] += pc[d];
+        }
       }
     }
     for (int t = 0; t < G; ++t) {
       if (have && g == t) {
-        if (cut < 0) {
+        const int mn = ad.y >> 8;
+        if (mn == 0) {
+          const unsigned slots = (unsigned)ad.z;
 #pragma unroll
           for (int lb = 0; lb < NPE; ++lb) {
             double* ak = slab + ((slots >> (8 * lb)) & 255) * DIM * DIM;
 #pragma unroll
-            for (int i = 0; i < DIM * DIM; ++i) ak[i] += (double)kv[lb][i / DIM][i % DIM];
+            for (int i = 0; i < DIM * DIM; ++i) ak[i] += kv[lb][i / DIM][i % DIM];
           }
         } else {
-          const int mn = __ldg(&P.cut_node_off[cut + 1]) - __ldg(&P.cut_node_off[cut]);
-          const double* kb = P.ke + __ldg(&P.ke_off[cut]) + (size_t)la * mn * DIM * DIM;
-          const int so = __ldg(&P.adj_slot_off[s]);
+          const double* kb = P.ke + ad.w;
           for (int lb = 0; lb < mn; ++lb) {
-            double* ak = slab + __ldg(&P.adj_slots[so + lb]) * DIM * DIM;
+            double* ak = slab + __ldg(&P.adj_slots[ad.z + lb]) * DIM * DIM;
 #pragma unroll
             for (int i = 0; i < DIM * DIM; ++i) ak[i] += kb[lb * DIM * DIM + i];
+          }
+          // cohesive blocks: sgn N_a1 N_a2 (w R^T D R) summed over the cohesive element's points
+          const int la = ad.y & 255;
+          const int cc = __ldg(&P.aresd[gd.x + idx]);
+          const int ce0 = __ldg(&P.cut_coh_off[cc]), ce1 = __ldg(&P.cut_coh_off[cc + 1]);
+          for (int ce = ce0; ce < ce1; ++ce) {
+            const int nh = __ldg(&P.coh_nh[ce]);
+            const int* cl = P.coh_local + __ldg(&P.coh_local_off[ce]);
+            int n1 = -1;
+            for (int k = 0; k < 2 * nh; ++k) if (__ldg(&cl[k]) == la) n1 = k;
+            if (n1 < 0) continue;
+            const int cqa = __ldg(&P.coh_qp_off[ce]), cqb = __ldg(&P.coh_qp_off[ce + 1]);
+            for (int n2 = 0; n2 < 2 * nh; ++n2) {
+              const double sgn = ((n1 >= nh) == (n2 >= nh)) ? 1.0 : -1.0;
+              double kc[DIM * DIM];
+#pragma unroll
+              for (int i = 0; i < DIM * DIM; ++i) kc[i] = 0.0;
+              for (int cq = cqa; cq < cqb; ++cq) {
+                const double nn = __ldg(&P.cqp_N[(size_t)cq * nh + n1 % nh]) * __ldg(&P.cqp_N[(size_t)cq * nh + n2 % nh]);
+                const double* wr = P.cpt + (size_t)cq * (DIM * DIM + DIM);
+#pragma unroll
+                for (int i = 0; i < DIM * DIM; ++i) kc[i] += sgn * (nn * wr[i]);
+              }
+              double* ak = slab + __ldg(&P.adj_slots[ad.z + __ldg(&cl[n2])]) * DIM * DIM;
+#pragma unroll
+              for (int i = 0; i < DIM * DIM; ++i) ak[i] += kc[i];
+            }
           }
         }
       }
       __syncwarp();
     }
   }
-  // residual: fixed-order tree over the group's lanes
 #pragma unroll
   for (int q = 0; q < DIM; ++q)
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) r[q] += __shfl_down_sync(0xffffffffu, r[q], o, G);
   if (!valid) return;
-  const int na = __ldg(&P.dn_node[a]);
-  const int nb0 = __ldg(&P.dn_nbr_off[a]);
-  const uint8_t* masks = P.dn_nbr_mask + nb0;
+  const int nn = gd.w;
+  const uint8_t* masks = P.dn_nbr_mask + gd.z;
+  const int* rd = P.growd + (size_t)node * 3 * DIM;
 #pragma unroll
   for (int q = 0; q < DIM; ++q) {
-    const int gdof = __ldg(&P.node_dof[(size_t)na * DIM + q]);
+    const int gdof = __ldg(&rd[q]);
     const bool rf = gdof < P.n_free;
-    const int rr = rf ? gdof : gdof - P.n_free;
     if (P.flags & FLAG_JAC) {
-      const int bF = rf ? 0 : 2, bC = rf ? 1 : 3;
-      double* vF = P.val[bF] + __ldg(&P.rp[bF][rr]);
-      double* vC = P.val[bC] + __ldg(&P.rp[bC][rr]);
+      double* vF = P.val[rf ? 0 : 2] + __ldg(&rd[DIM + q]);
+      double* vC = P.val[rf ? 1 : 3] + __ldg(&rd[2 * DIM + q]);
       for (int k = g; k < nn; k += G) {
         int pf = 0;
         for (int k2 = 0; k2 < k; ++k2) pf += __popc(__ldg(&masks[k2]));
@@ -299,10 +354,9 @@ __global__ void __launch_bounds__(128) k_rows(DevProblem P, const int* __restric
       }
     }
     if ((P.flags & FLAG_FUNC) && g == 0) {
-      if (rf) P.Pf[rr] = r[q]; else P.Pp[rr] = r[q];
+      if (rf) P.Pf[gdof] = r[q]; else P.Pp[gdof - P.n_free] = r[q];
     }
   }
-  (void)lane;
 }
 
 // Cohesive law at every cohesive quadrature point.  Output per point: w R^T D R (dim x dim) then
@@ -376,52 +430,31 @@ __global__ void __launch_bounds__(128) k_coh_points(DevProblem P) {
   if (bad) atomicOr(P.err, ERR_NONFINITE);
 }
 
-// Element blocks of the cut elements (see the file comment).  The element's quadrature data
-// (gradients over all its nodes, weights, materials), its nodal displacements and the stress at
-// every quadrature point are staged in shared memory first; the dynamic shared size is
-// cut_smem_doubles(max points, max nodes).
-__host__ __device__ inline int cut_smem_doubles(int nq, int mn, int dim) {
-  const int nv = (dim == 2) ? 3 : 6;
-  return nq * mn * dim + 2 * nq + nq * nv + mn * dim + 8;
-}
+// State-independent part of the cut elements, computed once at set-up: the volumetric element
+// matrix K_vol = sum over sub-element points of w B_i^T D B_j with the enriched gradients
+// (src/Assembler.cpp:223-274; the bulk law is linear, so this block does not change between
+// assemblies) and the macroscale-strain response G_i = sum w B_i^T D (R_i = K_vol,i U +
+// G_i eps_macro).  One block per cut element, one thread per node pair; the element's gradients,
+// weights and materials are staged in shared memory.  Blocks go to the cache in (i, j) block
+// order so a block row is contiguous.  FP64.
+__host__ __device__ inline int cut_smem_doubles(int nq, int mn, int dim) { return nq * mn * dim + 2 * nq + 2 * 36 + 8; }
 template <int DIM>
-__global__ void __launch_bounds__(64) k_cut_blocks(DevProblem P) {
+__global__ void __launch_bounds__(64) k_cut_volumetric(DevProblem P, const int* __restrict__ list, int n_list, double* gmac) {
   constexpr int NV = (DIM == 2) ? 3 : 6;
   extern __shared__ double sm[];
-  const int c = blockIdx.x;
-  if (c >= P.ncut) return;
-  const int o0 = __ldg(&P.cut_node_off[c]);
-  const int mn = __ldg(&P.cut_node_off[c + 1]) - o0;
+  if ((int)blockIdx.x >= n_list) return;
+  const int c = __ldg(&list[blockIdx.x]);
+  const int mn = __ldg(&P.cut_node_off[c + 1]) - __ldg(&P.cut_node_off[c]);
   const int q0 = __ldg(&P.cut_qp_off[c]), q1 = __ldg(&P.cut_qp_off[c + 1]);
   const int nq = q1 - q0;
-  const int ce0 = __ldg(&P.cut_coh_off[c]), ce1 = __ldg(&P.cut_coh_off[c + 1]);
-  double* sg = sm;                          // nq x mn x DIM
-  double* sw = sg + (size_t)nq * mn * DIM;  // nq weights
-  double* smat = sw + nq;                   // nq materials (as doubles)
-  double* ssig = smat + nq;                 // nq x NV stresses
-  double* su = ssig + (size_t)nq * NV;      // mn x DIM displacements
-  const int* nodes = P.cut_nodes + o0;
+  double* sg = sm;
+  double* sw = sg + (size_t)nq * mn * DIM;
+  double* smat = sw + nq;
+  double* sD = smat + nq;
   const int gbase = __ldg(&P.qp_grad_off[q0]);
   for (int i = threadIdx.x; i < nq * mn * DIM; i += blockDim.x) sg[i] = __ldg(&P.qp_grad[gbase + i]);
   for (int i = threadIdx.x; i < nq; i += blockDim.x) { sw[i] = __ldg(&P.qp_wgt[q0 + i]); smat[i] = (double)__ldg(&P.qp_mat[q0 + i]); }
-  for (int i = threadIdx.x; i < mn * DIM; i += blockDim.x) su[i] = P.U[(size_t)__ldg(&nodes[i / DIM]) * DIM + (i % DIM)];
-  __syncthreads();
-  for (int qq = threadIdx.x; qq < nq; qq += blockDim.x) {
-    const double* g = sg + (size_t)qq * mn * DIM;
-    double eps[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) eps[v] = 0.0;
-    for (int n = 0; n < mn; ++n) add_strain<DIM, double>(g + n * DIM, su + n * DIM, eps);
-    if (P.subscale) {
-#pragma unroll
-      for (int v = 0; v < NV; ++v) eps[v] += P.eps_macro[v];
-    }
-    double D[NV * NV];
-    const int m = (int)smat[qq];
-#pragma unroll
-    for (int i = 0; i < NV * NV; ++i) D[i] = __ldg(&P.Dd[m * 36 + i]);
-    lei_stress<DIM, double>(D, eps, ssig + (size_t)qq * NV);
-  }
+  for (int i = threadIdx.x; i < 72; i += blockDim.x) sD[i] = __ldg(&P.Dd[i]);
   __syncthreads();
   double* kout = P.ke + __ldg(&P.ke_off[c]);
   bool bad = false;
@@ -434,10 +467,7 @@ __global__ void __launch_bounds__(64) k_cut_blocks(DevProblem P) {
       for (int y = 0; y < DIM; ++y) kb[x][y] = 0.0;
     for (int qq = 0; qq < nq; ++qq) {
       const double w = sw[qq];
-      const int m = (int)smat[qq];
-      double D[NV * NV];
-#pragma unroll
-      for (int x = 0; x < NV * NV; ++x) D[x] = __ldg(&P.Dd[m * 36 + x]);
+      const double* D = sD + 36 * (int)smat[qq];
       const double* gi = sg + ((size_t)qq * mn + i) * DIM;
       const double* gj = sg + ((size_t)qq * mn + j) * DIM;
 #pragma unroll
@@ -448,67 +478,34 @@ __global__ void __launch_bounds__(64) k_cut_blocks(DevProblem P) {
         for (int q2 = 0; q2 < DIM; ++q2) kb[q][q2] += w * part_b<DIM, double>(part, gj, q2);
       }
     }
-    for (int ce = ce0; ce < ce1; ++ce) {
-      const int nh = __ldg(&P.coh_nh[ce]);
-      const int* cl = P.coh_local + __ldg(&P.coh_local_off[ce]);
-      int n1 = -1, n2 = -1;
-      for (int k = 0; k < 2 * nh; ++k) {
-        const int v = __ldg(&cl[k]);
-        if (v == i) n1 = k;
-        if (v == j) n2 = k;
-      }
-      if (n1 < 0 || n2 < 0) continue;
-      const int a1 = n1 % nh, a2 = n2 % nh;
-      const double sgn = ((n1 >= nh) == (n2 >= nh)) ? 1.0 : -1.0;
-      const int cq0 = __ldg(&P.coh_qp_off[ce]), cq1 = __ldg(&P.coh_qp_off[ce + 1]);
-      for (int cq = cq0; cq < cq1; ++cq) {
-        const double* N = P.cqp_N + (size_t)cq * nh;
-        const double* wr = P.cpt + (size_t)cq * (DIM * DIM + DIM);
-        const double nn = N[a1] * N[a2];
-#pragma unroll
-        for (int x = 0; x < DIM; ++x)
-#pragma unroll
-          for (int y = 0; y < DIM; ++y) kb[x][y] += sgn * (nn * wr[x * DIM + y]);
-      }
-    }
     double* o = kout + (size_t)p * DIM * DIM;
 #pragma unroll
     for (int x = 0; x < DIM; ++x)
 #pragma unroll
       for (int y = 0; y < DIM; ++y) { o[x * DIM + y] = kb[x][y]; bad |= !isfinite(kb[x][y]); }
   }
+  double* gout = gmac + (size_t)__ldg(&P.re_off[c]) / DIM * DIM * NV;
   for (int i = threadIdx.x; i < mn; i += blockDim.x) {
-    double r[DIM];
+    double gacc[DIM][NV];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) r[d] = 0.0;
+    for (int q = 0; q < DIM; ++q)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) gacc[q][v] = 0.0;
     for (int qq = 0; qq < nq; ++qq) {
       const double* gi = sg + ((size_t)qq * mn + i) * DIM;
+      const double* D = sD + 36 * (int)smat[qq];
 #pragma unroll
-      for (int q = 0; q < DIM; ++q) r[q] += sw[qq] * bt_sig<DIM, double>(gi, ssig + (size_t)qq * NV, q);
-    }
-    for (int ce = ce0; ce < ce1; ++ce) {
-      const int nh = __ldg(&P.coh_nh[ce]);
-      const int* cl = P.coh_local + __ldg(&P.coh_local_off[ce]);
-      int n1 = -1;
-      for (int k = 0; k < 2 * nh; ++k) if (__ldg(&cl[k]) == i) n1 = k;
-      if (n1 < 0) continue;
-      const double sgn = (n1 >= nh) ? 1.0 : -1.0;
-      const int cq0 = __ldg(&P.coh_qp_off[ce]), cq1 = __ldg(&P.coh_qp_off[ce + 1]);
-      double pc[DIM];
+      for (int q = 0; q < DIM; ++q) {
+        double part[NV];
+        bt_d_row<DIM, double>(D, gi, q, part);
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) pc[d] = 0.0;
-      for (int cq = cq0; cq < cq1; ++cq) {
-        const double* N = P.cqp_N + (size_t)cq * nh;
-        const double* wt = P.cpt + (size_t)cq * (DIM * DIM + DIM) + DIM * DIM;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) pc[d] += sgn * (N[n1 % nh] * wt[d]);
+        for (int v = 0; v < NV; ++v) gacc[q][v] += sw[qq] * part[v];
       }
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) r[d] += pc[d];
     }
-    double* ro = P.re + __ldg(&P.re_off[c]) + i * DIM;
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) { ro[d] = r[d]; bad |= !isfinite(r[d]); }
+    for (int q = 0; q < DIM; ++q)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) gout[((size_t)i * DIM + q) * NV + v] = gacc[q][v];
   }
   if (bad) atomicOr(P.err, ERR_NONFINITE);
 }
