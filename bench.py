@@ -109,6 +109,13 @@ def fast_kernel_bytes(P, fp32: bool) -> float:
     return float(total)
 
 
+def launches_per_step(P) -> int:
+    """Kernels one assembly launches: cohesive points, stencil rows and general rows, each only
+    when it has work (the L2 flush between steps is a torch fill, not counted)."""
+    s = P.sizes
+    return int(s["n_coh_qp"] > 0) + int(len(P.debug("fast_dn")) > 0) + int(len(P.debug("slow_dn")) > 0)
+
+
 class Clocks:
     """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -318,12 +325,12 @@ def main():
                           "rows_general": float(kt64[2]), "assembly": float(kt64[3])},
             "algorithmic_bytes_per_step": alg["total"], "algorithmic_bytes_per_element": alg["total"] / ne,
             "algorithmic_gbs": alg["total"] / (ms64 / args.steps * 1e-3) / 1e9,
-            "roofline": {"bound": "hbm", "kernel": "k_rows_fast<2,9,double> (runs concurrently with the cut-element kernels)", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": "k_rows_stencil<2,double> (side stream, concurrent with k_coh_points and k_rows_general)", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": None, "bytes_per_launch": fk_bytes},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_ms / args.steps},
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": launches_per_step(P) * args.steps,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }

@@ -86,12 +86,6 @@ const double kTri4[4][3] = {
     {0.200000000000000000000000000000000, 0.200000000000000000000000000000000, 0.260416666666666666666666666666665},
     {0.200000000000000000000000000000000, 0.600000000000000000000000000000000, 0.260416666666666666666666666666665},
     {0.600000000000000000000000000000000, 0.200000000000000000000000000000000, 0.260416666666666666666666666666665}};
-// Tri3 order 5 (src/tri3.cpp:131-141), used by Polygon sub-elements (default order 5).
-const double kTri7[7][3] = {
-    {0.33333333333333, 0.33333333333333, 0.112500000000000}, {0.47014206410511, 0.47014206410511, 0.066197076394255},
-    {0.47014206410511, 0.05971587178977, 0.066197076394255}, {0.05971587178977, 0.47014206410511, 0.066197076394255},
-    {0.10128650732346, 0.10128650732346, 0.062969590272415}, {0.10128650732346, 0.79742698535309, 0.062969590272415},
-    {0.79742698535309, 0.10128650732346, 0.062969590272415}};
 // Gauss-Legendre 2-point (edge order 3).
 const double kGauss2 = 0.57735026918962576450914878050196;
 
@@ -121,20 +115,22 @@ void poly_points(int nn, double px[], double py[]) {
   }
 }
 void poly_tri(int nn, int t, int tri[3]) { tri[0] = nn; tri[1] = t; tri[2] = (t == nn - 1) ? 0 : t + 1; }
+// Reached through an Elem* in Mesh::store_shape_functions, so the order is Elem's default 3, not
+// Polygon's own default: 4 points (tri3 order 3) on each triangle of the fan.
 void poly_qp(int nn, int qp, double* r, double* s, double* w) {
   double px[32], py[32];
   poly_points(nn, px, py);
   px[nn] = 0.0; py[nn] = 0.0;
-  const int t = qp / 7, q = qp % 7;
+  const int t = qp / 4, q = qp % 4;
   double tN[3], tdN[6];
-  tri3_shape(kTri7[q][0], kTri7[q][1], tN, tdN);
+  tri3_shape(kTri4[q][0], kTri4[q][1], tN, tdN);
   int tri[3]; poly_tri(nn, t, tri);
   double J0[2][2] = {{0, 0}, {0, 0}};
   for (int i = 0; i < 2; ++i)
     for (int j = 0; j < 2; ++j)
       for (int n = 0; n < 3; ++n) J0[i][j] += (i == 0 ? px[tri[n]] : py[tri[n]]) * tdN[n * 2 + j];
   double dJ = J0[0][0] * J0[1][1] - J0[0][1] * J0[1][0];
-  *w = dJ * kTri7[q][2];
+  *w = dJ * kTri4[q][2];
   double cx = 0.0, cy = 0.0;
   for (int n = 0; n < 3; ++n) { cx += tN[n] * px[tri[n]]; cy += tN[n] * py[tri[n]]; }
   *r = cx; *s = cy;
@@ -366,6 +362,13 @@ int build_setup(const ProblemDesc& d, Setup& s) {
   // ---------------- structured mesh (Mesh::generate_mesh)
   const int Nx = d.n[0], Ny = d.n[1], Nz = (dim == 3) ? d.n[2] : 0;
   if (Nx <= 0 || Ny <= 0 || (dim == 3 && Nz <= 0)) { s.error = "grid counts must be positive"; return 2; }
+  for (int q = 0; q < dim; ++q)
+    if (!(d.hi[q] > d.lo[q])) { s.error = "domain box must have hi > lo in every direction"; return 2; }
+  if (d.incl.size() % (dim + 1) != 0) { s.error = "inclusion array has a partial record"; return 2; }
+  for (size_t f = 0; f < d.incl.size() / (dim + 1); ++f) {
+    const double r = d.incl[f * (dim + 1) + dim];
+    if (!(r > 0.0) || !std::isfinite(r)) { s.error = "inclusion radius must be positive and finite"; return 2; }
+  }
   const double hx = (d.hi[0] - d.lo[0]) / Nx, hy = (d.hi[1] - d.lo[1]) / Ny;
   const double hz = (dim == 3) ? (d.hi[2] - d.lo[2]) / Nz : 0.0;
   const long long nstd_ll = (long long)(Nx + 1) * (Ny + 1) * (Nz + 1);
@@ -622,7 +625,7 @@ int build_setup(const ProblemDesc& d, Setup& s) {
       int nqp = 0;
       if (stype == SUB_TRI3) nqp = 4;
       else if (stype == SUB_QUAD4) nqp = 4;
-      else if (stype == SUB_POLYGON) nqp = 7 * nsn;
+      else if (stype == SUB_POLYGON) nqp = 4 * nsn;
       else { s.error = "3D sub-elements are not supported here"; return 4; }
       for (int qp = 0; qp < nqp; ++qp) {
         double r, t, w, cN[32], cdN[64], cdNdx[64], cJ;

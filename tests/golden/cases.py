@@ -53,6 +53,12 @@ CASES = {
     "coh_bl_two_fibers_one_element": dict(elem_type=0, n=(8, 8), incl=[[0.3817, 0.5123, 0.1031], [0.6022, 0.4871, 0.1017]],
                                           coh_law=1, coh=BL, subscale=0, u_scale=1e-6, isv_scale=0.0, seed=13,
                                           open=(1e-7, 1.2e-2)),
+    # two fibers 0.0076 apart: elements with a node in each fiber and one in the matrix are split
+    # into two triangles and a Wachspress pentagon (4-point rule on each triangle of its fan)
+    "lin_tri3_polygon": dict(elem_type=0, n=(8, 8), incl=[[0.5533, 0.6147, 0.1452], [0.8061, 0.5055, 0.0803]],
+                             coh_law=0, coh=(0, 0, 0, 0), subscale=0, u_scale=1e-3, isv_scale=0.0, seed=17),
+    "coh_bl_polygon": dict(elem_type=0, n=(8, 8), incl=[[0.5533, 0.6147, 0.1452], [0.8061, 0.5055, 0.0803]],
+                           coh_law=1, coh=BL, subscale=0, u_scale=1e-6, isv_scale=0.0, seed=18, open=(1e-7, 1.2e-2)),
 }
 
 

@@ -16,11 +16,11 @@ from cases import CASES, case_arrays, cohesive_state, spec_kwargs  # noqa: E402
 from oracle import ref  # noqa: E402
 
 
-def main(names=None):
-    for name, c in CASES.items():
-        if names and name not in names:
-            continue
-        R = ref.RefProblem(ref.ProblemSpec(**spec_kwargs(c)))
+def generate(name):
+    """The fixture arrays of one case, computed by the reference's own CPU assembly."""
+    c = CASES[name]
+    R = ref.RefProblem(ref.ProblemSpec(**spec_kwargs(c)))
+    try:
         n_isv = int(R.get("isv_off")[-1])
         if c["coh_law"]:
             U = cohesive_state(c, R.get("node_dofs"), R.n_free, R.n_const, R.get("elem_node_off"), R.get("elem_nodes"),
@@ -43,9 +43,19 @@ def main(names=None):
         for b in ("K_ff", "K_fp", "K_pf", "K_pp"):
             rp, ci, v, sh = R.csr(b)
             out[b + "_rowptr"], out[b + "_cols"], out[b + "_vals"] = rp, ci, v
-        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
-        print(name, "free", R.n_free, "const", R.n_const, "nnz_ff", len(out["K_ff_vals"]), "isv", n_isv)
+        out = {k: np.array(v, copy=True) for k, v in out.items()}
+        return out, (R.n_free, R.n_const, n_isv)
+    finally:
         R.close()
+
+
+def main(names=None):
+    for name in CASES:
+        if names and name not in names:
+            continue
+        out, (n_free, n_const, n_isv) = generate(name)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        print(name, "free", n_free, "const", n_const, "nnz_ff", len(out["K_ff_vals"]), "isv", n_isv)
 
 
 if __name__ == "__main__":
