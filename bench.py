@@ -44,7 +44,7 @@ L2_FLUSH_BYTES = 256 << 20
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=300)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--grid", type=int, default=512)
@@ -128,7 +128,7 @@ class Clocks:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -160,6 +160,22 @@ class Clocks:
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+def profiled_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/*.md lines
+    'traffic_bytes_per_launch <kernel> <bytes>'), or None."""
+    pdir = os.path.join(ROOT, "profiles")
+    try:
+        for fn in sorted(os.listdir(pdir)):
+            with open(os.path.join(pdir, fn)) as f:
+                for line in f:
+                    t = line.split()
+                    if len(t) == 3 and t[0] == "traffic_bytes_per_launch" and t[1] == kernel:
+                        return float(t[2])
+    except OSError:
+        pass
+    return None
 
 
 def measured_peak_hbm():
@@ -263,8 +279,8 @@ def main():
         torch.cuda.synchronize()
         return ms, kt / steps
 
-    with Clocks(local) as clk:
-        ms64, kt64 = timed(capi.FUNC | capi.JAC, args.steps, args.warmup, kernel_times=True)
+    clk = Clocks(local).__enter__()
+    ms64, kt64 = timed(capi.FUNC | capi.JAC, args.steps, args.warmup, kernel_times=True)
     ms32, kt32 = timed(capi.FUNC | capi.JAC | capi.FP32, args.steps, args.warmup, kernel_times=True)
     value = ws * ne * args.steps / (ms64 * 1e-3)
     value32 = ws * ne * args.steps / (ms32 * 1e-3)
@@ -295,6 +311,7 @@ def main():
         t = torch.tensor([e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
+    clk.__exit__(None, None, None)
     e2e_value = ws * ne * args.steps / (e2e_ms * 1e-3)
     h2d = U.nbytes
     d2h = 8 * (sum(P.nnz) + P.n_free + P.n_const)
@@ -327,7 +344,8 @@ def main():
             "algorithmic_gbs": alg["total"] / (ms64 / args.steps * 1e-3) / 1e9,
             "roofline": {"bound": "hbm", "kernel": "k_rows_stencil<2,double> (side stream, concurrent with k_coh_points and k_rows_general)", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                         "traffic": None, "bytes_per_launch": fk_bytes},
+                         "traffic": profiled_traffic("k_rows_stencil<2,double>"), "bytes_per_launch": fk_bytes,
+                         "traffic_note": "ncu dram read+write per launch, cold cache; row writes still in L2 at kernel end are not counted"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_ms / args.steps},
             "gpu_launches": launches_per_step(P) * args.steps,
