@@ -28,6 +28,7 @@ extern "C" {
 #define PG_ERR_DEVICE 10      /* CUDA error or out of device memory */
 #define PG_ERR_NONFINITE 11   /* a NaN/Inf produced in K or R */
 #define PG_ERR_STATE 12       /* call out of order */
+#define PG_ERR_CAPACITY 13    /* input larger than a fixed-size buffer allows (pg_norm2_noalloc) */
 
 /* assembly flags */
 #define PG_FUNC 1   /* assemble the internal-force vector P_int (assembleFunc) */
@@ -129,6 +130,21 @@ int pg_get_damage_zones(const pg_ctx* ctx, uint8_t* zones);
 /* Residual norm ||F_ext,f - P_f||_2 on the device in FP64 with a fixed-order reduction
  * (SolverNonlinearKSP.cpp:81-84); F_ext is zero for the reference's drivers. */
 int pg_residual_norm(pg_ctx* ctx, double* out);
+
+/* ||x||_2 of a device vector of n doubles, written to the device double *d_out, enqueued on
+ * `stream` (a cudaStream_t; NULL = legacy default stream).  No counterpart in the reference.
+ * It allocates nothing: the block partials and a completion counter live in a fixed 32 KiB
+ * __device__ array, so n is limited to PG_NORM_NOALLOC_MAX_N (PG_ERR_CAPACITY beyond it).
+ * For callers that must not allocate device memory: a request served against a fixed device
+ * memory budget (an allocation would fall outside the admitted budget, and cudaFree
+ * synchronises the whole device, stalling the other requests in flight), and a caller holding
+ * a raw device vector without a pg_ctx whose scratch it could borrow.  The sum runs in a fixed
+ * order, so the result is bitwise reproducible for the same n and data.  The first call on a
+ * device looks up the scratch address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  Calls on one device share the scratch: calls that may overlap in time (different
+ * streams without ordering, or host threads) race and must be serialised by the caller. */
+#define PG_NORM_NOALLOC_MAX_N 33554432
+int pg_norm2_noalloc(const double* d_x, int64_t n, double* d_out, void* stream);
 
 #ifdef __cplusplus
 }
