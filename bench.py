@@ -37,7 +37,6 @@ sys.path.insert(0, ROOT)
 
 METRIC = "assembled elems/s (K+R) FP64 vs FP32-mixed; served RVE req/s with p50/p99"
 UNIT = "elements/s"
-WORKLOAD = "cohesive_2d_512: 512x512 tri3 split (524,288 tri3), 200 circular fibers, bilinear cohesive interfaces"
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -49,7 +48,11 @@ def parse():
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--grid", type=int, default=512)
     p.add_argument("--fibers", type=int, default=200)
+    p.add_argument("--workload", choices=("cohesive_2d_512", "linear_3d_64"), default="cohesive_2d_512")
+    p.add_argument("--grid3d", type=int, default=64)
+    p.add_argument("--spheres", type=int, default=50)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (default: --steps)")
     return p.parse_args()
 
 
@@ -187,46 +190,88 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def build_problem(args, rank):
+WORKLOADS = {
+    "cohesive_2d_512": "cohesive_2d_512: 512x512 tri3 split (524,288 tri3), 200 circular fibers, bilinear cohesive interfaces",
+    "linear_3d_64": "linear_3d_64: 64^3 hexes split into 6 tet4 (1,572,864 tet4), 50 spheres, periodic, one K and six unit-strain right-hand sides",
+}
+
+
+def build_problem(args, rank, device=True):
     from pigfem_b200 import capi, rve
+    if args.workload == "linear_3d_64":
+        R = rve.linear_3d(n=args.grid3d, n_spheres=args.spheres, seed=1, request=rank)
+        P = capi.Problem(R.desc, device=device)
+        U = np.zeros(P.n_nodes * 3)
+        return R, P, U
     R = rve.cohesive_2d(n=args.grid, n_fibers=args.fibers, seed=1, request=rank)
-    P = capi.Problem(R.desc)
+    P = capi.Problem(R.desc, device=device)
     U = rve.interface_state(P, seed=rank)
     return R, P, U
 
 
+UNIT_STRAINS_3D = [tuple(1.0 if i == k else 0.0 for i in range(6)) for k in range(6)]
+
+
+def reference_problem(R, P, U):
+    """The reference's own Problem (oracle/_ref) for the same RVE and state; returns it and the DOF
+    vector (free then constrained) of U."""
+    import dataclasses
+    from oracle import ref
+    RP = ref.RefProblem(ref.ProblemSpec(**{f.name: getattr(R.desc, f.name) for f in dataclasses.fields(R.desc)}))
+    _, dofs, _ = P.nodes()
+    Ud = np.zeros(RP.n_free + RP.n_const)
+    Ud[dofs.reshape(-1)] = U
+    return RP, Ud
+
+
+def reference_step_seconds(args, RP, Ud, budget_s: float, max_steps: int):
+    """Times the reference's Assembler::assemble for one step of the workload (2D: one K + R;
+    3D: one K + R and five residual-only assemblies for the other unit strains), repeated while
+    the budget lasts (at most max_steps).  Returns (seconds per step, steps timed)."""
+    three_d = args.workload == "linear_3d_64"
+    if three_d:
+        RP.set_macro(UNIT_STRAINS_3D[0])
+    RP.assemble(Ud, None, 1.0)                       # warm-up (and the state for the timed calls)
+    times = []
+    spent = 0.0
+    while len(times) < max_steps and (not times or spent < budget_s):
+        if three_d:
+            t = 0.0
+            for k, e in enumerate(UNIT_STRAINS_3D):
+                RP.set_macro(e)
+                t += RP.assemble(Ud, None, 1.0, func=True, jac=(k == 0))
+        else:
+            t = RP.assemble(Ud, None, 1.0)
+        times.append(t)
+        spent += t
+    return float(np.mean(times)), len(times)
+
+
 def run_reference(args, ws, rank):
-    """The reference's own CPU assembly (oracle/_ref, built from its sources) on rank 0."""
+    """The reference's own CPU assembly (oracle/_ref, built from its sources) on rank 0.  The
+    reference assembles serially (one MPI rank; no threads in its assembly), so it uses one core."""
     if rank != 0:
         return
     from oracle import ref
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libpigfem_ref.so not built (make -C oracle)"}))
         return
-    from pigfem_b200 import rve
-    R = rve.cohesive_2d(n=args.grid, n_fibers=args.fibers, seed=1, request=0)
-    RP = ref.RefProblem(ref.ProblemSpec(elem_type=0, n=(args.grid, args.grid), inclusions=R.fibers,
-                                        coh_law=R.desc.coh_law, coh=R.desc.coh, app_strain=R.desc.app_strain))
     from pigfem_b200 import capi
-    P = capi.Problem(R.desc, device=False)
-    U = rve.interface_state(P, seed=0)
-    _, dofs, _ = P.nodes()
-    Ud = np.zeros(RP.n_free + RP.n_const)
-    Ud[dofs.reshape(-1)] = U
-    RP.assemble(Ud, None, 1.0)
-    for _ in range(args.warmup):
-        RP.time_assemble(1)
-    t = [RP.time_assemble(1) for _ in range(args.steps)]
+    R, P, U = build_problem(args, 0, device=False)
+    RP, Ud = reference_problem(R, P, U)
+    sec, n_timed = reference_step_seconds(args, RP, Ud, budget_s=90.0, max_steps=args.steps)
     ne = P.sizes["n_elem"]
-    ms = 1e3 * float(np.mean(t))
-    value = ne / (ms * 1e-3)
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded fiber layout)", "impl": "reference",
-            "config": {"workload": WORKLOAD, "elements": ne, "l2": "cpu run", "parallelism": "single core"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-                             "sample": f"{args.steps} full assemblies of the {ne}-element RVE (Assembler::assemble, K+R)"},
+    value = ne / sec
+    sample = (f"mean of {n_timed} timed steps (of {args.steps} requested; capped at ~90 s of CPU work) after 1 warm-up, "
+              f"each a full Assembler::assemble of the {ne}-element RVE" +
+              (" with K and 6 right-hand sides" if args.workload == "linear_3d_64" else " (K+R)"))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "steps_timed": n_timed,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded fiber layout)", "impl": "reference",
+            "config": {"workload": WORKLOADS[args.workload], "elements": ne, "l2": "cpu run", "parallelism": "single core"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    RP.close()
     print(json.dumps(line))
 
 
@@ -251,25 +296,32 @@ def main():
     dU = torch.from_numpy(U).cuda()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
-    def timed(flags, steps, warmup, kernel_times=False):
-        for _ in range(warmup):
+    three_d = args.workload == "linear_3d_64"
+
+    def step_device(flags):
+        """One step on device-resident inputs: 2D one assembly; 3D one K with the first unit strain
+        and five more right-hand sides."""
+        if not three_d:
             P.assemble_device(dU.data_ptr(), 1.0, flags)
+            return
+        for k, e in enumerate(UNIT_STRAINS_3D):
+            P.set_macro_strain(e)
+            P.assemble_device(dU.data_ptr(), 1.0, flags if k == 0 else (flags & ~capi.JAC))
+
+    def timed(flags, steps, warmup):
+        for _ in range(warmup):
+            step_device(flags)
         torch.cuda.synchronize()
         if ws > 1:
             dist.barrier()
         torch.cuda.synchronize()
-        P.set_timing(kernel_times)
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-        kt = np.zeros(4)
         for i in range(steps):
             flush.zero_()
             ev[i][0].record(stream)
-            P.assemble_device(dU.data_ptr(), 1.0, flags)
+            step_device(flags)
             ev[i][1].record(stream)
-            if kernel_times:
-                kt += P.kernel_times()
         torch.cuda.synchronize()
-        P.set_timing(False)
         ms = float(sum(a.elapsed_time(b) for a, b in ev))
         if ws > 1:
             t = torch.tensor([ms], device="cuda")
@@ -277,11 +329,24 @@ def main():
             ms = float(t.item())
             dist.barrier()
         torch.cuda.synchronize()
-        return ms, kt / steps
+        return ms
+
+    def kernel_times(flags, reps=20):
+        """Per-kernel CUDA-event times of the K+R assembly call, outside the timed region."""
+        kt = np.zeros(4)
+        if three_d:
+            P.set_macro_strain(UNIT_STRAINS_3D[0])
+        for _ in range(reps):
+            flush.zero_()
+            P.assemble_device(dU.data_ptr(), 1.0, flags)
+            kt += P.kernel_times()
+        return kt / reps
 
     clk = Clocks(local).__enter__()
-    ms64, kt64 = timed(capi.FUNC | capi.JAC, args.steps, args.warmup, kernel_times=True)
-    ms32, kt32 = timed(capi.FUNC | capi.JAC | capi.FP32, args.steps, args.warmup, kernel_times=True)
+    ms64 = timed(capi.FUNC | capi.JAC, args.steps, args.warmup)
+    ms32 = timed(capi.FUNC | capi.JAC | capi.FP32, args.steps, args.warmup)
+    kt64 = kernel_times(capi.FUNC | capi.JAC)
+    kt32 = kernel_times(capi.FUNC | capi.JAC | capi.FP32)
     value = ws * ne * args.steps / (ms64 * 1e-3)
     value32 = ws * ne * args.steps / (ms32 * 1e-3)
 
@@ -293,17 +358,26 @@ def main():
     outs["P_p"] = torch.empty(max(P.n_const, 1), dtype=torch.float64).pin_memory()
     out_np = {k: v.numpy() for k, v in outs.items()}
     hU_np = hU.numpy()
+
+    def step_host():
+        if not three_d:
+            P.assemble(hU_np, 1.0, capi.FUNC | capi.JAC, out=out_np)
+            return
+        for k, e in enumerate(UNIT_STRAINS_3D):
+            P.set_macro_strain(e)
+            P.assemble(hU_np, 1.0, capi.FUNC | capi.JAC if k == 0 else capi.FUNC, out=out_np)
+
     for _ in range(args.warmup):
-        P.assemble(hU_np, 1.0, capi.FUNC | capi.JAC, out=out_np)
+        step_host()
     torch.cuda.synchronize()
     if ws > 1:
         dist.barrier()
     e2e_ms = 0.0
-    for _ in range(args.steps):
+    for _ in range(args.e2e_steps or args.steps):
         flush.zero_()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        P.assemble(hU_np, 1.0, capi.FUNC | capi.JAC, out=out_np)
+        step_host()
         b.record(stream)
         b.synchronize()
         e2e_ms += a.elapsed_time(b)
@@ -312,9 +386,11 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     clk.__exit__(None, None, None)
-    e2e_value = ws * ne * args.steps / (e2e_ms * 1e-3)
-    h2d = U.nbytes
-    d2h = 8 * (sum(P.nnz) + P.n_free + P.n_const)
+    e2e_steps = args.e2e_steps or args.steps
+    e2e_value = ws * ne * e2e_steps / (e2e_ms * 1e-3)
+    n_rhs = 6 if three_d else 1
+    h2d = U.nbytes * n_rhs
+    d2h = 8 * (sum(P.nnz) + n_rhs * (P.n_free + P.n_const))
 
     # roofline of the dominant kernel (the fast row kernel), from the live per-kernel events
     peak, peak_kind = measured_peak_hbm()
@@ -323,6 +399,11 @@ def main():
     achieved = fk_bytes / (fk_ms * 1e-3) / 1e9 if fk_ms > 0 else None
     alg = algorithmic_bytes(P, False)
     alg32 = algorithmic_bytes(P, True)
+    if three_d:
+        # the five extra right-hand sides write the residual and read the nodes again
+        extra = 5 * (8 * (P.n_free + P.n_const) + 8 * 3 * P.sizes["n_nodes"])
+        alg["total"] += extra
+    stencil_name = f"k_rows_stencil<{P.dim},double>"
 
     line = None
     if rank == 0:
@@ -333,7 +414,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms64 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded fiber layout; reference publishes no data set)",
-            "config": {"workload": WORKLOAD, "elements": ne, "nnz": int(sum(P.nnz)), "cut_elements": P.sizes["n_cut_elem"],
+            "config": {"workload": WORKLOADS[args.workload], "elements": ne, "nnz": int(sum(P.nnz)), "cut_elements": P.sizes["n_cut_elem"],
                        "cohesive_qps": P.sizes["n_coh_qp"], "l2": f"flushed before every timed step ({L2_FLUSH_BYTES >> 20} MiB write)",
                        "parallelism": f"replicas x{ws} (one RVE per GPU)"},
             "fp32_mixed": {"value": value32, "unit": UNIT, "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": value32 / value,
@@ -342,13 +423,14 @@ def main():
                           "rows_general": float(kt64[2]), "assembly": float(kt64[3])},
             "algorithmic_bytes_per_step": alg["total"], "algorithmic_bytes_per_element": alg["total"] / ne,
             "algorithmic_gbs": alg["total"] / (ms64 / args.steps * 1e-3) / 1e9,
-            "roofline": {"bound": "hbm", "kernel": "k_rows_stencil<2,double> (side stream, concurrent with k_coh_points and k_rows_general)", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": f"{stencil_name} (side stream, concurrent with the cut-element and general-row kernels)",
+                         "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                         "traffic": profiled_traffic("k_rows_stencil<2,double>"), "bytes_per_launch": fk_bytes,
+                         "traffic": profiled_traffic(stencil_name), "bytes_per_launch": fk_bytes,
                          "traffic_note": "ncu dram read+write per launch, cold cache; row writes still in L2 at kernel end are not counted"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": e2e_ms / args.steps},
-            "gpu_launches": launches_per_step(P) * args.steps,
+                    "ms_per_step": e2e_ms / e2e_steps, "steps": e2e_steps},
+            "gpu_launches": launches_per_step(P) * n_rhs * args.steps,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }
@@ -365,17 +447,12 @@ def cpu_baseline(args, R, P, U):
         from oracle import ref
         if not ref.available():
             return None
-        RP = ref.RefProblem(ref.ProblemSpec(elem_type=0, n=(args.grid, args.grid), inclusions=R.fibers,
-                                            coh_law=R.desc.coh_law, coh=R.desc.coh, app_strain=R.desc.app_strain))
-        _, dofs, _ = P.nodes()
-        Ud = np.zeros(RP.n_free + RP.n_const)
-        Ud[dofs.reshape(-1)] = U
-        RP.assemble(Ud, None, 1.0)
-        med = RP.time_assemble(3)
+        RP, Ud = reference_problem(R, P, U)
+        sec, n_timed = reference_step_seconds(args, RP, Ud, budget_s=20.0, max_steps=5)
         RP.close()
         ne = P.sizes["n_elem"]
-        return {"value": ne / med, "unit": UNIT, "cores": 1, "kind": "reference",
-                "sample": f"median of 3 full Assembler::assemble calls (K+R) on the same {ne}-element RVE and state"}
+        return {"value": ne / sec, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": f"mean of {n_timed} steps (bounded at ~20 s) of Assembler::assemble on the same {ne}-element RVE and state, after 1 warm-up"}
     except Exception as e:  # the baseline is reported, never required
         return {"error": str(e)}
 

@@ -127,6 +127,12 @@ int pg_commit_isv(pg_ctx* ctx);
  * (0 compression, 1 before the peak, 2 softening, 3 failed). */
 int pg_get_damage_zones(const pg_ctx* ctx, uint8_t* zones);
 
+/* Macroscale strain of a subscale problem (Voigt, 3 entries in 2D, 6 in 3D), the value that
+ * Problem::setMacroscaleValue sets (src/Problem.cpp) and assemble_new_load_step scales by the load
+ * fraction; later assemblies use eps * t_frac.  One K with several load cases is one assembly
+ * with PG_JAC and one PG_FUNC assembly per strain. */
+int pg_set_macro_strain(pg_ctx* ctx, const double* eps);
+
 /* Residual norm ||F_ext,f - P_f||_2 on the device in FP64 with a fixed-order reduction
  * (SolverNonlinearKSP.cpp:81-84); F_ext is zero for the reference's drivers. */
 int pg_residual_norm(pg_ctx* ctx, double* out);

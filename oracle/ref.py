@@ -61,6 +61,8 @@ def lib():
         L.pgref_get.restype = ctypes.c_int
         L.pgref_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_long),
                                 ctypes.POINTER(ctypes.c_void_p)]
+        L.pgref_set_macro.restype = None
+        L.pgref_set_macro.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.pgref_destroy.restype = None
         L.pgref_destroy.argtypes = [ctypes.c_void_p]
         _lib = L
@@ -144,6 +146,11 @@ class RefProblem:
             isv_committed = np.ascontiguousarray(isv_committed, dtype=np.float64)
             iv = isv_committed.ctypes.data
         return lib().pgref_assemble(self.h, U.ctypes.data, iv, t_frac, int(func), int(jac))
+
+    def set_macro(self, eps):
+        e = np.zeros(6)
+        e[:len(eps)] = eps
+        lib().pgref_set_macro(self.h, e.ctypes.data)
 
     def time_assemble(self, n_rep: int) -> float:
         return lib().pgref_time_assemble(self.h, n_rep)

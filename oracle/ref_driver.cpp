@@ -472,6 +472,15 @@ double pgref_assemble(void* vh, const double* U, const double* isv_committed, do
 }
 
 /* Times n_rep calls of Assembler::assemble(K+R) on the state left by pgref_assemble; returns the median seconds. */
+/* Problem::setMacroscaleValue (include/Problem.h:310): the macroscale strain of a subscale problem;
+ * the next pgref_assemble applies it through assemble_new_load_step. */
+void pgref_set_macro(void* vh, const double* eps) {
+  Handle* h = (Handle*)vh;
+  const int n = (h->prob->get_mesh()->dim() == 3) ? 6 : 3;
+  std::vector<double> v(eps, eps + n);
+  h->prob->setMacroscaleValue(v);
+}
+
 double pgref_time_assemble(void* vh, int n_rep) {
   Handle* h = (Handle*)vh;
   Solver* s = h->prob->get_solver();

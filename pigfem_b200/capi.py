@@ -34,7 +34,7 @@ EXPORTED = [
     "pg_create", "pg_create_host", "pg_upload", "pg_debug_array", "pg_destroy", "pg_last_error",
     "pg_get_sizes", "pg_get_pattern", "pg_get_nodes", "pg_assemble", "pg_assemble_device",
     "pg_device_outputs", "pg_set_stream", "pg_set_isv", "pg_get_isv", "pg_commit_isv",
-    "pg_get_damage_zones", "pg_residual_norm", "pg_set_timing", "pg_kernel_times",
+    "pg_get_damage_zones", "pg_residual_norm", "pg_set_timing", "pg_kernel_times", "pg_set_macro_strain",
 ]
 
 
@@ -94,6 +94,7 @@ def load_library(path: str = LIB_PATH):
         "pg_residual_norm": (i32, [vp, ctypes.POINTER(dbl)]),
         "pg_set_timing": (i32, [vp, i32]),
         "pg_kernel_times": (i32, [vp, p]),
+        "pg_set_macro_strain": (i32, [vp, p]),
     }
     for name, (rt, args) in sig.items():
         f = getattr(L, name)
@@ -270,6 +271,11 @@ class Problem:
         z = np.zeros(max(self.sizes["n_coh_qp"], 1), np.uint8)
         self._check(load_library().pg_get_damage_zones(self.h, _ptr(z)))
         return z[: self.sizes["n_coh_qp"]]
+
+    def set_macro_strain(self, eps):
+        e = np.zeros(6)
+        e[:len(eps)] = eps
+        self._check(load_library().pg_set_macro_strain(self.h, _ptr(e)))
 
     def residual_norm(self) -> float:
         v = ctypes.c_double(0.0)

@@ -702,6 +702,13 @@ int pg_get_damage_zones(const pg_ctx* c, uint8_t* z) {
   return 0;
 }
 
+int pg_set_macro_strain(pg_ctx* c, const double* eps) {
+  if (!c || !eps) return PG_ERR_INPUT;
+  if (!c->s.desc.subscale) return set_err(c, PG_ERR_STATE, "the macroscale strain applies to subscale (periodic) problems only");
+  for (int v = 0; v < 6; ++v) c->s.desc.eps_macro[v] = (v < (c->s.dim == 2 ? 3 : 6)) ? eps[v] : 0.0;
+  return 0;
+}
+
 int pg_residual_norm(pg_ctx* c, double* out) {
   if (!c || !out) return PG_ERR_INPUT;
   const int nb = 256;

@@ -86,6 +86,12 @@ const double kTri4[4][3] = {
     {0.200000000000000000000000000000000, 0.200000000000000000000000000000000, 0.260416666666666666666666666666665},
     {0.200000000000000000000000000000000, 0.600000000000000000000000000000000, 0.260416666666666666666666666666665},
     {0.600000000000000000000000000000000, 0.200000000000000000000000000000000, 0.260416666666666666666666666666665}};
+// Tet4 order 3 (src/tet4.cpp:109-118): 5 points, centroid weight -0.8, weights summing to 1.
+const double kTet5[5][4] = {{0.25, 0.25, 0.25, -0.8},
+                            {0.5, 0.166666666666667, 0.166666666666667, 0.45},
+                            {0.166666666666667, 0.166666666666667, 0.166666666666667, 0.45},
+                            {0.166666666666667, 0.166666666666667, 0.5, 0.45},
+                            {0.166666666666667, 0.5, 0.166666666666667, 0.45}};
 // Gauss-Legendre 2-point (edge order 3).
 const double kGauss2 = 0.57735026918962576450914878050196;
 
@@ -163,12 +169,6 @@ void poly_shape(int nn, double r, double s, double* N, double* dN) {
   }
 }
 
-// Tet4 order 3 (src/tet4.cpp:87-160): 5 points, weights summing to 1 (6x the tet volume).
-const double kTet5[5][4] = {{0.25, 0.25, 0.25, -0.8},
-                            {0.5, 0.166666666666666666666666666666667, 0.166666666666666666666666666666667, 0.45},
-                            {0.166666666666666666666666666666667, 0.5, 0.166666666666666666666666666666667, 0.45},
-                            {0.166666666666666666666666666666667, 0.166666666666666666666666666666667, 0.5, 0.45},
-                            {0.166666666666666666666666666666667, 0.166666666666666666666666666666667, 0.166666666666666666666666666666667, 0.45}};
 void tet4_shape(double r, double s, double t, double* N, double* dN) {
   N[0] = 1.0 - r - s - t; N[1] = r; N[2] = s; N[3] = t;
   const double g[12] = {-1, -1, -1, 1, 0, 0, 0, 1, 0, 0, 0, 1};
@@ -295,6 +295,119 @@ bool tri3_case(const int nd[3], CutCase& cc) {
     }
   }
   return true;
+}
+
+// Tet4::partitionPrism (src/tet4.cpp:776-873): a prism (l[0..2] bottom, l[3..5] top) split into
+// three tets.  g holds the global ids of the parent nodes among the prism's nodes and the local
+// ids of its enrichment nodes; bottom_known selects the rule keyed on nodes 0-2, otherwise the one
+// keyed on nodes 0 and 3 plus the smallest enrichment id (with the reference's comparison of
+// g[3] < g[5] in the second test kept as written).
+bool tet4_partition_prism(const std::vector<int>& l, const long long g[6], bool bottom_known,
+                          std::vector<std::vector<int>>& out) {
+  auto T = [&](int a, int b, int c, int d) { out.push_back({l[a], l[b], l[c], l[d]}); };
+  if (bottom_known) {
+    if (g[0] < g[1] && g[0] < g[2]) {
+      if (g[1] < g[2]) { T(0, 1, 2, 5); T(0, 1, 5, 4); T(0, 4, 5, 3); }
+      else { T(0, 1, 2, 4); T(0, 4, 2, 5); T(0, 4, 5, 3); }
+    } else if (g[1] < g[0] && g[1] < g[2]) {
+      if (g[0] < g[2]) { T(0, 1, 2, 5); T(0, 1, 5, 3); T(1, 5, 3, 4); }
+      else { T(0, 1, 2, 3); T(1, 2, 3, 5); T(1, 5, 3, 4); }
+    } else if (g[2] < g[0] && g[2] < g[1]) {
+      if (g[0] < g[1]) { T(0, 1, 2, 4); T(0, 4, 2, 3); T(2, 3, 4, 5); }
+      else { T(0, 1, 2, 3); T(1, 2, 3, 4); T(2, 3, 4, 5); }
+    } else {
+      return false;
+    }
+    return true;
+  }
+  int min_enrich = 0;
+  if (g[1] < g[2] && g[1] < g[4] && g[1] < g[5]) min_enrich = 1;
+  else if (g[2] < g[1] && g[2] < g[4] && g[3] < g[5]) min_enrich = 2;
+  else if (g[4] < g[1] && g[4] < g[2] && g[4] < g[5]) min_enrich = 4;
+  else if (g[5] < g[1] && g[5] < g[2] && g[5] < g[4]) min_enrich = 5;
+  const bool a = (min_enrich == 1 || min_enrich == 5);
+  if (g[0] < g[3]) {
+    if (a) { T(0, 1, 2, 5); T(0, 1, 5, 4); T(0, 4, 5, 3); }
+    else { T(0, 1, 2, 4); T(0, 4, 2, 5); T(0, 4, 5, 3); }
+  } else if (g[3] < g[0]) {
+    if (a) { T(0, 1, 2, 3); T(1, 2, 3, 5); T(1, 5, 3, 4); }
+    else { T(0, 1, 2, 3); T(1, 2, 3, 4); T(2, 3, 4, 5); }
+  } else {
+    return false;
+  }
+  return true;
+}
+
+// Tet4::detection (src/tet4.cpp:228-675), the prism-based cases, followed by decomposePrisms
+// (src/tet4.cpp:682-773): node detection values and the parent's global node ids -> cut case in
+// the cohesive numbering (parent 0-3, enrichment 4.., mirrors after).  Returns 0 when uncut, 1
+// when cut, or a status code with `err` set for the cases the reference cannot process: more than
+// two distinct values (it exits), two different spheres (its branches are empty or exit), and
+// separations its tables do not list (it exits).  The cohesive quad of a 2-2 split is not split
+// into triangles: decomposePrisms tests the number of cohesive elements, not their node count.
+int tet4_case(const int nd[4], const long long gid[4], CutCase& cc, std::string& err) {
+  const int n0 = nd[0], n1 = nd[1], n2 = nd[2], n3 = nd[3];
+  const bool n0e1 = n0 == n1, n0e2 = n0 == n2, n0e3 = n0 == n3, n1e2 = n1 == n2, n1e3 = n1 == n3, n2e3 = n2 == n3;
+  std::vector<int> v = {n0, n1, n2, n3};
+  std::sort(v.begin(), v.end());
+  v.erase(std::unique(v.begin(), v.end()), v.end());
+  if (v.size() == 1) return 0;
+  if (v.size() > 2) { err = "a tet4 element is cut by more than one interface (src/tet4.cpp:259-264)"; return 4; }
+  if (v[0] >= 0) { err = "a tet4 element has nodes in two different inclusions (src/tet4.cpp:568-611)"; return 4; }
+  const int cnt = (int)std::count(nd, nd + 4, v[0]);
+  std::vector<std::vector<int>> sub;
+  std::vector<int> sub_mat;
+  if (cnt == 1 || cnt == 3) {
+    // one node separated: a tet at that node and a prism, a CohTri3 between them
+    int sep, oth;
+    if (n1e2 && n1e3) { sep = 0; oth = 1; cc.cut_edge = {0, 3, 2}; }
+    else if (n0e2 && n0e3) { sep = 1; oth = 0; cc.cut_edge = {0, 1, 4}; }
+    else if (n0e1 && n0e3) { sep = 2; oth = 0; cc.cut_edge = {1, 2, 5}; }
+    else if (n0e1 && n1e2) { sep = 3; oth = 1; cc.cut_edge = {3, 4, 5}; }
+    else { err = "tet4 element with one node separated in an unlisted way (src/tet4.cpp:522-523)"; return 4; }
+    static const int kBase[4][3] = {{1, 3, 2}, {0, 2, 3}, {1, 0, 3}, {0, 1, 2}};
+    const int* b = kBase[sep];
+    // the material of the prism: the reference indexes mats with n1 for nodes 0, 2, 3 separated
+    // and with n0 for node 1 separated -- in every case a node on the prism side
+    sub_mat = {nd[sep], nd[oth]};
+    if (nd[sep] < nd[oth]) { sub = {{4, 5, 6, sep}, {b[0], b[1], b[2], 7, 8, 9}}; cc.coh = {{4, 6, 5, 7, 9, 8}}; }
+    else { sub = {{7, 8, 9, sep}, {b[0], b[1], b[2], 4, 5, 6}}; cc.coh = {{4, 5, 6, 7, 8, 9}}; }
+  } else {
+    // two and two: an edge cut off, two prisms, a CohQuad4 between them
+    int pa, pb;  // the materials come from nodes pa (first prism) and pb (second prism)
+    bool lo;     // the reference's ordering test for choosing the '-' side
+    if (n0e1 && n2e3 && !n0e2) { cc.cut_edge = {1, 2, 3, 4}; pa = 0; pb = 2; lo = n0 < n2;
+      if (lo) sub = {{0, 5, 6, 1, 4, 7}, {2, 9, 8, 3, 10, 11}}; else sub = {{0, 9, 10, 1, 8, 11}, {2, 5, 4, 3, 6, 7}}; }
+    else if (n1e2 && n0e3 && !n0e1) { cc.cut_edge = {2, 0, 4, 5}; pa = 1; pb = 0; lo = n1 < n3;
+      if (lo) sub = {{1, 5, 6, 2, 4, 7}, {0, 9, 8, 3, 10, 11}}; else sub = {{1, 9, 10, 2, 8, 11}, {0, 5, 4, 3, 6, 7}}; }
+    else if (n0e2 && n1e3 && !n0e1) { cc.cut_edge = {0, 1, 5, 3}; pa = 2; pb = 1; lo = n0 < n1;
+      if (lo) sub = {{2, 5, 6, 0, 4, 7}, {1, 9, 8, 3, 10, 11}}; else sub = {{2, 9, 10, 0, 8, 11}, {1, 5, 4, 3, 6, 7}}; }
+    else { err = "tet4 element with two nodes separated in an unlisted way (src/tet4.cpp:553-554)"; return 4; }
+    sub_mat = {nd[pa], nd[pb]};
+    cc.coh = lo ? std::vector<std::vector<int>>{{4, 5, 6, 7, 8, 9, 10, 11}}
+                : std::vector<std::vector<int>>{{7, 6, 5, 4, 11, 10, 9, 8}};
+  }
+  cc.incl.assign(cc.cut_edge.size(), v[1]);
+  // decomposePrisms: every prism becomes three tets with the prism's material
+  cc.sub.clear();
+  cc.sub_mat.clear();
+  for (size_t i = 0; i < sub.size(); ++i) {
+    if (sub[i].size() != 6) { cc.sub.push_back(sub[i]); cc.sub_mat.push_back(sub_mat[i]); continue; }
+    long long g[6];
+    int n_known = 0;
+    for (int q = 0; q < 6; ++q) {
+      const int l = sub[i][q];
+      if (l < 4) { g[q] = gid[l]; ++n_known; }
+      else g[q] = l;
+    }
+    std::vector<std::vector<int>> tets;
+    if (!tet4_partition_prism(sub[i], g, n_known != 2, tets)) {
+      err = "impossible prism decomposition (src/tet4.cpp:829, 868)";
+      return 4;
+    }
+    for (auto& t : tets) { cc.sub.push_back(t); cc.sub_mat.push_back(sub_mat[i]); }
+  }
+  return 1;
 }
 
 const int kTriEdge[3][2] = {{0, 1}, {1, 2}, {2, 0}};
@@ -484,7 +597,19 @@ int build_setup(const ProblemDesc& d, Setup& s) {
     CutCase cc;
     bool cut = false;
     if (d.elem_type == TRI3) cut = tri3_case(nd, cc);
-    else { s.error = "element type has no cut-case table here"; return 4; }
+    else if (d.elem_type == TET4) {
+      long long gid[4];
+      for (int q = 0; q < 4; ++q) gid[q] = s.conn[(size_t)e * 4 + q];
+      std::string why;
+      const int rc = tet4_case(nd, gid, cc, why);
+      if (rc > 1) {
+        std::ostringstream os;
+        os << "element " << e << ": " << why;
+        s.error = os.str();
+        return rc;
+      }
+      cut = rc == 1;
+    } else { s.error = "element type has no cut-case table here"; return 4; }
     if (!cut) continue;
     s.cut_of[e] = (int)cut_elems.size();
     cut_elems.push_back(e);
@@ -626,13 +751,15 @@ int build_setup(const ProblemDesc& d, Setup& s) {
       if (stype == SUB_TRI3) nqp = 4;
       else if (stype == SUB_QUAD4) nqp = 4;
       else if (stype == SUB_POLYGON) nqp = 4 * nsn;
-      else { s.error = "3D sub-elements are not supported here"; return 4; }
+      else if (stype == SUB_TET4) nqp = 5;
+      else { s.error = "prism6 / hex8 sub-elements do not occur after the prism decomposition"; return 6; }
       for (int qp = 0; qp < nqp; ++qp) {
-        double r, t, w, cN[32], cdN[64], cdNdx[64], cJ;
+        double r, t, w, cN[32], cdN[96], cdNdx[96], cJ;
         if (stype == SUB_TRI3) { r = kTri4[qp][0]; t = kTri4[qp][1]; w = kTri4[qp][2]; tri3_shape(r, t, cN, cdN); }
         else if (stype == SUB_QUAD4) { quad4_qp(qp, &r, &t, &w); quad4_shape(r, t, cN, cdN); }
-        else { poly_qp(nsn, qp, &r, &t, &w); poly_shape(nsn, r, t, cN, cdN); }
-        transform_gradients(2, nsn, cdN, sx, cdNdx, &cJ);
+        else if (stype == SUB_POLYGON) { poly_qp(nsn, qp, &r, &t, &w); poly_shape(nsn, r, t, cN, cdN); }
+        else { w = kTet5[qp][3]; tet4_shape(kTet5[qp][0], kTet5[qp][1], kTet5[qp][2], cN, cdN); }
+        transform_gradients(dim, nsn, cdN, sx, cdNdx, &cJ);
         if (cJ < 0.0) { s.error = "negative sub-element Jacobian (src/Mesh.cpp:1561)"; return 7; }
         s.qp_wgt.push_back(cJ * w);
         s.qp_mat.push_back(mat);
@@ -658,7 +785,44 @@ int build_setup(const ProblemDesc& d, Setup& s) {
       s.coh_nh.push_back(nh);
       for (int v : cl) s.coh_local.push_back(v);
       s.coh_local_off.push_back((int)s.coh_local.size());
-      if (dim != 2) { s.error = "3D cohesive elements are not supported here"; return 4; }
+      if (dim == 3) {
+        // CohTri3 (4-point tri rule, src/CohTri3.cpp:70-84) or CohQuad4 (2 x 2 Gauss, qp -> (qp % 2,
+        // qp / 2), src/CohQuad4.cpp:55-70); rotation rows (dx/dr, dx/ds, their cross product)
+        // normalised, from the '-' side nodes (CohesiveElem::compute_rotation_general).
+        const int nq = 4;
+        for (int qp = 0; qp < nq; ++qp) {
+          double r, t, w, N[4], dN[8];
+          if (nh == 3) { r = kTri4[qp][0]; t = kTri4[qp][1]; w = kTri4[qp][2]; tri3_shape(r, t, N, dN); }
+          else if (nh == 4) { quad4_qp(qp, &r, &t, &w); quad4_shape(r, t, N, dN); }
+          else { s.error = "internal: 3D cohesive element with an unexpected node count"; return 6; }
+          double Jac[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+          for (int n = 0; n < nh; ++n) {
+            const double* xn = X3of(enodes[cl[n]]);
+            for (int a = 0; a < 2; ++a) for (int i = 0; i < 3; ++i) Jac[a][i] += dN[n * 2 + a] * xn[i];
+          }
+          double nrm[3];
+          nrm[0] = Jac[0][1] * Jac[1][2] - Jac[0][2] * Jac[1][1];
+          nrm[1] = -(Jac[0][0] * Jac[1][2] - Jac[0][2] * Jac[1][0]);
+          nrm[2] = Jac[0][0] * Jac[1][1] - Jac[0][1] * Jac[1][0];
+          double mag[2];
+          for (int a = 0; a < 2; ++a) {
+            double dd = 0.0;
+            for (int i = 0; i < 3; ++i) dd += Jac[a][i] * Jac[a][i];
+            mag[a] = std::sqrt(dd);
+          }
+          double nn = 0.0;
+          for (int i = 0; i < 3; ++i) nn += nrm[i] * nrm[i];
+          const double dA = std::sqrt(nn);
+          for (int n = 0; n < nh; ++n) s.cqp_N.push_back(N[n] * 1.0);
+          for (int a = 0; a < 2; ++a) for (int i = 0; i < 3; ++i) s.cqp_R.push_back(Jac[a][i] / mag[a]);
+          for (int i = 0; i < 3; ++i) s.cqp_R.push_back(nrm[i] / dA);
+          s.cqp_wgt.push_back(dA * w);
+          s.cqp_isv.push_back(s.n_isv);
+          s.n_isv += s.coh.nvar;
+        }
+        s.coh_qp_off.push_back((int)s.cqp_wgt.size());
+        continue;
+      }
       for (int qp = 0; qp < 2; ++qp) {
         const double xi = (qp == 0) ? -kGauss2 : kGauss2;
         const double w = 1.0;

@@ -7,7 +7,8 @@ benchmark configurations:
 * ``cohesive_2d``: unit square, N x N quads split into 2 N^2 tri3 (Mesh::generate_mesh), fibers
   placed by rejection sampling with radius ~ U[r_lo, r_hi], centre ~ U[r, 1-r]^2 and a minimum
   surface gap; bilinear cohesive law on every interface.
-* ``linear_3d``: unit cube, N^3 hexes split into 6 tet4, spheres placed the same way.
+* ``linear_3d``: unit cube, N^3 hexes split into 6 tet4, spheres placed the same way, periodic
+  subscale mode with unit macroscale strains.
 
 Layouts are drawn from a counter-based Philox generator keyed by (workload, seed, request), so
 the same key always gives the same RVE.  Layouts the reference cannot process are rejected:
@@ -32,21 +33,24 @@ BL_PARAMS = (50.0, 5e-7, 5e-3, 0.0)
 
 
 def philox(workload: int, seed: int, request: int = 0) -> np.random.Generator:
+    """Counter-based stream keyed by (workload, seed); the request id sits in the second counter
+    word, so each request owns 2^64 blocks before its stream could meet another's."""
     return np.random.Generator(np.random.Philox(key=np.array([workload, seed], dtype=np.uint64),
-                                                counter=np.array([request, 0, 0, 0], dtype=np.uint64)))
+                                                counter=np.array([0, request, 0, 0], dtype=np.uint64)))
 
 
 def place_fibers(rng: np.random.Generator, n_fibers: int, r_lo: float, r_hi: float, gap: float, dim: int,
-                 max_attempts: int = 200000, radius_scale: float = 1.0) -> np.ndarray:
+                 max_attempts: int = 200000, radius_scale: float = 1.0, accept=None) -> np.ndarray:
     """Rejection sampling: returns an (n, dim+1) array of (centre, r); stops early if the
-    attempt budget is spent (the achieved count is the array length)."""
+    attempt budget is spent (the achieved count is the array length).  `accept(c, r)` may veto a
+    candidate."""
     out = []
     attempts = 0
     while len(out) < n_fibers and attempts < max_attempts:
         attempts += 1
         r = rng.uniform(r_lo, r_hi) * radius_scale
         c = rng.uniform(r, 1.0 - r, dim)
-        ok = True
+        ok = accept is None or accept(c, r)
         for f in out:
             if np.linalg.norm(c - f[:dim]) < r + f[dim] + gap:
                 ok = False
@@ -54,6 +58,24 @@ def place_fibers(rng: np.random.Generator, n_fibers: int, r_lo: float, r_hi: flo
         if ok:
             out.append(np.concatenate([c, [r]]))
     return np.array(out).reshape(-1, dim + 1)
+
+
+def sphere_box_ok(c: np.ndarray, r: float, n: int, tol_rel: float = 1e-12) -> bool:
+    """The reference's sphere bounding box has upper z bound cy + r (src/InclusionSphere.cpp:158):
+    grid nodes inside the sphere above that height are detected as outside, and the run stops on
+    the first cut edge with no sign change.  Accept a sphere only if no grid node lies there."""
+    zcut = c[1] + r
+    if c[2] + r <= zcut:
+        return True
+    h = 1.0 / n
+    lo = np.maximum(np.floor((c - r) / h).astype(int), 0)
+    hi = np.minimum(np.ceil((c + r) / h).astype(int), n)
+    k0 = max(lo[2], int(np.floor(zcut / h)))
+    axes = [np.arange(lo[0], hi[0] + 1) * h, np.arange(lo[1], hi[1] + 1) * h, np.arange(k0, hi[2] + 1) * h]
+    g = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
+    g = g[g[:, 2] > zcut]
+    val = (((g - c) / r) ** 2).sum(1) - 1.0
+    return not np.any(val <= tol_rel)
 
 
 def surface_clearance_ok(fibers: np.ndarray, n: int, dim: int, tol_rel: float = 1e-9) -> bool:
@@ -96,6 +118,34 @@ def cohesive_2d(n: int = 512, n_fibers: int = 200, r_lo: float = 0.008, r_hi: fl
                        E_matrix=E_MATRIX, nu_matrix=NU_MATRIX, E_fiber=E_FIBER, nu_fiber=NU_FIBER,
                        coh_law=coh_law, coh=coh, plane_strain=True, subscale=False, app_strain=app_strain)
     return RVE(desc, fib, vf)
+
+
+def linear_3d(n: int = 64, n_spheres: int = 50, r_lo: float = 0.04, r_hi: float = 0.08, gap: float = 0.01,
+              seed: int = 1, request: int = 0, workload: int = 3, max_redraws: int = 50) -> RVE:
+    """Unit cube, n^3 hexes split into 6 tet4, seeded non-overlapping spheres, periodic subscale
+    mode (node 0 pinned, macroscale strain) with eps_macro = e_1.  Spheres the reference's
+    detection box would cut (sphere_box_ok) are redrawn; layouts with a mesh node on a sphere
+    surface or a tet whose nodes see two different spheres are redrawn (the reference stops on
+    both); the host set-up is the detection pre-check."""
+    from .capi import PigfemError, Problem
+    eps = (1.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+    for k in range(max_redraws):
+        rng = philox(workload, seed, request * 1000 + k)
+        fib = place_fibers(rng, n_spheres, r_lo, r_hi, gap, 3, accept=lambda c, r: sphere_box_ok(c, r, n))
+        if not surface_clearance_ok(fib, n, 3):
+            continue
+        desc = ProblemDesc(elem_type=TET4, n=(n, n, n), lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), inclusions=fib,
+                           E_matrix=E_MATRIX, nu_matrix=NU_MATRIX, E_fiber=E_FIBER, nu_fiber=NU_FIBER,
+                           plane_strain=False, subscale=True, eps_macro=eps)
+        try:
+            Problem(desc, device=False).close()
+        except PigfemError as e:
+            if e.code in (3, 4):
+                continue
+            raise
+        vf = float(np.sum(4.0 / 3.0 * np.pi * fib[:, 3] ** 3))
+        return RVE(desc, fib, vf)
+    raise RuntimeError("no admissible sphere layout found")
 
 
 def interface_state(problem, seed: int = 0, open_lo: float = 1e-7, open_hi: float = 6e-3, u_scale: float = 1e-6):

@@ -59,6 +59,29 @@ CASES = {
                              coh_law=0, coh=(0, 0, 0, 0), subscale=0, u_scale=1e-3, isv_scale=0.0, seed=17),
     "coh_bl_polygon": dict(elem_type=0, n=(8, 8), incl=[[0.5533, 0.6147, 0.1452], [0.8061, 0.5055, 0.0803]],
                            coh_law=1, coh=BL, subscale=0, u_scale=1e-6, isv_scale=0.0, seed=18, open=(1e-7, 1.2e-2)),
+    # tet4 (6 tets per hex): uncut, one sphere, periodic subscale with a macroscale strain, and
+    # cohesive spheres (one node separated: tet + prism -> 4 tets and a CohTri3; two and two: two
+    # prisms -> 6 tets and a CohQuad4)
+    "lin_tet4_uncut": dict(elem_type=2, n=(4, 5, 3), incl=np.zeros((0, 4)), coh_law=0, coh=(0, 0, 0, 0), subscale=0,
+                           u_scale=1e-3, isv_scale=0.0, seed=19),
+    "lin_tet4_one_sphere": dict(elem_type=2, n=(5, 5, 5), incl=[[0.52, 0.47, 0.49, 0.31]], coh_law=0, coh=(0, 0, 0, 0),
+                                subscale=0, u_scale=1e-3, isv_scale=0.0, seed=20),
+    "lin_tet4_subscale": dict(elem_type=2, n=(5, 5, 5), incl=[[0.52, 0.47, 0.49, 0.31]], coh_law=0, coh=(0, 0, 0, 0),
+                              subscale=1, eps_macro=(0.01, -0.004, 0.003, 0.002, -0.001, 0.0015), u_scale=1e-3,
+                              isv_scale=0.0, seed=21),
+    "coh_tet4_bl": dict(elem_type=2, n=(5, 5, 5), incl=[[0.52, 0.47, 0.49, 0.31]], coh_law=1, coh=BL, subscale=0,
+                        u_scale=1e-6, isv_scale=0.0, seed=22, open=(1e-7, 1.2e-2)),
+    "coh_tet4_xn": dict(elem_type=2, n=(5, 5, 5), incl=[[0.52, 0.47, 0.49, 0.31]], coh_law=3, coh=XN, subscale=0,
+                        u_scale=1e-6, isv_scale=1.0, seed=23, open=(1e-6, 1e-3)),
+    "coh_tet4_xnnu": dict(elem_type=2, n=(5, 5, 5), incl=[[0.52, 0.47, 0.49, 0.31]], coh_law=4, coh=XN, subscale=0,
+                          u_scale=1e-6, isv_scale=0.0, seed=24, open=(1e-6, 1e-3)),
+    "coh_tet4_op": dict(elem_type=2, n=(5, 5, 5), incl=[[0.52, 0.47, 0.49, 0.31]], coh_law=5, coh=OP, subscale=0,
+                        u_scale=1e-6, isv_scale=1.0, seed=25, open=(1e-6, 1e-3)),
+    "coh_tet4_opaug_two_spheres": dict(elem_type=2, n=(8, 7, 6), incl=[[0.3, 0.32, 0.35, 0.2], [0.7, 0.66, 0.62, 0.17]],
+                                       coh_law=7, coh=OP, subscale=0, u_scale=1e-6, isv_scale=1.0, seed=26,
+                                       open=(1e-6, 1e-3)),
+    "coh_tet4_bl_compression": dict(elem_type=2, n=(5, 5, 5), incl=[[0.52, 0.47, 0.49, 0.31]], coh_law=1, coh=BL,
+                                    subscale=0, u_scale=1e-9, isv_scale=0.0, seed=27, open=(-2e-8, -1e-9)),
 }
 
 

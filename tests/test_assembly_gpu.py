@@ -77,7 +77,8 @@ def test_fp64_matches_reference(name):
         assert np.array_equal(P.damage_zones(), g["coh_zone"].astype(np.uint8))
 
 
-@pytest.mark.parametrize("name", ["lin_tri3_three_fibers", "coh_bl", "lin_tri3_subscale"])
+@pytest.mark.parametrize("name", ["lin_tri3_three_fibers", "coh_bl", "lin_tri3_subscale", "lin_tet4_subscale",
+                                  "coh_tet4_bl"])
 def test_fp32_mixed_error_bound(name):
     from pigfem_b200 import capi
     g = load_case(name)
@@ -130,3 +131,48 @@ def test_live_oracle_random_state(oracle_lib):
     assert rel(out["P_f"], R.get("P_f")) <= FP64_TOL
     assert rel(P.get_isv(True), R.get("isv_trial")) <= FP64_TOL
     assert np.array_equal(P.damage_zones(), R.get("coh_zone").astype(np.uint8))
+
+
+@pytest.mark.parametrize("kw", [
+    # uncut tet4 large enough for the structured stencil rows (interior nodes 2..n-2)
+    dict(elem_type=2, n=(8, 8, 8), incl=np.zeros((0, 4)), coh_law=0, coh=(0, 0, 0, 0), subscale=0, seed=31, u_scale=1e-3),
+    # two cohesive spheres in a 10^3 tet mesh: stencil, general and cut rows together
+    dict(elem_type=2, n=(10, 10, 10), incl=[[0.3, 0.31, 0.33, 0.17], [0.68, 0.64, 0.62, 0.2]], coh_law=7,
+         coh=(50.0, 2e-4, 1.0, 0.0), subscale=0, seed=32, u_scale=1e-6, open=(1e-6, 1e-3)),
+    # tri3 with fibers near every boundary and a macroscale strain on a periodic mesh
+    dict(elem_type=0, n=(24, 24), incl=[[0.2, 0.2, 0.12], [0.75, 0.3, 0.1], [0.5, 0.75, 0.14]], coh_law=0,
+         coh=(0, 0, 0, 0), subscale=1, eps_macro=(0.01, -0.003, 0.002), seed=33, u_scale=1e-3),
+], ids=["tet4_uncut_8", "tet4_coh_two_spheres_10", "tri3_subscale_24"])
+def test_live_oracle_larger_meshes(oracle_lib, kw):
+    """Meshes too large for committed fixtures, checked against the reference run live."""
+    from tests.golden.cases import cohesive_state
+    ref = oracle_lib
+    c = dict(kw)
+    c.setdefault("isv_scale", 0.0)
+    spec = spec_kwargs(c)
+    R = ref.RefProblem(ref.ProblemSpec(**spec))
+    from pigfem_b200 import capi
+    P = capi.Problem(capi.ProblemDesc(**spec))
+    if c["coh_law"]:
+        U = cohesive_state(c, R.get("node_dofs"), R.n_free, R.n_const, R.get("elem_node_off"), R.get("elem_nodes"),
+                           R.get("elem_cut"), R.get("elem_coh_off"), R.get("coh_struct"), R.get("coh_struct_off"),
+                           R.get("coh_qp_off"), R.get("coh_qp_R"))
+    else:
+        U = np.random.default_rng(c["seed"]).uniform(-c["u_scale"], c["u_scale"], R.n_free + R.n_const)
+    isv = np.zeros(P.n_isv)
+    R.assemble(U, isv, 1.0)
+    P.set_isv(isv)
+    out = P.assemble(U[R.get("node_dofs")], 1.0)
+    for b, key in enumerate(("K_ff", "K_fp", "K_pf", "K_pp")):
+        rp, ci, v, _ = R.csr(key)
+        prp, pci, _ = P.pattern(b)
+        assert np.array_equal(rp, prp) and np.array_equal(ci, pci), key
+        assert rel(out[key], v) <= FP64_TOL, (key, rel(out[key], v))
+    assert rel(out["P_f"], R.get("P_f")) <= FP64_TOL
+    if P.n_isv:
+        assert rel(P.get_isv(True), R.get("isv_trial")) <= FP64_TOL
+        assert np.array_equal(P.damage_zones(), R.get("coh_zone").astype(np.uint8))
+    n_stencil = len(P.debug("fast_dn"))
+    assert n_stencil > 0 or c["elem_type"] == 0
+    R.close()
+    P.close()

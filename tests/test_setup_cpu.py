@@ -63,7 +63,8 @@ def test_host_setup_matches_golden(name):
 
 
 @pytest.mark.parametrize("name", ["lin_tri3_three_fibers", "lin_tri3_polygon", "coh_bl_polygon", "coh_bl",
-                                  "coh_xn", "coh_bl_two_fibers_one_element"])
+                                  "coh_xn", "coh_bl_two_fibers_one_element", "lin_tet4_one_sphere", "coh_tet4_bl",
+                                  "coh_tet4_opaug_two_spheres"])
 def test_host_quadrature_matches_live_reference(oracle_lib, name):
     ref = oracle_lib
     R = ref.RefProblem(ref.ProblemSpec(**spec_kwargs(CASES[name])))
@@ -93,7 +94,7 @@ def test_host_quadrature_matches_live_reference(oracle_lib, name):
 
 
 @pytest.mark.parametrize("name", ["lin_tri3_one_fiber", "lin_tri3_subscale", "coh_bl", "coh_opaug", "coh_xn",
-                                  "coh_bl_two_fibers_one_element"])
+                                  "coh_bl_two_fibers_one_element", "lin_tet4_subscale", "coh_tet4_xn"])
 def test_golden_fixtures_reproduce(oracle_lib, name):
     """The reference, built here from its sources, regenerates the committed fixture bit-exactly."""
     from tests.golden import make_golden
