@@ -137,6 +137,24 @@ int pg_set_macro_strain(pg_ctx* ctx, const double* eps);
  * (SolverNonlinearKSP.cpp:81-84); F_ext is zero for the reference's drivers. */
 int pg_residual_norm(pg_ctx* ctx, double* out);
 
+/* Jacobi-preconditioned conjugate gradients on K_ff of the last assembly (FP64, on the device).
+ * d_b: nrhs right-hand sides of n_free entries each, one after another; d_x: initial guesses in,
+ * solutions out (same layout).  Stops each right-hand side at ||b - K x|| <= rtol ||b|| (checked
+ * every iteration on the device; the host looks every 16 iterations, so at most max_it + 15
+ * iterations run).  Inner products are fixed-order reductions: a right-hand side's result does not
+ * depend on the others solved with it.  iters / relres (host, nrhs entries, may be NULL) get each
+ * right-hand side's iteration count and final relative residual.  PG_ERR_STATE if any right-hand
+ * side missed the tolerance.  The reference solves with a direct Cholesky factorisation (PETSc
+ * KSPPREONLY + PCCHOLESKY through MUMPS, src/Solver.cpp:108-194); this is the device solver that
+ * replaces it for linear requests and Newton corrections. */
+int pg_pcg_solve(pg_ctx* ctx, const double* d_b, double* d_x, int nrhs, double rtol, int max_it, int* iters,
+                 double* relres);
+
+/* Volume average of the stress over the volumetric quadrature points (Problem::homogenize,
+ * src/Problem.cpp:471-484): out[0..nv-1] = sum(J W sigma) / sum(J W), out[nv] = sum(J W), with
+ * sigma from d_U (device, node-major) plus the macroscale strain eps_macro * t_frac. */
+int pg_homogenize(pg_ctx* ctx, const double* d_U, double t_frac, double* out);
+
 /* ||x||_2 of a device vector of n doubles, written to the device double *d_out, enqueued on
  * `stream` (a cudaStream_t; NULL = legacy default stream).  No counterpart in the reference.
  * It allocates nothing: the block partials and a completion counter live in a fixed 32 KiB

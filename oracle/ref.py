@@ -61,6 +61,8 @@ def lib():
         L.pgref_get.restype = ctypes.c_int
         L.pgref_get.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_long),
                                 ctypes.POINTER(ctypes.c_void_p)]
+        L.pgref_homogenize.restype = None
+        L.pgref_homogenize.argtypes = [ctypes.c_void_p]
         L.pgref_set_macro.restype = None
         L.pgref_set_macro.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.pgref_destroy.restype = None
@@ -146,6 +148,10 @@ class RefProblem:
             isv_committed = np.ascontiguousarray(isv_committed, dtype=np.float64)
             iv = isv_committed.ctypes.data
         return lib().pgref_assemble(self.h, U.ctypes.data, iv, t_frac, int(func), int(jac))
+
+    def homogenize(self) -> np.ndarray:
+        lib().pgref_homogenize(self.h)
+        return self.get("homogenized")
 
     def set_macro(self, eps):
         e = np.zeros(6)

@@ -472,6 +472,15 @@ double pgref_assemble(void* vh, const double* U, const double* isv_committed, do
 }
 
 /* Times n_rep calls of Assembler::assemble(K+R) on the state left by pgref_assemble; returns the median seconds. */
+/* Problem::homogenize (src/Problem.cpp:471-484) on the state left by the last pgref_assemble;
+ * exports "homogenized" (the volume-averaged stress, Voigt). */
+void pgref_homogenize(void* vh) {
+  Handle* h = (Handle*)vh;
+  h->prob->homogenize();
+  Export& e = put_d(h, "homogenized");
+  e.f64 = h->prob->getHomogenizedValue();
+}
+
 /* Problem::setMacroscaleValue (include/Problem.h:310): the macroscale strain of a subscale problem;
  * the next pgref_assemble applies it through assemble_new_load_step. */
 void pgref_set_macro(void* vh, const double* eps) {

@@ -35,6 +35,7 @@ EXPORTED = [
     "pg_get_sizes", "pg_get_pattern", "pg_get_nodes", "pg_assemble", "pg_assemble_device",
     "pg_device_outputs", "pg_set_stream", "pg_set_isv", "pg_get_isv", "pg_commit_isv",
     "pg_get_damage_zones", "pg_residual_norm", "pg_set_timing", "pg_kernel_times", "pg_set_macro_strain",
+    "pg_pcg_solve", "pg_homogenize", "pg_norm2_noalloc",
 ]
 
 
@@ -95,6 +96,9 @@ def load_library(path: str = LIB_PATH):
         "pg_set_timing": (i32, [vp, i32]),
         "pg_kernel_times": (i32, [vp, p]),
         "pg_set_macro_strain": (i32, [vp, p]),
+        "pg_pcg_solve": (i32, [vp, vp, vp, i32, dbl, i32, p, p]),
+        "pg_homogenize": (i32, [vp, vp, dbl, p]),
+        "pg_norm2_noalloc": (i32, [vp, ctypes.c_int64, vp, vp]),
     }
     for name, (rt, args) in sig.items():
         f = getattr(L, name)
@@ -102,6 +106,17 @@ def load_library(path: str = LIB_PATH):
         f.argtypes = args
     _lib = L
     return L
+
+
+def device_view(ptr: int, n: int, typestr: str = "<f8"):
+    """A torch tensor viewing n elements of device memory the library owns (e.g. the K values or
+    P_f of a context, from Problem.device_outputs); valid while the context lives."""
+    import torch
+
+    class _View:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (int(ptr), False), "version": 3,
+                                    "strides": None}
+    return torch.as_tensor(_View(), device="cuda")
 
 
 def _ptr(a: Optional[np.ndarray]):
@@ -276,6 +291,21 @@ class Problem:
         e = np.zeros(6)
         e[:len(eps)] = eps
         self._check(load_library().pg_set_macro_strain(self.h, _ptr(e)))
+
+    def pcg_solve(self, d_b: int, d_x: int, nrhs: int = 1, rtol: float = 1e-10, max_it: int = 100000):
+        """Jacobi-PCG on K_ff of the last assembly; d_b / d_x are device pointers to nrhs blocks of
+        n_free doubles (x: initial guess in, solution out).  Returns (iterations, relative residuals)."""
+        it = np.zeros(nrhs, np.int32)
+        rr = np.zeros(nrhs)
+        self._check(load_library().pg_pcg_solve(self.h, ctypes.c_void_p(d_b), ctypes.c_void_p(d_x), int(nrhs),
+                                                float(rtol), int(max_it), _ptr(it), _ptr(rr)))
+        return it, rr
+
+    def homogenize(self, d_U: int, t_frac: float = 1.0) -> np.ndarray:
+        """Volume-averaged stress (Voigt) and the integrated volume as the last entry."""
+        out = np.zeros(7)
+        self._check(load_library().pg_homogenize(self.h, ctypes.c_void_p(d_U), float(t_frac), _ptr(out)))
+        return out[: (3 if self.dim == 2 else 6) + 1]
 
     def residual_norm(self) -> float:
         v = ctypes.c_double(0.0)

@@ -4,9 +4,7 @@
 // quadrature tables, the CSR structure and values of the four blocks, the residual, the
 // committed and trial internal variables and the cut-element scratch.  The caller owns its
 // host arrays; pointers are never retained across calls.
-#include "pg_stencil.cuh"
-#include "pg_setup.h"
-#include "../../include/pigfem_b200.h"
+#include "pg_ctx.h"
 
 #include <algorithm>
 #include <cstdio>
@@ -14,43 +12,9 @@
 #include <string>
 #include <vector>
 
-struct pg_ctx {
-  pg::Setup s;
-  std::string err;
-  cudaStream_t stream = 0;
-  std::vector<void*> allocs;
-  pgd::DevProblem P{};
-  double* d_U = nullptr;
-  double* d_isv_committed = nullptr;
-  double* d_isv_trial = nullptr;
-  uint8_t* d_zone = nullptr;
-  int* d_err = nullptr;
-  double* d_red = nullptr;  // residual-norm partials
-  long long cut_scratch = 0;
-  int max_nd = 0;
-  int maxnb_fast = 0;
-  int n_coh_qp = 0;
-  bool assembled = false;
-  std::vector<int> fast_dn, slow_dn;
-  int tile_nodes = 128;
-  int max_cut_qp = 1, max_cut_nodes = 1;
-  const int* cut_list[2] = {nullptr, nullptr};
-  int n_cut_list[2] = {0, 0};
-  int cut_cls_qp[2] = {1, 1}, cut_cls_nodes[2] = {1, 1};
-  const int4* stencil = nullptr;
-  int n_stencil = 0;
-  pgd::GridInfo grid{0, 0, 0};
-  bool timing = false;
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-};
-
 namespace {
 
-int set_err(pg_ctx* c, int code, const std::string& m) {
-  if (c) c->err = m;
-  return code;
-}
+int set_err(pg_ctx* c, int code, const std::string& m) { return pg_set_err(c, code, m); }
 
 template <typename T>
 int upload(pg_ctx* c, const std::vector<T>& h, const T** out) {
@@ -66,16 +30,7 @@ int upload(pg_ctx* c, const std::vector<T>& h, const T** out) {
 }
 
 template <typename T>
-int dalloc(pg_ctx* c, size_t n, T** out) {
-  *out = nullptr;
-  if (n == 0) n = 1;
-  void* p = nullptr;
-  if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "cudaMalloc failed");
-  c->allocs.push_back(p);
-  cudaMemset(p, 0, n * sizeof(T));
-  *out = (T*)p;
-  return 0;
-}
+int dalloc(pg_ctx* c, size_t n, T** out) { return pg_dalloc(c, n, out); }
 
 #define PG_TRY(x) do { int _e = (x); if (_e) return _e; } while (0)
 
@@ -124,7 +79,7 @@ int launch(pg_ctx* c, double t_frac, int flags) {
   // the stencil rows run on the side stream, concurrently with the cohesive points and general rows
   if (c->n_stencil > 0) {
     const int tpb = 128;
-    const int nthreads = (dim == 2) ? c->n_stencil : 3 * c->n_stencil;
+    const int nthreads = (dim == 2) ? c->n_stencil : 3 * 32 * ((c->n_stencil + 31) / 32);
     const int grid = (nthreads + tpb - 1) / tpb;
     if (dim == 2) {
       if (fp32) pgd::k_rows_stencil<2, float><<<grid, tpb, 0, c->side>>>(P, c->grid, c->stencil, c->n_stencil);
@@ -162,6 +117,11 @@ int launch(pg_ctx* c, double t_frac, int flags) {
 }
 
 }  // namespace
+
+int pg_set_err(pg_ctx* c, int code, const std::string& m) {
+  if (c) c->err = m;
+  return code;
+}
 
 extern "C" {
 
@@ -381,13 +341,8 @@ int pg_upload(pg_ctx* c) {
       int qp = s.cut_qp_off[cc];
       for (int sb = s.cut_sub_off[cc]; sb < s.cut_sub_off[cc + 1]; ++sb) {
         const int st = s.sub_type[sb];
-        const int nsn = s.sub_node_off[sb + 1] - s.sub_node_off[sb];
-        int nq = 0;
-        if (st == pg::SUB_TRI3 || st == pg::SUB_QUAD4) nq = 4;
-        else if (st == pg::SUB_POLYGON) nq = 7 * nsn;
-        else if (st == pg::SUB_TET4) nq = 5;
-        else if (st == pg::SUB_PRISM6) nq = 8;
-        else nq = 8;
+        const int nq = s.sub_qp_off[sb + 1] - s.sub_qp_off[sb];
+        if (s.sub_qp_off[sb] != qp) return set_err(c, PG_ERR_STATE, "internal: quadrature offsets out of order");
         const bool affine = (st == pg::SUB_TRI3 || st == pg::SUB_TET4);
         if (affine) {
           double w = 0.0;
@@ -440,6 +395,18 @@ int pg_upload(pg_ctx* c) {
   PG_TRY(upload(c, s.coh_local, &P.coh_local));
   PG_TRY(upload(c, s.coh_qp_off, &P.coh_qp_off));
   PG_TRY(upload(c, s.cqp_N, &P.cqp_N));
+  {
+    std::vector<int> noff;
+    noff.reserve(s.cqp_wgt.size() + 1);
+    for (size_t ce = 0; ce + 1 < s.coh_qp_off.size(); ++ce)
+      for (int cq = s.coh_qp_off[ce]; cq < s.coh_qp_off[ce + 1]; ++cq) noff.push_back(0);
+    // running offsets: each point of cohesive element ce holds coh_nh[ce] shape values
+    int o = 0, k = 0;
+    for (size_t ce = 0; ce + 1 < s.coh_qp_off.size(); ++ce)
+      for (int cq = s.coh_qp_off[ce]; cq < s.coh_qp_off[ce + 1]; ++cq) { noff[k++] = o; o += s.coh_nh[ce]; }
+    if (o != (int)s.cqp_N.size()) return set_err(c, PG_ERR_STATE, "internal: cohesive shape-value count mismatch");
+    PG_TRY(upload(c, noff, &P.cqp_noff));
+  }
   PG_TRY(upload(c, s.cqp_R, &P.cqp_R));
   PG_TRY(upload(c, s.cqp_wgt, &P.cqp_wgt));
   PG_TRY(upload(c, s.cqp_isv, &P.cqp_isv));
@@ -583,6 +550,9 @@ int pg_kernel_times(pg_ctx* c, float* ms) {
 
 void pg_destroy(pg_ctx* c) {
   if (!c) return;
+  if (c->pcg.stream) cudaStreamDestroy(c->pcg.stream);
+  if (c->pcg.ev) cudaEventDestroy(c->pcg.ev);
+  if (c->pcg.hflag) cudaFreeHost(c->pcg.hflag);
   for (int i = 0; i < 6; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->side) cudaStreamDestroy(c->side);
   for (void* p : c->allocs) cudaFree(p);

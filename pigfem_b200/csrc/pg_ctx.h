@@ -1,0 +1,77 @@
+// pg_ctx.h -- the context behind the C ABI's opaque pg_ctx (internal to libpigfem_b200).
+//
+// A pg_ctx owns every device buffer of one problem: geometry, topology, the cut-element
+// quadrature tables, the CSR structure and values of the four blocks, the residual, the
+// committed and trial internal variables, the cut-element scratch and the solver workspace.
+#pragma once
+
+#include "pg_stencil.cuh"
+#include "pg_setup.h"
+#include "../../include/pigfem_b200.h"
+
+#include <string>
+#include <vector>
+
+// Workspace of the Jacobi-preconditioned CG on K_ff (pg_solver.cu), allocated on first use.
+struct PcgWork {
+  int n = 0, cap_rhs = 0, nb = 0;
+  double* dinv = nullptr;                       // n: inverse diagonal of K_ff
+  const int* ci = nullptr;                      // column indices of K_ff
+  double *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;  // cap_rhs x n each
+  double* part = nullptr;                       // partial sums: 3 x cap_rhs x nb
+  double* sc = nullptr;                         // scalars per rhs (see pg_solver.cu)
+  int* flag = nullptr;                          // per rhs: done, iterations; [2*cap_rhs] = active count
+  int* hflag = nullptr;                         // pinned host copy of flag
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev = nullptr;
+  bool diag_ready = false;
+};
+
+struct pg_ctx {
+  pg::Setup s;
+  std::string err;
+  cudaStream_t stream = 0;
+  std::vector<void*> allocs;
+  pgd::DevProblem P{};
+  double* d_U = nullptr;
+  double* d_isv_committed = nullptr;
+  double* d_isv_trial = nullptr;
+  uint8_t* d_zone = nullptr;
+  int* d_err = nullptr;
+  double* d_red = nullptr;  // residual-norm partials
+  long long cut_scratch = 0;
+  int max_nd = 0;
+  int maxnb_fast = 0;
+  int n_coh_qp = 0;
+  bool assembled = false;
+  std::vector<int> fast_dn, slow_dn;
+  int tile_nodes = 128;
+  int max_cut_qp = 1, max_cut_nodes = 1;
+  const int* cut_list[2] = {nullptr, nullptr};
+  int n_cut_list[2] = {0, 0};
+  int cut_cls_qp[2] = {1, 1}, cut_cls_nodes[2] = {1, 1};
+  const int4* stencil = nullptr;
+  int n_stencil = 0;
+  pgd::GridInfo grid{0, 0, 0};
+  bool timing = false;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  PcgWork pcg;
+  double* d_hom = nullptr;  // homogenization partials
+};
+
+// Shared helpers of the translation units of the library.
+int pg_set_err(pg_ctx* c, int code, const std::string& m);
+template <typename T>
+int pg_dalloc(pg_ctx* c, size_t n, T** out) {
+  *out = nullptr;
+  if (n == 0) n = 1;
+  void* p = nullptr;
+  if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return pg_set_err(c, PG_ERR_DEVICE, "cudaMalloc failed");
+  c->allocs.push_back(p);
+  cudaMemset(p, 0, n * sizeof(T));
+  *out = (T*)p;
+  return 0;
+}
+
+

@@ -53,6 +53,7 @@ struct DevProblem {
   const int* cut_qp_off; const double* qp_wgt; const int* qp_mat; const int* qp_grad_off; const double* qp_grad;
   const int* cut_coh_off; const int* coh_nh; const int* coh_local_off; const int* coh_local;
   const int* coh_qp_off; const double* cqp_N; const double* cqp_R; const double* cqp_wgt; const int* cqp_isv;
+  const int* cqp_noff;  // first shape value of each cohesive point in cqp_N (CohTri3 3, CohQuad4 4, CohEdge2 2)
   const long long* ke_off;  // per cut element: offset of its element matrix in the scratch
   const int* re_off;        // per cut element: offset of its element vector in the scratch
   double* ke;               // cache: volumetric element matrices of the cut elements (set-up)

@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(128) k_rows_general(DevProblem P, int slab_slo
 #pragma unroll
           for (int d = 0; d < DIM; ++d) pc[d] = 0.0;
           for (int cq = __ldg(&P.coh_qp_off[ce]); cq < __ldg(&P.coh_qp_off[ce + 1]); ++cq) {
-            const double nv = __ldg(&P.cqp_N[(size_t)cq * nh + n1 % nh]);
+            const double nv = __ldg(&P.cqp_N[__ldg(&P.cqp_noff[cq]) + n1 % nh]);
             const double* wt = P.cpt + (size_t)cq * (DIM * DIM + DIM) + DIM * DIM;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) pc[d] += sgn * (nv * wt[d]);
@@ -311,7 +311,8 @@ __global__ void __launch_bounds__(128) k_rows_general(DevProblem P, int slab_slo
 #pragma unroll
               for (int i = 0; i < DIM * DIM; ++i) kc[i] = 0.0;
               for (int cq = cqa; cq < cqb; ++cq) {
-                const double nn = __ldg(&P.cqp_N[(size_t)cq * nh + n1 % nh]) * __ldg(&P.cqp_N[(size_t)cq * nh + n2 % nh]);
+                const int no = __ldg(&P.cqp_noff[cq]);
+                const double nn = __ldg(&P.cqp_N[no + n1 % nh]) * __ldg(&P.cqp_N[no + n2 % nh]);
                 const double* wr = P.cpt + (size_t)cq * (DIM * DIM + DIM);
 #pragma unroll
                 for (int i = 0; i < DIM * DIM; ++i) kc[i] += sgn * (nn * wr[i]);
@@ -369,7 +370,7 @@ __global__ void __launch_bounds__(128) k_coh_points(DevProblem P) {
   const int nh = __ldg(&P.coh_nh[ce]);
   const int* cl = P.coh_local + __ldg(&P.coh_local_off[ce]);
   const int* nodes = P.cut_nodes + __ldg(&P.cut_node_off[c]);
-  const double* N = P.cqp_N + (size_t)cq * nh;
+  const double* N = P.cqp_N + __ldg(&P.cqp_noff[cq]);
   const double* R = P.cqp_R + (size_t)cq * DIM * DIM;
   double d0[DIM];
 #pragma unroll

@@ -680,6 +680,7 @@ int build_setup(const ProblemDesc& d, Setup& s) {
   s.cut_node_off.push_back(0);
   s.cut_sub_off.push_back(0);
   s.sub_node_off.push_back(0);
+  s.sub_qp_off.push_back(0);
   s.cut_qp_off.push_back(0);
   s.qp_grad_off.push_back(0);
   s.cut_coh_off.push_back(0);
@@ -774,6 +775,7 @@ int build_setup(const ProblemDesc& d, Setup& s) {
         }
         s.qp_grad_off.push_back((int)s.qp_grad.size());
       }
+      s.sub_qp_off.push_back((int)s.qp_wgt.size());
     }
     s.cut_sub_off.push_back((int)s.sub_type.size());
     s.cut_qp_off.push_back((int)s.qp_wgt.size());

@@ -76,6 +76,7 @@ struct Setup {
   std::vector<int> cut_elem;                  // cut index -> element
   std::vector<int> cut_node_off, cut_nodes;   // parent nodes then enrichment nodes (global node ids)
   std::vector<int> cut_sub_off, sub_type, sub_mat, sub_node_off, sub_nodes;  // sub-elements (global node ids)
+  std::vector<int> sub_qp_off;  // first quadrature point of each sub-element (into qp_wgt)
   std::vector<int> cut_qp_off;                // volumetric quadrature points per cut element
   std::vector<double> qp_wgt;                 // J * W of each volumetric qp
   std::vector<int> qp_mat;                    // material of each qp

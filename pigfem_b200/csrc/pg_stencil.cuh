@@ -114,6 +114,7 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
   constexpr int QB = (Q < 0) ? 0 : Q, QE = (Q < 0) ? DIM : Q + 1;
   const int sx = gi.nx + 1, sxy = sx * (gi.ny + 1);
   const int i = nid % sx, j = (nid / sx) % (gi.ny + 1), k = nid / sxy;
+  const bool jac = (P.flags & FLAG_JAC) != 0;  // uniform over the launch
   T dm[2][ND];
   iso_d<DIM, T>(P, 0, dm[0]);
   iso_d<DIM, T>(P, 1, dm[1]);
@@ -161,13 +162,15 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
     const int la = S::ent(a, 4);
 #pragma unroll
     for (int q = QB; q < QE; ++q) {
-      T part[NV];
-      part_iso<DIM, T>(d, g[la], q, part);
       r[q - QB] += (double)(w * bt_sig<DIM, T>(g[la], sig, q));
+      if (jac) {
+        T part[NV];
+        part_iso<DIM, T>(d, g[la], q, part);
 #pragma unroll
-      for (int lb = 0; lb < NPE; ++lb)
+        for (int lb = 0; lb < NPE; ++lb)
 #pragma unroll
-        for (int q2 = 0; q2 < DIM; ++q2) acc[S::ent(a, 5 + lb)][q - QB][q2] += (double)(w * part_b<DIM, T>(part, g[lb], q2));
+          for (int q2 = 0; q2 < DIM; ++q2) acc[S::ent(a, 5 + lb)][q - QB][q2] += (double)(w * part_b<DIM, T>(part, g[lb], q2));
+      }
     }
   }
 #pragma unroll
@@ -183,8 +186,9 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
   }
 }
 
-// One thread per stencil node (2D) or per (stencil node, row) (3D).  st: {node id, first free
-// DOF, first CSR slot of its first row, class} per node, class-sorted.
+// One thread per stencil node (2D) or per (stencil node, row) (3D, rows interleaved by warp so the
+// row is warp-uniform).  st: {node id, first free DOF, first CSR slot of its first row, class} per
+// node, class-sorted.
 template <int DIM, typename T>
 __global__ void __launch_bounds__(128) k_rows_stencil(DevProblem P, GridInfo gi, const int4* __restrict__ st, int n) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -194,8 +198,10 @@ __global__ void __launch_bounds__(128) k_rows_stencil(DevProblem P, GridInfo gi,
     if (v.w == 0) stencil_rows<Tri3Stencil0, 2, T, -1>(P, gi, v.x, v.y, v.z);
     else stencil_rows<Tri3Stencil1, 2, T, -1>(P, gi, v.x, v.y, v.z);
   } else {
-    if (t >= 3 * n) return;
-    const int node = t / 3, q = t - node * 3;
+    // a warp takes one row (q) of 32 consecutive stencil nodes, so q is uniform within a warp
+    const int w = t >> 5, lane = t & 31;
+    const int q = w % 3, node = (w / 3) * 32 + lane;
+    if (node >= n) return;
     const int4 v = __ldg(&st[node]);
     if (q == 0) stencil_rows<Tet4Stencil0, 3, T, 0>(P, gi, v.x, v.y, v.z);
     else if (q == 1) stencil_rows<Tet4Stencil0, 3, T, 1>(P, gi, v.x, v.y, v.z);
