@@ -155,6 +155,29 @@ int pg_pcg_solve(pg_ctx* ctx, const double* d_b, double* d_x, int nrhs, double r
  * sigma from d_U (device, node-major) plus the macroscale strain eps_macro * t_frac. */
 int pg_homogenize(pg_ctx* ctx, const double* d_U, double t_frac, double* out);
 
+/* ---- Batches: many contexts assembled by one set of persistent launches replayed from a CUDA
+ * graph.  No counterpart in the reference (it assembles one mesh per process).  Each context's
+ * results are bitwise those of pg_assemble_device on the same inputs. */
+typedef struct pg_batch pg_batch;
+/* The contexts must be uploaded and of one dimension; they stay owned by the caller and must
+ * outlive the batch. */
+int pg_batch_create(pg_ctx* const* ctxs, int n, pg_batch** out);
+/* Enqueues one assembly of every context: d_U[i] (device, node-major) with load fraction
+ * t_frac[i] (NULL: 1.0 for all) and the common flags (PG_FUNC | PG_JAC | PG_FP32).  Asynchronous
+ * on the batch's own stream; outputs land in each context's device buffers. */
+int pg_batch_assemble(pg_batch* b, const double* const* d_U, const double* t_frac, int flags);
+/* Waits for the last pg_batch_assemble; ms (may be NULL) gets its device time. */
+int pg_batch_wait(pg_batch* b, float* ms);
+/* Autotuner: times every candidate launch shape (stencil nodes per block, general-row lanes per
+ * node, persistent blocks per SM) over `reps` assemblies of this batch and keeps the fastest;
+ * best[3] (may be NULL) gets {nodes per stencil block, lanes per general node, blocks per SM}. */
+int pg_batch_tune(pg_batch* b, const double* const* d_U, int flags, int reps, int* best);
+/* info[8]: contexts, elements, nodes per stencil block, lanes per general node, blocks per SM,
+ * cohesive-point chunks, stencil chunks, general chunks. */
+int pg_batch_info(const pg_batch* b, int64_t* info);
+const char* pg_batch_last_error(const pg_batch* b);
+void pg_batch_destroy(pg_batch* b);
+
 /* ||x||_2 of a device vector of n doubles, written to the device double *d_out, enqueued on
  * `stream` (a cudaStream_t; NULL = legacy default stream).  No counterpart in the reference.
  * It allocates nothing: the block partials and a completion counter live in a fixed 32 KiB

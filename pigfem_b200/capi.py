@@ -36,6 +36,8 @@ EXPORTED = [
     "pg_device_outputs", "pg_set_stream", "pg_set_isv", "pg_get_isv", "pg_commit_isv",
     "pg_get_damage_zones", "pg_residual_norm", "pg_set_timing", "pg_kernel_times", "pg_set_macro_strain",
     "pg_pcg_solve", "pg_homogenize", "pg_norm2_noalloc",
+    "pg_batch_create", "pg_batch_assemble", "pg_batch_wait", "pg_batch_tune", "pg_batch_info",
+    "pg_batch_last_error", "pg_batch_destroy",
 ]
 
 
@@ -99,6 +101,13 @@ def load_library(path: str = LIB_PATH):
         "pg_pcg_solve": (i32, [vp, vp, vp, i32, dbl, i32, p, p]),
         "pg_homogenize": (i32, [vp, vp, dbl, p]),
         "pg_norm2_noalloc": (i32, [vp, ctypes.c_int64, vp, vp]),
+        "pg_batch_create": (i32, [p, i32, ctypes.POINTER(vp)]),
+        "pg_batch_assemble": (i32, [vp, p, p, i32]),
+        "pg_batch_wait": (i32, [vp, ctypes.POINTER(ctypes.c_float)]),
+        "pg_batch_tune": (i32, [vp, p, i32, i32, p]),
+        "pg_batch_info": (i32, [vp, p]),
+        "pg_batch_last_error": (ctypes.c_char_p, [vp]),
+        "pg_batch_destroy": (None, [vp]),
     }
     for name, (rt, args) in sig.items():
         f = getattr(L, name)
@@ -325,6 +334,69 @@ class Problem:
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:
             load_library().pg_destroy(self.h)
+            self.h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Several uploaded contexts assembled together by persistent launches replayed from a CUDA
+    graph (pg_batch_*).  The Problems must outlive the Batch."""
+
+    def __init__(self, problems):
+        L = load_library()
+        self.problems = list(problems)
+        hs = (ctypes.c_void_p * len(self.problems))(*[p.h.value for p in self.problems])
+        self._hs = hs
+        h = ctypes.c_void_p(0)
+        rc = L.pg_batch_create(ctypes.cast(hs, ctypes.c_void_p), len(self.problems), ctypes.byref(h))
+        self.h = h
+        if rc:
+            msg = L.pg_batch_last_error(h).decode() if h.value else "invalid batch"
+            self.close()
+            raise PigfemError(rc, msg)
+        self._u = None
+
+    def _check(self, rc):
+        if rc:
+            raise PigfemError(rc, load_library().pg_batch_last_error(self.h).decode())
+
+    def _uptrs(self, d_U):
+        arr = (ctypes.c_void_p * len(self.problems))(*[int(u) for u in d_U])
+        self._u = arr      # kept alive until the next call
+        return ctypes.cast(arr, ctypes.c_void_p)
+
+    def assemble(self, d_U, flags: int = FUNC | JAC, t_frac=None):
+        tf = None
+        if t_frac is not None:
+            tf = np.ascontiguousarray(t_frac, dtype=np.float64)
+            self._tf = tf
+        self._check(load_library().pg_batch_assemble(self.h, self._uptrs(d_U), _ptr(tf), int(flags)))
+
+    def wait(self) -> float:
+        ms = ctypes.c_float(0.0)
+        self._check(load_library().pg_batch_wait(self.h, ctypes.byref(ms)))
+        return ms.value
+
+    def tune(self, d_U, flags: int = FUNC | JAC, reps: int = 3):
+        best = np.zeros(3, np.int32)
+        self._check(load_library().pg_batch_tune(self.h, self._uptrs(d_U), int(flags), int(reps), _ptr(best)))
+        return tuple(int(x) for x in best)
+
+    def info(self) -> dict:
+        v = np.zeros(8, np.int64)
+        self._check(load_library().pg_batch_info(self.h, _ptr(v)))
+        keys = ("contexts", "elements", "stencil_nodes_per_block", "general_lanes_per_node", "blocks_per_sm",
+                "coh_chunks", "stencil_chunks", "general_chunks")
+        return {k: int(x) for k, x in zip(keys, v)}
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            load_library().pg_batch_destroy(self.h)
             self.h = ctypes.c_void_p(0)
 
     def __del__(self):

@@ -193,16 +193,15 @@ __device__ __forceinline__ void simplex_block_row(const DevProblem& P, int e, in
 //   adesc[entry]     int4 {element, local node | nodes of a cut element << 8, slots (uncut: 8 bits per
 //                    node; cut: offset into adj_slots), material (uncut) / block-row offset (cut)}
 //   aresd[entry]     element-vector offset of the cut element's row (cut entries)
+// Rows of general node `node` (an index into the general-node descriptors) for the lane group of
+// the calling thread (G lanes, 128 / G groups per 128-thread block).  Every lane of the warp must
+// call it (valid = false for lanes without a node) because of the warp-wide shuffles.  slab: this
+// group's shared-memory slab of slab_slots x DIM x DIM doubles.
 template <int DIM, int G>
-__global__ void __launch_bounds__(128) k_rows_general(DevProblem P, int slab_slots) {
+__device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool valid, double* slab) {
   constexpr int NPE = DIM + 1;
   constexpr int NV = (DIM == 2) ? 3 : 6;
-  constexpr int NB = 128 / G;
-  extern __shared__ double smem[];
-  const int grp = threadIdx.x / G, g = threadIdx.x % G;
-  const int node = blockIdx.x * NB + grp;
-  const bool valid = node < P.n_slow_dn;
-  double* slab = smem + (size_t)grp * slab_slots * DIM * DIM;
+  const int g = threadIdx.x % G;
   int4 gd = make_int4(0, 0, 0, 0);
   if (valid) {
     gd = __ldg(&P.gdesc[node]);
@@ -360,12 +359,19 @@ __global__ void __launch_bounds__(128) k_rows_general(DevProblem P, int slab_slo
   }
 }
 
+template <int DIM, int G>
+__global__ void __launch_bounds__(128) k_rows_general(DevProblem P, int slab_slots) {
+  constexpr int NB = 128 / G;
+  extern __shared__ double smem[];
+  const int grp = threadIdx.x / G;
+  const int node = blockIdx.x * NB + grp;
+  general_rows<DIM, G>(P, node, node < P.n_slow_dn, smem + (size_t)grp * slab_slots * DIM * DIM);
+}
+
 // Cohesive law at every cohesive quadrature point.  Output per point: w R^T D R (dim x dim) then
 // w R^T T (dim).
 template <int DIM>
-__global__ void __launch_bounds__(128) k_coh_points(DevProblem P) {
-  const int cq = blockIdx.x * blockDim.x + threadIdx.x;
-  if (cq >= P.n_coh_qp) return;
+__device__ __forceinline__ void coh_point(const DevProblem& P, int cq) {
   const int c = __ldg(&P.cqp_cut[cq]), ce = __ldg(&P.cqp_ce[cq]);
   const int nh = __ldg(&P.coh_nh[ce]);
   const int* cl = P.coh_local + __ldg(&P.coh_local_off[ce]);
@@ -429,6 +435,12 @@ __global__ void __launch_bounds__(128) k_coh_points(DevProblem P) {
     bad |= !isfinite(s);
   }
   if (bad) atomicOr(P.err, ERR_NONFINITE);
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(128) k_coh_points(DevProblem P) {
+  const int cq = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cq < P.n_coh_qp) coh_point<DIM>(P, cq);
 }
 
 // State-independent part of the cut elements, computed once at set-up: the volumetric element

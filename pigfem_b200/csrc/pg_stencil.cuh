@@ -115,9 +115,14 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
   const int sx = gi.nx + 1, sxy = sx * (gi.ny + 1);
   const int i = nid % sx, j = (nid / sx) % (gi.ny + 1), k = nid / sxy;
   const bool jac = (P.flags & FLAG_JAC) != 0;  // uniform over the launch
-  T dm[2][ND];
-  iso_d<DIM, T>(P, 0, dm[0]);
-  iso_d<DIM, T>(P, 1, dm[1]);
+  double dm[2][ND];
+  iso_d<DIM, double>(P, 0, dm[0]);
+  iso_d<DIM, double>(P, 1, dm[1]);
+  T dmk[2][ND];   // the tangent's D in the element-stiffness precision
+#pragma unroll
+  for (int m = 0; m < 2; ++m)
+#pragma unroll
+    for (int k2 = 0; k2 < ND; ++k2) dmk[m][k2] = (T)dm[m][k2];
   double acc[S::NN][QE - QB][DIM];
 #pragma unroll
   for (int s = 0; s < S::NN; ++s)
@@ -133,43 +138,51 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
     const int ci = i + S::ent(a, 0), cj = j + S::ent(a, 1), ck = k + S::ent(a, 2);
     const int e = (DIM == 2) ? 2 * (cj * gi.nx + ci) + S::ent(a, 3) : 6 * ((ck * gi.ny + cj) * gi.nx + ci) + S::ent(a, 3);
     const int m = __ldg(&P.emat[e]);
-    T x[NPE][DIM], u[NPE][DIM], g[NPE][DIM], J;
+    double x[NPE][DIM], u[NPE][DIM], g[NPE][DIM], J;
 #pragma unroll
     for (int n = 0; n < NPE; ++n) {
       const int sl = S::ent(a, 5 + n);
       const int id = nid + S::off(sl, 0) + S::off(sl, 1) * sx + S::off(sl, 2) * sxy;
 #pragma unroll
       for (int d = 0; d < DIM; ++d) {
-        if (sizeof(T) == 4) x[n][d] = (T)__ldg(&P.Xf[(size_t)id * DIM + d]);
-        else x[n][d] = (T)__ldg(&P.X[(size_t)id * DIM + d]);
-        u[n][d] = (T)__ldg(&P.U[(size_t)id * DIM + d]);
+        x[n][d] = __ldg(&P.X[(size_t)id * DIM + d]);
+        u[n][d] = __ldg(&P.U[(size_t)id * DIM + d]);
       }
     }
-    simplex_geom<DIM, T>(x, g, &J);
-    const T w = J * (T)((DIM == 2) ? tri4_wsum() : tet5_wsum());
-    T eps[NV];
+    // geometry, strain, stress and the internal force in FP64 (the Newton residual)
+    simplex_geom<DIM, double>(x, g, &J);
+    const double w = J * ((DIM == 2) ? tri4_wsum() : tet5_wsum());
+    double eps[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) eps[v] = 0;
 #pragma unroll
-    for (int n = 0; n < NPE; ++n) add_strain<DIM, T>(g[n], u[n], eps);
+    for (int n = 0; n < NPE; ++n) add_strain<DIM, double>(g[n], u[n], eps);
     if (P.subscale) {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) eps[v] += (T)P.eps_macro[v];
+      for (int v = 0; v < NV; ++v) eps[v] += P.eps_macro[v];
     }
-    const T* d = m ? dm[1] : dm[0];
-    T sig[NV];
-    lei_stress_iso<DIM, T>(d, eps, sig);
+    const double* d = m ? dm[1] : dm[0];
+    double sig[NV];
+    lei_stress_iso<DIM, double>(d, eps, sig);
     const int la = S::ent(a, 4);
+    // the stiffness block products in T (FP32 in the mixed path), accumulated in FP64
+    T gk[NPE][DIM];
+#pragma unroll
+    for (int n = 0; n < NPE; ++n)
+#pragma unroll
+      for (int dd = 0; dd < DIM; ++dd) gk[n][dd] = (T)g[n][dd];
+    const T wk = (T)w;
+    const T* dk = m ? dmk[1] : dmk[0];
 #pragma unroll
     for (int q = QB; q < QE; ++q) {
-      r[q - QB] += (double)(w * bt_sig<DIM, T>(g[la], sig, q));
+      r[q - QB] += w * bt_sig<DIM, double>(g[la], sig, q);
       if (jac) {
         T part[NV];
-        part_iso<DIM, T>(d, g[la], q, part);
+        part_iso<DIM, T>(dk, gk[la], q, part);
 #pragma unroll
         for (int lb = 0; lb < NPE; ++lb)
 #pragma unroll
-          for (int q2 = 0; q2 < DIM; ++q2) acc[S::ent(a, 5 + lb)][q - QB][q2] += (double)(w * part_b<DIM, T>(part, g[lb], q2));
+          for (int q2 = 0; q2 < DIM; ++q2) acc[S::ent(a, 5 + lb)][q - QB][q2] += (double)(wk * part_b<DIM, T>(part, gk[lb], q2));
       }
     }
   }

@@ -46,6 +46,7 @@ class SolveResult:
     steps: List[StepRecord]
     U_free: np.ndarray
     isv: np.ndarray
+    failed: str = ""      # why the run stopped early (raise_on_failure=False), else empty
 
 
 class LoadStepper:
@@ -94,12 +95,24 @@ class LoadStepper:
             if increase >= 3:
                 return False, res, norms
 
-    def solve(self) -> "SolveResult":
-        """SolverNonlinear::solve."""
+    def solve(self, raise_on_failure: bool = True) -> "SolveResult":
+        """SolverNonlinear::solve.  With raise_on_failure=False a run the reference would hand to
+        its explicit solver returns the records so far with `failed` set."""
+        try:
+            return self._solve()
+        except NewtonFailure as e:
+            if raise_on_failure:
+                raise
+            res = self.result(self._records)
+            res.failed = str(e)
+            return res
+
+    def _solve(self) -> "SolveResult":
         dt = self.max_dt
         t = 0.0
         step_iter = 0
         records: List[StepRecord] = []
+        self._records = records
         self.save()
         while t < self.T_final:
             repeat = 0

@@ -148,6 +148,32 @@ def linear_3d(n: int = 64, n_spheres: int = 50, r_lo: float = 0.04, r_hi: float 
     raise RuntimeError("no admissible sphere layout found")
 
 
+def cohesive_batch(count: int = 256, seed: int = 1, n_lo: int = 32, n_hi: int = 256, fib_lo: int = 5,
+                   fib_hi: int = 120, vf_lo: float = 0.2, vf_hi: float = 0.5, gap: float = 0.002,
+                   workload: int = 4, max_attempts: int = 20000):
+    """Independent 2D cohesive RVEs of uneven size: grid side N ~ log-uniform[n_lo, n_hi], fiber
+    count ~ U{fib_lo..fib_hi}, radii U[0.8, 1.2] x the mean radius of a volume fraction drawn from
+    U[vf_lo, vf_hi]; rejection sampling with capped attempts (the achieved volume fraction is
+    recorded); bilinear cohesive interfaces as in cohesive_2d.  RVE k is keyed by request k."""
+    out = []
+    for k in range(count):
+        rng = philox(workload, seed, k)
+        n = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))
+        nf = int(rng.integers(fib_lo, fib_hi + 1))
+        vf = float(rng.uniform(vf_lo, vf_hi))
+        r_mean = math.sqrt(vf / (nf * math.pi))
+        for _ in range(20):
+            fib = place_fibers(rng, nf, 0.8 * r_mean, 1.2 * r_mean, gap, 2, max_attempts=max_attempts)
+            if len(fib) and surface_clearance_ok(fib, n, 2):
+                break
+        vf_got = float(np.sum(np.pi * fib[:, 2] ** 2))
+        desc = ProblemDesc(elem_type=TRI3, n=(n, n), lo=(0.0, 0.0), hi=(1.0, 1.0), inclusions=fib,
+                           E_matrix=E_MATRIX, nu_matrix=NU_MATRIX, E_fiber=E_FIBER, nu_fiber=NU_FIBER,
+                           coh_law=COH_BL, coh=BL_PARAMS, plane_strain=True, subscale=False, app_strain=0.02)
+        out.append(RVE(desc, fib, vf_got))
+    return out
+
+
 def interface_state(problem, seed: int = 0, open_lo: float = 1e-7, open_hi: float = 6e-3, u_scale: float = 1e-6):
     """A displacement field (node-major) with seeded tensile openings at every cohesive interface:
     each '+' enrichment node is displaced from its '-' partner along the interface normal by a
@@ -155,23 +181,32 @@ def interface_state(problem, seed: int = 0, open_lo: float = 1e-7, open_hi: floa
     softening and failed branches.  Bulk displacements are small random values."""
     rng = np.random.default_rng(seed)
     dim = problem.dim
-    X, dofs, _ = problem.nodes()
-    U = rng.uniform(-u_scale, u_scale, X.shape[0] * dim).reshape(-1, dim)
+    n_nodes = problem.n_nodes
+    U = rng.uniform(-u_scale, u_scale, n_nodes * dim).reshape(-1, dim)
     cut_node_off = problem.debug("cut_node_off")
     cut_nodes = problem.debug("cut_nodes")
     cut_coh_off = problem.debug("cut_coh_off")
     coh_local_off = problem.debug("coh_local_off")
     coh_local = problem.debug("coh_local")
     coh_qp_off = problem.debug("coh_qp_off")
+    n_ce = len(coh_local_off) - 1
+    if n_ce <= 0:
+        return np.ascontiguousarray(U.reshape(-1))
     R = problem.debug("cqp_R").reshape(-1, dim, dim)
+    # cut element of every cohesive element, its mean rotation, and the '-' / '+' node pairs
+    ce_cut = np.repeat(np.arange(len(cut_coh_off) - 1), np.diff(cut_coh_off))
+    Rm = np.add.reduceat(R, coh_qp_off[:-1], axis=0) / np.diff(coh_qp_off)[:, None, None]
+    nh = np.diff(coh_local_off) // 2
     a, b = math.log(open_lo), math.log(open_hi)
-    for c in range(len(cut_node_off) - 1):
-        nodes = cut_nodes[cut_node_off[c]:cut_node_off[c + 1]]
-        for ce in range(cut_coh_off[c], cut_coh_off[c + 1]):
-            cl = coh_local[coh_local_off[ce]:coh_local_off[ce + 1]]
-            nh = len(cl) // 2
-            Rm = R[coh_qp_off[ce]:coh_qp_off[ce + 1]].mean(axis=0)
-            for k in range(nh):
-                dn = math.exp(rng.uniform(a, b))
-                U[nodes[cl[k + nh]]] = U[nodes[cl[k]]] + dn * Rm[dim - 1] + rng.uniform(-0.3, 0.3) * dn * Rm[0]
+    # one opening per (cohesive element, node pair) in element order, pairs in node order
+    pair_ce = np.repeat(np.arange(n_ce), nh)
+    pair_k = np.arange(len(pair_ce)) - np.repeat(np.cumsum(nh) - nh, nh)
+    draws = rng.uniform(0.0, 1.0, (len(pair_ce), 2))
+    dn = np.exp(a + (b - a) * draws[:, 0])
+    dt = (-0.3 + 0.6 * draws[:, 1]) * dn
+    base = coh_local_off[pair_ce]
+    minus = cut_nodes[cut_node_off[ce_cut[pair_ce]] + coh_local[base + pair_k]]
+    plus = cut_nodes[cut_node_off[ce_cut[pair_ce]] + coh_local[base + pair_k + nh[pair_ce]]]
+    # later pairs overwrite earlier ones that share a '+' node, as a sequential loop would
+    U[plus] = U[minus] + dn[:, None] * Rm[pair_ce, dim - 1] + dt[:, None] * Rm[pair_ce, 0]
     return np.ascontiguousarray(U.reshape(-1))
