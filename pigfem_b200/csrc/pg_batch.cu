@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(128) k_batch_general(const BatchItem* __restri
                                                        int n_chunks, int slab_slots) {
   extern __shared__ double smem[];
   const int grp = threadIdx.x / G;
-  double* slab = smem + (size_t)grp * slab_slots * DIM * DIM;
+  double* slab = smem + (size_t)grp * pgd::general_slab_doubles(slab_slots, DIM);
   for (int c = blockIdx.x; c < n_chunks; c += gridDim.x) {
     const int4 ch = chunks[c];
     pgd::general_rows<DIM, G>(items[ch.x].P, ch.y + grp, grp < ch.z, slab);
@@ -151,7 +151,7 @@ int upload_vec(pg_batch* b, const std::vector<T>& h, T** d) {
 }
 
 template <int DIM, int G>
-size_t general_smem(const pg_batch* b) { return (size_t)(128 / G) * b->slab_slots * DIM * DIM * sizeof(double); }
+size_t general_smem(const pg_batch* b) { return (size_t)(128 / G) * pgd::general_slab_doubles(b->slab_slots, DIM) * sizeof(double); }
 
 template <int DIM, int G>
 void general_attr(const pg_batch* b) {

@@ -20,11 +20,13 @@ template <typename T>
 int upload(pg_ctx* c, const std::vector<T>& h, const T** out) {
   *out = nullptr;
   if (h.empty()) return 0;
+  if (int rc = pg_alloc_stream(c)) return rc;
   void* p = nullptr;
-  if (cudaMalloc(&p, h.size() * sizeof(T)) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "cudaMalloc failed");
+  if (cudaMallocAsync(&p, h.size() * sizeof(T), c->up) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "device allocation failed");
   c->allocs.push_back(p);
-  if (cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
-    return set_err(c, PG_ERR_DEVICE, "cudaMemcpy failed");
+  // pageable source: the call returns once the data is staged, so `h` may go away afterwards
+  if (cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, c->up) != cudaSuccess)
+    return set_err(c, PG_ERR_DEVICE, "host-to-device copy failed");
   *out = (const T*)p;
   return 0;
 }
@@ -96,13 +98,13 @@ int launch(pg_ctx* c, double t_frac, int flags) {
     if (dim == 2) {
       constexpr int G = 4;
       const int grid = (P.n_slow_dn + (128 / G) - 1) / (128 / G);
-      const size_t smem = (size_t)(128 / G) * slots * 4 * sizeof(double);
+      const size_t smem = (size_t)(128 / G) * pgd::general_slab_doubles(slots, 2) * sizeof(double);
       cudaFuncSetAttribute(pgd::k_rows_general<2, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       pgd::k_rows_general<2, G><<<grid, 128, smem, c->stream>>>(P, slots);
     } else {
       constexpr int G = 32;
       const int grid = (P.n_slow_dn + (128 / G) - 1) / (128 / G);
-      const size_t smem = (size_t)(128 / G) * slots * 9 * sizeof(double);
+      const size_t smem = (size_t)(128 / G) * pgd::general_slab_doubles(slots, 3) * sizeof(double);
       cudaFuncSetAttribute(pgd::k_rows_general<3, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       pgd::k_rows_general<3, G><<<grid, 128, smem, c->stream>>>(P, slots);
     }
@@ -121,6 +123,29 @@ int launch(pg_ctx* c, double t_frac, int flags) {
 int pg_set_err(pg_ctx* c, int code, const std::string& m) {
   if (c) c->err = m;
   return code;
+}
+
+int pg_alloc_stream(pg_ctx* c) {
+  if (c->up) return 0;
+  static bool pool_ready = false;
+  if (!pool_ready) {
+    // keep freed blocks in the pool for the next context instead of returning them to the driver
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t thr = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    pool_ready = true;
+  }
+  if (cudaStreamCreateWithFlags(&c->up, cudaStreamNonBlocking) != cudaSuccess)
+    return pg_set_err(c, PG_ERR_DEVICE, "allocation stream creation failed");
+  return 0;
+}
+
+int pg_alloc_sync(pg_ctx* c) {
+  if (c->up && cudaStreamSynchronize(c->up) != cudaSuccess) return pg_set_err(c, PG_ERR_DEVICE, "device allocation failed");
+  return 0;
 }
 
 extern "C" {
@@ -481,16 +506,16 @@ int pg_upload(pg_ctx* c) {
       if (n == 0) continue;
       const size_t smem = (size_t)pgd::cut_smem_doubles(c->cut_cls_qp[cls], c->cut_cls_nodes[cls], dim) * sizeof(double);
       if (dim == 2) { cudaFuncSetAttribute(pgd::k_cut_volumetric<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                      pgd::k_cut_volumetric<2><<<n, 64, smem>>>(P, c->cut_list[cls], n, dg); }
+                      pgd::k_cut_volumetric<2><<<n, 64, smem, c->up>>>(P, c->cut_list[cls], n, dg); }
       else { cudaFuncSetAttribute(pgd::k_cut_volumetric<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-             pgd::k_cut_volumetric<3><<<n, 64, smem>>>(P, c->cut_list[cls], n, dg); }
+             pgd::k_cut_volumetric<3><<<n, 64, smem, c->up>>>(P, c->cut_list[cls], n, dg); }
     }
     int herr = 0;
-    if (cudaDeviceSynchronize() != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "cut-element set-up kernel failed");
-    cudaMemcpy(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpyAsync(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->up);
+    if (cudaStreamSynchronize(c->up) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "cut-element set-up kernel failed");
     if (herr) return set_err(c, PG_ERR_NONFINITE, "non-finite cut-element stiffness at set-up");
   }
-  return 0;
+  return pg_alloc_sync(c);
 }
 
 int pg_create(const pg_problem_desc* d, pg_ctx** out) {
@@ -550,12 +575,17 @@ int pg_kernel_times(pg_ctx* c, float* ms) {
 
 void pg_destroy(pg_ctx* c) {
   if (!c) return;
+  // work of this context still in flight finishes before its memory goes back to the pool
+  cudaStreamSynchronize(c->stream);
+  if (c->side) cudaStreamSynchronize(c->side);
+  if (c->pcg.stream) cudaStreamSynchronize(c->pcg.stream);
   if (c->pcg.stream) cudaStreamDestroy(c->pcg.stream);
   if (c->pcg.ev) cudaEventDestroy(c->pcg.ev);
   if (c->pcg.hflag) cudaFreeHost(c->pcg.hflag);
   for (int i = 0; i < 6; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->side) cudaStreamDestroy(c->side);
-  for (void* p : c->allocs) cudaFree(p);
+  for (void* p : c->allocs) cudaFreeAsync(p, c->up);
+  if (c->up) cudaStreamDestroy(c->up);   // released once the frees have run
   delete c;
 }
 
@@ -644,8 +674,8 @@ int pg_device_outputs(pg_ctx* c, double** K, double** Pf, double** Pp) {
 int pg_set_isv(pg_ctx* c, const double* v) {
   if (!c || (!v && c->s.n_isv)) return PG_ERR_INPUT;
   if (c->s.n_isv == 0) return 0;
-  if (cudaMemcpy(c->d_isv_committed, v, (size_t)c->s.n_isv * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
-    return set_err(c, PG_ERR_DEVICE, "copy of internal variables failed");
+  cudaMemcpyAsync(c->d_isv_committed, v, (size_t)c->s.n_isv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "copy of internal variables failed");
   return 0;
 }
 
@@ -653,7 +683,9 @@ int pg_get_isv(const pg_ctx* c, int trial, double* out) {
   if (!c || (!out && c->s.n_isv)) return PG_ERR_INPUT;
   if (c->s.n_isv == 0) return 0;
   cudaStreamSynchronize(c->stream);
-  cudaMemcpy(out, trial ? c->d_isv_trial : c->d_isv_committed, (size_t)c->s.n_isv * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaMemcpyAsync(out, trial ? c->d_isv_trial : c->d_isv_committed, (size_t)c->s.n_isv * sizeof(double), cudaMemcpyDeviceToHost,
+                  c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return PG_ERR_DEVICE;
   return 0;
 }
 
@@ -668,7 +700,8 @@ int pg_get_damage_zones(const pg_ctx* c, uint8_t* z) {
   if (!c || (!z && c->n_coh_qp)) return PG_ERR_INPUT;
   if (!c->n_coh_qp) return 0;
   cudaStreamSynchronize(c->stream);
-  cudaMemcpy(z, c->d_zone, (size_t)c->n_coh_qp, cudaMemcpyDeviceToHost);
+  cudaMemcpyAsync(z, c->d_zone, (size_t)c->n_coh_qp, cudaMemcpyDeviceToHost, c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return PG_ERR_DEVICE;
   return 0;
 }
 

@@ -58,20 +58,31 @@ struct pg_ctx {
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   PcgWork pcg;
   double* d_hom = nullptr;  // homogenization partials
+  // Device memory comes from the stream-ordered pool on this stream (cudaMallocAsync /
+  // cudaFreeAsync): creating and destroying contexts does not synchronise the device, so other
+  // contexts' work in flight (the serving loop) keeps running.
+  cudaStream_t up = nullptr;
 };
+
+// The allocation stream of a context (created on first use).
+int pg_alloc_stream(pg_ctx* c);
 
 // Shared helpers of the translation units of the library.
 int pg_set_err(pg_ctx* c, int code, const std::string& m);
+// Zero-filled device array of n T on the context's allocation stream; ready for other streams
+// after pg_alloc_sync(c).
 template <typename T>
 int pg_dalloc(pg_ctx* c, size_t n, T** out) {
   *out = nullptr;
   if (n == 0) n = 1;
+  if (int rc = pg_alloc_stream(c)) return rc;
   void* p = nullptr;
-  if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return pg_set_err(c, PG_ERR_DEVICE, "cudaMalloc failed");
+  if (cudaMallocAsync(&p, n * sizeof(T), c->up) != cudaSuccess) return pg_set_err(c, PG_ERR_DEVICE, "device allocation failed");
   c->allocs.push_back(p);
-  cudaMemset(p, 0, n * sizeof(T));
+  cudaMemsetAsync(p, 0, n * sizeof(T), c->up);
   *out = (T*)p;
   return 0;
 }
+int pg_alloc_sync(pg_ctx* c);
 
 

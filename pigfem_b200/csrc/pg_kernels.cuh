@@ -193,32 +193,40 @@ __device__ __forceinline__ void simplex_block_row(const DevProblem& P, int e, in
 //   adesc[entry]     int4 {element, local node | nodes of a cut element << 8, slots (uncut: 8 bits per
 //                    node; cut: offset into adj_slots), material (uncut) / block-row offset (cut)}
 //   aresd[entry]     element-vector offset of the cut element's row (cut entries)
+// Shared-memory doubles of one lane group's slab: slab_slots blocks of DIM x DIM plus the node's
+// residual (4 doubles reserved).
+__host__ __device__ inline int general_slab_doubles(int slab_slots, int dim) { return slab_slots * dim * dim + 4; }
+
 // Rows of general node `node` (an index into the general-node descriptors) for the lane group of
 // the calling thread (G lanes, 128 / G groups per 128-thread block).  Every lane of the warp must
 // call it (valid = false for lanes without a node) because of the warp-wide shuffles.  slab: this
-// group's shared-memory slab of slab_slots x DIM x DIM doubles.
+// group's shared-memory slab of general_slab_doubles(slab_slots, DIM) doubles.  The K blocks and
+// the residual are both summed over the adjacent elements in adjacency order, one lane after
+// another, so the result does not depend on G.
 template <int DIM, int G>
 __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool valid, double* slab) {
   constexpr int NPE = DIM + 1;
   constexpr int NV = (DIM == 2) ? 3 : 6;
   const int g = threadIdx.x % G;
   int4 gd = make_int4(0, 0, 0, 0);
+  double* rs = nullptr;   // the node's residual, after the slab blocks
   if (valid) {
     gd = __ldg(&P.gdesc[node]);
-    for (int i = g; i < gd.w * DIM * DIM; i += G) slab[i] = 0.0;
+    rs = slab + gd.w * DIM * DIM;
+    for (int i = g; i < gd.w * DIM * DIM + DIM; i += G) slab[i] = 0.0;
   }
   int passes = (gd.y + G - 1) / G;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) passes = max(passes, __shfl_xor_sync(0xffffffffu, passes, o));
   __syncwarp();
-  double r[DIM];
-#pragma unroll
-  for (int q = 0; q < DIM; ++q) r[q] = 0.0;
   for (int pass = 0; pass < passes; ++pass) {
     const int idx = pass * G + g;
     const bool have = valid && idx < gd.y;
     int4 ad = make_int4(0, 0, 0, 0);
     double kv[NPE][DIM][DIM];
+    double r[DIM];   // this entry's residual contribution
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) r[q] = 0.0;
     if (have) {
       ad = __ldg(&P.adesc[gd.x + idx]);
       const int la = ad.y & 255, mn = ad.y >> 8;
@@ -277,6 +285,8 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
     }
     for (int t = 0; t < G; ++t) {
       if (have && g == t) {
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) rs[q] += r[q];
         const int mn = ad.y >> 8;
         if (mn == 0) {
           const unsigned slots = (unsigned)ad.z;
@@ -326,10 +336,6 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
       __syncwarp();
     }
   }
-#pragma unroll
-  for (int q = 0; q < DIM; ++q)
-#pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) r[q] += __shfl_down_sync(0xffffffffu, r[q], o, G);
   if (!valid) return;
   const int nn = gd.w;
   const uint8_t* masks = P.dn_nbr_mask + gd.z;
@@ -354,7 +360,7 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
       }
     }
     if ((P.flags & FLAG_FUNC) && g == 0) {
-      if (rf) P.Pf[gdof] = r[q]; else P.Pp[gdof - P.n_free] = r[q];
+      if (rf) P.Pf[gdof] = rs[q]; else P.Pp[gdof - P.n_free] = rs[q];
     }
   }
 }
@@ -365,7 +371,7 @@ __global__ void __launch_bounds__(128) k_rows_general(DevProblem P, int slab_slo
   extern __shared__ double smem[];
   const int grp = threadIdx.x / G;
   const int node = blockIdx.x * NB + grp;
-  general_rows<DIM, G>(P, node, node < P.n_slow_dn, smem + (size_t)grp * slab_slots * DIM * DIM);
+  general_rows<DIM, G>(P, node, node < P.n_slow_dn, smem + (size_t)grp * general_slab_doubles(slab_slots, DIM));
 }
 
 // Cohesive law at every cohesive quadrature point.  Output per point: w R^T D R (dim x dim) then

@@ -256,7 +256,7 @@ int pcg_reserve(pg_ctx* c, int nrhs) {
     int* ci = nullptr;
     rc |= pg_dalloc(c, c->s.ci[0].size(), &ci);
     if (!rc && !c->s.ci[0].empty() &&
-        cudaMemcpy(ci, c->s.ci[0].data(), c->s.ci[0].size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+        cudaMemcpyAsync(ci, c->s.ci[0].data(), c->s.ci[0].size() * sizeof(int), cudaMemcpyHostToDevice, c->up) != cudaSuccess)
       rc = 1;
     w.ci = ci;
   }
@@ -267,7 +267,8 @@ int pcg_reserve(pg_ctx* c, int nrhs) {
   rc |= pg_dalloc(c, (size_t)3 * nrhs * w.nb, &w.part);
   rc |= pg_dalloc(c, (size_t)S_NSC * nrhs, &w.sc);
   rc |= pg_dalloc(c, (size_t)2 * nrhs + 1, &w.flag);
-  return rc ? PG_ERR_DEVICE : 0;
+  if (rc) return PG_ERR_DEVICE;
+  return pg_alloc_sync(c);
 }
 
 // ---------------------------------------------------------------- homogenization
@@ -420,7 +421,7 @@ int pg_pcg_solve(pg_ctx* c, const double* d_b, double* d_x, int nrhs, double rto
 int pg_homogenize(pg_ctx* c, const double* d_U, double t_frac, double* out) {
   if (!c || !d_U || !out) return PG_ERR_INPUT;
   const int dim = c->s.dim, nv = dim == 2 ? 3 : 6;
-  if (!c->d_hom && pg_dalloc(c, (size_t)(nv + 2) * kHomBlocks + 8, &c->d_hom)) return PG_ERR_DEVICE;
+  if (!c->d_hom && (pg_dalloc(c, (size_t)(nv + 2) * kHomBlocks + 8, &c->d_hom) || pg_alloc_sync(c))) return PG_ERR_DEVICE;
   pgd::DevProblem P = c->P;
   for (int v = 0; v < 6; ++v) P.eps_macro[v] = c->s.desc.eps_macro[v] * t_frac;
   if (dim == 2) k_homogenize<2><<<kHomBlocks, kThreads, 0, c->stream>>>(P, d_U, c->d_hom);

@@ -176,9 +176,11 @@ def cohesive_batch(count: int = 256, seed: int = 1, n_lo: int = 32, n_hi: int = 
 
 def interface_state(problem, seed: int = 0, open_lo: float = 1e-7, open_hi: float = 6e-3, u_scale: float = 1e-6):
     """A displacement field (node-major) with seeded tensile openings at every cohesive interface:
-    each '+' enrichment node is displaced from its '-' partner along the interface normal by a
-    log-uniform opening in [open_lo, open_hi], so the bilinear law runs through its loading,
-    softening and failed branches.  Bulk displacements are small random values."""
+    each '+' enrichment node is displaced from its '-' partner along the mean normal of the
+    cohesive elements that hold the pair, by a log-uniform opening in [open_lo, open_hi] plus a
+    tangential slip of up to 0.3 of it, so the bilinear law runs through its loading, softening
+    and failed branches while every cohesive point stays in tension.  Bulk displacements are small
+    random values."""
     rng = np.random.default_rng(seed)
     dim = problem.dim
     n_nodes = problem.n_nodes
@@ -193,20 +195,28 @@ def interface_state(problem, seed: int = 0, open_lo: float = 1e-7, open_hi: floa
     if n_ce <= 0:
         return np.ascontiguousarray(U.reshape(-1))
     R = problem.debug("cqp_R").reshape(-1, dim, dim)
-    # cut element of every cohesive element, its mean rotation, and the '-' / '+' node pairs
     ce_cut = np.repeat(np.arange(len(cut_coh_off) - 1), np.diff(cut_coh_off))
     Rm = np.add.reduceat(R, coh_qp_off[:-1], axis=0) / np.diff(coh_qp_off)[:, None, None]
     nh = np.diff(coh_local_off) // 2
-    a, b = math.log(open_lo), math.log(open_hi)
-    # one opening per (cohesive element, node pair) in element order, pairs in node order
+    # every ('-', '+') node pair of every cohesive element
     pair_ce = np.repeat(np.arange(n_ce), nh)
     pair_k = np.arange(len(pair_ce)) - np.repeat(np.cumsum(nh) - nh, nh)
-    draws = rng.uniform(0.0, 1.0, (len(pair_ce), 2))
+    base = coh_local_off[pair_ce]
+    first = cut_node_off[ce_cut[pair_ce]]
+    minus = cut_nodes[first + coh_local[base + pair_k]]
+    plus = cut_nodes[first + coh_local[base + pair_k + nh[pair_ce]]]
+    # mean normal and tangent of each '+' node over the cohesive elements holding it
+    nsum = np.zeros((n_nodes, dim))
+    tsum = np.zeros((n_nodes, dim))
+    np.add.at(nsum, plus, Rm[pair_ce, dim - 1])
+    np.add.at(tsum, plus, Rm[pair_ce, 0])
+    nodes_p, idx = np.unique(plus, return_index=True)
+    nodes_m = minus[idx]
+    nrm = nsum[nodes_p] / np.linalg.norm(nsum[nodes_p], axis=1)[:, None]
+    tng = tsum[nodes_p] / np.maximum(np.linalg.norm(tsum[nodes_p], axis=1), 1e-300)[:, None]
+    a, b = math.log(open_lo), math.log(open_hi)
+    draws = rng.uniform(0.0, 1.0, (len(nodes_p), 2))
     dn = np.exp(a + (b - a) * draws[:, 0])
     dt = (-0.3 + 0.6 * draws[:, 1]) * dn
-    base = coh_local_off[pair_ce]
-    minus = cut_nodes[cut_node_off[ce_cut[pair_ce]] + coh_local[base + pair_k]]
-    plus = cut_nodes[cut_node_off[ce_cut[pair_ce]] + coh_local[base + pair_k + nh[pair_ce]]]
-    # later pairs overwrite earlier ones that share a '+' node, as a sequential loop would
-    U[plus] = U[minus] + dn[:, None] * Rm[pair_ce, dim - 1] + dt[:, None] * Rm[pair_ce, 0]
+    U[nodes_p] = U[nodes_m] + dn[:, None] * nrm + dt[:, None] * tng
     return np.ascontiguousarray(U.reshape(-1))
