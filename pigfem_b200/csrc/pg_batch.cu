@@ -1,9 +1,9 @@
 // pg_batch.cu -- many RVEs in one set of persistent launches, replayed from a CUDA graph.
 //
 // A batch holds the device descriptors (DevProblem) of n assembled-ready contexts and three work
-// lists that cover all of them: chunks of cohesive points, of structured stencil nodes and of
+// lists that cover all of them: chunks of cohesive elements, of structured stencil nodes and of
 // general DOF nodes, each chunk {context, first item, count}.  One assembly of the whole batch is
-// three persistent kernels (cohesive points and general rows on the batch stream, stencil rows
+// three persistent kernels (cohesive elements and general rows on the batch stream, stencil rows
 // concurrently on a side stream) that stride over the chunk lists; the whole sequence, including
 // the upload of the per-call parameters (each context's displacement pointer, flags and
 // macroscale strain), is captured once into a CUDA graph and replayed.  Every CSR value and
@@ -11,7 +11,7 @@
 // single-context launches, so each context's results are bitwise those of pg_assemble_device.
 //
 // The autotuner (pg_batch_tune) times the candidate launch shapes on the batch itself and keeps
-// the fastest: stencil nodes per block (64 / 128 / 256), general-row lanes per node (2D: 2 / 4 / 8,
+// the fastest: stencil nodes per block (64 / 128 / 256), general-row lanes per node (2D: 4 / 8 / 16,
 // 3D: 8 / 16 / 32) and the persistent grid (2 / 4 / 8 blocks per SM).
 #include "pg_ctx.h"
 
@@ -54,12 +54,15 @@ __global__ void k_batch_errors(const BatchItem* items, int n, int* out) {
   if ((threadIdx.x & 31) == 0 && e) atomicOr(out, e);
 }
 
+// chunk = 128 / CQ cohesive elements, CQ lanes each
 template <int DIM>
 __global__ void __launch_bounds__(128) k_batch_coh(const BatchItem* __restrict__ items, const int4* __restrict__ chunks,
                                                    int n_chunks) {
+  constexpr int CQ = pgd::CohLanes<DIM>::CQ;
+  const int e = threadIdx.x / CQ, qi = threadIdx.x % CQ;
   for (int c = blockIdx.x; c < n_chunks; c += gridDim.x) {
     const int4 ch = chunks[c];
-    if ((int)threadIdx.x < ch.z) pgd::coh_point<DIM>(items[ch.x].P, ch.y + threadIdx.x);
+    pgd::coh_element<DIM>(items[ch.x].P, ch.y + e, qi, e < ch.z);
   }
 }
 
@@ -89,10 +92,10 @@ __global__ void __launch_bounds__(256) k_batch_stencil(const BatchItem* __restri
 
 template <int DIM, int G>
 __global__ void __launch_bounds__(128) k_batch_general(const BatchItem* __restrict__ items, const int4* __restrict__ chunks,
-                                                       int n_chunks, int slab_slots) {
+                                                       int n_chunks, int slab_slots, int max_mn) {
   extern __shared__ double smem[];
   const int grp = threadIdx.x / G;
-  double* slab = smem + (size_t)grp * pgd::general_slab_doubles(slab_slots, DIM);
+  double* slab = smem + (size_t)grp * pgd::general_slab_doubles(slab_slots, DIM, max_mn);
   for (int c = blockIdx.x; c < n_chunks; c += gridDim.x) {
     const int4 ch = chunks[c];
     pgd::general_rows<DIM, G>(items[ch.x].P, ch.y + grp, grp < ch.z, slab);
@@ -112,6 +115,7 @@ struct pg_batch {
   int* d_err = nullptr;   // OR of the contexts' device error words of the last call
   int n_coh = 0, n_sten = 0, n_gen = 0;
   int slab_slots = 1;
+  int max_mn = 1;
   int tpb = 128, G = 4, mult = 4;   // launch shape (autotuned)
   cudaStream_t stream = nullptr, side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr, t0 = nullptr, t1 = nullptr;
@@ -151,7 +155,9 @@ int upload_vec(pg_batch* b, const std::vector<T>& h, T** d) {
 }
 
 template <int DIM, int G>
-size_t general_smem(const pg_batch* b) { return (size_t)(128 / G) * pgd::general_slab_doubles(b->slab_slots, DIM) * sizeof(double); }
+size_t general_smem(const pg_batch* b) {
+  return (size_t)(128 / G) * pgd::general_slab_doubles(b->slab_slots, DIM, b->max_mn) * sizeof(double);
+}
 
 template <int DIM, int G>
 void general_attr(const pg_batch* b) {
@@ -160,7 +166,7 @@ void general_attr(const pg_batch* b) {
 
 // set before any capture: the dynamic shared memory of the general-row kernel of the current shape
 void set_attributes(const pg_batch* b) {
-  if (b->dim == 2) { if (b->G == 2) general_attr<2, 2>(b); else if (b->G == 4) general_attr<2, 4>(b); else general_attr<2, 8>(b); }
+  if (b->dim == 2) { if (b->G == 4) general_attr<2, 4>(b); else if (b->G == 8) general_attr<2, 8>(b); else general_attr<2, 16>(b); }
   else { if (b->G == 8) general_attr<3, 8>(b); else if (b->G == 16) general_attr<3, 16>(b); else general_attr<3, 32>(b); }
 }
 
@@ -173,7 +179,9 @@ int build_chunks(pg_batch* b) {
   const int gen_chunk = 128 / b->G;
   for (int i = 0; i < (int)b->ctx.size(); ++i) {
     const pg_ctx* c = b->ctx[i];
-    for (int f = 0; f < c->n_coh_qp; f += 128) coh.push_back(make_int4(i, f, std::min(128, c->n_coh_qp - f), 0));
+    const int coh_chunk = 128 / ((b->dim == 2) ? pgd::CohLanes<2>::CQ : pgd::CohLanes<3>::CQ);
+    for (int f = 0; f < c->P.n_coh_el; f += coh_chunk)
+      coh.push_back(make_int4(i, f, std::min(coh_chunk, c->P.n_coh_el - f), 0));
     for (int f = 0; f < c->n_stencil; f += sten_chunk)
       sten.push_back(make_int4(i, f, std::min(sten_chunk, c->n_stencil - f), 0));
     for (int f = 0; f < c->P.n_slow_dn; f += gen_chunk)
@@ -191,7 +199,8 @@ int build_chunks(pg_batch* b) {
 
 template <int DIM, int G>
 void launch_general(pg_batch* b, cudaStream_t st, int grid) {
-  k_batch_general<DIM, G><<<grid, 128, general_smem<DIM, G>(b), st>>>(b->d_items, b->d_gen, b->n_gen, b->slab_slots);
+  k_batch_general<DIM, G><<<grid, 128, general_smem<DIM, G>(b), st>>>(b->d_items, b->d_gen, b->n_gen, b->slab_slots,
+                                                                     b->max_mn);
 }
 
 void enqueue(pg_batch* b, bool fp32) {
@@ -221,9 +230,9 @@ void enqueue(pg_batch* b, bool fp32) {
   if (b->n_gen) {
     const int grid = std::min(b->n_gen, cap);
     if (b->dim == 2) {
-      if (b->G == 2) launch_general<2, 2>(b, st, grid);
-      else if (b->G == 4) launch_general<2, 4>(b, st, grid);
-      else launch_general<2, 8>(b, st, grid);
+      if (b->G == 4) launch_general<2, 4>(b, st, grid);
+      else if (b->G == 8) launch_general<2, 8>(b, st, grid);
+      else launch_general<2, 16>(b, st, grid);
     } else {
       if (b->G == 8) launch_general<3, 8>(b, st, grid);
       else if (b->G == 16) launch_general<3, 16>(b, st, grid);
@@ -282,6 +291,7 @@ int pg_batch_create(pg_ctx* const* ctxs, int n, pg_batch** out) {
     items[i].stencil = c->stencil;
     items[i].n_stencil = c->n_stencil;
     b->slab_slots = std::max(b->slab_slots, c->P.maxnb_general);
+    b->max_mn = std::max(b->max_mn, c->P.max_mn);
     b->n_elem += c->s.ne;
   }
   if (cudaMalloc(&b->d_items, sizeof(BatchItem) * n) != cudaSuccess) return berr(b, PG_ERR_DEVICE, "cudaMalloc failed");
@@ -332,7 +342,7 @@ int pg_batch_wait(pg_batch* b, float* ms) {
 int pg_batch_tune(pg_batch* b, const double* const* d_U, int flags, int reps, int* best) {
   if (!b || !d_U || reps < 1) return PG_ERR_INPUT;
   const int tpbs[3] = {64, 128, 256};
-  const int gs2[3] = {2, 4, 8}, gs3[3] = {8, 16, 32};
+  const int gs2[3] = {4, 8, 16}, gs3[3] = {8, 16, 32};   // at least one lane per element node
   const int mults[3] = {2, 4, 8};
   float best_ms = 1e30f;
   int bt = b->tpb, bg = b->G, bm = b->mult;

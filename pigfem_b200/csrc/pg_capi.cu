@@ -72,11 +72,12 @@ int launch(pg_ctx* c, double t_frac, int flags) {
   // cut-element kernels and the general rows on the main stream
   cudaEventRecord(c->ev[0], c->stream);
   cudaStreamWaitEvent(c->side, c->ev[0], 0);
-  if (P.n_coh_qp > 0) {
+  if (P.n_coh_el > 0) {
     const int tpb = 128;
-    const int grid = (P.n_coh_qp + tpb - 1) / tpb;
-    if (dim == 2) pgd::k_coh_points<2><<<grid, tpb, 0, c->stream>>>(P);
-    else pgd::k_coh_points<3><<<grid, tpb, 0, c->stream>>>(P);
+    const int lanes = (dim == 2) ? pgd::CohLanes<2>::CQ : pgd::CohLanes<3>::CQ;
+    const int grid = (int)(((long long)P.n_coh_el * lanes + tpb - 1) / tpb);
+    if (dim == 2) pgd::k_coh_elements<2><<<grid, tpb, 0, c->stream>>>(P);
+    else pgd::k_coh_elements<3><<<grid, tpb, 0, c->stream>>>(P);
   }
   // the stencil rows run on the side stream, concurrently with the cohesive points and general rows
   if (c->n_stencil > 0) {
@@ -98,15 +99,15 @@ int launch(pg_ctx* c, double t_frac, int flags) {
     if (dim == 2) {
       constexpr int G = 4;
       const int grid = (P.n_slow_dn + (128 / G) - 1) / (128 / G);
-      const size_t smem = (size_t)(128 / G) * pgd::general_slab_doubles(slots, 2) * sizeof(double);
+      const size_t smem = (size_t)(128 / G) * pgd::general_slab_doubles(slots, 2, P.max_mn) * sizeof(double);
       cudaFuncSetAttribute(pgd::k_rows_general<2, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      pgd::k_rows_general<2, G><<<grid, 128, smem, c->stream>>>(P, slots);
+      pgd::k_rows_general<2, G><<<grid, 128, smem, c->stream>>>(P, slots, P.max_mn);
     } else {
       constexpr int G = 32;
       const int grid = (P.n_slow_dn + (128 / G) - 1) / (128 / G);
-      const size_t smem = (size_t)(128 / G) * pgd::general_slab_doubles(slots, 3) * sizeof(double);
+      const size_t smem = (size_t)(128 / G) * pgd::general_slab_doubles(slots, 3, P.max_mn) * sizeof(double);
       cudaFuncSetAttribute(pgd::k_rows_general<3, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      pgd::k_rows_general<3, G><<<grid, 128, smem, c->stream>>>(P, slots);
+      pgd::k_rows_general<3, G><<<grid, 128, smem, c->stream>>>(P, slots, P.max_mn);
     }
   }
   cudaEventRecord(c->ev[4], c->stream);
@@ -209,10 +210,14 @@ int pg_upload(pg_ctx* c) {
         for (int q = s.cut_node_off[cc]; q < s.cut_node_off[cc + 1]; ++q) en.push_back(s.cut_nodes[q]);
       }
       slot_off[k] = (int)slots.size();
+      const size_t first_slot = slots.size();
       for (size_t lb = 0; lb < en.size(); ++lb) {
         const int db = s.node_dn[en[lb]];
         const int pos = (int)(std::lower_bound(nb, nb + nn, db) - nb);
         if (pos >= nn || nb[pos] != db) return set_err(c, PG_ERR_STATE, "internal: adjacency without neighbour slot");
+        // the lanes of a row group add an element's blocks concurrently: its nodes need distinct slots
+        for (size_t k2 = first_slot; k2 < slots.size(); ++k2)
+          if (slots[k2] == pos) return set_err(c, PG_ERR_UNSUPPORTED, "an element holds a node and its periodic image");
         slots.push_back((uint8_t)pos);
         if (s.cut_of[e] < 0) slot32[k] |= pos << (8 * lb);
       }
@@ -471,18 +476,45 @@ int pg_upload(pg_ctx* c) {
   PG_TRY(upload(c, growd, &P.growd));
   PG_TRY(upload(c, adesc, &P.adesc));
   PG_TRY(upload(c, aresd, &P.aresd));
-  // cohesive points: owning cut element and cohesive element
+  // cohesive elements: owning cut element, scratch offsets of their blocks, and the cohesive
+  // position of every cut-element local node (a node is on at most one cohesive element)
   {
-    std::vector<int> cqp_cut(c->n_coh_qp), cqp_ce(c->n_coh_qp);
+    const int n_ce = (int)s.coh_nh.size();
+    if ((long long)n_ce * 32 > 2147483647LL) return set_err(c, PG_ERR_UNSUPPORTED, "too many cohesive elements");
+    std::vector<int> ce_cut(n_ce), kc_off(n_ce + 1, 0), cohpos(s.cut_nodes.size(), -1);
     for (int cc = 0; cc < s.ncut; ++cc)
-      for (int ce = s.cut_coh_off[cc]; ce < s.cut_coh_off[cc + 1]; ++ce)
-        for (int q = s.coh_qp_off[ce]; q < s.coh_qp_off[ce + 1]; ++q) { cqp_cut[q] = cc; cqp_ce[q] = ce; }
-    PG_TRY(upload(c, cqp_cut, &P.cqp_cut));
-    PG_TRY(upload(c, cqp_ce, &P.cqp_ce));
-    double* dcpt;
-    PG_TRY(dalloc(c, (size_t)c->n_coh_qp * (dim * dim + dim), &dcpt));
-    P.cpt = dcpt;
+      for (int ce = s.cut_coh_off[cc]; ce < s.cut_coh_off[cc + 1]; ++ce) {
+        ce_cut[ce] = cc;
+        const int nh = s.coh_nh[ce];
+        if (2 * nh > 32) return set_err(c, PG_ERR_UNSUPPORTED, "cohesive element with more than 32 nodes");
+        kc_off[ce + 1] = kc_off[ce] + nh * nh * dim * dim + nh * dim;
+        for (int k = 0; k < 2 * nh; ++k) {
+          const int ln = s.coh_local[s.coh_local_off[ce] + k];
+          int& slot = cohpos[s.cut_node_off[cc] + ln];
+          if (slot >= 0) return set_err(c, PG_ERR_STATE, "internal: a node on two cohesive elements of one cut element");
+          slot = ce * 32 + k;
+        }
+      }
+    PG_TRY(upload(c, ce_cut, &P.ce_cut));
+    PG_TRY(upload(c, kc_off, &P.kc_off));
+    PG_TRY(upload(c, cohpos, &P.cohpos));
+    double* dk;
+    PG_TRY(dalloc(c, (size_t)kc_off[n_ce], &dk));
+    P.kcoh = dk;
+    P.n_coh_el = n_ce;
     P.n_coh_qp = c->n_coh_qp;
+    int max_mn = 1;
+    for (int cc = 0; cc < s.ncut; ++cc) max_mn = std::max(max_mn, s.cut_node_off[cc + 1] - s.cut_node_off[cc]);
+    P.max_mn = max_mn;
+  }
+  // row positions: free DOFs of the earlier neighbours of every neighbour slot
+  {
+    std::vector<int> pre(s.dn_nbr.size(), 0);
+    for (int a = 0; a < s.n_dn; ++a) {
+      int acc = 0;
+      for (int k = s.dn_nbr_off[a]; k < s.dn_nbr_off[a + 1]; ++k) { pre[k] = acc; acc += __builtin_popcount(nbr_mask[k]); }
+    }
+    PG_TRY(upload(c, pre, &P.nbr_pre));
   }
   if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess)
     return set_err(c, PG_ERR_DEVICE, "stream creation failed");

@@ -75,8 +75,13 @@ struct DevProblem {
   const int4* gdesc; const int* growd; const int4* adesc; const int* aresd;  // k_rows_general descriptors
   // cohesive points
   int n_coh_qp;
-  const int* cqp_cut; const int* cqp_ce;
-  double* cpt;                                   // per cohesive point: w R^T D R, w R^T T
+  int n_coh_el;                                  // cohesive elements
+  const int* ce_cut;                             // cut element of each cohesive element
+  const int* kc_off;                             // per cohesive element: offset of its blocks in kcoh
+  double* kcoh;                                  // per call: cohesive blocks B_ab and tractions t_a
+  const int* cohpos;                             // per cut-element local node: (cohesive element << 5 | position) or -1
+  const int* nbr_pre;                            // per neighbour slot: free DOFs of the earlier neighbours
+  int max_mn;                                    // most nodes of a cut element
   // outputs: CSR values of the four blocks and the two residual parts
   const int* rp[4];
   double* val[4];

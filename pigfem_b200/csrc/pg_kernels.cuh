@@ -1,8 +1,9 @@
 // pg_kernels.cuh -- the assembly kernels.
 //
-//   k_coh_points     one thread per cohesive quadrature point: opening delta = R sum_n N_n (U+ - U-),
-//                    the traction-separation law with its internal-variable update and damage
-//                    zone, and the weighted R^T D R / R^T T (src/Utilities.cpp:528-594).  FP64.
+//   k_coh_elements   one lane per cohesive quadrature point, the lanes of an element together:
+//                    opening delta = R sum_n N_n (U+ - U-), the traction-separation law with its
+//                    internal-variable update and damage zone, and the element's cohesive blocks
+//                    and tractions (src/Utilities.cpp:528-594).  FP64.
 //   k_cut_volumetric run once at set-up: the cut elements' volumetric (linear, state-independent)
 //                    element matrices from sub-element quadrature with enriched B-matrices
 //                    (src/Assembler.cpp:223-274), cached for every later assembly.  FP64.
@@ -10,7 +11,7 @@
 //                    path (pg_stencil.cuh) does not take: boundary rows, nodes of cut elements and
 //                    enrichment nodes; uncut elements are recomputed from node coordinates; for cut
 //                    elements the cached volumetric block row is combined with the nodal
-//                    displacements and the cohesive points' blocks (src/Assembler.cpp:278-365).
+//                    displacements and the cohesive elements' blocks (src/Assembler.cpp:278-365).
 //                    Every CSR value is written once.
 // No atomics anywhere: every row has one owner and sums in a fixed order, so results are
 // bit-reproducible from run to run.
@@ -128,217 +129,195 @@ __device__ __forceinline__ void add_strain(const T* g, const T* u, T* e) {
 __device__ __host__ inline double tri4_wsum() { return ((-0.28125 + 0.260416666666666666666666666666665) + 0.260416666666666666666666666666665) + 0.260416666666666666666666666666665; }
 __device__ __host__ inline double tet5_wsum() { return (((-0.8 + 0.45) + 0.45) + 0.45) + 0.45; }
 
-// Block row of an uncut simplex for local node la: kv[lb][q][q2] = w (B_la^T D B_lb)[q][q2],
-// rv[q] = w (B_la^T sigma)[q].
-template <int DIM, typename T>
-__device__ __forceinline__ void simplex_block_row(const DevProblem& P, int e, int la, const T* D, T (*kv)[DIM][DIM], T* rv) {
+// Block (la, lb) of an uncut simplex: kb = w (B_la^T D B_lb); with want_r also the residual of
+// row la, rv = w (B_la^T sigma).  Geometry from the node coordinates, stress from U (+ eps_macro).
+template <int DIM>
+__device__ __forceinline__ void simplex_block(const DevProblem& P, int e, int la, int lb, const double* D,
+                                              double (*kb)[DIM], double* rv, bool want_r) {
   constexpr int NPE = DIM + 1;
   constexpr int NV = (DIM == 2) ? 3 : 6;
   int nd[NPE];
 #pragma unroll
   for (int n = 0; n < NPE; ++n) nd[n] = __ldg(&P.conn[(size_t)e * NPE + n]);
-  T x[NPE][DIM], u[NPE][DIM], g[NPE][DIM], J;
+  double x[NPE][DIM], g[NPE][DIM], J;
 #pragma unroll
   for (int n = 0; n < NPE; ++n)
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      if (sizeof(T) == 4) x[n][d] = (T)__ldg(&P.Xf[(size_t)nd[n] * DIM + d]);
-      else x[n][d] = (T)__ldg(&P.X[(size_t)nd[n] * DIM + d]);
-      u[n][d] = (T)__ldg(&P.U[(size_t)nd[n] * DIM + d]);
-    }
-  simplex_geom<DIM, T>(x, g, &J);
-  const T wgt = J * (T)((DIM == 2) ? tri4_wsum() : tet5_wsum());
-  T eps[NV];
+    for (int d = 0; d < DIM; ++d) x[n][d] = __ldg(&P.X[(size_t)nd[n] * DIM + d]);
+  simplex_geom<DIM, double>(x, g, &J);
+  const double wgt = J * ((DIM == 2) ? tri4_wsum() : tet5_wsum());
+  double ga[DIM], gb[DIM];
 #pragma unroll
-  for (int v = 0; v < NV; ++v) eps[v] = 0;
+  for (int d = 0; d < DIM; ++d) { ga[d] = g[0][d]; gb[d] = g[0][d]; }
 #pragma unroll
-  for (int n = 0; n < NPE; ++n) add_strain<DIM, T>(g[n], u[n], eps);
-  if (P.subscale) {
-#pragma unroll
-    for (int v = 0; v < NV; ++v) eps[v] += (T)P.eps_macro[v];
-  }
-  T sig[NV];
-  lei_stress<DIM, T>(D, eps, sig);
-  // la is a runtime index: copy its gradient once
-  T ga[DIM];
-#pragma unroll
-  for (int d = 0; d < DIM; ++d) ga[d] = g[0][d];
-#pragma unroll
-  for (int n = 1; n < NPE; ++n)
+  for (int n = 1; n < NPE; ++n) {
     if (la == n)
 #pragma unroll
       for (int d = 0; d < DIM; ++d) ga[d] = g[n][d];
+    if (lb == n)
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) gb[d] = g[n][d];
+  }
 #pragma unroll
   for (int q = 0; q < DIM; ++q) {
-    T part[NV];
-    bt_d_row<DIM, T>(D, ga, q, part);
-    rv[q] = wgt * bt_sig<DIM, T>(ga, sig, q);
+    double part[NV];
+    bt_d_row<DIM, double>(D, ga, q, part);
 #pragma unroll
-    for (int lb = 0; lb < NPE; ++lb)
+    for (int q2 = 0; q2 < DIM; ++q2) kb[q][q2] = wgt * part_b<DIM, double>(part, gb, q2);
+  }
+  if (want_r) {
+    double eps[NV];
 #pragma unroll
-      for (int q2 = 0; q2 < DIM; ++q2) kv[lb][q][q2] = wgt * part_b<DIM, T>(part, g[lb], q2);
+    for (int v = 0; v < NV; ++v) eps[v] = 0.0;
+#pragma unroll
+    for (int n = 0; n < NPE; ++n) {
+      double u[DIM];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) u[d] = __ldg(&P.U[(size_t)nd[n] * DIM + d]);
+      add_strain<DIM, double>(g[n], u, eps);
+    }
+    if (P.subscale) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) eps[v] += P.eps_macro[v];
+    }
+    double sig[NV];
+    lei_stress<DIM, double>(D, eps, sig);
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) rv[q] = wgt * bt_sig<DIM, double>(ga, sig, q);
   }
 }
 
+// Shared-memory doubles of one lane group: slab_slots blocks of DIM x DIM, the node's residual (4
+// doubles reserved) and the per-block residual partials of one cut element (max_mn x DIM).
+__host__ __device__ inline int general_slab_doubles(int slab_slots, int dim, int max_mn) {
+  return slab_slots * dim * dim + 4 + max_mn * dim;
+}
+
 // Row assembly for the DOF nodes the stencil path does not take (boundary rows, nodes of cut
-// elements, enrichment nodes): one lane group of G threads per DOF node.  Each lane takes one
-// adjacent element (uncut: geometry recomputed from the node coordinates; cut: its block row from
-// the scratch), the lanes add their block rows into the node's shared-memory slab one after
-// another in adjacency order (deterministic, no atomics), the residual is reduced with a fixed
-// shuffle tree, and the group writes every CSR value of the node's rows exactly once.
-// Everything a node or an adjacency entry needs is packed into descriptors so the dependent
-// loads are: node descriptor -> adjacency descriptors -> element data.
+// elements, enrichment nodes): one lane group of G threads per DOF node.  The group walks the
+// node's adjacent elements in adjacency order; for each element its lanes take the element's
+// nodes (lane b: block (la, b)) and add the blocks into the node's shared-memory slab -- the blocks
+// of one element go to distinct neighbour slots, so no two lanes write the same entry -- and the
+// residual contributions are summed in a fixed order.  Every sum is therefore in adjacency order
+// and independent of G.  Uncut elements are recomputed from the node coordinates; a cut element
+// contributes its cached volumetric block row (K_vol, state independent) times the displacements,
+// its macroscale-strain response and, when the row node is on its cohesive element, the cohesive
+// blocks and traction that k_coh_elements left for it.  Finally the group writes every CSR value
+// of the node's rows exactly once.
 //   gdesc[node]      int4 {adjacency begin, adjacency count, neighbour begin, neighbour count}
 //   growd[node]      3*DIM ints: global DOF of each row, first slot in the row's F block, in its C block
 //   adesc[entry]     int4 {element, local node | nodes of a cut element << 8, slots (uncut: 8 bits per
 //                    node; cut: offset into adj_slots), material (uncut) / block-row offset (cut)}
-//   aresd[entry]     element-vector offset of the cut element's row (cut entries)
-// Shared-memory doubles of one lane group's slab: slab_slots blocks of DIM x DIM plus the node's
-// residual (4 doubles reserved).
-__host__ __device__ inline int general_slab_doubles(int slab_slots, int dim) { return slab_slots * dim * dim + 4; }
-
-// Rows of general node `node` (an index into the general-node descriptors) for the lane group of
-// the calling thread (G lanes, 128 / G groups per 128-thread block).  Every lane of the warp must
-// call it (valid = false for lanes without a node) because of the warp-wide shuffles.  slab: this
-// group's shared-memory slab of general_slab_doubles(slab_slots, DIM) doubles.  The K blocks and
-// the residual are both summed over the adjacent elements in adjacency order, one lane after
-// another, so the result does not depend on G.
+//   aresd[entry]     cut element index (cut entries)
+//   nbr_pre[slot]    free DOFs of the node's neighbours before this one (row positions)
+// Every lane of the warp must call it (valid = false for lanes without a node): the entry loop and
+// its warp synchronisations are warp-uniform.  G >= DIM + 1.
 template <int DIM, int G>
 __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool valid, double* slab) {
   constexpr int NPE = DIM + 1;
   constexpr int NV = (DIM == 2) ? 3 : 6;
+  constexpr int D2 = DIM * DIM;
+  static_assert(G >= NPE, "one lane per element node");
   const int g = threadIdx.x % G;
   int4 gd = make_int4(0, 0, 0, 0);
-  double* rs = nullptr;   // the node's residual, after the slab blocks
-  if (valid) {
-    gd = __ldg(&P.gdesc[node]);
-    rs = slab + gd.w * DIM * DIM;
-    for (int i = g; i < gd.w * DIM * DIM + DIM; i += G) slab[i] = 0.0;
-  }
-  int passes = (gd.y + G - 1) / G;
+  if (valid) gd = __ldg(&P.gdesc[node]);
+  double* rs = slab + gd.w * D2;           // residual of the node's rows
+  double* part = rs + 4;                    // per-block residual partials of one cut element
+  if (valid)
+    for (int i = g; i < gd.w * D2 + DIM; i += G) slab[i] = 0.0;
+  int n_ent = gd.y;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) passes = max(passes, __shfl_xor_sync(0xffffffffu, passes, o));
+  for (int o = 16; o > 0; o >>= 1) n_ent = max(n_ent, __shfl_xor_sync(0xffffffffu, n_ent, o));
   __syncwarp();
-  for (int pass = 0; pass < passes; ++pass) {
-    const int idx = pass * G + g;
-    const bool have = valid && idx < gd.y;
+  for (int ei = 0; ei < n_ent; ++ei) {
+    const bool have = valid && ei < gd.y;
     int4 ad = make_int4(0, 0, 0, 0);
-    double kv[NPE][DIM][DIM];
-    double r[DIM];   // this entry's residual contribution
-#pragma unroll
-    for (int q = 0; q < DIM; ++q) r[q] = 0.0;
+    int cc = -1;
     if (have) {
-      ad = __ldg(&P.adesc[gd.x + idx]);
-      const int la = ad.y & 255, mn = ad.y >> 8;
-      if (mn == 0) {
-        double D[NV * NV];
-#pragma unroll
-        for (int i = 0; i < NV * NV; ++i) D[i] = __ldg(&P.Dd[ad.w * 36 + i]);
-        double rv[DIM];
-        simplex_block_row<DIM, double>(P, ad.x, la, D, kv, rv);
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) r[q] += rv[q];
-      } else {
-        // cut element: K_vol (state independent, cached at set-up) times the element's nodal
-        // displacements, the macroscale-strain response, and the cohesive internal forces
-        const int cc = __ldg(&P.aresd[gd.x + idx]);
-        const double* kb = P.ke + ad.w;
-        const int* cn = P.cut_nodes + __ldg(&P.cut_node_off[cc]);
-        for (int lb = 0; lb < mn; ++lb) {
-          const int nd = __ldg(&cn[lb]);
-          double u[DIM];
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) u[d] = P.U[(size_t)nd * DIM + d];
-#pragma unroll
-          for (int q = 0; q < DIM; ++q)
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) r[q] += kb[lb * DIM * DIM + q * DIM + d] * u[d];
-        }
-        if (P.subscale) {
-          const double* gm = P.gmac + __ldg(&P.re_off[cc]) / DIM * DIM * NV + (size_t)la * DIM * NV;
-#pragma unroll
-          for (int q = 0; q < DIM; ++q)
-#pragma unroll
-            for (int v = 0; v < NV; ++v) r[q] += gm[q * NV + v] * P.eps_macro[v];
-        }
-        const int ce0 = __ldg(&P.cut_coh_off[cc]), ce1 = __ldg(&P.cut_coh_off[cc + 1]);
-        for (int ce = ce0; ce < ce1; ++ce) {
-          const int nh = __ldg(&P.coh_nh[ce]);
-          const int* cl = P.coh_local + __ldg(&P.coh_local_off[ce]);
-          int n1 = -1;
-          for (int k = 0; k < 2 * nh; ++k) if (__ldg(&cl[k]) == la) n1 = k;
-          if (n1 < 0) continue;
-          const double sgn = (n1 >= nh) ? 1.0 : -1.0;
-          double pc[DIM];
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) pc[d] = 0.0;
-          for (int cq = __ldg(&P.coh_qp_off[ce]); cq < __ldg(&P.coh_qp_off[ce + 1]); ++cq) {
-            const double nv = __ldg(&P.cqp_N[__ldg(&P.cqp_noff[cq]) + n1 % nh]);
-            const double* wt = P.cpt + (size_t)cq * (DIM * DIM + DIM) + DIM * DIM;
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) pc[d] += sgn * (nv * wt[d]);
-          }
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) r[d] += pc[d];
-        }
-      }
+      ad = __ldg(&P.adesc[gd.x + ei]);
+      if ((ad.y >> 8) > 0) cc = __ldg(&P.aresd[gd.x + ei]);
     }
-    for (int t = 0; t < G; ++t) {
-      if (have && g == t) {
+    const int la = ad.y & 255, mn = ad.y >> 8;
+    if (have && mn == 0) {
+      if (g < NPE) {
+        double kb[DIM][DIM], rv[DIM];
+        simplex_block<DIM>(P, ad.x, la, g, P.Dd + 36 * ad.w, kb, rv, g == 0);
+        double* ak = slab + ((((unsigned)ad.z) >> (8 * g)) & 255) * D2;
 #pragma unroll
-        for (int q = 0; q < DIM; ++q) rs[q] += r[q];
-        const int mn = ad.y >> 8;
-        if (mn == 0) {
-          const unsigned slots = (unsigned)ad.z;
+        for (int i = 0; i < D2; ++i) ak[i] += kb[i / DIM][i % DIM];
+        if (g == 0)
 #pragma unroll
-          for (int lb = 0; lb < NPE; ++lb) {
-            double* ak = slab + ((slots >> (8 * lb)) & 255) * DIM * DIM;
+          for (int q = 0; q < DIM; ++q) rs[q] += rv[q];
+      }
+    } else if (have) {
+      const int base = __ldg(&P.cut_node_off[cc]);
+      const int* cn = P.cut_nodes + base;
+      const double* kr = P.ke + ad.w;                 // block row la of K_vol
+      const int cpa = __ldg(&P.cohpos[base + la]);    // (cohesive element << 5 | position) or -1
+      for (int b = g; b < mn; b += G) {
+        double blk[D2];
 #pragma unroll
-            for (int i = 0; i < DIM * DIM; ++i) ak[i] += kv[lb][i / DIM][i % DIM];
-          }
-        } else {
-          const double* kb = P.ke + ad.w;
-          for (int lb = 0; lb < mn; ++lb) {
-            double* ak = slab + __ldg(&P.adj_slots[ad.z + lb]) * DIM * DIM;
+        for (int i = 0; i < D2; ++i) blk[i] = kr[b * D2 + i];
+        const int nb = __ldg(&cn[b]);
+        double u[DIM];
 #pragma unroll
-            for (int i = 0; i < DIM * DIM; ++i) ak[i] += kb[lb * DIM * DIM + i];
-          }
-          // cohesive blocks: sgn N_a1 N_a2 (w R^T D R) summed over the cohesive element's points
-          const int la = ad.y & 255;
-          const int cc = __ldg(&P.aresd[gd.x + idx]);
-          const int ce0 = __ldg(&P.cut_coh_off[cc]), ce1 = __ldg(&P.cut_coh_off[cc + 1]);
-          for (int ce = ce0; ce < ce1; ++ce) {
+        for (int d = 0; d < DIM; ++d) u[d] = P.U[(size_t)nb * DIM + d];
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) {
+          double s = 0.0;
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) s += blk[q * DIM + d] * u[d];
+          part[b * DIM + q] = s;
+        }
+        if (cpa >= 0) {
+          const int cpb = __ldg(&P.cohpos[base + b]);
+          if (cpb >= 0 && (cpb >> 5) == (cpa >> 5)) {
+            const int ce = cpa >> 5, n1 = cpa & 31, n2 = cpb & 31;
             const int nh = __ldg(&P.coh_nh[ce]);
-            const int* cl = P.coh_local + __ldg(&P.coh_local_off[ce]);
-            int n1 = -1;
-            for (int k = 0; k < 2 * nh; ++k) if (__ldg(&cl[k]) == la) n1 = k;
-            if (n1 < 0) continue;
-            const int cqa = __ldg(&P.coh_qp_off[ce]), cqb = __ldg(&P.coh_qp_off[ce + 1]);
-            for (int n2 = 0; n2 < 2 * nh; ++n2) {
-              const double sgn = ((n1 >= nh) == (n2 >= nh)) ? 1.0 : -1.0;
-              double kc[DIM * DIM];
+            const double sgn = ((n1 >= nh) == (n2 >= nh)) ? 1.0 : -1.0;
+            const double* B = P.kcoh + __ldg(&P.kc_off[ce]) + ((n1 % nh) * nh + (n2 % nh)) * D2;
 #pragma unroll
-              for (int i = 0; i < DIM * DIM; ++i) kc[i] = 0.0;
-              for (int cq = cqa; cq < cqb; ++cq) {
-                const int no = __ldg(&P.cqp_noff[cq]);
-                const double nn = __ldg(&P.cqp_N[no + n1 % nh]) * __ldg(&P.cqp_N[no + n2 % nh]);
-                const double* wr = P.cpt + (size_t)cq * (DIM * DIM + DIM);
-#pragma unroll
-                for (int i = 0; i < DIM * DIM; ++i) kc[i] += sgn * (nn * wr[i]);
-              }
-              double* ak = slab + __ldg(&P.adj_slots[ad.z + __ldg(&cl[n2])]) * DIM * DIM;
-#pragma unroll
-              for (int i = 0; i < DIM * DIM; ++i) ak[i] += kc[i];
-            }
+            for (int i = 0; i < D2; ++i) blk[i] += sgn * B[i];
           }
         }
+        double* ak = slab + __ldg(&P.adj_slots[ad.z + b]) * D2;
+#pragma unroll
+        for (int i = 0; i < D2; ++i) ak[i] += blk[i];
       }
-      __syncwarp();
     }
+    __syncwarp();
+    if (have && mn > 0 && g == 0) {
+      double r[DIM];
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) r[q] = 0.0;
+      for (int b = 0; b < mn; ++b)
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) r[q] += part[b * DIM + q];
+      if (P.subscale) {
+        const double* gm = P.gmac + __ldg(&P.re_off[cc]) / DIM * DIM * NV + (size_t)la * DIM * NV;
+#pragma unroll
+        for (int q = 0; q < DIM; ++q)
+#pragma unroll
+          for (int v = 0; v < NV; ++v) r[q] += gm[q * NV + v] * P.eps_macro[v];
+      }
+      const int cpa = __ldg(&P.cohpos[__ldg(&P.cut_node_off[cc]) + la]);
+      if (cpa >= 0) {
+        const int ce = cpa >> 5, n1 = cpa & 31;
+        const int nh = __ldg(&P.coh_nh[ce]);
+        const double sgn = (n1 >= nh) ? 1.0 : -1.0;
+        const double* t = P.kcoh + __ldg(&P.kc_off[ce]) + nh * nh * D2 + (n1 % nh) * DIM;
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) r[q] += sgn * t[q];
+      }
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) rs[q] += r[q];
+    }
+    __syncwarp();
   }
   if (!valid) return;
   const int nn = gd.w;
   const uint8_t* masks = P.dn_nbr_mask + gd.z;
+  const int* pre = P.nbr_pre + gd.z;
   const int* rd = P.growd + (size_t)node * 3 * DIM;
 #pragma unroll
   for (int q = 0; q < DIM; ++q) {
@@ -348,8 +327,7 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
       double* vF = P.val[rf ? 0 : 2] + __ldg(&rd[DIM + q]);
       double* vC = P.val[rf ? 1 : 3] + __ldg(&rd[2 * DIM + q]);
       for (int k = g; k < nn; k += G) {
-        int pf = 0;
-        for (int k2 = 0; k2 < k; ++k2) pf += __popc(__ldg(&masks[k2]));
+        int pf = __ldg(&pre[k]);
         int pc = k * DIM - pf;
         const int mk = __ldg(&masks[k]);
 #pragma unroll
@@ -366,87 +344,156 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
 }
 
 template <int DIM, int G>
-__global__ void __launch_bounds__(128) k_rows_general(DevProblem P, int slab_slots) {
+__global__ void __launch_bounds__(128) k_rows_general(DevProblem P, int slab_slots, int max_mn) {
   constexpr int NB = 128 / G;
   extern __shared__ double smem[];
   const int grp = threadIdx.x / G;
   const int node = blockIdx.x * NB + grp;
-  general_rows<DIM, G>(P, node, node < P.n_slow_dn, smem + (size_t)grp * general_slab_doubles(slab_slots, DIM));
+  general_rows<DIM, G>(P, node, node < P.n_slow_dn, smem + (size_t)grp * general_slab_doubles(slab_slots, DIM, max_mn));
 }
 
-// Cohesive law at every cohesive quadrature point.  Output per point: w R^T D R (dim x dim) then
-// w R^T T (dim).
+// Cohesive elements, one lane per quadrature point (CQ lanes per element: 2 in 2D for CohEdge2, 4
+// in 3D for CohTri3 / CohQuad4).  Lane qi forms the opening delta = R sum_n N_n (U+ - U-) of its
+// point, runs the traction-separation law with its internal-variable update and damage zone
+// (src/Utilities.cpp:528-594, the Material_*Cohesive* files) and forms w R^T D R and w R^T T; the
+// lanes then exchange these by shuffles and each writes some of the element's blocks
+// B_ab = sum_qp N_a N_b w R^T D R (a, b < nh) and tractions t_a = sum_qp N_a w R^T T (sums in point
+// order) to the scratch at kc_off[ce].  The element's stiffness block (n1, n2) is
+// sgn * B_{n1 % nh, n2 % nh} and its internal force at n1 is sgn * t_{n1 % nh}, the signs following
+// cohesiveKFast / cohesiveInternalForceFast.  Every lane of the warp must call it (valid = false
+// for lanes past the last element).
 template <int DIM>
-__device__ __forceinline__ void coh_point(const DevProblem& P, int cq) {
-  const int c = __ldg(&P.cqp_cut[cq]), ce = __ldg(&P.cqp_ce[cq]);
-  const int nh = __ldg(&P.coh_nh[ce]);
-  const int* cl = P.coh_local + __ldg(&P.coh_local_off[ce]);
-  const int* nodes = P.cut_nodes + __ldg(&P.cut_node_off[c]);
-  const double* N = P.cqp_N + __ldg(&P.cqp_noff[cq]);
-  const double* R = P.cqp_R + (size_t)cq * DIM * DIM;
-  double d0[DIM];
-#pragma unroll
-  for (int d = 0; d < DIM; ++d) {
-    double s = 0.0;
-    for (int n = 0; n < nh; ++n) {
-      const int np = __ldg(&nodes[__ldg(&cl[n + nh])]), nm = __ldg(&nodes[__ldg(&cl[n])]);
-      s += N[n] * (P.U[(size_t)np * DIM + d] - P.U[(size_t)nm * DIM + d]);
-    }
-    d0[d] = s;
+struct CohLanes { static constexpr int CQ = (DIM == 2) ? 2 : 4; };
+
+template <int DIM>
+__device__ __forceinline__ void coh_element(const DevProblem& P, int ce, int qi, bool valid) {
+  constexpr int D2 = DIM * DIM;
+  constexpr int CQ = CohLanes<DIM>::CQ;
+  const int lane = threadIdx.x & 31, base_lane = lane & ~(CQ - 1);
+  int c = 0, nh = 0, q0 = 0, nq = 0;
+  if (valid) {
+    c = __ldg(&P.ce_cut[ce]);
+    nh = __ldg(&P.coh_nh[ce]);
+    q0 = __ldg(&P.coh_qp_off[ce]);
+    nq = min(CQ, __ldg(&P.coh_qp_off[ce + 1]) - q0);
   }
-  double dl[DIM], T[DIM], Dc[DIM * DIM];
+  double W[D2], Tr[DIM];
 #pragma unroll
-  for (int i = 0; i < DIM; ++i) {
-    double s = 0.0;
+  for (int i = 0; i < D2; ++i) W[i] = 0.0;
 #pragma unroll
-    for (int j = 0; j < DIM; ++j) s += R[i * DIM + j] * d0[j];
-    dl[i] = s;
-  }
-  const int iv = __ldg(&P.cqp_isv[cq]);
-  double isv[2] = {0.0, 0.0};
-  for (int v = 0; v < P.coh.nvar; ++v) isv[v] = P.isv_committed[iv + v];
-  uint8_t z;
-  coh_law(P.coh, DIM, dl, T, Dc, isv, &z);
-  for (int v = 0; v < P.coh.nvar; ++v) P.isv_trial[iv + v] = isv[v];
-  P.zone[cq] = z;
-  double RtD[DIM * DIM];
-#pragma unroll
-  for (int i = 0; i < DIM; ++i)
-#pragma unroll
-    for (int k = 0; k < DIM; ++k) {
-      double s = 0.0;
-#pragma unroll
-      for (int j = 0; j < DIM; ++j) s += R[j * DIM + i] * Dc[j * DIM + k];
-      RtD[i * DIM + k] = s;
-    }
-  const double w = P.cqp_wgt[cq];
-  double* out = P.cpt + (size_t)cq * (DIM * DIM + DIM);
+  for (int i = 0; i < DIM; ++i) Tr[i] = 0.0;
   bool bad = false;
+  if (valid && qi < nq) {
+    const int* cl = P.coh_local + __ldg(&P.coh_local_off[ce]);
+    const int* nodes = P.cut_nodes + __ldg(&P.cut_node_off[c]);
+    const int cq = q0 + qi;
+    const double* N = P.cqp_N + __ldg(&P.cqp_noff[cq]);
+    const double* R = P.cqp_R + (size_t)cq * D2;
+    double d0[DIM];
 #pragma unroll
-  for (int i = 0; i < DIM; ++i)
+    for (int d = 0; d < DIM; ++d) {
+      double s = 0.0;
+      for (int n = 0; n < nh; ++n) {
+        const int np = __ldg(&nodes[__ldg(&cl[n + nh])]), nm = __ldg(&nodes[__ldg(&cl[n])]);
+        s += N[n] * (P.U[(size_t)np * DIM + d] - P.U[(size_t)nm * DIM + d]);
+      }
+      d0[d] = s;
+    }
+    double dl[DIM], T[DIM], Dc[D2];
 #pragma unroll
-    for (int l = 0; l < DIM; ++l) {
+    for (int i = 0; i < DIM; ++i) {
       double s = 0.0;
 #pragma unroll
-      for (int k = 0; k < DIM; ++k) s += RtD[i * DIM + k] * R[k * DIM + l];
-      out[i * DIM + l] = w * s;
+      for (int j = 0; j < DIM; ++j) s += R[i * DIM + j] * d0[j];
+      dl[i] = s;
+    }
+    const int iv = __ldg(&P.cqp_isv[cq]);
+    double isv[2] = {0.0, 0.0};
+    for (int v = 0; v < P.coh.nvar; ++v) isv[v] = P.isv_committed[iv + v];
+    uint8_t z;
+    coh_law(P.coh, DIM, dl, T, Dc, isv, &z);
+    for (int v = 0; v < P.coh.nvar; ++v) P.isv_trial[iv + v] = isv[v];
+    P.zone[cq] = z;
+    double RtD[D2];
+#pragma unroll
+    for (int i = 0; i < DIM; ++i)
+#pragma unroll
+      for (int k = 0; k < DIM; ++k) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < DIM; ++j) s += R[j * DIM + i] * Dc[j * DIM + k];
+        RtD[i * DIM + k] = s;
+      }
+    const double w = P.cqp_wgt[cq];
+#pragma unroll
+    for (int i = 0; i < DIM; ++i)
+#pragma unroll
+      for (int l = 0; l < DIM; ++l) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) s += RtD[i * DIM + k] * R[k * DIM + l];
+        W[i * DIM + l] = w * s;
+        bad |= !isfinite(s);
+      }
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) {
+      double s = 0.0;
+#pragma unroll
+      for (int j = 0; j < DIM; ++j) s += R[j * DIM + i] * T[j];
+      Tr[i] = w * s;
       bad |= !isfinite(s);
     }
+  }
+  // every point's w R^T D R and w R^T T to every lane of the element
+  double Wa[CQ][D2], Ta[CQ][DIM];
 #pragma unroll
-  for (int i = 0; i < DIM; ++i) {
-    double s = 0.0;
+  for (int j = 0; j < CQ; ++j) {
 #pragma unroll
-    for (int j = 0; j < DIM; ++j) s += R[j * DIM + i] * T[j];
-    out[DIM * DIM + i] = w * s;
-    bad |= !isfinite(s);
+    for (int i = 0; i < D2; ++i) Wa[j][i] = __shfl_sync(0xffffffffu, W[i], base_lane + j);
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) Ta[j][i] = __shfl_sync(0xffffffffu, Tr[i], base_lane + j);
   }
   if (bad) atomicOr(P.err, ERR_NONFINITE);
+  if (!valid) return;
+  double* out = P.kcoh + __ldg(&P.kc_off[ce]);
+  for (int p = qi; p < nh * nh; p += CQ) {
+    const int a = p / nh, b = p - a * nh;
+    double blk[D2];
+#pragma unroll
+    for (int i = 0; i < D2; ++i) blk[i] = 0.0;
+#pragma unroll
+    for (int j = 0; j < CQ; ++j) {
+      if (j >= nq) break;
+      const double* N = P.cqp_N + __ldg(&P.cqp_noff[q0 + j]);
+      const double nn = N[a] * N[b];
+#pragma unroll
+      for (int i = 0; i < D2; ++i) blk[i] += nn * Wa[j][i];
+    }
+#pragma unroll
+    for (int i = 0; i < D2; ++i) out[p * D2 + i] = blk[i];
+  }
+  for (int a = qi; a < nh; a += CQ) {
+    double t[DIM];
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) t[i] = 0.0;
+#pragma unroll
+    for (int j = 0; j < CQ; ++j) {
+      if (j >= nq) break;
+      const double na = P.cqp_N[__ldg(&P.cqp_noff[q0 + j]) + a];
+#pragma unroll
+      for (int i = 0; i < DIM; ++i) t[i] += na * Ta[j][i];
+    }
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) out[nh * nh * D2 + a * DIM + i] = t[i];
+  }
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(128) k_coh_points(DevProblem P) {
-  const int cq = blockIdx.x * blockDim.x + threadIdx.x;
-  if (cq < P.n_coh_qp) coh_point<DIM>(P, cq);
+__global__ void __launch_bounds__(128) k_coh_elements(DevProblem P) {
+  constexpr int CQ = CohLanes<DIM>::CQ;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ce = t / CQ;
+  coh_element<DIM>(P, ce, t % CQ, ce < P.n_coh_el);
 }
 
 // State-independent part of the cut elements, computed once at set-up: the volumetric element
