@@ -71,18 +71,23 @@ __global__ void __launch_bounds__(128) k_batch_coh(const BatchItem* __restrict__
 template <int DIM, typename T>
 __global__ void __launch_bounds__(256) k_batch_stencil(const BatchItem* __restrict__ items, const int4* __restrict__ chunks,
                                                        int n_chunks) {
+  extern __shared__ double stage[];
   for (int c = blockIdx.x; c < n_chunks; c += gridDim.x) {
     const int4 ch = chunks[c];
     const BatchItem& it = items[ch.x];
     if (DIM == 2) {
-      if ((int)threadIdx.x >= ch.z) continue;
-      const int4 v = __ldg(&it.stencil[ch.y + threadIdx.x]);
-      if (v.w == 0) pgd::stencil_rows<pgd::Tri3Stencil0, 2, T, -1>(it.P, it.gi, v.x, v.y, v.z);
-      else pgd::stencil_rows<pgd::Tri3Stencil1, 2, T, -1>(it.P, it.gi, v.x, v.y, v.z);
+      // chunks start at multiples of 32 of the padded list, so every warp has one class
+      if ((int)(threadIdx.x & ~31u) >= ch.z) continue;
+      const bool in = (int)threadIdx.x < ch.z;
+      const int4 v = in ? __ldg(&it.stencil[ch.y + threadIdx.x]) : make_int4(-1, 0, 0, 0);
+      const int cls = __shfl_sync(0xffffffffu, v.w, 0);
+      if (cls == 0) pgd::stencil_rows_staged<pgd::Tri3Stencil0, T>(it.P, it.gi, v, v.x >= 0, stage);
+      else pgd::stencil_rows_staged<pgd::Tri3Stencil1, T>(it.P, it.gi, v, v.x >= 0, stage);
     } else {
       const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
       if (lane >= ch.z || w > 2) continue;
       const int4 v = __ldg(&it.stencil[ch.y + lane]);
+      if (v.x < 0) continue;
       if (w == 0) pgd::stencil_rows<pgd::Tet4Stencil0, 3, T, 0>(it.P, it.gi, v.x, v.y, v.z);
       else if (w == 1) pgd::stencil_rows<pgd::Tet4Stencil0, 3, T, 1>(it.P, it.gi, v.x, v.y, v.z);
       else pgd::stencil_rows<pgd::Tet4Stencil0, 3, T, 2>(it.P, it.gi, v.x, v.y, v.z);
@@ -164,8 +169,10 @@ void general_attr(const pg_batch* b) {
   cudaFuncSetAttribute(k_batch_general<DIM, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)general_smem<DIM, G>(b));
 }
 
-// set before any capture: the dynamic shared memory of the general-row kernel of the current shape
+// set before any capture: the dynamic shared memory of the kernels of the current shape
 void set_attributes(const pg_batch* b) {
+  cudaFuncSetAttribute(k_batch_stencil<2, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pgd::stencil_stage_bytes(256));
+  cudaFuncSetAttribute(k_batch_stencil<2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pgd::stencil_stage_bytes(256));
   if (b->dim == 2) { if (b->G == 4) general_attr<2, 4>(b); else if (b->G == 8) general_attr<2, 8>(b); else general_attr<2, 16>(b); }
   else { if (b->G == 8) general_attr<3, 8>(b); else if (b->G == 16) general_attr<3, 16>(b); else general_attr<3, 32>(b); }
 }
@@ -220,8 +227,9 @@ void enqueue(pg_batch* b, bool fp32) {
   if (b->n_sten) {
     const int grid = std::min(b->n_sten, cap);
     if (b->dim == 2) {
-      if (fp32) k_batch_stencil<2, float><<<grid, b->tpb, 0, b->side>>>(b->d_items, b->d_sten, b->n_sten);
-      else k_batch_stencil<2, double><<<grid, b->tpb, 0, b->side>>>(b->d_items, b->d_sten, b->n_sten);
+      const size_t smem = pgd::stencil_stage_bytes(b->tpb);
+      if (fp32) k_batch_stencil<2, float><<<grid, b->tpb, smem, b->side>>>(b->d_items, b->d_sten, b->n_sten);
+      else k_batch_stencil<2, double><<<grid, b->tpb, smem, b->side>>>(b->d_items, b->d_sten, b->n_sten);
     } else {
       if (fp32) k_batch_stencil<3, float><<<grid, 96, 0, b->side>>>(b->d_items, b->d_sten, b->n_sten);
       else k_batch_stencil<3, double><<<grid, 96, 0, b->side>>>(b->d_items, b->d_sten, b->n_sten);

@@ -85,8 +85,9 @@ int launch(pg_ctx* c, double t_frac, int flags) {
     const int nthreads = (dim == 2) ? c->n_stencil : 3 * 32 * ((c->n_stencil + 31) / 32);
     const int grid = (nthreads + tpb - 1) / tpb;
     if (dim == 2) {
-      if (fp32) pgd::k_rows_stencil<2, float><<<grid, tpb, 0, c->side>>>(P, c->grid, c->stencil, c->n_stencil);
-      else pgd::k_rows_stencil<2, double><<<grid, tpb, 0, c->side>>>(P, c->grid, c->stencil, c->n_stencil);
+      const size_t smem = pgd::stencil_stage_bytes(tpb);
+      if (fp32) pgd::k_rows_stencil<2, float><<<grid, tpb, smem, c->side>>>(P, c->grid, c->stencil, c->n_stencil);
+      else pgd::k_rows_stencil<2, double><<<grid, tpb, smem, c->side>>>(P, c->grid, c->stencil, c->n_stencil);
     } else {
       if (fp32) pgd::k_rows_stencil<3, float><<<grid, tpb, 0, c->side>>>(P, c->grid, c->stencil, c->n_stencil);
       else pgd::k_rows_stencil<3, double><<<grid, tpb, 0, c->side>>>(P, c->grid, c->stencil, c->n_stencil);
@@ -280,14 +281,21 @@ int pg_upload(pg_ctx* c) {
       by_class[cls].push_back(make_int4(nid, g0, row0, cls));
       in_stencil[a] = 1;
     }
-    for (auto& v : by_class) stencil.insert(stencil.end(), v.begin(), v.end());
+    // each class segment padded to whole warps (entries with node -1): a warp's nodes then share
+    // one class and one row length, which the staged row stores of the 2D kernel rely on
+    for (int cls = 0; cls < 2; ++cls) {
+      auto& v = by_class[cls];
+      if (v.empty()) continue;
+      stencil.insert(stencil.end(), v.begin(), v.end());
+      while (stencil.size() % 32) stencil.push_back(make_int4(-1, 0, 0, cls));
+    }
     std::vector<int> rest;
     maxnb_general = 1;
     for (int a = 0; a < s.n_dn; ++a)
       if (!in_stencil[a]) { rest.push_back(a); maxnb_general = std::max(maxnb_general, s.dn_nbr_off[a + 1] - s.dn_nbr_off[a]); }
     slow.swap(rest);
     fast.clear();
-    for (auto& v : stencil) fast.push_back(s.node_dn[v.x]);
+    for (auto& v : stencil) if (v.x >= 0) fast.push_back(s.node_dn[v.x]);
     c->grid = pgd::GridInfo{Nx, Ny, Nz};
   }
   // cut-element scratch layout

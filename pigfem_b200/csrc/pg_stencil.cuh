@@ -107,7 +107,8 @@ __device__ __forceinline__ void iso_d(const DevProblem& P, int m, T* d) {
 
 // Rows of one stencil node.  Q < 0: all dim rows in one thread; Q >= 0: row Q only.
 template <class S, int DIM, typename T, int Q>
-__device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo& gi, int nid, int g0, int row0) {
+__device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo& gi, int nid, int g0, int row0,
+                                             double* stage = nullptr) {
   constexpr int NPE = DIM + 1;
   constexpr int NV = (DIM == 2) ? 3 : 6;
   constexpr int ND = (DIM == 2) ? 5 : 12;
@@ -189,7 +190,8 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
 #pragma unroll
   for (int q = QB; q < QE; ++q) {
     if (P.flags & FLAG_JAC) {
-      double* v = P.val[0] + row0 + (size_t)q * S::NN * DIM;
+      // rows go to the caller's stage when it has one, else straight to the CSR
+      double* v = stage ? stage + (size_t)q * S::NN * DIM : P.val[0] + row0 + (size_t)q * S::NN * DIM;
 #pragma unroll
       for (int s = 0; s < S::NN; ++s)
 #pragma unroll
@@ -199,23 +201,53 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
   }
 }
 
+// 2D rows of the stencil node of this lane, staged: the lane's two rows (2 x NN x 2 values, one
+// contiguous run of the CSR since a node's rows follow each other) go to the warp's shared-memory
+// stage, then the warp writes the 32 runs with consecutive lanes on consecutive addresses, so a
+// store instruction touches a few sectors instead of one per lane.  Every lane of the warp calls it
+// (valid = false for padding entries); the warp's entries share one class.
+constexpr int kStageStride = 37;   // doubles per lane in the stage (>= the longest run, 36; odd)
+__host__ __device__ inline size_t stencil_stage_bytes(int threads) { return (size_t)threads * kStageStride * sizeof(double); }
+
+template <class S, typename T>
+__device__ __forceinline__ void stencil_rows_staged(const DevProblem& P, const GridInfo& gi, int4 v, bool valid,
+                                                    double* stage) {
+  constexpr int RUN = 2 * S::NN * 2;
+  const int lane = threadIdx.x & 31;
+  double* my = stage + (size_t)(threadIdx.x & ~31) * kStageStride;
+  if (valid) stencil_rows<S, 2, T, -1>(P, gi, v.x, v.y, v.z, my + lane * kStageStride);
+  if (!(P.flags & FLAG_JAC)) return;
+  __syncwarp();
+  const unsigned ok = __ballot_sync(0xffffffffu, valid);
+  double* out = P.val[0];
+  for (int i = lane; i < 32 * RUN; i += 32) {
+    const int k = i / RUN, o = i - k * RUN;
+    const int r0 = __shfl_sync(0xffffffffu, v.z, k);
+    if ((ok >> k) & 1u) out[(size_t)r0 + o] = my[k * kStageStride + o];
+  }
+  __syncwarp();
+}
+
 // One thread per stencil node (2D) or per (stencil node, row) (3D, rows interleaved by warp so the
 // row is warp-uniform).  st: {node id, first free DOF, first CSR slot of its first row, class} per
-// node, class-sorted.
+// node, class-sorted, each class padded to whole warps with node -1.  2D launches carry
+// stencil_stage_bytes(blockDim.x) of dynamic shared memory.
 template <int DIM, typename T>
 __global__ void __launch_bounds__(128) k_rows_stencil(DevProblem P, GridInfo gi, const int4* __restrict__ st, int n) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (DIM == 2) {
-    if (t >= n) return;
+    extern __shared__ double stage[];
+    if (t - (int)(threadIdx.x & 31) >= n) return;   // whole warps only: n is a multiple of 32
     const int4 v = __ldg(&st[t]);
-    if (v.w == 0) stencil_rows<Tri3Stencil0, 2, T, -1>(P, gi, v.x, v.y, v.z);
-    else stencil_rows<Tri3Stencil1, 2, T, -1>(P, gi, v.x, v.y, v.z);
+    if (v.w == 0) stencil_rows_staged<Tri3Stencil0, T>(P, gi, v, v.x >= 0, stage);
+    else stencil_rows_staged<Tri3Stencil1, T>(P, gi, v, v.x >= 0, stage);
   } else {
     // a warp takes one row (q) of 32 consecutive stencil nodes, so q is uniform within a warp
     const int w = t >> 5, lane = t & 31;
     const int q = w % 3, node = (w / 3) * 32 + lane;
     if (node >= n) return;
     const int4 v = __ldg(&st[node]);
+    if (v.x < 0) return;   // padding entry
     if (q == 0) stencil_rows<Tet4Stencil0, 3, T, 0>(P, gi, v.x, v.y, v.z);
     else if (q == 1) stencil_rows<Tet4Stencil0, 3, T, 1>(P, gi, v.x, v.y, v.z);
     else stencil_rows<Tet4Stencil0, 3, T, 2>(P, gi, v.x, v.y, v.z);
