@@ -293,6 +293,18 @@ int pg_upload(pg_ctx* c) {
     maxnb_general = 1;
     for (int a = 0; a < s.n_dn; ++a)
       if (!in_stencil[a]) { rest.push_back(a); maxnb_general = std::max(maxnb_general, s.dn_nbr_off[a + 1] - s.dn_nbr_off[a]); }
+    // general nodes grouped by shape (cut adjacent elements, then all adjacent elements, both
+    // descending; node order within a group) so the lane groups of a warp walk alike entries
+    auto n_cut_adj = [&](int a) {
+      int k = 0;
+      for (int j = s.dn_adj_off[a]; j < s.dn_adj_off[a + 1]; ++j) k += s.cut_of[s.dn_adj[j] >> 5] >= 0;
+      return k;
+    };
+    std::stable_sort(rest.begin(), rest.end(), [&](int x, int y) {
+      const int cx = n_cut_adj(x), cy = n_cut_adj(y);
+      if (cx != cy) return cx > cy;
+      return (s.dn_adj_off[x + 1] - s.dn_adj_off[x]) > (s.dn_adj_off[y + 1] - s.dn_adj_off[y]);
+    });
     slow.swap(rest);
     fast.clear();
     for (auto& v : stencil) if (v.x >= 0) fast.push_back(s.node_dn[v.x]);
@@ -327,9 +339,12 @@ int pg_upload(pg_ctx* c) {
       rows[2][q] = rf ? s.rp[1][rr] : s.rp[3][rr];
     }
     for (int t = 0; t < 3; ++t) for (int q = 0; q < dim; ++q) growd.push_back(rows[t][q]);
+    // cut elements first, then uncut ones, each in adjacency order
+    for (int pass = 0; pass < 2; ++pass)
     for (int k = s.dn_adj_off[a]; k < s.dn_adj_off[a + 1]; ++k) {
       const int e = s.dn_adj[k] >> 5, la = s.dn_adj[k] & 31;
       const int cc = s.cut_of[e];
+      if ((cc >= 0) != (pass == 0)) continue;
       if (cc < 0) {
         adesc.push_back(make_int4(e, la, slot32[k], s.elem_mat[e]));
         aresd.push_back(0);

@@ -190,7 +190,7 @@ __device__ __forceinline__ void simplex_block(const DevProblem& P, int e, int la
 // Shared-memory doubles of one lane group: slab_slots blocks of DIM x DIM, the node's residual (4
 // doubles reserved) and the per-block residual partials of one cut element (max_mn x DIM).
 __host__ __device__ inline int general_slab_doubles(int slab_slots, int dim, int max_mn) {
-  return slab_slots * dim * dim + 4 + max_mn * dim;
+  return (slab_slots * dim * dim + 4 + max_mn * dim) | 1;   // odd: groups start on different banks
 }
 
 // Row assembly for the DOF nodes the stencil path does not take (boundary rows, nodes of cut
@@ -229,14 +229,15 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) n_ent = max(n_ent, __shfl_xor_sync(0xffffffffu, n_ent, o));
   __syncwarp();
+  // the next entry's descriptors are loaded while the current one is processed
+  int4 ad_next = make_int4(0, 0, 0, 0);
+  int cc_next = -1;
+  if (valid && gd.y > 0) { ad_next = __ldg(&P.adesc[gd.x]); cc_next = __ldg(&P.aresd[gd.x]); }
   for (int ei = 0; ei < n_ent; ++ei) {
     const bool have = valid && ei < gd.y;
-    int4 ad = make_int4(0, 0, 0, 0);
-    int cc = -1;
-    if (have) {
-      ad = __ldg(&P.adesc[gd.x + ei]);
-      if ((ad.y >> 8) > 0) cc = __ldg(&P.aresd[gd.x + ei]);
-    }
+    const int4 ad = ad_next;
+    const int cc = ((ad.y >> 8) > 0) ? cc_next : -1;
+    if (valid && ei + 1 < gd.y) { ad_next = __ldg(&P.adesc[gd.x + ei + 1]); cc_next = __ldg(&P.aresd[gd.x + ei + 1]); }
     const int la = ad.y & 255, mn = ad.y >> 8;
     if (have && mn == 0) {
       if (g < NPE) {
