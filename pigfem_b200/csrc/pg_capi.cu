@@ -324,7 +324,8 @@ int pg_upload(pg_ctx* c) {
 
   // descriptors of the general rows (k_rows_general)
   std::vector<int4> gdesc, adesc;
-  std::vector<int> growd, aresd;
+  std::vector<int> growd;
+  std::vector<int4> aresd;   // per entry: uncut {element nodes}, cut {cut element, first node, cohesive place, 0}
   for (int a : slow) {
     const int na = s.dn_node[a];
     gdesc.push_back(make_int4((int)adesc.size(), s.dn_adj_off[a + 1] - s.dn_adj_off[a], s.dn_nbr_off[a],
@@ -347,13 +348,19 @@ int pg_upload(pg_ctx* c) {
       if ((cc >= 0) != (pass == 0)) continue;
       if (cc < 0) {
         adesc.push_back(make_int4(e, la, slot32[k], s.elem_mat[e]));
-        aresd.push_back(0);
+        const int* en = &s.conn[(size_t)e * s.npe];
+        aresd.push_back(make_int4(en[0], en[1], en[2], s.npe > 3 ? en[3] : -1));
       } else {
         const int mn = s.cut_node_off[cc + 1] - s.cut_node_off[cc];
         const long long kro = ke_off[cc] + (long long)la * mn * dim * dim;
         if (kro > 2147483647LL) return set_err(c, PG_ERR_UNSUPPORTED, "cut-element scratch beyond 2^31 doubles");
         adesc.push_back(make_int4(e, la | (mn << 8), slot_off[k], (int)kro));
-        aresd.push_back(cc);
+        // the row node's place on a cohesive element of this cut element: (element << 5 | position)
+        int cpa = -1;
+        for (int ce = s.cut_coh_off[cc]; ce < s.cut_coh_off[cc + 1] && cpa < 0; ++ce)
+          for (int j = s.coh_local_off[ce]; j < s.coh_local_off[ce + 1]; ++j)
+            if (s.coh_local[j] == la) { cpa = ce * 32 + (j - s.coh_local_off[ce]); break; }
+        aresd.push_back(make_int4(cc, s.cut_node_off[cc], cpa, 0));
       }
     }
   }

@@ -72,7 +72,7 @@ struct DevProblem {
   const uint16_t* adj_local;                     // tile-local index of each adjacency entry's element
   const int* slow_dn; int n_slow_dn;             // the remaining DOF nodes
   int maxnb_general;                             // slab slots per node in k_rows_general
-  const int4* gdesc; const int* growd; const int4* adesc; const int* aresd;  // k_rows_general descriptors
+  const int4* gdesc; const int* growd; const int4* adesc; const int4* aresd;  // k_rows_general descriptors
   // cohesive points
   int n_coh_qp;
   int n_coh_el;                                  // cohesive elements

@@ -129,16 +129,15 @@ __device__ __forceinline__ void add_strain(const T* g, const T* u, T* e) {
 __device__ __host__ inline double tri4_wsum() { return ((-0.28125 + 0.260416666666666666666666666666665) + 0.260416666666666666666666666666665) + 0.260416666666666666666666666666665; }
 __device__ __host__ inline double tet5_wsum() { return (((-0.8 + 0.45) + 0.45) + 0.45) + 0.45; }
 
-// Block (la, lb) of an uncut simplex: kb = w (B_la^T D B_lb); with want_r also the residual of
+// Block (la, lb) of an uncut simplex with the given nodes: kb = w (B_la^T D B_lb); with want_r
+// also the residual of
 // row la, rv = w (B_la^T sigma).  Geometry from the node coordinates, stress from U (+ eps_macro).
 template <int DIM>
-__device__ __forceinline__ void simplex_block(const DevProblem& P, int e, int la, int lb, const double* D,
+__device__ __forceinline__ void simplex_block(const DevProblem& P, int4 nodes, int la, int lb, const double* D,
                                               double (*kb)[DIM], double* rv, bool want_r) {
   constexpr int NPE = DIM + 1;
   constexpr int NV = (DIM == 2) ? 3 : 6;
-  int nd[NPE];
-#pragma unroll
-  for (int n = 0; n < NPE; ++n) nd[n] = __ldg(&P.conn[(size_t)e * NPE + n]);
+  const int nd[4] = {nodes.x, nodes.y, nodes.z, nodes.w};
   double x[NPE][DIM], g[NPE][DIM], J;
 #pragma unroll
   for (int n = 0; n < NPE; ++n)
@@ -208,7 +207,8 @@ __host__ __device__ inline int general_slab_doubles(int slab_slots, int dim, int
 //   growd[node]      3*DIM ints: global DOF of each row, first slot in the row's F block, in its C block
 //   adesc[entry]     int4 {element, local node | nodes of a cut element << 8, slots (uncut: 8 bits per
 //                    node; cut: offset into adj_slots), material (uncut) / block-row offset (cut)}
-//   aresd[entry]     cut element index (cut entries)
+//   aresd[entry]     int4: uncut {element nodes (-1 padded)}; cut {cut element, its first node in
+//                    cut_nodes, the row node's cohesive place (element << 5 | position) or -1, 0}
 //   nbr_pre[slot]    free DOFs of the node's neighbours before this one (row positions)
 // Every lane of the warp must call it (valid = false for lanes without a node): the entry loop and
 // its warp synchronisations are warp-uniform.  G >= DIM + 1.
@@ -230,19 +230,18 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
   for (int o = 16; o > 0; o >>= 1) n_ent = max(n_ent, __shfl_xor_sync(0xffffffffu, n_ent, o));
   __syncwarp();
   // the next entry's descriptors are loaded while the current one is processed
-  int4 ad_next = make_int4(0, 0, 0, 0);
-  int cc_next = -1;
-  if (valid && gd.y > 0) { ad_next = __ldg(&P.adesc[gd.x]); cc_next = __ldg(&P.aresd[gd.x]); }
+  int4 ad_next = make_int4(0, 0, 0, 0), ax_next = make_int4(0, 0, 0, 0);
+  if (valid && gd.y > 0) { ad_next = __ldg(&P.adesc[gd.x]); ax_next = __ldg(&P.aresd[gd.x]); }
   for (int ei = 0; ei < n_ent; ++ei) {
     const bool have = valid && ei < gd.y;
-    const int4 ad = ad_next;
-    const int cc = ((ad.y >> 8) > 0) ? cc_next : -1;
-    if (valid && ei + 1 < gd.y) { ad_next = __ldg(&P.adesc[gd.x + ei + 1]); cc_next = __ldg(&P.aresd[gd.x + ei + 1]); }
+    const int4 ad = ad_next, ax = ax_next;
+    const int cc = ax.x;
+    if (valid && ei + 1 < gd.y) { ad_next = __ldg(&P.adesc[gd.x + ei + 1]); ax_next = __ldg(&P.aresd[gd.x + ei + 1]); }
     const int la = ad.y & 255, mn = ad.y >> 8;
     if (have && mn == 0) {
       if (g < NPE) {
         double kb[DIM][DIM], rv[DIM];
-        simplex_block<DIM>(P, ad.x, la, g, P.Dd + 36 * ad.w, kb, rv, g == 0);
+        simplex_block<DIM>(P, ax, la, g, P.Dd + 36 * ad.w, kb, rv, g == 0);
         double* ak = slab + ((((unsigned)ad.z) >> (8 * g)) & 255) * D2;
 #pragma unroll
         for (int i = 0; i < D2; ++i) ak[i] += kb[i / DIM][i % DIM];
@@ -251,10 +250,10 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
           for (int q = 0; q < DIM; ++q) rs[q] += rv[q];
       }
     } else if (have) {
-      const int base = __ldg(&P.cut_node_off[cc]);
+      const int base = ax.y;
       const int* cn = P.cut_nodes + base;
       const double* kr = P.ke + ad.w;                 // block row la of K_vol
-      const int cpa = __ldg(&P.cohpos[base + la]);    // (cohesive element << 5 | position) or -1
+      const int cpa = ax.z;                           // (cohesive element << 5 | position) or -1
       for (int b = g; b < mn; b += G) {
         double blk[D2];
 #pragma unroll
@@ -301,7 +300,7 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
 #pragma unroll
           for (int v = 0; v < NV; ++v) r[q] += gm[q * NV + v] * P.eps_macro[v];
       }
-      const int cpa = __ldg(&P.cohpos[__ldg(&P.cut_node_off[cc]) + la]);
+      const int cpa = ax.z;
       if (cpa >= 0) {
         const int ce = cpa >> 5, n1 = cpa & 31;
         const int nh = __ldg(&P.coh_nh[ce]);

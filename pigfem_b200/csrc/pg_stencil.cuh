@@ -91,6 +91,16 @@ __device__ __forceinline__ void part_iso(const T* d, const T* ga, int q, T* part
   }
 }
 
+// the nonzero entries of an isotropic D (36 entries, row-major) in lei_stress_iso's order
+template <int DIM, typename T>
+__device__ __forceinline__ void iso_from(const T* D, T* d) {
+  constexpr int n = (DIM == 2) ? 5 : 12;
+  constexpr int i2[5] = {0, 1, 3, 4, 8};
+  constexpr int i3[12] = {0, 1, 2, 6, 7, 8, 12, 13, 14, 21, 28, 35};
+#pragma unroll
+  for (int k = 0; k < n; ++k) d[k] = D[(DIM == 2) ? i2[k] : i3[k]];
+}
+
 template <int DIM, typename T>
 __device__ __forceinline__ void iso_d(const DevProblem& P, int m, T* d) {
   const int* idx;
@@ -116,14 +126,6 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
   const int sx = gi.nx + 1, sxy = sx * (gi.ny + 1);
   const int i = nid % sx, j = (nid / sx) % (gi.ny + 1), k = nid / sxy;
   const bool jac = (P.flags & FLAG_JAC) != 0;  // uniform over the launch
-  double dm[2][ND];
-  iso_d<DIM, double>(P, 0, dm[0]);
-  iso_d<DIM, double>(P, 1, dm[1]);
-  T dmk[2][ND];   // the tangent's D in the element-stiffness precision
-#pragma unroll
-  for (int m = 0; m < 2; ++m)
-#pragma unroll
-    for (int k2 = 0; k2 < ND; ++k2) dmk[m][k2] = (T)dm[m][k2];
   double acc[S::NN][QE - QB][DIM];
 #pragma unroll
   for (int s = 0; s < S::NN; ++s)
@@ -162,7 +164,10 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
 #pragma unroll
       for (int v = 0; v < NV; ++v) eps[v] += P.eps_macro[v];
     }
-    const double* d = m ? dm[1] : dm[0];
+    // D of the element's material from the descriptor (kernel parameter space), per element:
+    // keeping both materials' D in registers costs more registers than the loads
+    double d[ND];
+    iso_from<DIM, double>(P.D[m], d);
     double sig[NV];
     lei_stress_iso<DIM, double>(d, eps, sig);
     const int la = S::ent(a, 4);
@@ -173,7 +178,14 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
 #pragma unroll
       for (int dd = 0; dd < DIM; ++dd) gk[n][dd] = (T)g[n][dd];
     const T wk = (T)w;
-    const T* dk = m ? dmk[1] : dmk[0];
+    T dkv[ND];   // the tangent's D in the element-stiffness precision
+    if constexpr (sizeof(T) == sizeof(double)) {
+#pragma unroll
+      for (int k2 = 0; k2 < ND; ++k2) dkv[k2] = (T)d[k2];
+    } else {
+      iso_from<DIM, T>(P.Df[m], dkv);
+    }
+    const T* dk = dkv;
 #pragma unroll
     for (int q = QB; q < QE; ++q) {
       r[q - QB] += w * bt_sig<DIM, double>(g[la], sig, q);
