@@ -103,8 +103,8 @@ int pg_get_nodes(const pg_ctx* ctx, double* coords, int32_t* node_dofs, double* 
  * trial = committed, updated by the cohesive laws (read with pg_get_isv). */
 int pg_assemble(pg_ctx* ctx, const double* U_node_major, double t_frac, int flags,
                 double* K_ff, double* K_fp, double* K_pf, double* K_pp, double* P_f, double* P_p);
-/* Same, on device-resident data: d_U is a device pointer (n_nodes*dim); results stay in the
- * context's device buffers (pg_device_outputs). */
+/* Same, on device-resident data: d_U is a 16-byte aligned device pointer (n_nodes*dim); results
+ * stay in the context's device buffers (pg_device_outputs). */
 int pg_assemble_device(pg_ctx* ctx, const double* d_U, double t_frac, int flags);
 /* Device pointers of the outputs: K values (4 blocks), P_f, P_p. */
 int pg_device_outputs(pg_ctx* ctx, double** K_vals4, double** P_f, double** P_p);

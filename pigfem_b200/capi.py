@@ -67,11 +67,13 @@ class _Sizes(ctypes.Structure):
 _lib = None
 
 
-def load_library(path: str = LIB_PATH):
-    """Load libpigfem_b200.so and declare its signatures; raises if it is missing."""
+def load_library(path: Optional[str] = None):
+    """Load libpigfem_b200.so (or the build named by PIGFEM_B200_LIB) and declare its signatures;
+    raises if it is missing."""
     global _lib
     if _lib is not None:
         return _lib
+    path = path or os.environ.get("PIGFEM_B200_LIB") or LIB_PATH
     if not os.path.exists(path):
         raise FileNotFoundError(f"{path} is missing: build it first (make -C pigfem_b200/csrc)")
     L = ctypes.CDLL(path)

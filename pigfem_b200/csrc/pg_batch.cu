@@ -322,8 +322,10 @@ int pg_batch_create(pg_ctx* const* ctxs, int n, pg_batch** out) {
 int pg_batch_assemble(pg_batch* b, const double* const* d_U, const double* t_frac, int flags) {
   if (!b || !d_U) return PG_ERR_INPUT;
   if (b->launched && cudaEventSynchronize(b->t1) != cudaSuccess) return berr(b, PG_ERR_DEVICE, "previous batch failed");
-  for (size_t i = 0; i < b->ctx.size(); ++i)
+  for (size_t i = 0; i < b->ctx.size(); ++i) {
     if (!d_U[i]) return berr(b, PG_ERR_INPUT, "missing displacement pointer");
+    if (reinterpret_cast<uintptr_t>(d_U[i]) % 16) return berr(b, PG_ERR_INPUT, "displacement arrays must be 16-byte aligned");
+  }
   fill_call(b, d_U, t_frac, flags);
   cudaGraphExec_t e;
   if (int rc = graph_for(b, (flags & PG_FP32) != 0, &e)) return rc;

@@ -687,6 +687,7 @@ int pg_set_stream(pg_ctx* c, void* stream) {
 
 int pg_assemble_device(pg_ctx* c, const double* d_U, double t_frac, int flags) {
   if (!c || !d_U) return PG_ERR_INPUT;
+  if (reinterpret_cast<uintptr_t>(d_U) % 16) return set_err(c, PG_ERR_INPUT, "the displacement array must be 16-byte aligned");
   if (!(flags & (PG_FUNC | PG_JAC))) return 0;
   double* keep = c->d_U;
   c->d_U = const_cast<double*>(d_U);

@@ -250,6 +250,21 @@ __device__ inline void coh_law(const CohConst& c, int dim, double* delta, double
   }
 }
 
+// The DIM components of a node-major array at `node` (coordinates, displacements): one 16-byte
+// load in 2D (the arrays are 16-byte aligned; pg_assemble_device checks a caller's U), DIM loads
+// in 3D.  Read-only for the whole kernel.
+template <int DIM>
+__device__ __forceinline__ void load_node(const double* __restrict__ A, int node, double* v) {
+  if constexpr (DIM == 2) {
+    const double2 t = __ldg(reinterpret_cast<const double2*>(A) + node);
+    v[0] = t.x;
+    v[1] = t.y;
+  } else {
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = __ldg(&A[(size_t)node * DIM + d]);
+  }
+}
+
 // Voigt B-matrix entry B(r, k*dim + q) for a node with gradient g (dim entries).
 template <typename T>
 __device__ inline T bmat(int dim, int r, int q, const T* g) {

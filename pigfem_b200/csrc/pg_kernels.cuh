@@ -140,9 +140,7 @@ __device__ __forceinline__ void simplex_block(const DevProblem& P, int4 nodes, i
   const int nd[4] = {nodes.x, nodes.y, nodes.z, nodes.w};
   double x[NPE][DIM], g[NPE][DIM], J;
 #pragma unroll
-  for (int n = 0; n < NPE; ++n)
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) x[n][d] = __ldg(&P.X[(size_t)nd[n] * DIM + d]);
+  for (int n = 0; n < NPE; ++n) load_node<DIM>(P.X, nd[n], x[n]);
   simplex_geom<DIM, double>(x, g, &J);
   const double wgt = J * ((DIM == 2) ? tri4_wsum() : tet5_wsum());
   double ga[DIM], gb[DIM];
@@ -171,8 +169,7 @@ __device__ __forceinline__ void simplex_block(const DevProblem& P, int4 nodes, i
 #pragma unroll
     for (int n = 0; n < NPE; ++n) {
       double u[DIM];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) u[d] = __ldg(&P.U[(size_t)nd[n] * DIM + d]);
+      load_node<DIM>(P.U, nd[n], u);
       add_strain<DIM, double>(g[n], u, eps);
     }
     if (P.subscale) {
@@ -189,7 +186,23 @@ __device__ __forceinline__ void simplex_block(const DevProblem& P, int4 nodes, i
 // Shared-memory doubles of one lane group: slab_slots blocks of DIM x DIM, the node's residual (4
 // doubles reserved) and the per-block residual partials of one cut element (max_mn x DIM).
 __host__ __device__ inline int general_slab_doubles(int slab_slots, int dim, int max_mn) {
-  return (slab_slots * dim * dim + 4 + max_mn * dim) | 1;   // odd: groups start on different banks
+  // even (16-byte aligned groups) and 2 mod 4, so consecutive groups start on different banks
+  int n = (slab_slots * dim * dim + 4 + max_mn * dim + 1) & ~1;
+  return (n % 4 == 0) ? n + 2 : n;
+}
+
+// slab block += v (DIM x DIM); 16-byte shared-memory accesses in 2D
+template <int DIM>
+__device__ __forceinline__ void slab_add(double* ak, const double* v) {
+  if constexpr (DIM == 2) {
+    double2* a2 = reinterpret_cast<double2*>(ak);
+    double2 t0 = a2[0], t1 = a2[1];
+    t0.x += v[0]; t0.y += v[1]; t1.x += v[2]; t1.y += v[3];
+    a2[0] = t0; a2[1] = t1;
+  } else {
+#pragma unroll
+    for (int i = 0; i < DIM * DIM; ++i) ak[i] += v[i];
+  }
 }
 
 // Row assembly for the DOF nodes the stencil path does not take (boundary rows, nodes of cut
@@ -243,8 +256,7 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
         double kb[DIM][DIM], rv[DIM];
         simplex_block<DIM>(P, ax, la, g, P.Dd + 36 * ad.w, kb, rv, g == 0);
         double* ak = slab + ((((unsigned)ad.z) >> (8 * g)) & 255) * D2;
-#pragma unroll
-        for (int i = 0; i < D2; ++i) ak[i] += kb[i / DIM][i % DIM];
+        slab_add<DIM>(ak, &kb[0][0]);
         if (g == 0)
 #pragma unroll
           for (int q = 0; q < DIM; ++q) rs[q] += rv[q];
@@ -256,12 +268,17 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
       const int cpa = ax.z;                           // (cohesive element << 5 | position) or -1
       for (int b = g; b < mn; b += G) {
         double blk[D2];
+        if constexpr (DIM == 2) {   // a 2 x 2 block: 32 bytes, 32-byte aligned in the cache
+          const double2 b0 = __ldg(reinterpret_cast<const double2*>(kr + b * D2));
+          const double2 b1 = __ldg(reinterpret_cast<const double2*>(kr + b * D2) + 1);
+          blk[0] = b0.x; blk[1] = b0.y; blk[2] = b1.x; blk[3] = b1.y;
+        } else {
 #pragma unroll
-        for (int i = 0; i < D2; ++i) blk[i] = kr[b * D2 + i];
+          for (int i = 0; i < D2; ++i) blk[i] = kr[b * D2 + i];
+        }
         const int nb = __ldg(&cn[b]);
         double u[DIM];
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) u[d] = P.U[(size_t)nb * DIM + d];
+        load_node<DIM>(P.U, nb, u);
 #pragma unroll
         for (int q = 0; q < DIM; ++q) {
           double s = 0.0;
@@ -281,8 +298,7 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
           }
         }
         double* ak = slab + __ldg(&P.adj_slots[ad.z + b]) * D2;
-#pragma unroll
-        for (int i = 0; i < D2; ++i) ak[i] += blk[i];
+        slab_add<DIM>(ak, blk);
       }
     }
     __syncwarp();

@@ -146,11 +146,8 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
     for (int n = 0; n < NPE; ++n) {
       const int sl = S::ent(a, 5 + n);
       const int id = nid + S::off(sl, 0) + S::off(sl, 1) * sx + S::off(sl, 2) * sxy;
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        x[n][d] = __ldg(&P.X[(size_t)id * DIM + d]);
-        u[n][d] = __ldg(&P.U[(size_t)id * DIM + d]);
-      }
+      load_node<DIM>(P.X, id, x[n]);
+      load_node<DIM>(P.U, id, u[n]);
     }
     // geometry, strain, stress and the internal force in FP64 (the Newton residual)
     simplex_geom<DIM, double>(x, g, &J);
