@@ -35,6 +35,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from pigfem_b200 import replicas  # noqa: E402  (no torch / CUDA import at module load)
+
 METRIC = "assembled elems/s (K+R) FP64 vs FP32-mixed; served RVE req/s with p50/p99"
 UNIT = "elements/s"
 L2_FLUSH_BYTES = 256 << 20
@@ -61,10 +63,7 @@ def parse():
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    return replicas.dist_env()
 
 
 def algorithmic_bytes(P, fp32: bool) -> dict:
@@ -286,7 +285,6 @@ def main_batched(args, ws, rank, local):
     autotuned shape) in FP32-mixed (the value) and FP64, beside the plain path (one
     pg_assemble_device call per RVE, FP64)."""
     import torch
-    import torch.distributed as dist
     from concurrent.futures import ThreadPoolExecutor
     from pigfem_b200 import capi, rve
     t_setup = time.time()
@@ -311,8 +309,7 @@ def main_batched(args, ws, rank, local):
         for _ in range(warmup):
             B.assemble(ptrs, flags)
             B.wait()
-        if ws > 1:
-            dist.barrier()
+        replicas.barrier()
         total = 0.0
         for _ in range(steps):
             flush.zero_()
@@ -376,18 +373,15 @@ def main_batched(args, ws, rank, local):
         if it > 0:
             e2e_ms += a.elapsed_time(b)
     clk.__exit__(None, None, None)
-    value32 = ws * ne * args.steps / (ms32 * 1e-3)
-    value64 = ws * ne * args.steps / (ms64 * 1e-3)
-    value_plain = ws * ne * plain_steps / (ms_plain * 1e-3)
-    e2e_value = ws * ne * e2e_steps / (e2e_ms * 1e-3)
+    ms32, ms64, ms_plain, e2e_ms = replicas.max_over_ranks([ms32, ms64, ms_plain, e2e_ms], "cuda")
+    value32 = replicas.aggregate_rate(ne * args.steps, ws, ms32)
+    value64 = replicas.aggregate_rate(ne * args.steps, ws, ms64)
+    value_plain = replicas.aggregate_rate(ne * plain_steps, ws, ms_plain)
+    e2e_value = replicas.aggregate_rate(ne * e2e_steps, ws, e2e_ms)
     alg = sum(algorithmic_bytes(P, True)["total"] for P in probs)
     peak, peak_kind = measured_peak_hbm()
     achieved = alg / (ms32 / args.steps * 1e-3) / 1e9
-    if ws > 1:
-        t = torch.tensor([ms32, ms64, ms_plain, e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish()
     if rank != 0:
         return
     line = {
@@ -447,6 +441,9 @@ def main_serving(args, ws, rank, local):
         summ["mean_gpu_s"] = float(np.mean([r.done - r.admitted for r in res]))
         sweep.append(summ)
     clk.__exit__(None, None, None)
+    # whole-job request rates: each rank serves its own stream
+    for summ in sweep:
+        summ["req_per_s"] = replicas.sum_over_ranks([summ["req_per_s"] or 0.0], "cuda")[0]
     best = max(sweep, key=lambda x: x["req_per_s"] or 0)
     if rank != 0:
         return
@@ -474,25 +471,21 @@ def main():
         run_reference(args, ws, rank)
         return
     if args.workload == "serving":
+        import torch
+        torch.cuda.set_device(local)
+        replicas.init("nccl", local, timeout_s=600)
         main_serving(args, ws, rank, local)
+        replicas.finish()
         return
     if args.workload == "batched_2d_256":
         import torch
-        import torch.distributed as dist
         torch.cuda.set_device(local)
-        if ws > 1:
-            import datetime
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                    device_id=torch.device("cuda", local))
+        replicas.init("nccl", local, timeout_s=300)
         main_batched(args, ws, rank, local)
         return
     import torch
-    import torch.distributed as dist
     torch.cuda.set_device(local)
-    if ws > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    replicas.init("nccl", local)
     from pigfem_b200 import capi
     R, P, U = build_problem(args, rank)
     ne = P.sizes["n_elem"]
@@ -517,8 +510,7 @@ def main():
         for _ in range(warmup):
             step_device(flags)
         torch.cuda.synchronize()
-        if ws > 1:
-            dist.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         for i in range(steps):
@@ -528,11 +520,8 @@ def main():
             ev[i][1].record(stream)
         torch.cuda.synchronize()
         ms = float(sum(a.elapsed_time(b) for a, b in ev))
-        if ws > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-            dist.barrier()
+        ms = replicas.max_over_ranks([ms], "cuda")[0]
+        replicas.barrier()
         torch.cuda.synchronize()
         return ms
 
@@ -575,8 +564,7 @@ def main():
     for _ in range(args.warmup):
         step_host()
     torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
+    replicas.barrier()
     e2e_ms = 0.0
     for _ in range(args.e2e_steps or args.steps):
         flush.zero_()
@@ -586,10 +574,7 @@ def main():
         b.record(stream)
         b.synchronize()
         e2e_ms += a.elapsed_time(b)
-    if ws > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = replicas.max_over_ranks([e2e_ms], "cuda")[0]
     clk.__exit__(None, None, None)
     e2e_steps = args.e2e_steps or args.steps
     e2e_value = ws * ne * e2e_steps / (e2e_ms * 1e-3)
@@ -639,9 +624,7 @@ def main():
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }
-    if ws > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish()
     if line is not None:
         print(json.dumps(line))
 
