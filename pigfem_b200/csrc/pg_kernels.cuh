@@ -254,7 +254,7 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
     if (have && mn == 0) {
       if (g < NPE) {
         double kb[DIM][DIM], rv[DIM];
-        simplex_block<DIM>(P, ax, la, g, P.Dd + 36 * ad.w, kb, rv, g == 0);
+        simplex_block<DIM>(P, ax, la, g, P.D[ad.w], kb, rv, g == 0);   // D from the parameter space
         double* ak = slab + ((((unsigned)ad.z) >> (8 * g)) & 255) * D2;
         slab_add<DIM>(ak, &kb[0][0]);
         if (g == 0)
