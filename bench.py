@@ -115,6 +115,34 @@ def fast_kernel_bytes(P, fp32: bool) -> float:
     return float(total)
 
 
+def general_kernel_bytes(P, fp32: bool) -> float:
+    """Algorithmic bytes of the general-row kernel (boundary rows, nodes of cut elements and
+    enrichment nodes): the CSR values and residual entries of its rows, connectivity/material of
+    the elements adjacent to them, a 4 B sub-element table index per cut element, and the
+    coordinates and U of the nodes their rows couple to."""
+    s = P.sizes
+    dim = s["dim"]
+    comp = 4 if fp32 else 8
+    slow = P.debug("slow_dn")
+    dn_node = P.debug("dn_node")
+    _, dofs, _ = P.nodes()
+    nf = P.n_free
+    rows = dofs[dn_node[slow]].reshape(-1)
+    total = 0
+    for blocks, sel, off in (((0, 1), rows < nf, 0), ((2, 3), rows >= nf, nf)):
+        r = rows[sel] - off
+        for b in blocks:
+            rp, _, _ = P.pattern(b)
+            total += 8 * int(np.sum(rp[r + 1] - rp[r]))
+    total += 8 * len(rows)
+    ao, adj = P.debug("dn_adj_off"), P.debug("dn_adj")
+    no, nbr = P.debug("dn_nbr_off"), P.debug("dn_nbr")
+    elems = np.unique(np.concatenate([adj[ao[a]:ao[a + 1]] >> 5 for a in slow])) if len(slow) else np.zeros(0, int)
+    nodes = np.unique(np.concatenate([nbr[no[a]:no[a + 1]] for a in slow])) if len(slow) else np.zeros(0, int)
+    total += (4 * (dim + 1) + 4) * len(elems) + 4 * s["n_cut_elem"] + 2 * comp * dim * len(nodes)
+    return float(total)
+
+
 def launches_per_step(P) -> int:
     """Kernels one assembly launches: cohesive points, stencil rows and general rows, each only
     when it has work (the L2 flush between steps is a torch fill, not counted)."""
@@ -594,6 +622,10 @@ def main():
         extra = 5 * (8 * (P.n_free + P.n_const) + 8 * 3 * P.sizes["n_nodes"])
         alg["total"] += extra
     stencil_name = f"k_rows_stencil<{P.dim},double>"
+    general_name = f"k_rows_general<{P.dim},{4 if P.dim == 2 else 32}>"
+    gk_bytes = general_kernel_bytes(P, False)
+    gk_ms = float(kt64[2])
+    g_achieved = gk_bytes / (gk_ms * 1e-3) / 1e9 if gk_ms > 0 else None
 
     line = None
     if rank == 0:
@@ -618,6 +650,11 @@ def main():
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": profiled_traffic(stencil_name), "bytes_per_launch": fk_bytes,
                          "traffic_note": "ncu dram read+write per launch, cold cache; row writes still in L2 at kernel end are not counted"},
+            # the longest-running kernel (the stencil kernel above moves most of the bytes)
+            "roofline_general": {"bound": "hbm", "kernel": f"{general_name} (main stream, after the cohesive elements, sharing the SMs with the stencil rows)",
+                                 "achieved": g_achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                                 "frac": (g_achieved / peak) if g_achieved else None,
+                                 "traffic": profiled_traffic(general_name), "bytes_per_launch": gk_bytes},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_ms / e2e_steps, "steps": e2e_steps},
             "gpu_launches": launches_per_step(P) * n_rhs * args.steps,
