@@ -63,6 +63,8 @@ def lib():
                                 ctypes.POINTER(ctypes.c_void_p)]
         L.pgref_homogenize.restype = None
         L.pgref_homogenize.argtypes = [ctypes.c_void_p]
+        L.pgref_write_homogenization.restype = None
+        L.pgref_write_homogenization.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_double, ctypes.c_int]
         L.pgref_set_macro.restype = None
         L.pgref_set_macro.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.pgref_destroy.restype = None
@@ -152,6 +154,10 @@ class RefProblem:
     def homogenize(self) -> np.ndarray:
         lib().pgref_homogenize(self.h)
         return self.get("homogenized")
+
+    def write_homogenization(self, filename: str, t: float, step: int):
+        """The reference's WriterHomogenization::writeConsecutive on the current state."""
+        lib().pgref_write_homogenization(self.h, filename.encode(), float(t), int(step))
 
     def set_macro(self, eps):
         e = np.zeros(6)

@@ -70,6 +70,7 @@
 #include "Utilities.h"
 #include "CohesiveElem.h"
 #include "pgshim_objects.h"
+#include "WriterHomogenization.h"
 #undef protected
 #undef private
 
@@ -479,6 +480,14 @@ void pgref_homogenize(void* vh) {
   h->prob->homogenize();
   Export& e = put_d(h, "homogenized");
   e.f64 = h->prob->getHomogenizedValue();
+}
+
+/* WriterHomogenization::writeConsecutive (src/WriterHomogenization.cpp:41-61) on the current
+ * macroscale value and the last pgref_homogenize result: the reference's homogenization CSV. */
+void pgref_write_homogenization(void* vh, const char* filename, double t, int step) {
+  Handle* h = (Handle*)vh;
+  WriterHomogenization w(h->prob);
+  w.writeConsecutive(filename, t, (id_type)step);
 }
 
 /* Problem::setMacroscaleValue (include/Problem.h:310): the macroscale strain of a subscale problem;

@@ -17,6 +17,7 @@ step below min_dt) is not restated: the driver stops with NewtonFailure there in
 from __future__ import annotations
 
 import math
+import time
 from dataclasses import dataclass, field
 from typing import List
 
@@ -39,6 +40,7 @@ class StepRecord:
     convergence: int
     res_norm: float
     nr_norms: List[float] = field(default_factory=list)
+    nr_times: List[float] = field(default_factory=list)   # seconds of each Newton correction
 
 
 @dataclass
@@ -47,6 +49,10 @@ class SolveResult:
     U_free: np.ndarray
     isv: np.ndarray
     failed: str = ""      # why the run stopped early (raise_on_failure=False), else empty
+
+    def log(self) -> str:
+        """The run's solver log in the reference's text (format_log)."""
+        return format_log(self.steps)
 
 
 class LoadStepper:
@@ -76,10 +82,14 @@ class LoadStepper:
         res = self.assemble(t_frac)
         res0 = res
         norms = [res]
+        self._times = times = []
         it = 0
         increase = 0
         while True:
-            if not self.correct():
+            t0 = time.perf_counter()
+            ok = self.correct()
+            times.append(time.perf_counter() - t0)
+            if not ok:
                 return False, float("nan"), norms
             prev = res
             res = self.assemble(t_frac)
@@ -131,7 +141,7 @@ class LoadStepper:
                 else:
                     conv = -1
                     self.restore()
-                records.append(StepRecord(step_iter + 1, t, dt, repeat, conv, res, norms))
+                records.append(StepRecord(step_iter + 1, t, dt, repeat, conv, res, norms, list(self._times)))
                 dt, t = self._update_time_step(dt, t, converged, repeat)
             self.commit()
             self.save()
@@ -249,21 +259,55 @@ class NewtonSolver(LoadStepper):
         return SolveResult(records, self.U[: self.nf].cpu().numpy(), isv)
 
 
+LOG_HEADER = ("\n\nStarting time step algorithm.\n"
+              "Cnv cheatsheet:\n  1: Converged\n -1: NR-diverged\n -2: Large damage rate\n"
+              "LStp      T(s)      TStep(s)    Rpt   Cnv    Res\n"
+              "----   ----------   --------    ---   ---  --------\n")
+
+
+def _g(x: float) -> str:
+    """A double as a C++ stream prints it by default (%g, 6 significant digits)."""
+    return "%g" % x
+
+
+def format_log(records: List[StepRecord]) -> str:
+    """The solver log of a run in the reference's own text: the table header
+    (src/SolverNonlinear.cpp:111-114), the Newton lines of every attempt
+    (src/SolverNonlinearKSP.cpp:89, 117), "REPEATING LOADSTEP" after an attempt that failed
+    (src/SolverNonlinear.cpp:225) and the load-step line (src/SolverNonlinear.cpp:241-246), so that
+    a run's log reads, and parses, like a reference run's."""
+    out = [LOG_HEADER]
+    for r in records:
+        for k, res in enumerate(r.nr_norms):
+            if k == 0:
+                out.append("\tNR iteration: 0 Residual: %s\n" % _g(res))
+            else:
+                dt = r.nr_times[k - 1] if k - 1 < len(r.nr_times) else 0.0
+                out.append("\tNR iteration: %d Iteration_Time: %s \tResidual: %s\n" % (k, _g(dt), _g(res)))
+        if r.convergence != 1:
+            out.append("REPEATING LOADSTEP\n")
+        out.append(" %d     %1.5e  %1.2e     %d     %d   %1.2e\n" % (r.step, r.t, r.dt, r.repeat, r.convergence,
+                                                                      r.res_norm))
+    return "".join(out)
+
+
 def parse_reference_log(log: str):
     """Load-step table and Newton norms from the reference's solver log (the lines printed by
     src/SolverNonlinear.cpp:241-246 and src/SolverNonlinearKSP.cpp:71, 106)."""
-    steps, nr = [], []
+    steps, nr, times = [], [], []
     for line in log.splitlines():
         s = line.strip()
         if s.startswith("NR iteration:"):
             nr.append(float(s.split("Residual:")[-1]))
+            if "Iteration_Time:" in s:
+                times.append(float(s.split("Iteration_Time:")[1].split()[0]))
             continue
         parts = s.split()
         if len(parts) == 6 and parts[0].isdigit():
             try:
                 steps.append(StepRecord(int(parts[0]), float(parts[1]), float(parts[2]), int(parts[3]), int(parts[4]),
-                                        float(parts[5]), nr))
+                                        float(parts[5]), nr, times))
             except ValueError:
                 continue
-            nr = []
+            nr, times = [], []
     return steps

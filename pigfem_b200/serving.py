@@ -175,6 +175,15 @@ def run_request(P: capi.Problem, req: Request, stream) -> Dict[str, np.ndarray]:
         return {"residual_norm": np.array([res]), "zones": np.bincount(zones, minlength=4).astype(np.int64)}
 
 
+def homogenization_csv(result: Result) -> str:
+    """A homogenization request's result as the reference's homogenization CSV
+    (WriterHomogenization): one row per unit macroscale strain e_k at t = 1, ``1, e_k..., C[:, k]...``."""
+    from . import writers
+    C = result.values["C"]
+    nv = C.shape[0]
+    return writers.homogenization_table(1.0, np.eye(nv), C.T)
+
+
 def run_alone(req: Request) -> Result:
     """One request by itself: set-up, upload, work, free (the one-at-a-time plain FP64 call)."""
     import torch
