@@ -40,7 +40,8 @@ extern "C" {
 #define PG_QUAD4 1
 #define PG_TET4 2
 
-/* cohesive laws: bilinear, Xu-Needleman, Ortiz-Pandolfi (plain, no-unloading "NU", augmented "AUG") */
+/* cohesive laws: bilinear, Xu-Needleman, Ortiz-Pandolfi (plain, no-unloading "NU", augmented
+ * "AUG"), trilinear and smoothed trilinear (plain and "NU") */
 #define PG_COH_NONE 0
 #define PG_COH_BL 1
 #define PG_COH_BLNU 2
@@ -50,6 +51,10 @@ extern "C" {
 #define PG_COH_OPNU 6
 #define PG_COH_OPAUG 7
 #define PG_COH_OPNUAUG 8
+#define PG_COH_TL 9         /* TrilinearCohesiveMaterial (src/Material_TrilinearCohesive.cpp) */
+#define PG_COH_TLNU 10      /* TrilinearCohesiveNUMaterial (src/Material_TrilinearCohesiveNU.cpp) */
+#define PG_COH_STL 11       /* TrilinearSmoothedCohesiveMaterial (src/Material_SmoothedTrilinearCohesive.cpp) */
+#define PG_COH_STLNU 12     /* TrilinearSmoothedCohesiveNUMaterial (src/Material_SmoothedTrilinearCohesiveNU.cpp) */
 
 typedef struct pg_ctx pg_ctx;
 
@@ -62,7 +67,8 @@ typedef struct {
   const double* incl;           /* circles: cx, cy, r; spheres: cx, cy, cz, r */
   double E_matrix, nu_matrix, E_fiber, nu_fiber;
   int32_t coh_law;              /* PG_COH_*; applied to every fiber/matrix interface */
-  double coh[4];                /* BL: sigma_c, delta_c1, delta_c2; XN: sigma_c, delta_cn, delta_ct, q; OP: sigma_c, delta_c, beta */
+  double coh[4];                /* BL: sigma_c, delta_c1, delta_c2; XN: sigma_c, delta_cn, delta_ct, q; OP: sigma_c, delta_c, beta;
+                                   TL, STL: sigma_c, delta_c1, delta_c2, delta_c3 (0 < delta_c1 <= delta_c2 <= delta_c3) */
   int32_t plane_strain;
   int32_t subscale;             /* 1: periodic mesh, macroscale strain eps_macro, node 0 pinned */
   double eps_macro[6];          /* Voigt (xx, yy, xy) or (xx, yy, zz, yz, xz, xy), engineering shear */

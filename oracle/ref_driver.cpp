@@ -64,6 +64,10 @@
 #include "Material_OPCohesiveNU.h"
 #include "Material_OPCohesiveAug.h"
 #include "Material_OPCohesiveNUAug.h"
+#include "Material_TrilinearCohesive.h"
+#include "Material_TrilinearCohesiveNU.h"
+#include "Material_SmoothedTrilinearCohesive.h"
+#include "Material_SmoothedTrilinearCohesiveNU.h"
 #include "InclusionCircle.h"
 #include "InclusionSphere.h"
 #include "Options.h"
@@ -89,7 +93,11 @@ enum {
   PGREF_COH_OP = 5,      /* OPCohesiveMaterial:        SIGMA_C, DELTA_C, BETA */
   PGREF_COH_OPNU = 6,    /* OPCohesiveNUMaterial */
   PGREF_COH_OPAUG = 7,   /* OPCohesiveAugMaterial */
-  PGREF_COH_OPNUAUG = 8  /* OPCohesiveNUAugMaterial */
+  PGREF_COH_OPNUAUG = 8, /* OPCohesiveNUAugMaterial */
+  PGREF_COH_TL = 9,      /* TrilinearCohesiveMaterial: SIGMA_C, DELTA_C1, DELTA_C2, DELTA_C3 */
+  PGREF_COH_TLNU = 10,   /* TrilinearCohesiveNUMaterial */
+  PGREF_COH_STL = 11,    /* TrilinearSmoothedCohesiveMaterial */
+  PGREF_COH_STLNU = 12   /* TrilinearSmoothedCohesiveNUMaterial */
 };
 
 typedef struct {
@@ -161,11 +169,18 @@ Material* make_cohesive(int law, const double* p) {
     case PGREF_COH_OPNU: m = new OPCohesiveNUMaterial; break;
     case PGREF_COH_OPAUG: m = new OPCohesiveAugMaterial; break;
     case PGREF_COH_OPNUAUG: m = new OPCohesiveNUAugMaterial; break;
+    case PGREF_COH_TL: m = new TrilinearCohesiveMaterial; break;
+    case PGREF_COH_TLNU: m = new TrilinearCohesiveNUMaterial; break;
+    case PGREF_COH_STL: m = new TrilinearSmoothedCohesiveMaterial; break;
+    case PGREF_COH_STLNU: m = new TrilinearSmoothedCohesiveNUMaterial; break;
     default: return nullptr;
   }
   m->set_name("Interface");
   if (law == PGREF_COH_BL || law == PGREF_COH_BLNU) {
     m->set_parameter("SIGMA_C", p[0]); m->set_parameter("DELTA_C1", p[1]); m->set_parameter("DELTA_C2", p[2]);
+  } else if (law >= PGREF_COH_TL) {
+    m->set_parameter("SIGMA_C", p[0]); m->set_parameter("DELTA_C1", p[1]); m->set_parameter("DELTA_C2", p[2]);
+    m->set_parameter("DELTA_C3", p[3]);
   } else if (law == PGREF_COH_XN || law == PGREF_COH_XNNU) {
     m->set_parameter("SIGMA_C", p[0]); m->set_parameter("DELTA_CN", p[1]); m->set_parameter("DELTA_CT", p[2]); m->set_parameter("Q", p[3]);
   } else {

@@ -25,6 +25,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libpigfem_b200.so")
 
 TRI3, QUAD4, TET4 = 0, 1, 2
 COH_NONE, COH_BL, COH_BLNU, COH_XN, COH_XNNU, COH_OP, COH_OPNU, COH_OPAUG, COH_OPNUAUG = range(9)
+COH_TL, COH_TLNU, COH_STL, COH_STLNU = range(9, 13)   # trilinear and smoothed trilinear
 FUNC, JAC, FP32 = 1, 2, 4
 ERRORS = {2: "PG_ERR_INPUT", 3: "PG_ERR_GEOMETRY", 4: "PG_ERR_UNSUPPORTED", 7: "PG_ERR_JACOBIAN",
           10: "PG_ERR_DEVICE", 11: "PG_ERR_NONFINITE", 12: "PG_ERR_STATE"}

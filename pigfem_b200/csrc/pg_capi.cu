@@ -373,7 +373,7 @@ int pg_upload(pg_ctx* c) {
   for (int m = 0; m < 2; ++m) for (int i = 0; i < 36; ++i) { P.D[m][i] = s.D[m][i]; P.Df[m][i] = (float)s.D[m][i]; }
   P.coh.law = s.coh.law; P.coh.nvar = s.coh.nvar; P.coh.sigma_c = s.coh.sigma_c; P.coh.delta_c1 = s.coh.delta_c1;
   P.coh.delta_c2 = s.coh.delta_c2; P.coh.delta_cn = s.coh.delta_cn; P.coh.delta_ct = s.coh.delta_ct; P.coh.q = s.coh.q;
-  P.coh.delta_c = s.coh.delta_c; P.coh.beta2 = s.coh.beta2; P.coh.alpha = s.coh.alpha;
+  P.coh.delta_c = s.coh.delta_c; P.coh.beta2 = s.coh.beta2; P.coh.alpha = s.coh.alpha; P.coh.delta_c3 = s.coh.delta_c3;
   {
     std::vector<double> Dh(72);
     std::vector<float> Dfh(72);

@@ -19,13 +19,15 @@ namespace pgd {
 
 constexpr int kMaxNodesCut = 32;  // element-local node slots (parent + enrichment); matches the set-up encoding
 
-enum { COH_NONE = 0, COH_BL = 1, COH_BLNU = 2, COH_XN = 3, COH_XNNU = 4, COH_OP = 5, COH_OPNU = 6, COH_OPAUG = 7, COH_OPNUAUG = 8 };
+enum { COH_NONE = 0, COH_BL = 1, COH_BLNU = 2, COH_XN = 3, COH_XNNU = 4, COH_OP = 5, COH_OPNU = 6, COH_OPAUG = 7, COH_OPNUAUG = 8,
+       COH_TL = 9, COH_TLNU = 10, COH_STL = 11, COH_STLNU = 12 };
 enum { FLAG_FUNC = 1, FLAG_JAC = 2, FLAG_FP32 = 4 };
 enum { ERR_NONFINITE = 1, ERR_CUT_OVERFLOW = 2, ERR_BAD_SLOT = 4 };
 
 struct CohConst {
   int law, nvar;
   double sigma_c, delta_c1, delta_c2, delta_cn, delta_ct, q, delta_c, beta2, alpha;
+  double delta_c3;
 };
 
 // Everything one assembly launch reads or writes, as device pointers.
@@ -95,6 +97,39 @@ struct DevProblem {
 // ---------------------------------------------------------------- cohesive laws (FP64)
 // x^2 as one correctly rounded product (what pow(x, 2) returns on the reference's host).
 __device__ __forceinline__ double sq(double x) { return x * x; }
+
+// Effective traction of the trilinear laws at effective opening d: linear rise to sigma_c at
+// delta_c1, plateau to delta_c2, linear fall to 0 at delta_c3
+// (src/Material_TrilinearCohesiveNU.cpp:90-113); the smoothed laws rise along 2v - v^2 and fall
+// along 2v^3 - 3v^2 + 1 (src/Material_SmoothedTrilinearCohesiveNU.cpp:98-121).  `unload` gives
+// the traction at a historical maximum as the unloading branches write it
+// (src/Material_TrilinearCohesive.cpp:90-98, src/Material_SmoothedTrilinearCohesive.cpp:97-113).
+__device__ inline void trilinear_curve(const CohConst& c, bool smooth, bool unload, double d, double* t, double* dt) {
+  *dt = 0.0;
+  if (d >= 0 && d < c.delta_c1) {
+    if (smooth) {
+      const double v = d / c.delta_c1;
+      *t = c.sigma_c * (2.0 * v - sq(v));
+      *dt = c.sigma_c * ((2.0 / c.delta_c1) * (1.0 - v));
+    } else {
+      *t = unload ? d * (c.sigma_c / c.delta_c1) : c.sigma_c * (d / c.delta_c1);
+      *dt = c.sigma_c / c.delta_c1;
+    }
+  } else if (d >= c.delta_c1 && d < c.delta_c2) {
+    *t = c.sigma_c;
+  } else if (d >= c.delta_c2 && d < c.delta_c3) {
+    if (smooth) {
+      const double v = (d - c.delta_c2) / (c.delta_c3 - c.delta_c2);
+      *t = c.sigma_c * (2.0 * pow(v, 3.0) - 3.0 * sq(v) + 1.0);
+      *dt = c.sigma_c * (6.0 * (v / (c.delta_c3 - c.delta_c2)) * (v - 1.0));
+    } else {
+      *t = c.sigma_c * (1 - (d - c.delta_c2) / (c.delta_c3 - c.delta_c2));
+      *dt = -1.0 * (c.sigma_c / (c.delta_c3 - c.delta_c2));
+    }
+  } else {
+    *t = 0.0;
+  }
+}
 // delta (dim entries, tangential first, normal last) may be overwritten by the 1e-20 clamp, as the
 // reference's getDeltaEff / getDnDt do.  T gets the traction, Dm the dim x dim tangent (row-major),
 // isv the trial internal variables of this quadrature point (updated in place), zone the damage zone.
@@ -178,7 +213,27 @@ __device__ inline void coh_law(const CohConst& c, int dim, double* delta, double
   deff = sqrt(deff);
   double trac = 0.0, dtrac = 0.0;
   double dmax_copy = 0.0;
-  if (law == COH_BL || law == COH_BLNU) {
+  double tl_c = 0.0;           // trilinear: compression-penalty coefficient
+  if (law >= COH_TL) {
+    // Trilinear laws.  The plain ones read delta_max but never write it (like the bilinear one),
+    // and their max_traction is set only on the unloading branch, so a compressed point on the
+    // loading branch with delta_max > 0 gets a zero penalty (src/Material_TrilinearCohesive.cpp:
+    // 40-128, src/Material_SmoothedTrilinearCohesive.cpp:40-140).
+    const bool smooth = (law == COH_STL || law == COH_STLNU);
+    const bool memory = (law == COH_TL || law == COH_STL);
+    const double delta_max = memory ? isv[0] : 0.0;
+    double max_traction = 0.0;
+    if (!memory || deff >= delta_max || deff < 0.0) {
+      trilinear_curve(c, smooth, false, deff, &trac, &dtrac);
+    } else {
+      double unused;
+      trilinear_curve(c, smooth, true, delta_max, &max_traction, &unused);
+      trac = max_traction * (deff / delta_max);
+      dtrac = max_traction / delta_max;
+    }
+    if (memory && delta_max > 0.0) tl_c = (max_traction / c.alpha) * (c.delta_c1 / delta_max);
+    else tl_c = (smooth ? 2.0 * c.sigma_c : c.sigma_c) / c.alpha;
+  } else if (law == COH_BL || law == COH_BLNU) {
     // BilinearCohesiveMaterial never writes delta_max, so both variants follow the loading curve.
     const double delta_max = (law == COH_BL) ? isv[0] : 0.0;
     if (law == COH_BLNU || deff >= delta_max || deff < 0.0) {
@@ -240,10 +295,16 @@ __device__ inline void coh_law(const CohConst& c, int dim, double* delta, double
     } else if (law == COH_OPNUAUG) {
       for (int i = 0; i < dim - 1; ++i) Dm[(dim - 1) * dim + i] = 0.0;
       Dm[(dim - 1) * dim + dim - 1] = (c.sigma_c * exp(1.0) / c.delta_c) * cosh(c.alpha * delta[dim - 1] / c.delta_c);
+    } else if (law >= COH_TL) {
+      T[dim - 1] = tl_c * sinh(c.alpha * delta[dim - 1] / c.delta_c1);
+      for (int i = 0; i < dim - 1; ++i) Dm[(dim - 1) * dim + i] = 0.0;
+      Dm[(dim - 1) * dim + dim - 1] = tl_c * (c.alpha / c.delta_c1) * cosh(c.alpha * delta[dim - 1] / c.delta_c1);
     }
   }
   if (law == COH_BL || law == COH_BLNU) {
     *zone = compress ? 0 : (deff <= c.delta_c1 ? 1 : (deff <= c.delta_c2 ? 2 : 3));
+  } else if (law >= COH_TL) {
+    *zone = compress ? 0 : (deff <= c.delta_c1 ? 1 : (deff <= c.delta_c3 ? 2 : 3));
   } else {
     const double nf = deff / c.delta_c;
     *zone = (nf <= 0) ? 0 : (nf <= 1 ? 1 : (nf <= 5.0 ? 2 : 3));

@@ -469,7 +469,19 @@ int build_setup(const ProblemDesc& d, Setup& s) {
     case COH_OP: case COH_OPNU: case COH_OPAUG: case COH_OPNUAUG:
       s.coh.sigma_c = d.coh[0]; s.coh.delta_c = d.coh[1]; s.coh.beta2 = d.coh[2] * d.coh[2];
       s.coh.nvar = (d.coh_law == COH_OP || d.coh_law == COH_OPAUG) ? 1 : 0; break;
-    default: break;
+    // The trilinear copies pass ALPHA as sqrt(alpha) too (src/Material_TrilinearCohesiveNU.cpp:40,
+    // src/Material_SmoothedTrilinearCohesiveNU.cpp:40; set_alpha stores its argument), and the
+    // setters stop the reference on parameters out of order (set_dc1 .. set_dc3, set_sc).
+    case COH_TL: case COH_TLNU: case COH_STL: case COH_STLNU:
+      s.coh.sigma_c = d.coh[0]; s.coh.delta_c1 = d.coh[1]; s.coh.delta_c2 = d.coh[2]; s.coh.delta_c3 = d.coh[3];
+      if (!(d.coh[0] > 0 && d.coh[1] > 0 && d.coh[2] >= d.coh[1] && d.coh[3] >= d.coh[2])) {
+        s.error = "trilinear cohesive law needs sigma_c > 0 and 0 < delta_c1 <= delta_c2 <= delta_c3";
+        return 2;
+      }
+      s.coh.alpha = std::sqrt(50.0);
+      s.coh.nvar = (d.coh_law == COH_TL || d.coh_law == COH_STL) ? 1 : 0; break;
+    case COH_NONE: break;
+    default: s.error = "unknown cohesive law"; return 2;
   }
 
   // ---------------- structured mesh (Mesh::generate_mesh)

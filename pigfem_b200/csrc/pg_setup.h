@@ -17,7 +17,8 @@ enum ElemType : int { TRI3 = 0, QUAD4 = 1, TET4 = 2 };
 enum SubType : int { SUB_TRI3 = 0, SUB_QUAD4 = 1, SUB_POLYGON = 2, SUB_TET4 = 3, SUB_PRISM6 = 4, SUB_HEX8 = 5 };
 enum CohLaw : int {
   COH_NONE = 0, COH_BL = 1, COH_BLNU = 2, COH_XN = 3, COH_XNNU = 4,
-  COH_OP = 5, COH_OPNU = 6, COH_OPAUG = 7, COH_OPNUAUG = 8
+  COH_OP = 5, COH_OPNU = 6, COH_OPAUG = 7, COH_OPNUAUG = 8,
+  COH_TL = 9, COH_TLNU = 10, COH_STL = 11, COH_STLNU = 12
 };
 
 // Problem description (the reference's Tests/Main.cpp inputs).
@@ -40,7 +41,8 @@ struct ProblemDesc {
 struct CohParams {
   int law = COH_NONE;
   int nvar = 0;  // internal variables per cohesive quadrature point
-  double sigma_c = 0, delta_c1 = 0, delta_c2 = 0;  // bilinear
+  double sigma_c = 0, delta_c1 = 0, delta_c2 = 0;  // bilinear (and trilinear)
+  double delta_c3 = 0;                             // trilinear
   double delta_cn = 0, delta_ct = 0, q = 0;        // Xu-Needleman
   double delta_c = 0;                              // Ortiz-Pandolfi
   double beta2 = 1.0, alpha = 50.0;

@@ -17,6 +17,7 @@ E_M, NU_M, E_F, NU_F = 3.5e3, 0.35, 72e3, 0.22
 BL = (50.0, 5e-7, 5e-3, 0.0)
 XN = (50.0, 2e-4, 3e-4, 1.7)
 OP = (50.0, 2e-4, 1.0, 0.0)
+TL = (50.0, 5e-7, 1e-3, 5e-3)
 
 CASES = {
     # name: dict(elem_type, n, incl, coh_law, coh, subscale, eps_macro, u_scale, isv_scale, seed)
@@ -44,6 +45,22 @@ CASES = {
                       subscale=0, u_scale=1e-6, isv_scale=1.0, seed=11, open=(1e-6, 1e-3)),
     "coh_opnuaug": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=8, coh=OP,
                         subscale=0, u_scale=1e-6, isv_scale=0.0, seed=12, open=(1e-6, 1e-3)),
+    # trilinear and smoothed trilinear: openings across rise, plateau, fall and failure; the plain
+    # laws read (never write) a committed maximum drawn over the same range, so points unload too
+    "coh_tl": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=9, coh=TL,
+                   subscale=0, u_scale=1e-6, isv_scale=6e-3, seed=28, open=(1e-7, 1.2e-2)),
+    "coh_tlnu": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=10, coh=TL,
+                     subscale=0, u_scale=1e-6, isv_scale=0.0, seed=29, open=(1e-7, 1.2e-2)),
+    "coh_stl": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=11, coh=TL,
+                    subscale=0, u_scale=1e-6, isv_scale=6e-3, seed=30, open=(1e-7, 1.2e-2)),
+    "coh_stlnu": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=12, coh=TL,
+                      subscale=0, u_scale=1e-6, isv_scale=0.0, seed=31, open=(1e-7, 1.2e-2)),
+    # compression under a committed maximum: unloading points get the scaled penalty, loading points
+    # with a maximum > 0 none (max_traction is only set on the unloading branch)
+    "coh_stl_compression": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=11,
+                                coh=TL, subscale=0, u_scale=1e-9, isv_scale=4e-8, seed=32, open=(-2e-8, -1e-9)),
+    "coh_tlnu_compression": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=10,
+                                 coh=TL, subscale=0, u_scale=1e-9, isv_scale=0.0, seed=33, open=(-2e-8, -1e-9)),
     "coh_bl_compression": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=1, coh=BL,
                                subscale=0, u_scale=1e-9, isv_scale=0.0, seed=14, open=(-2e-8, -1e-9)),
     "coh_opaug_compression": dict(elem_type=0, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=7, coh=OP,
@@ -80,6 +97,10 @@ CASES = {
     "coh_tet4_opaug_two_spheres": dict(elem_type=2, n=(8, 7, 6), incl=[[0.3, 0.32, 0.35, 0.2], [0.7, 0.66, 0.62, 0.17]],
                                        coh_law=7, coh=OP, subscale=0, u_scale=1e-6, isv_scale=1.0, seed=26,
                                        open=(1e-6, 1e-3)),
+    "coh_tet4_tl": dict(elem_type=2, n=(5, 5, 5), incl=[[0.52, 0.47, 0.49, 0.31]], coh_law=9, coh=TL, subscale=0,
+                        u_scale=1e-6, isv_scale=6e-3, seed=34, open=(1e-7, 1.2e-2)),
+    "coh_tet4_stlnu": dict(elem_type=2, n=(5, 5, 5), incl=[[0.52, 0.47, 0.49, 0.31]], coh_law=12, coh=TL, subscale=0,
+                           u_scale=1e-6, isv_scale=0.0, seed=35, open=(1e-7, 1.2e-2)),
     "coh_tet4_bl_compression": dict(elem_type=2, n=(5, 5, 5), incl=[[0.52, 0.47, 0.49, 0.31]], coh_law=1, coh=BL,
                                     subscale=0, u_scale=1e-9, isv_scale=0.0, seed=27, open=(-2e-8, -1e-9)),
 }

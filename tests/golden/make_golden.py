@@ -16,6 +16,21 @@ from cases import CASES, case_arrays, cohesive_state, spec_kwargs  # noqa: E402
 from oracle import ref  # noqa: E402
 
 
+def effective_openings(c, U, R):
+    """The effective opening of every cohesive point under U.  Laws that write their maximum
+    opening report it as the trial internal variable of the assembly R just ran; the plain
+    trilinear laws never write it, so an Ortiz-Pandolfi twin of the same mesh (one internal
+    variable per point, set to the effective opening on first loading) measures it."""
+    if c["coh_law"] not in (9, 11):
+        return R.get("isv_trial")
+    twin = ref.RefProblem(ref.ProblemSpec(**spec_kwargs(dict(c, coh_law=5, coh=(50.0, 2e-4, 1.0, 0.0)))))
+    try:
+        twin.assemble(U, np.zeros(len(R.get("isv_trial"))), 1.0)
+        return twin.get("isv_trial")
+    finally:
+        twin.close()
+
+
 def generate(name):
     """The fixture arrays of one case, computed by the reference's own CPU assembly."""
     c = CASES[name]
@@ -31,7 +46,7 @@ def generate(name):
                 # committed maxima around the current openings: about half the points unload
                 R.assemble(U, isv, 1.0)
                 rng = np.random.default_rng(c["seed"] + 1000)
-                isv = R.get("isv_trial") * rng.uniform(0.5, 1.5, n_isv)
+                isv = effective_openings(c, U, R) * rng.uniform(0.5, 1.5, n_isv)
         else:
             U, isv = case_arrays(c, R.n_free, R.n_const, n_isv)
         t_frac = 1.0

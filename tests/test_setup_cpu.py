@@ -118,6 +118,13 @@ def test_setup_errors_are_status_codes():
     with pytest.raises(capi.PigfemError) as e:
         capi.Problem(capi.ProblemDesc(n=(8, 8), inclusions=np.array([[0.5, 0.5, -0.1]])), device=False)
     assert e.value.code == 2
+    # an unknown cohesive law, and trilinear parameters out of order (the reference's setters stop there)
+    with pytest.raises(capi.PigfemError) as e:
+        capi.Problem(capi.ProblemDesc(n=(8, 8), coh_law=13, coh=(50.0, 1e-6, 1e-3, 5e-3)), device=False)
+    assert e.value.code == 2
+    with pytest.raises(capi.PigfemError) as e:
+        capi.Problem(capi.ProblemDesc(n=(8, 8), coh_law=capi.COH_TL, coh=(50.0, 1e-3, 5e-7, 5e-3)), device=False)
+    assert e.value.code == 2
 
 
 def test_uncut_sizes():
