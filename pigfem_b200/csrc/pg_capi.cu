@@ -68,6 +68,7 @@ int launch(pg_ctx* c, double t_frac, int flags) {
   for (int v = 0; v < 6; ++v) P.eps_macro[v] = c->s.desc.eps_macro[v] * t_frac;
   const int dim = c->s.dim;
   const bool fp32 = (flags & PG_FP32) != 0;
+  const bool jac = (flags & PG_JAC) != 0;   // without it: the residual-only kernels
   // fork: the fast rows (uncut elements only) run on the side stream, concurrently with the
   // cut-element kernels and the general rows on the main stream
   cudaEventRecord(c->ev[0], c->stream);
@@ -80,7 +81,12 @@ int launch(pg_ctx* c, double t_frac, int flags) {
     else pgd::k_coh_elements<3><<<grid, tpb, 0, c->stream>>>(P);
   }
   // the stencil rows run on the side stream, concurrently with the cohesive points and general rows
-  if (c->n_stencil > 0) {
+  if (c->n_stencil > 0 && !jac) {
+    const int tpb = 128;
+    const int grid = (c->n_stencil + tpb - 1) / tpb;
+    if (dim == 2) pgd::k_rows_stencil<2, double, false><<<grid, tpb, 0, c->side>>>(P, c->grid, c->stencil, c->n_stencil);
+    else pgd::k_rows_stencil<3, double, false><<<grid, tpb, 0, c->side>>>(P, c->grid, c->stencil, c->n_stencil);
+  } else if (c->n_stencil > 0) {
     const int tpb = 128;
     const int nthreads = (dim == 2) ? c->n_stencil : 3 * 32 * ((c->n_stencil + 31) / 32);
     const int grid = (nthreads + tpb - 1) / tpb;
@@ -95,7 +101,21 @@ int launch(pg_ctx* c, double t_frac, int flags) {
   }
   cudaEventRecord(c->ev[1], c->side);
   cudaEventRecord(c->ev[3], c->stream);
-  if (P.n_slow_dn > 0) {
+  if (P.n_slow_dn > 0 && !jac) {
+    if (dim == 2) {
+      constexpr int G = 4;
+      const int grid = (P.n_slow_dn + (128 / G) - 1) / (128 / G);
+      const size_t smem = (size_t)(128 / G) * pgd::general_slab_doubles(0, 2, P.max_mn) * sizeof(double);
+      cudaFuncSetAttribute(pgd::k_rows_general<2, G, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      pgd::k_rows_general<2, G, false><<<grid, 128, smem, c->stream>>>(P, 0, P.max_mn);
+    } else {
+      constexpr int G = 8;
+      const int grid = (P.n_slow_dn + (128 / G) - 1) / (128 / G);
+      const size_t smem = (size_t)(128 / G) * pgd::general_slab_doubles(0, 3, P.max_mn) * sizeof(double);
+      cudaFuncSetAttribute(pgd::k_rows_general<3, G, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      pgd::k_rows_general<3, G, false><<<grid, 128, smem, c->stream>>>(P, 0, P.max_mn);
+    }
+  } else if (P.n_slow_dn > 0) {
     const int slots = P.maxnb_general;
     if (dim == 2) {
       constexpr int G = 4;
@@ -104,7 +124,7 @@ int launch(pg_ctx* c, double t_frac, int flags) {
       cudaFuncSetAttribute(pgd::k_rows_general<2, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       pgd::k_rows_general<2, G><<<grid, 128, smem, c->stream>>>(P, slots, P.max_mn);
     } else {
-      constexpr int G = 32;
+      constexpr int G = 8;
       const int grid = (P.n_slow_dn + (128 / G) - 1) / (128 / G);
       const size_t smem = (size_t)(128 / G) * pgd::general_slab_doubles(slots, 3, P.max_mn) * sizeof(double);
       cudaFuncSetAttribute(pgd::k_rows_general<3, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

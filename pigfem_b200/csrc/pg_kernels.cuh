@@ -129,10 +129,10 @@ __device__ __forceinline__ void add_strain(const T* g, const T* u, T* e) {
 __device__ __host__ inline double tri4_wsum() { return ((-0.28125 + 0.260416666666666666666666666666665) + 0.260416666666666666666666666666665) + 0.260416666666666666666666666666665; }
 __device__ __host__ inline double tet5_wsum() { return (((-0.8 + 0.45) + 0.45) + 0.45) + 0.45; }
 
-// Block (la, lb) of an uncut simplex with the given nodes: kb = w (B_la^T D B_lb); with want_r
-// also the residual of
-// row la, rv = w (B_la^T sigma).  Geometry from the node coordinates, stress from U (+ eps_macro).
-template <int DIM>
+// Block (la, lb) of an uncut simplex with the given nodes: kb = w (B_la^T D B_lb) (WANT_K); with
+// want_r also the residual of row la, rv = w (B_la^T sigma).  Geometry from the node coordinates,
+// stress from U (+ eps_macro).
+template <int DIM, bool WANT_K = true>
 __device__ __forceinline__ void simplex_block(const DevProblem& P, int4 nodes, int la, int lb, const double* D,
                                               double (*kb)[DIM], double* rv, bool want_r) {
   constexpr int NPE = DIM + 1;
@@ -155,12 +155,14 @@ __device__ __forceinline__ void simplex_block(const DevProblem& P, int4 nodes, i
 #pragma unroll
       for (int d = 0; d < DIM; ++d) gb[d] = g[n][d];
   }
+  if constexpr (WANT_K) {
 #pragma unroll
-  for (int q = 0; q < DIM; ++q) {
-    double part[NV];
-    bt_d_row<DIM, double>(D, ga, q, part);
+    for (int q = 0; q < DIM; ++q) {
+      double part[NV];
+      bt_d_row<DIM, double>(D, ga, q, part);
 #pragma unroll
-    for (int q2 = 0; q2 < DIM; ++q2) kb[q][q2] = wgt * part_b<DIM, double>(part, gb, q2);
+      for (int q2 = 0; q2 < DIM; ++q2) kb[q][q2] = wgt * part_b<DIM, double>(part, gb, q2);
+    }
   }
   if (want_r) {
     double eps[NV];
@@ -224,8 +226,10 @@ __device__ __forceinline__ void slab_add(double* ak, const double* v) {
 //                    cut_nodes, the row node's cohesive place (element << 5 | position) or -1, 0}
 //   nbr_pre[slot]    free DOFs of the node's neighbours before this one (row positions)
 // Every lane of the warp must call it (valid = false for lanes without a node): the entry loop and
-// its warp synchronisations are warp-uniform.  G >= DIM + 1.
-template <int DIM, int G>
+// its warp synchronisations are warp-uniform.  G >= DIM + 1.  JAC = false compiles the residual
+// alone: no slab of blocks (the group's shared memory is general_slab_doubles(0, ...)), no CSR
+// writes; the residual sums are the same operations in the same order.
+template <int DIM, int G, bool JAC = true>
 __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool valid, double* slab) {
   constexpr int NPE = DIM + 1;
   constexpr int NV = (DIM == 2) ? 3 : 6;
@@ -234,10 +238,10 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
   const int g = threadIdx.x % G;
   int4 gd = make_int4(0, 0, 0, 0);
   if (valid) gd = __ldg(&P.gdesc[node]);
-  double* rs = slab + gd.w * D2;           // residual of the node's rows
+  double* rs = JAC ? slab + gd.w * D2 : slab;   // residual of the node's rows
   double* part = rs + 4;                    // per-block residual partials of one cut element
   if (valid)
-    for (int i = g; i < gd.w * D2 + DIM; i += G) slab[i] = 0.0;
+    for (int i = g; i < (JAC ? gd.w * D2 : 0) + DIM; i += G) slab[i] = 0.0;
   int n_ent = gd.y;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) n_ent = max(n_ent, __shfl_xor_sync(0xffffffffu, n_ent, o));
@@ -252,11 +256,13 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
     if (valid && ei + 1 < gd.y) { ad_next = __ldg(&P.adesc[gd.x + ei + 1]); ax_next = __ldg(&P.aresd[gd.x + ei + 1]); }
     const int la = ad.y & 255, mn = ad.y >> 8;
     if (have && mn == 0) {
-      if (g < NPE) {
+      if (JAC ? g < NPE : g == 0) {
         double kb[DIM][DIM], rv[DIM];
-        simplex_block<DIM>(P, ax, la, g, P.D[ad.w], kb, rv, g == 0);   // D from the parameter space
-        double* ak = slab + ((((unsigned)ad.z) >> (8 * g)) & 255) * D2;
-        slab_add<DIM>(ak, &kb[0][0]);
+        simplex_block<DIM, JAC>(P, ax, la, g, P.D[ad.w], kb, rv, g == 0);   // D from the parameter space
+        if constexpr (JAC) {
+          double* ak = slab + ((((unsigned)ad.z) >> (8 * g)) & 255) * D2;
+          slab_add<DIM>(ak, &kb[0][0]);
+        }
         if (g == 0)
 #pragma unroll
           for (int q = 0; q < DIM; ++q) rs[q] += rv[q];
@@ -286,7 +292,7 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
           for (int d = 0; d < DIM; ++d) s += blk[q * DIM + d] * u[d];
           part[b * DIM + q] = s;
         }
-        if (cpa >= 0) {
+        if (JAC && cpa >= 0) {
           const int cpb = __ldg(&P.cohpos[base + b]);
           if (cpb >= 0 && (cpb >> 5) == (cpa >> 5)) {
             const int ce = cpa >> 5, n1 = cpa & 31, n2 = cpb & 31;
@@ -297,8 +303,10 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
             for (int i = 0; i < D2; ++i) blk[i] += sgn * B[i];
           }
         }
-        double* ak = slab + __ldg(&P.adj_slots[ad.z + b]) * D2;
-        slab_add<DIM>(ak, blk);
+        if constexpr (JAC) {
+          double* ak = slab + __ldg(&P.adj_slots[ad.z + b]) * D2;
+          slab_add<DIM>(ak, blk);
+        }
       }
     }
     __syncwarp();
@@ -339,7 +347,7 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
   for (int q = 0; q < DIM; ++q) {
     const int gdof = __ldg(&rd[q]);
     const bool rf = gdof < P.n_free;
-    if (P.flags & FLAG_JAC) {
+    if (JAC && (P.flags & FLAG_JAC)) {
       double* vF = P.val[rf ? 0 : 2] + __ldg(&rd[DIM + q]);
       double* vC = P.val[rf ? 1 : 3] + __ldg(&rd[2 * DIM + q]);
       for (int k = g; k < nn; k += G) {
@@ -359,13 +367,15 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
   }
 }
 
-template <int DIM, int G>
+// slab_slots = 0 with JAC = false (residual only).
+template <int DIM, int G, bool JAC = true>
 __global__ void __launch_bounds__(128) k_rows_general(DevProblem P, int slab_slots, int max_mn) {
   constexpr int NB = 128 / G;
   extern __shared__ double smem[];
   const int grp = threadIdx.x / G;
   const int node = blockIdx.x * NB + grp;
-  general_rows<DIM, G>(P, node, node < P.n_slow_dn, smem + (size_t)grp * general_slab_doubles(slab_slots, DIM, max_mn));
+  general_rows<DIM, G, JAC>(P, node, node < P.n_slow_dn,
+                            smem + (size_t)grp * general_slab_doubles(slab_slots, DIM, max_mn));
 }
 
 // Cohesive elements, one lane per quadrature point (CQ lanes per element: 2 in 2D for CohEdge2, 4

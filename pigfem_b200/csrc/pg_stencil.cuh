@@ -115,8 +115,9 @@ __device__ __forceinline__ void iso_d(const DevProblem& P, int m, T* d) {
   (void)idx;
 }
 
-// Rows of one stencil node.  Q < 0: all dim rows in one thread; Q >= 0: row Q only.
-template <class S, int DIM, typename T, int Q>
+// Rows of one stencil node.  Q < 0: all dim rows in one thread; Q >= 0: row Q only.  JAC = false
+// compiles the residual alone (no stiffness accumulators, no CSR writes).
+template <class S, int DIM, typename T, int Q, bool JAC = true>
 __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo& gi, int nid, int g0, int row0,
                                              double* stage = nullptr) {
   constexpr int NPE = DIM + 1;
@@ -125,14 +126,16 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
   constexpr int QB = (Q < 0) ? 0 : Q, QE = (Q < 0) ? DIM : Q + 1;
   const int sx = gi.nx + 1, sxy = sx * (gi.ny + 1);
   const int i = nid % sx, j = (nid / sx) % (gi.ny + 1), k = nid / sxy;
-  const bool jac = (P.flags & FLAG_JAC) != 0;  // uniform over the launch
-  double acc[S::NN][QE - QB][DIM];
+  const bool jac = JAC && (P.flags & FLAG_JAC) != 0;  // uniform over the launch
+  double acc[JAC ? S::NN : 1][QE - QB][DIM];
+  if constexpr (JAC) {
 #pragma unroll
-  for (int s = 0; s < S::NN; ++s)
+    for (int s = 0; s < S::NN; ++s)
 #pragma unroll
-    for (int q = 0; q < QE - QB; ++q)
+      for (int q = 0; q < QE - QB; ++q)
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) acc[s][q][d] = 0.0;
+        for (int d = 0; d < DIM; ++d) acc[s][q][d] = 0.0;
+  }
   double r[QE - QB];
 #pragma unroll
   for (int q = 0; q < QE - QB; ++q) r[q] = 0.0;
@@ -186,7 +189,7 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
 #pragma unroll
     for (int q = QB; q < QE; ++q) {
       r[q - QB] += w * bt_sig<DIM, double>(g[la], sig, q);
-      if (jac) {
+      if constexpr (JAC) if (jac) {
         T part[NV];
         part_iso<DIM, T>(dk, gk[la], q, part);
 #pragma unroll
@@ -198,7 +201,7 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
   }
 #pragma unroll
   for (int q = QB; q < QE; ++q) {
-    if (P.flags & FLAG_JAC) {
+    if constexpr (JAC) if (jac) {
       // rows go to the caller's stage when it has one, else straight to the CSR
       double* v = stage ? stage + (size_t)q * S::NN * DIM : P.val[0] + row0 + (size_t)q * S::NN * DIM;
 #pragma unroll
@@ -240,10 +243,23 @@ __device__ __forceinline__ void stencil_rows_staged(const DevProblem& P, const G
 // One thread per stencil node (2D) or per (stencil node, row) (3D, rows interleaved by warp so the
 // row is warp-uniform).  st: {node id, first free DOF, first CSR slot of its first row, class} per
 // node, class-sorted, each class padded to whole warps with node -1.  2D launches carry
-// stencil_stage_bytes(blockDim.x) of dynamic shared memory.
-template <int DIM, typename T>
+// stencil_stage_bytes(blockDim.x) of dynamic shared memory.  JAC = false (residual only): one
+// thread per stencil node in 2D and 3D, no shared memory.
+template <int DIM, typename T, bool JAC = true>
 __global__ void __launch_bounds__(128) k_rows_stencil(DevProblem P, GridInfo gi, const int4* __restrict__ st, int n) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if constexpr (!JAC) {
+    if (t >= n) return;
+    const int4 v = __ldg(&st[t]);
+    if (v.x < 0) return;   // padding entry
+    if constexpr (DIM == 2) {
+      if (v.w == 0) stencil_rows<Tri3Stencil0, 2, double, -1, false>(P, gi, v.x, v.y, v.z);
+      else stencil_rows<Tri3Stencil1, 2, double, -1, false>(P, gi, v.x, v.y, v.z);
+    } else {
+      stencil_rows<Tet4Stencil0, 3, double, -1, false>(P, gi, v.x, v.y, v.z);
+    }
+    return;
+  }
   if (DIM == 2) {
     extern __shared__ double stage[];
     if (t - (int)(threadIdx.x & 31) >= n) return;   // whole warps only: n is a multiple of 32
