@@ -622,7 +622,7 @@ def main():
         extra = 5 * (8 * (P.n_free + P.n_const) + 8 * 3 * P.sizes["n_nodes"])
         alg["total"] += extra
     stencil_name = f"k_rows_stencil<{P.dim},double>"
-    general_name = f"k_rows_general<{P.dim},{4 if P.dim == 2 else 32}>"
+    general_name = f"k_rows_general<{P.dim},{4 if P.dim == 2 else 8}>"
     gk_bytes = general_kernel_bytes(P, False)
     gk_ms = float(kt64[2])
     g_achieved = gk_bytes / (gk_ms * 1e-3) / 1e9 if gk_ms > 0 else None
@@ -641,17 +641,17 @@ def main():
                        "parallelism": f"replicas x{ws} (one RVE per GPU)"},
             "fp32_mixed": {"value": value32, "unit": UNIT, "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": value32 / value,
                            "kernel_ms": [float(x) for x in kt32]},
-            "kernel_ms": {"cut_elements": float(kt64[0]), "rows_fast_concurrent": float(kt64[1]),
+            "kernel_ms": {"cohesive_elements": float(kt64[0]), "rows_stencil": float(kt64[1]),
                           "rows_general": float(kt64[2]), "assembly": float(kt64[3])},
             "algorithmic_bytes_per_step": alg["total"], "algorithmic_bytes_per_element": alg["total"] / ne,
             "algorithmic_gbs": alg["total"] / (ms64 / args.steps * 1e-3) / 1e9,
-            "roofline": {"bound": "hbm", "kernel": f"{stencil_name} (side stream, concurrent with the cut-element and general-row kernels)",
+            "roofline": {"bound": "hbm", "kernel": f"{stencil_name} " + ("(side stream, concurrent with the cohesive and general-row kernels)" if P.dim == 2 else "(main stream, alone)"),
                          "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": profiled_traffic(stencil_name), "bytes_per_launch": fk_bytes,
                          "traffic_note": "ncu dram read+write per launch, cold cache; row writes still in L2 at kernel end are not counted"},
             # the longest-running kernel (the stencil kernel above moves most of the bytes)
-            "roofline_general": {"bound": "hbm", "kernel": f"{general_name} (main stream, after the cohesive elements, sharing the SMs with the stencil rows)",
+            "roofline_general": {"bound": "hbm", "kernel": f"{general_name} " + ("(main stream, after the cohesive elements, sharing the SMs with the stencil rows)" if P.dim == 2 else "(main stream, after the stencil rows, alone)"),
                                  "achieved": g_achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                                  "frac": (g_achieved / peak) if g_achieved else None,
                                  "traffic": profiled_traffic(general_name), "bytes_per_launch": gk_bytes},

@@ -118,8 +118,9 @@ int pg_device_outputs(pg_ctx* ctx, double** K_vals4, double** P_f, double** P_p)
 int pg_set_stream(pg_ctx* ctx, void* stream);
 
 /* Device timing of the last assembly from CUDA events the context records on its streams:
- * ms[0] cohesive points + cut-element blocks, ms[1] fast rows (side stream, concurrent with ms[0]),
- * ms[2] general rows, ms[3] the whole assembly (fork to join).  pg_set_timing is kept for callers
+ * ms[0] cohesive elements, ms[1] stencil rows (2D: side stream, concurrent with ms[0] and ms[2];
+ * 3D: after ms[0]), ms[2] general rows (2D: after ms[0]; 3D: after ms[1]), ms[3] the whole
+ * assembly (fork to join).  pg_set_timing is kept for callers
  * that toggle it; the events are always recorded. */
 int pg_set_timing(pg_ctx* ctx, int on);
 int pg_kernel_times(pg_ctx* ctx, float* ms);

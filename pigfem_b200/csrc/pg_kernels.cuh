@@ -226,10 +226,9 @@ __device__ __forceinline__ void slab_add(double* ak, const double* v) {
 //                    cut_nodes, the row node's cohesive place (element << 5 | position) or -1, 0}
 //   nbr_pre[slot]    free DOFs of the node's neighbours before this one (row positions)
 // Every lane of the warp must call it (valid = false for lanes without a node): the entry loop and
-// its warp synchronisations are warp-uniform.  G >= DIM + 1.  JAC = false compiles the residual
-// alone: no slab of blocks (the group's shared memory is general_slab_doubles(0, ...)), no CSR
-// writes; the residual sums are the same operations in the same order.
-template <int DIM, int G, bool JAC = true>
+// its warp synchronisations are warp-uniform.  G >= DIM + 1.  (Residual-only assemblies use
+// k_rows_general_resid.)
+template <int DIM, int G>
 __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool valid, double* slab) {
   constexpr int NPE = DIM + 1;
   constexpr int NV = (DIM == 2) ? 3 : 6;
@@ -238,10 +237,10 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
   const int g = threadIdx.x % G;
   int4 gd = make_int4(0, 0, 0, 0);
   if (valid) gd = __ldg(&P.gdesc[node]);
-  double* rs = JAC ? slab + gd.w * D2 : slab;   // residual of the node's rows
+  double* rs = slab + gd.w * D2;           // residual of the node's rows
   double* part = rs + 4;                    // per-block residual partials of one cut element
   if (valid)
-    for (int i = g; i < (JAC ? gd.w * D2 : 0) + DIM; i += G) slab[i] = 0.0;
+    for (int i = g; i < gd.w * D2 + DIM; i += G) slab[i] = 0.0;
   int n_ent = gd.y;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) n_ent = max(n_ent, __shfl_xor_sync(0xffffffffu, n_ent, o));
@@ -256,13 +255,11 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
     if (valid && ei + 1 < gd.y) { ad_next = __ldg(&P.adesc[gd.x + ei + 1]); ax_next = __ldg(&P.aresd[gd.x + ei + 1]); }
     const int la = ad.y & 255, mn = ad.y >> 8;
     if (have && mn == 0) {
-      if (JAC ? g < NPE : g == 0) {
+      if (g < NPE) {
         double kb[DIM][DIM], rv[DIM];
-        simplex_block<DIM, JAC>(P, ax, la, g, P.D[ad.w], kb, rv, g == 0);   // D from the parameter space
-        if constexpr (JAC) {
-          double* ak = slab + ((((unsigned)ad.z) >> (8 * g)) & 255) * D2;
-          slab_add<DIM>(ak, &kb[0][0]);
-        }
+        simplex_block<DIM>(P, ax, la, g, P.D[ad.w], kb, rv, g == 0);   // D from the parameter space
+        double* ak = slab + ((((unsigned)ad.z) >> (8 * g)) & 255) * D2;
+        slab_add<DIM>(ak, &kb[0][0]);
         if (g == 0)
 #pragma unroll
           for (int q = 0; q < DIM; ++q) rs[q] += rv[q];
@@ -292,7 +289,7 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
           for (int d = 0; d < DIM; ++d) s += blk[q * DIM + d] * u[d];
           part[b * DIM + q] = s;
         }
-        if (JAC && cpa >= 0) {
+        if (cpa >= 0) {
           const int cpb = __ldg(&P.cohpos[base + b]);
           if (cpb >= 0 && (cpb >> 5) == (cpa >> 5)) {
             const int ce = cpa >> 5, n1 = cpa & 31, n2 = cpb & 31;
@@ -303,10 +300,8 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
             for (int i = 0; i < D2; ++i) blk[i] += sgn * B[i];
           }
         }
-        if constexpr (JAC) {
-          double* ak = slab + __ldg(&P.adj_slots[ad.z + b]) * D2;
-          slab_add<DIM>(ak, blk);
-        }
+        double* ak = slab + __ldg(&P.adj_slots[ad.z + b]) * D2;
+        slab_add<DIM>(ak, blk);
       }
     }
     __syncwarp();
@@ -347,7 +342,7 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
   for (int q = 0; q < DIM; ++q) {
     const int gdof = __ldg(&rd[q]);
     const bool rf = gdof < P.n_free;
-    if (JAC && (P.flags & FLAG_JAC)) {
+    if (P.flags & FLAG_JAC) {
       double* vF = P.val[rf ? 0 : 2] + __ldg(&rd[DIM + q]);
       double* vC = P.val[rf ? 1 : 3] + __ldg(&rd[2 * DIM + q]);
       for (int k = g; k < nn; k += G) {
@@ -367,15 +362,93 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
   }
 }
 
-// slab_slots = 0 with JAC = false (residual only).
-template <int DIM, int G, bool JAC = true>
+// Residual-only rows of the general nodes, entry-parallel: L lanes per DOF node, lane k takes the
+// node's entries k, k + L, ... and forms each entry's whole contribution to the node's residual
+// (an uncut element's w B^T sigma; a cut element's block row of K_vol times the displacements in
+// block order, its macroscale-strain response and the cohesive traction at the node) -- the same
+// operations general_rows performs for that entry -- and the group adds the contributions in
+// entry (adjacency) order with shuffles.  Every entry's loads are in flight at once instead of
+// one entry after the other.  L divides 32.
+template <int DIM, int L>
+__global__ void __launch_bounds__(128) k_rows_general_resid(DevProblem P) {
+  constexpr int NV = (DIM == 2) ? 3 : 6;
+  constexpr int D2 = DIM * DIM;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int node = t / L, k = t % L;
+  const bool valid = node < P.n_slow_dn;   // uniform over each group of L lanes
+  const unsigned gmask = (L == 32) ? 0xffffffffu : (((1u << L) - 1u) << ((threadIdx.x & 31) / L * L));
+  if (__all_sync(0xffffffffu, !valid)) return;
+  int4 gd = make_int4(0, 0, 0, 0);
+  if (valid) gd = __ldg(&P.gdesc[node]);
+  double rs[DIM];
+#pragma unroll
+  for (int q = 0; q < DIM; ++q) rs[q] = 0.0;
+  for (int e0 = 0; e0 < gd.y; e0 += L) {          // gd.y is uniform over the group
+    const int ei = e0 + k;
+    double re[DIM];
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) re[q] = 0.0;
+    if (ei < gd.y) {
+      const int4 ad = __ldg(&P.adesc[gd.x + ei]);
+      const int4 ax = __ldg(&P.aresd[gd.x + ei]);
+      const int la = ad.y & 255, mn = ad.y >> 8;
+      if (mn == 0) {
+        double kb[DIM][DIM];
+        simplex_block<DIM, false>(P, ax, la, 0, P.D[ad.w], kb, re, true);
+      } else {
+        const int* cn = P.cut_nodes + ax.y;
+        const double* kr = P.ke + ad.w;             // block row la of K_vol
+        for (int b = 0; b < mn; ++b) {
+          const int nb = __ldg(&cn[b]);
+          double u[DIM];
+          load_node<DIM>(P.U, nb, u);
+#pragma unroll
+          for (int q = 0; q < DIM; ++q) {
+            double s = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) s += __ldg(&kr[b * D2 + q * DIM + d]) * u[d];
+            re[q] += s;
+          }
+        }
+        if (P.subscale) {
+          const double* gm = P.gmac + __ldg(&P.re_off[ax.x]) / DIM * DIM * NV + (size_t)la * DIM * NV;
+#pragma unroll
+          for (int q = 0; q < DIM; ++q)
+#pragma unroll
+            for (int v = 0; v < NV; ++v) re[q] += gm[q * NV + v] * P.eps_macro[v];
+        }
+        const int cpa = ax.z;
+        if (cpa >= 0) {
+          const int ce = cpa >> 5, n1 = cpa & 31;
+          const int nh = __ldg(&P.coh_nh[ce]);
+          const double sgn = (n1 >= nh) ? 1.0 : -1.0;
+          const double* tr = P.kcoh + __ldg(&P.kc_off[ce]) + nh * nh * D2 + (n1 % nh) * DIM;
+#pragma unroll
+          for (int q = 0; q < DIM; ++q) re[q] += sgn * tr[q];
+        }
+      }
+    }
+    // the node's sum in entry order
+    const int n_here = min(L, gd.y - e0);
+    for (int j = 0; j < n_here; ++j)
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) rs[q] += __shfl_sync(gmask, re[q], j, L);
+  }
+  if (!valid || k >= DIM || !(P.flags & FLAG_FUNC)) return;
+  double mine = rs[0];
+#pragma unroll
+  for (int q = 1; q < DIM; ++q) if (k == q) mine = rs[q];
+  const int gdof = __ldg(&P.growd[(size_t)node * 3 * DIM + k]);
+  if (gdof < P.n_free) P.Pf[gdof] = mine; else P.Pp[gdof - P.n_free] = mine;
+}
+
+template <int DIM, int G>
 __global__ void __launch_bounds__(128) k_rows_general(DevProblem P, int slab_slots, int max_mn) {
   constexpr int NB = 128 / G;
   extern __shared__ double smem[];
   const int grp = threadIdx.x / G;
   const int node = blockIdx.x * NB + grp;
-  general_rows<DIM, G, JAC>(P, node, node < P.n_slow_dn,
-                            smem + (size_t)grp * general_slab_doubles(slab_slots, DIM, max_mn));
+  general_rows<DIM, G>(P, node, node < P.n_slow_dn, smem + (size_t)grp * general_slab_doubles(slab_slots, DIM, max_mn));
 }
 
 // Cohesive elements, one lane per quadrature point (CQ lanes per element: 2 in 2D for CohEdge2, 4

@@ -115,8 +115,20 @@ __device__ __forceinline__ void iso_d(const DevProblem& P, int m, T* d) {
   (void)idx;
 }
 
+// The last adjacent element (in adjacency order) that has neighbour slot s among its nodes.
+template <class S, int NPE>
+__host__ __device__ constexpr int slot_last_touch(int s) {
+  int l = -1;
+  for (int a = 0; a < S::NADJ; ++a)
+    for (int n = 0; n < NPE; ++n)
+      if (S::ent(a, 5 + n) == s) l = a;
+  return l;
+}
+
 // Rows of one stencil node.  Q < 0: all dim rows in one thread; Q >= 0: row Q only.  JAC = false
-// compiles the residual alone (no stiffness accumulators, no CSR writes).
+// compiles the residual alone (no stiffness accumulators, no CSR writes).  Each neighbour block is
+// stored as soon as the last element touching it has been added (the slots are compile-time, so
+// the store points are too): its registers are free for the rest of the walk.
 template <class S, int DIM, typename T, int Q, bool JAC = true>
 __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo& gi, int nid, int g0, int row0,
                                              double* stage = nullptr) {
@@ -198,19 +210,24 @@ __device__ __forceinline__ void stencil_rows(const DevProblem& P, const GridInfo
           for (int q2 = 0; q2 < DIM; ++q2) acc[S::ent(a, 5 + lb)][q - QB][q2] += (double)(wk * part_b<DIM, T>(part, gk[lb], q2));
       }
     }
-  }
-#pragma unroll
-  for (int q = QB; q < QE; ++q) {
     if constexpr (JAC) if (jac) {
-      // rows go to the caller's stage when it has one, else straight to the CSR
-      double* v = stage ? stage + (size_t)q * S::NN * DIM : P.val[0] + row0 + (size_t)q * S::NN * DIM;
+      // the blocks no later element touches: to the caller's stage when it has one, else
+      // straight to the CSR (a node's rows are consecutive, NN x DIM values each)
 #pragma unroll
-      for (int s = 0; s < S::NN; ++s)
+      for (int s = 0; s < S::NN; ++s) {
+        if (slot_last_touch<S, NPE>(s) != a) continue;
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) v[s * DIM + d] = acc[s][q - QB][d];
+        for (int q = QB; q < QE; ++q) {
+          double* v = stage ? stage + (size_t)q * S::NN * DIM : P.val[0] + row0 + (size_t)q * S::NN * DIM;
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) v[s * DIM + d] = acc[s][q - QB][d];
+        }
+      }
     }
-    if (P.flags & FLAG_FUNC) P.Pf[g0 + q] = r[q - QB];
   }
+#pragma unroll
+  for (int q = QB; q < QE; ++q)
+    if (P.flags & FLAG_FUNC) P.Pf[g0 + q] = r[q - QB];
 }
 
 // 2D rows of the stencil node of this lane, staged: the lane's two rows (2 x NN x 2 values, one
