@@ -20,7 +20,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <map>
+#include <thread>
 #include <set>
 #include <sstream>
 #include <tuple>
@@ -28,6 +30,31 @@
 
 namespace pg {
 namespace {
+
+// Host threads for the set-up's independent loops: PIGFEM_SETUP_THREADS, else the hardware
+// concurrency, at most 8.  Results do not depend on the count: every parallel loop writes
+// disjoint outputs, and anything order-dependent is laid out from per-chunk counts first.
+int setup_threads() {
+  static const int n = [] {
+    const char* e = std::getenv("PIGFEM_SETUP_THREADS");
+    int v = e ? std::atoi(e) : (int)std::thread::hardware_concurrency();
+    return std::max(1, std::min(v, 8));
+  }();
+  return n;
+}
+
+// f(chunk, begin, end) over nt contiguous chunks of [0, n), chunk k on its own thread.
+template <class F>
+void chunked(int n, int nt, F f) {
+  if (nt <= 1 || n < 2) { f(0, 0, n); return; }
+  std::vector<std::thread> th;
+  const int step = (n + nt - 1) / nt;
+  for (int k = 0; k < nt; ++k) {
+    const int a = std::min(n, k * step), b = std::min(n, a + step);
+    th.emplace_back(f, k, a, b);
+  }
+  for (auto& t : th) t.join();
+}
 
 const double kPI = 3.14159265358979323846264338327950;
 
@@ -574,24 +601,33 @@ int build_setup(const ProblemDesc& d, Setup& s) {
   }
   const int ninc = (int)incs.size();
   s.node_detect.assign(s.n_std, -1);
-  for (int n = 0; n < s.n_std; ++n) {
-    const double* x = &X3[(size_t)n * 3];
-    int res = -1;
-    for (int j = ninc - 1; j >= 0; --j) {
-      if (!incs[j].in_box(x)) continue;
-      int r = incs[j].detect(x);
-      if (r == 0) continue;
-      if (r == 1) {
+  {
+    // nodes in parallel chunks; the first node on a surface (in node order) is the one reported
+    const int ntd = setup_threads();
+    std::vector<std::pair<int, int>> on_surface(ntd, {-1, -1});
+    chunked(s.n_std, ntd, [&](int k, int n0, int n1) {
+      for (int n = n0; n < n1; ++n) {
+        const double* x = &X3[(size_t)n * 3];
+        int res = -1;
+        for (int j = ninc - 1; j >= 0; --j) {
+          if (!incs[j].in_box(x)) continue;
+          int r = incs[j].detect(x);
+          if (r == 0) continue;
+          if (r == 1) { on_surface[k] = {n, j}; return; }
+          res = j;
+          break;
+        }
+        s.node_detect[n] = res;
+      }
+    });
+    for (const auto& f : on_surface)
+      if (f.first >= 0) {
         std::ostringstream os;
-        os << "node " << n << " lies on the surface of inclusion " << j
+        os << "node " << f.first << " lies on the surface of inclusion " << f.second
            << " (the reference stops here: src/Mesh.cpp:2904-2911)";
         s.error = os.str();
         return 3;
       }
-      res = j;
-      break;
-    }
-    s.node_detect[n] = res;
   }
 
   // ---------------- element detection (Tri3::detection / Tet4::detection)
@@ -689,177 +725,248 @@ int build_setup(const ProblemDesc& d, Setup& s) {
   };
 
   // ---------------- per cut element: nodes, sub-elements, quadrature data
-  s.cut_node_off.push_back(0);
-  s.cut_sub_off.push_back(0);
-  s.sub_node_off.push_back(0);
-  s.sub_qp_off.push_back(0);
-  s.cut_qp_off.push_back(0);
-  s.qp_grad_off.push_back(0);
-  s.cut_coh_off.push_back(0);
-  s.coh_local_off.push_back(0);
-  s.coh_qp_off.push_back(0);
-  for (int c = 0; c < s.ncut; ++c) {
-    const int e = cut_elems[c];
-    CutCase cc = cases[c];
-    const int ncut_e = (int)cc.cut_edge.size();
-    const int n_en = s.cohesive ? 2 * ncut_e : ncut_e;
-    // transformDetectionCohToReg: fold mirror indices back when the mesh is not cohesive
-    if (!s.cohesive) {
-      for (auto& sub : cc.sub)
-        for (int& v : sub)
-          if (v >= s.npe + ncut_e) v -= ncut_e;
-      cc.coh.clear();
-    }
-    // enrichment node of each slot (add_enrich_node_to_elem)
-    std::vector<int> slot(n_en, -1);
-    for (int i = 0; i < ncut_e; ++i) {
-      int a = s.conn[(size_t)e * s.npe + emap[cc.cut_edge[i]][0]], b = s.conn[(size_t)e * s.npe + emap[cc.cut_edge[i]][1]];
-      if (a > b) std::swap(a, b);
-      auto it = edge_index.find(std::make_tuple(a, b, cc.incl[i]));
-      if (it == edge_index.end()) { s.error = "internal: cut edge without enrichment node"; return 6; }
-      // first cut-edge entry with this (edge, inclusion) takes the node
-      int first = i;
-      for (int i2 = 0; i2 < i; ++i2) {
-        int a2 = s.conn[(size_t)e * s.npe + emap[cc.cut_edge[i2]][0]], b2 = s.conn[(size_t)e * s.npe + emap[cc.cut_edge[i2]][1]];
-        if (a2 > b2) std::swap(a2, b2);
-        if (a2 == a && b2 == b && cc.incl[i2] == cc.incl[i]) { first = i2; break; }
+  // The cut elements are independent: contiguous chunks of them run in parallel, each appending
+  // to its own accumulator with chunk-local offsets, and the chunks are then concatenated in
+  // order (offsets shifted by the earlier chunks' sizes), which gives exactly the arrays of one
+  // pass over the cut elements.
+  struct CutAcc {
+    std::vector<int> cut_nodes, cut_node_off, sub_type, sub_mat, sub_nodes, sub_node_off, qp_mat, qp_grad_off,
+        sub_qp_off, cut_sub_off, cut_qp_off, coh_nh, coh_local_off, coh_local, cqp_isv, coh_qp_off, cut_coh_off;
+    std::vector<double> qp_wgt, qp_grad, cqp_N, cqp_R, cqp_wgt;
+    int n_isv = 0;
+    std::string error;
+    int rc = 0;
+  };
+  const int ntc = setup_threads();
+  std::vector<CutAcc> accs(std::max(1, ntc));
+  auto cut_chunk = [&](int k, int c0, int c1) {
+    CutAcc& A = accs[k];
+    for (int c = c0; c < c1; ++c) {
+      const int e = cut_elems[c];
+      CutCase cc = cases[c];
+      const int ncut_e = (int)cc.cut_edge.size();
+      const int n_en = s.cohesive ? 2 * ncut_e : ncut_e;
+      // transformDetectionCohToReg: fold mirror indices back when the mesh is not cohesive
+      if (!s.cohesive) {
+        for (auto& sub : cc.sub)
+          for (int& v : sub)
+            if (v >= s.npe + ncut_e) v -= ncut_e;
+        cc.coh.clear();
       }
-      if (first != i) { s.error = "internal: repeated (edge, inclusion) in one element"; return 6; }
-      slot[i] = s.n_std + it->second;
-      if (s.cohesive) slot[i + ncut_e] = s.n_std + it->second + n_init;
-    }
-    // element node list: parent nodes then enrichment slots
-    std::vector<int> enodes;
-    for (int q = 0; q < s.npe; ++q) enodes.push_back(s.conn[(size_t)e * s.npe + q]);
-    for (int q = 0; q < n_en; ++q) enodes.push_back(slot[q]);
-    const int nall = (int)enodes.size();
-    for (int v : enodes) s.cut_nodes.push_back(v);
-    s.cut_node_off.push_back((int)s.cut_nodes.size());
-
-    // parent gradients (constant for the affine tri3 / tet4 parents)
-    double pxs[4 * 3], pdNdr[4 * 3], pdNdx[4 * 3], pN[4], pJ;
-    for (int q = 0; q < s.npe; ++q) for (int k = 0; k < dim; ++k) pxs[q * dim + k] = X3of(enodes[q])[k];
-    if (dim == 2) tri3_shape(0.0, 0.0, pN, pdNdr);
-    else tet4_shape(0.0, 0.0, 0.0, pN, pdNdr);
-    transform_gradients(dim, s.npe, pdNdr, pxs, pdNdx, &pJ);
-
-    for (size_t ie = 0; ie < cc.sub.size(); ++ie) {
-      const std::vector<int>& sub = cc.sub[ie];
-      const int nsn = (int)sub.size();
-      int stype;
-      if (dim == 2) stype = (nsn == 3) ? SUB_TRI3 : (nsn == 4 ? SUB_QUAD4 : SUB_POLYGON);
-      else stype = (nsn == 4) ? SUB_TET4 : (nsn == 6 ? SUB_PRISM6 : SUB_HEX8);
-      const int mat = (cc.sub_mat[ie] < 0) ? s.elem_mat[e] : 1;
-      s.sub_type.push_back(stype);
-      s.sub_mat.push_back(mat);
-      std::vector<int> gsub(nsn);
-      double sx[32 * 3];
-      for (int q = 0; q < nsn; ++q) {
-        gsub[q] = enodes[sub[q]];
-        s.sub_nodes.push_back(gsub[q]);
-        for (int k = 0; k < dim; ++k) sx[q * dim + k] = X3of(gsub[q])[k];
-      }
-      s.sub_node_off.push_back((int)s.sub_nodes.size());
-      int nqp = 0;
-      if (stype == SUB_TRI3) nqp = 4;
-      else if (stype == SUB_QUAD4) nqp = 4;
-      else if (stype == SUB_POLYGON) nqp = 4 * nsn;
-      else if (stype == SUB_TET4) nqp = 5;
-      else { s.error = "prism6 / hex8 sub-elements do not occur after the prism decomposition"; return 6; }
-      for (int qp = 0; qp < nqp; ++qp) {
-        double r, t, w, cN[32], cdN[96], cdNdx[96], cJ;
-        if (stype == SUB_TRI3) { r = kTri4[qp][0]; t = kTri4[qp][1]; w = kTri4[qp][2]; tri3_shape(r, t, cN, cdN); }
-        else if (stype == SUB_QUAD4) { quad4_qp(qp, &r, &t, &w); quad4_shape(r, t, cN, cdN); }
-        else if (stype == SUB_POLYGON) { poly_qp(nsn, qp, &r, &t, &w); poly_shape(nsn, r, t, cN, cdN); }
-        else { w = kTet5[qp][3]; tet4_shape(kTet5[qp][0], kTet5[qp][1], kTet5[qp][2], cN, cdN); }
-        transform_gradients(dim, nsn, cdN, sx, cdNdx, &cJ);
-        if (cJ < 0.0) { s.error = "negative sub-element Jacobian (src/Mesh.cpp:1561)"; return 7; }
-        s.qp_wgt.push_back(cJ * w);
-        s.qp_mat.push_back(mat);
-        // gradients over the element's nodes: parent gradients, then the child gradient of the
-        // sub-element node that is each enrichment node (zero when the sub-element lacks it)
-        for (int q = 0; q < s.npe; ++q) for (int k = 0; k < dim; ++k) s.qp_grad.push_back(pdNdx[q * dim + k]);
-        for (int en = 0; en < n_en; ++en) {
-          const int id = enodes[s.npe + en];
-          int found = -1;
-          for (int q = 0; q < nsn; ++q) if (gsub[q] == id) { found = q; break; }
-          for (int k = 0; k < dim; ++k) s.qp_grad.push_back(found >= 0 ? 1.0 * cdNdx[found * dim + k] : 0.0);
+      // enrichment node of each slot (add_enrich_node_to_elem)
+      std::vector<int> slot(n_en, -1);
+      for (int i = 0; i < ncut_e; ++i) {
+        int a = s.conn[(size_t)e * s.npe + emap[cc.cut_edge[i]][0]], b = s.conn[(size_t)e * s.npe + emap[cc.cut_edge[i]][1]];
+        if (a > b) std::swap(a, b);
+        auto it = edge_index.find(std::make_tuple(a, b, cc.incl[i]));
+        if (it == edge_index.end()) { A.error = "internal: cut edge without enrichment node"; A.rc = 6; return; }
+        // first cut-edge entry with this (edge, inclusion) takes the node
+        int first = i;
+        for (int i2 = 0; i2 < i; ++i2) {
+          int a2 = s.conn[(size_t)e * s.npe + emap[cc.cut_edge[i2]][0]], b2 = s.conn[(size_t)e * s.npe + emap[cc.cut_edge[i2]][1]];
+          if (a2 > b2) std::swap(a2, b2);
+          if (a2 == a && b2 == b && cc.incl[i2] == cc.incl[i]) { first = i2; break; }
         }
-        s.qp_grad_off.push_back((int)s.qp_grad.size());
+        if (first != i) { A.error = "internal: repeated (edge, inclusion) in one element"; A.rc = 6; return; }
+        slot[i] = s.n_std + it->second;
+        if (s.cohesive) slot[i + ncut_e] = s.n_std + it->second + n_init;
       }
-      s.sub_qp_off.push_back((int)s.qp_wgt.size());
-    }
-    s.cut_sub_off.push_back((int)s.sub_type.size());
-    s.cut_qp_off.push_back((int)s.qp_wgt.size());
+      // element node list: parent nodes then enrichment slots
+      std::vector<int> enodes;
+      for (int q = 0; q < s.npe; ++q) enodes.push_back(s.conn[(size_t)e * s.npe + q]);
+      for (int q = 0; q < n_en; ++q) enodes.push_back(slot[q]);
+      const int nall = (int)enodes.size();
+      for (int v : enodes) A.cut_nodes.push_back(v);
+      A.cut_node_off.push_back((int)A.cut_nodes.size());
 
-    // cohesive elements (CohEdge2, 2-point Gauss; rotation from the '-' side nodes)
-    for (size_t ce = 0; ce < cc.coh.size(); ++ce) {
-      const std::vector<int>& cl = cc.coh[ce];
-      const int nh = (int)cl.size() / 2;
-      s.coh_nh.push_back(nh);
-      for (int v : cl) s.coh_local.push_back(v);
-      s.coh_local_off.push_back((int)s.coh_local.size());
-      if (dim == 3) {
-        // CohTri3 (4-point tri rule, src/CohTri3.cpp:70-84) or CohQuad4 (2 x 2 Gauss, qp -> (qp % 2,
-        // qp / 2), src/CohQuad4.cpp:55-70); rotation rows (dx/dr, dx/ds, their cross product)
-        // normalised, from the '-' side nodes (CohesiveElem::compute_rotation_general).
-        const int nq = 4;
-        for (int qp = 0; qp < nq; ++qp) {
-          double r, t, w, N[4], dN[8];
-          if (nh == 3) { r = kTri4[qp][0]; t = kTri4[qp][1]; w = kTri4[qp][2]; tri3_shape(r, t, N, dN); }
-          else if (nh == 4) { quad4_qp(qp, &r, &t, &w); quad4_shape(r, t, N, dN); }
-          else { s.error = "internal: 3D cohesive element with an unexpected node count"; return 6; }
-          double Jac[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
-          for (int n = 0; n < nh; ++n) {
-            const double* xn = X3of(enodes[cl[n]]);
-            for (int a = 0; a < 2; ++a) for (int i = 0; i < 3; ++i) Jac[a][i] += dN[n * 2 + a] * xn[i];
-          }
-          double nrm[3];
-          nrm[0] = Jac[0][1] * Jac[1][2] - Jac[0][2] * Jac[1][1];
-          nrm[1] = -(Jac[0][0] * Jac[1][2] - Jac[0][2] * Jac[1][0]);
-          nrm[2] = Jac[0][0] * Jac[1][1] - Jac[0][1] * Jac[1][0];
-          double mag[2];
-          for (int a = 0; a < 2; ++a) {
-            double dd = 0.0;
-            for (int i = 0; i < 3; ++i) dd += Jac[a][i] * Jac[a][i];
-            mag[a] = std::sqrt(dd);
-          }
-          double nn = 0.0;
-          for (int i = 0; i < 3; ++i) nn += nrm[i] * nrm[i];
-          const double dA = std::sqrt(nn);
-          for (int n = 0; n < nh; ++n) s.cqp_N.push_back(N[n] * 1.0);
-          for (int a = 0; a < 2; ++a) for (int i = 0; i < 3; ++i) s.cqp_R.push_back(Jac[a][i] / mag[a]);
-          for (int i = 0; i < 3; ++i) s.cqp_R.push_back(nrm[i] / dA);
-          s.cqp_wgt.push_back(dA * w);
-          s.cqp_isv.push_back(s.n_isv);
-          s.n_isv += s.coh.nvar;
+      // parent gradients (constant for the affine tri3 / tet4 parents)
+      double pxs[4 * 3], pdNdr[4 * 3], pdNdx[4 * 3], pN[4], pJ;
+      for (int q = 0; q < s.npe; ++q) for (int k = 0; k < dim; ++k) pxs[q * dim + k] = X3of(enodes[q])[k];
+      if (dim == 2) tri3_shape(0.0, 0.0, pN, pdNdr);
+      else tet4_shape(0.0, 0.0, 0.0, pN, pdNdr);
+      transform_gradients(dim, s.npe, pdNdr, pxs, pdNdx, &pJ);
+
+      for (size_t ie = 0; ie < cc.sub.size(); ++ie) {
+        const std::vector<int>& sub = cc.sub[ie];
+        const int nsn = (int)sub.size();
+        int stype;
+        if (dim == 2) stype = (nsn == 3) ? SUB_TRI3 : (nsn == 4 ? SUB_QUAD4 : SUB_POLYGON);
+        else stype = (nsn == 4) ? SUB_TET4 : (nsn == 6 ? SUB_PRISM6 : SUB_HEX8);
+        const int mat = (cc.sub_mat[ie] < 0) ? s.elem_mat[e] : 1;
+        A.sub_type.push_back(stype);
+        A.sub_mat.push_back(mat);
+        std::vector<int> gsub(nsn);
+        double sx[32 * 3];
+        for (int q = 0; q < nsn; ++q) {
+          gsub[q] = enodes[sub[q]];
+          A.sub_nodes.push_back(gsub[q]);
+          for (int k = 0; k < dim; ++k) sx[q * dim + k] = X3of(gsub[q])[k];
         }
-        s.coh_qp_off.push_back((int)s.cqp_wgt.size());
-        continue;
+        A.sub_node_off.push_back((int)A.sub_nodes.size());
+        int nqp = 0;
+        if (stype == SUB_TRI3) nqp = 4;
+        else if (stype == SUB_QUAD4) nqp = 4;
+        else if (stype == SUB_POLYGON) nqp = 4 * nsn;
+        else if (stype == SUB_TET4) nqp = 5;
+        else { A.error = "prism6 / hex8 sub-elements do not occur after the prism decomposition"; A.rc = 6; return; }
+        for (int qp = 0; qp < nqp; ++qp) {
+          double r, t, w, cN[32], cdN[96], cdNdx[96], cJ;
+          if (stype == SUB_TRI3) { r = kTri4[qp][0]; t = kTri4[qp][1]; w = kTri4[qp][2]; tri3_shape(r, t, cN, cdN); }
+          else if (stype == SUB_QUAD4) { quad4_qp(qp, &r, &t, &w); quad4_shape(r, t, cN, cdN); }
+          else if (stype == SUB_POLYGON) { poly_qp(nsn, qp, &r, &t, &w); poly_shape(nsn, r, t, cN, cdN); }
+          else { w = kTet5[qp][3]; tet4_shape(kTet5[qp][0], kTet5[qp][1], kTet5[qp][2], cN, cdN); }
+          transform_gradients(dim, nsn, cdN, sx, cdNdx, &cJ);
+          if (cJ < 0.0) { A.error = "negative sub-element Jacobian (src/Mesh.cpp:1561)"; A.rc = 7; return; }
+          A.qp_wgt.push_back(cJ * w);
+          A.qp_mat.push_back(mat);
+          // gradients over the element's nodes: parent gradients, then the child gradient of the
+          // sub-element node that is each enrichment node (zero when the sub-element lacks it)
+          for (int q = 0; q < s.npe; ++q) for (int k = 0; k < dim; ++k) A.qp_grad.push_back(pdNdx[q * dim + k]);
+          for (int en = 0; en < n_en; ++en) {
+            const int id = enodes[s.npe + en];
+            int found = -1;
+            for (int q = 0; q < nsn; ++q) if (gsub[q] == id) { found = q; break; }
+            for (int k = 0; k < dim; ++k) A.qp_grad.push_back(found >= 0 ? 1.0 * cdNdx[found * dim + k] : 0.0);
+          }
+          A.qp_grad_off.push_back((int)A.qp_grad.size());
+        }
+        A.sub_qp_off.push_back((int)A.qp_wgt.size());
       }
-      for (int qp = 0; qp < 2; ++qp) {
-        const double xi = (qp == 0) ? -kGauss2 : kGauss2;
-        const double w = 1.0;
-        const double N0 = 0.5 * (1.0 - xi), N1 = 0.5 * (1 + xi);
-        const double* x0 = X3of(enodes[cl[0]]);
-        const double* x1 = X3of(enodes[cl[1]]);
-        double Jac[2] = {0.0, 0.0};
-        for (int i = 0; i < 2; ++i) { Jac[i] += -0.5 * x0[i]; Jac[i] += 0.5 * x1[i]; }
-        const double nrm[2] = {-Jac[1], Jac[0]};
-        const double mag = std::sqrt(Jac[0] * Jac[0] + Jac[1] * Jac[1]);
-        const double dA = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1]);
-        s.cqp_N.push_back(N0 * 1.0);
-        s.cqp_N.push_back(N1 * 1.0);
-        s.cqp_R.push_back(Jac[0] / mag); s.cqp_R.push_back(Jac[1] / mag);
-        s.cqp_R.push_back(nrm[0] / dA);  s.cqp_R.push_back(nrm[1] / dA);
-        s.cqp_wgt.push_back(dA * w);
-        s.cqp_isv.push_back(s.n_isv);
-        s.n_isv += s.coh.nvar;
+      A.cut_sub_off.push_back((int)A.sub_type.size());
+      A.cut_qp_off.push_back((int)A.qp_wgt.size());
+
+      // cohesive elements (CohEdge2, 2-point Gauss; rotation from the '-' side nodes)
+      for (size_t ce = 0; ce < cc.coh.size(); ++ce) {
+        const std::vector<int>& cl = cc.coh[ce];
+        const int nh = (int)cl.size() / 2;
+        A.coh_nh.push_back(nh);
+        for (int v : cl) A.coh_local.push_back(v);
+        A.coh_local_off.push_back((int)A.coh_local.size());
+        if (dim == 3) {
+          // CohTri3 (4-point tri rule, src/CohTri3.cpp:70-84) or CohQuad4 (2 x 2 Gauss, qp -> (qp % 2,
+          // qp / 2), src/CohQuad4.cpp:55-70); rotation rows (dx/dr, dx/ds, their cross product)
+          // normalised, from the '-' side nodes (CohesiveElem::compute_rotation_general).
+          const int nq = 4;
+          for (int qp = 0; qp < nq; ++qp) {
+            double r, t, w, N[4], dN[8];
+            if (nh == 3) { r = kTri4[qp][0]; t = kTri4[qp][1]; w = kTri4[qp][2]; tri3_shape(r, t, N, dN); }
+            else if (nh == 4) { quad4_qp(qp, &r, &t, &w); quad4_shape(r, t, N, dN); }
+            else { A.error = "internal: 3D cohesive element with an unexpected node count"; A.rc = 6; return; }
+            double Jac[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+            for (int n = 0; n < nh; ++n) {
+              const double* xn = X3of(enodes[cl[n]]);
+              for (int a = 0; a < 2; ++a) for (int i = 0; i < 3; ++i) Jac[a][i] += dN[n * 2 + a] * xn[i];
+            }
+            double nrm[3];
+            nrm[0] = Jac[0][1] * Jac[1][2] - Jac[0][2] * Jac[1][1];
+            nrm[1] = -(Jac[0][0] * Jac[1][2] - Jac[0][2] * Jac[1][0]);
+            nrm[2] = Jac[0][0] * Jac[1][1] - Jac[0][1] * Jac[1][0];
+            double mag[2];
+            for (int a = 0; a < 2; ++a) {
+              double dd = 0.0;
+              for (int i = 0; i < 3; ++i) dd += Jac[a][i] * Jac[a][i];
+              mag[a] = std::sqrt(dd);
+            }
+            double nn = 0.0;
+            for (int i = 0; i < 3; ++i) nn += nrm[i] * nrm[i];
+            const double dA = std::sqrt(nn);
+            for (int n = 0; n < nh; ++n) A.cqp_N.push_back(N[n] * 1.0);
+            for (int a = 0; a < 2; ++a) for (int i = 0; i < 3; ++i) A.cqp_R.push_back(Jac[a][i] / mag[a]);
+            for (int i = 0; i < 3; ++i) A.cqp_R.push_back(nrm[i] / dA);
+            A.cqp_wgt.push_back(dA * w);
+            A.cqp_isv.push_back(A.n_isv);
+            A.n_isv += s.coh.nvar;
+          }
+          A.coh_qp_off.push_back((int)A.cqp_wgt.size());
+          continue;
+        }
+        for (int qp = 0; qp < 2; ++qp) {
+          const double xi = (qp == 0) ? -kGauss2 : kGauss2;
+          const double w = 1.0;
+          const double N0 = 0.5 * (1.0 - xi), N1 = 0.5 * (1 + xi);
+          const double* x0 = X3of(enodes[cl[0]]);
+          const double* x1 = X3of(enodes[cl[1]]);
+          double Jac[2] = {0.0, 0.0};
+          for (int i = 0; i < 2; ++i) { Jac[i] += -0.5 * x0[i]; Jac[i] += 0.5 * x1[i]; }
+          const double nrm[2] = {-Jac[1], Jac[0]};
+          const double mag = std::sqrt(Jac[0] * Jac[0] + Jac[1] * Jac[1]);
+          const double dA = std::sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1]);
+          A.cqp_N.push_back(N0 * 1.0);
+          A.cqp_N.push_back(N1 * 1.0);
+          A.cqp_R.push_back(Jac[0] / mag); A.cqp_R.push_back(Jac[1] / mag);
+          A.cqp_R.push_back(nrm[0] / dA);  A.cqp_R.push_back(nrm[1] / dA);
+          A.cqp_wgt.push_back(dA * w);
+          A.cqp_isv.push_back(A.n_isv);
+          A.n_isv += s.coh.nvar;
+        }
+        A.coh_qp_off.push_back((int)A.cqp_wgt.size());
       }
-      s.coh_qp_off.push_back((int)s.cqp_wgt.size());
+      A.cut_coh_off.push_back((int)A.coh_nh.size());
     }
-    s.cut_coh_off.push_back((int)s.coh_nh.size());
+  };
+  chunked(s.ncut, ntc, cut_chunk);
+  for (const CutAcc& A : accs)
+    if (A.rc) { s.error = A.error; return A.rc; }
+  // Concatenation: every chunk's slice of each array starts after the earlier chunks' slices;
+  // offset arrays (one entry per item after a leading 0) are shifted by the earlier chunks' sizes
+  // of the array they index.  The chunks copy their slices in parallel.
+  struct Slice { size_t cut_nodes, sub_type, sub_nodes, qp_wgt, qp_grad, coh_nh, coh_local, cqp_wgt, cqp_N, cqp_R;
+                 size_t ncut, nsub, nqp, ncoh; int isv; };
+  std::vector<Slice> at(accs.size() + 1, Slice{0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0});
+  for (size_t k = 0; k < accs.size(); ++k) {
+    const CutAcc& A = accs[k];
+    Slice n = at[k];
+    n.cut_nodes += A.cut_nodes.size(); n.sub_type += A.sub_type.size(); n.sub_nodes += A.sub_nodes.size();
+    n.qp_wgt += A.qp_wgt.size(); n.qp_grad += A.qp_grad.size(); n.coh_nh += A.coh_nh.size();
+    n.coh_local += A.coh_local.size(); n.cqp_wgt += A.cqp_wgt.size(); n.cqp_N += A.cqp_N.size(); n.cqp_R += A.cqp_R.size();
+    n.ncut += A.cut_node_off.size(); n.nsub += A.sub_node_off.size(); n.nqp += A.qp_grad_off.size(); n.ncoh += A.coh_qp_off.size();
+    n.isv += A.n_isv;
+    at[k + 1] = n;
   }
+  const Slice& T = at[accs.size()];
+  if (T.qp_grad > 2147483647ULL || T.cqp_R > 2147483647ULL) { s.error = "cut-element tables beyond 2^31 entries"; return 2; }
+  s.cut_nodes.resize(T.cut_nodes); s.sub_type.resize(T.sub_type); s.sub_mat.resize(T.sub_type);
+  s.sub_nodes.resize(T.sub_nodes); s.qp_wgt.resize(T.qp_wgt); s.qp_mat.resize(T.qp_wgt); s.qp_grad.resize(T.qp_grad);
+  s.coh_nh.resize(T.coh_nh); s.coh_local.resize(T.coh_local); s.cqp_wgt.resize(T.cqp_wgt); s.cqp_isv.resize(T.cqp_wgt);
+  s.cqp_N.resize(T.cqp_N); s.cqp_R.resize(T.cqp_R);
+  s.cut_node_off.assign(T.ncut + 1, 0); s.cut_sub_off.assign(T.ncut + 1, 0); s.cut_qp_off.assign(T.ncut + 1, 0);
+  s.cut_coh_off.assign(T.ncut + 1, 0);
+  s.sub_node_off.assign(T.nsub + 1, 0); s.sub_qp_off.assign(T.nsub + 1, 0);
+  s.qp_grad_off.assign(T.nqp + 1, 0);
+  s.coh_local_off.assign(T.ncoh + 1, 0); s.coh_qp_off.assign(T.ncoh + 1, 0);
+  const int isv0 = s.n_isv;
+  chunked((int)accs.size(), (int)accs.size(), [&](int, int k0, int k1) {
+    for (int k = k0; k < k1; ++k) {
+      const CutAcc& A = accs[k];
+      const Slice& o = at[k];
+      auto put = [](std::vector<int>& dst, size_t pos, const std::vector<int>& src, long long base) {
+        for (size_t i = 0; i < src.size(); ++i) dst[pos + i] = (int)(base + src[i]);
+      };
+      put(s.cut_node_off, 1 + o.ncut, A.cut_node_off, (long long)o.cut_nodes);
+      put(s.cut_sub_off, 1 + o.ncut, A.cut_sub_off, (long long)o.sub_type);
+      put(s.cut_qp_off, 1 + o.ncut, A.cut_qp_off, (long long)o.qp_wgt);
+      put(s.cut_coh_off, 1 + o.ncut, A.cut_coh_off, (long long)o.coh_nh);
+      put(s.sub_node_off, 1 + o.nsub, A.sub_node_off, (long long)o.sub_nodes);
+      put(s.sub_qp_off, 1 + o.nsub, A.sub_qp_off, (long long)o.qp_wgt);
+      put(s.qp_grad_off, 1 + o.nqp, A.qp_grad_off, (long long)o.qp_grad);
+      put(s.coh_local_off, 1 + o.ncoh, A.coh_local_off, (long long)o.coh_local);
+      put(s.coh_qp_off, 1 + o.ncoh, A.coh_qp_off, (long long)o.cqp_wgt);
+      put(s.cqp_isv, o.cqp_wgt, A.cqp_isv, (long long)isv0 + o.isv);
+      std::copy(A.cut_nodes.begin(), A.cut_nodes.end(), s.cut_nodes.begin() + o.cut_nodes);
+      std::copy(A.sub_type.begin(), A.sub_type.end(), s.sub_type.begin() + o.sub_type);
+      std::copy(A.sub_mat.begin(), A.sub_mat.end(), s.sub_mat.begin() + o.sub_type);
+      std::copy(A.sub_nodes.begin(), A.sub_nodes.end(), s.sub_nodes.begin() + o.sub_nodes);
+      std::copy(A.qp_wgt.begin(), A.qp_wgt.end(), s.qp_wgt.begin() + o.qp_wgt);
+      std::copy(A.qp_mat.begin(), A.qp_mat.end(), s.qp_mat.begin() + o.qp_wgt);
+      std::copy(A.qp_grad.begin(), A.qp_grad.end(), s.qp_grad.begin() + o.qp_grad);
+      std::copy(A.coh_nh.begin(), A.coh_nh.end(), s.coh_nh.begin() + o.coh_nh);
+      std::copy(A.coh_local.begin(), A.coh_local.end(), s.coh_local.begin() + o.coh_local);
+      std::copy(A.cqp_wgt.begin(), A.cqp_wgt.end(), s.cqp_wgt.begin() + o.cqp_wgt);
+      std::copy(A.cqp_N.begin(), A.cqp_N.end(), s.cqp_N.begin() + o.cqp_N);
+      std::copy(A.cqp_R.begin(), A.cqp_R.end(), s.cqp_R.begin() + o.cqp_R);
+    }
+  });
+  s.n_isv += T.isv;
 
   // ---------------- DOF numbering (DofObject::set_local_owned_normal_dofs / _enrich_dofs)
   // Dirichlet conditions as Tests/Main.cpp:549-581 applies them.
@@ -903,44 +1010,83 @@ int build_setup(const ProblemDesc& d, Setup& s) {
   for (int n = 0; n < n_nodes; ++n)
     if (s.dnode[n] == n) { s.node_dn[n] = s.n_dn++; s.dn_node.push_back(n); }
   for (int n = 0; n < n_nodes; ++n) s.node_dn[n] = s.node_dn[s.dnode[n]];
-  std::vector<std::vector<int>> adj(s.n_dn);
-  std::vector<std::vector<int>> nb(s.n_dn);
-  auto elem_nodes = [&](int e, std::vector<int>& out) {
-    out.clear();
-    if (s.cut_of[e] < 0) for (int q = 0; q < s.npe; ++q) out.push_back(s.conn[(size_t)e * s.npe + q]);
-    else {
-      const int c = s.cut_of[e];
-      for (int k = s.cut_node_off[c]; k < s.cut_node_off[c + 1]; ++k) out.push_back(s.cut_nodes[k]);
-    }
+  // Adjacency of every DOF node in element order (element, local node) and its sorted distinct
+  // neighbours.  Elements are split into contiguous chunks; each chunk counts its entries per DOF
+  // node, the counts place every chunk's entries after the earlier chunks' (so each node's list
+  // stays in element order), and the chunks fill their places in parallel.
+  auto elem_n = [&](int e) {
+    const int c = s.cut_of[e];
+    return c < 0 ? s.npe : s.cut_node_off[c + 1] - s.cut_node_off[c];
   };
-  std::vector<int> en;
-  for (int e = 0; e < s.ne; ++e) {
-    elem_nodes(e, en);
-    if ((int)en.size() > 32) { s.error = "element with more than 32 nodes"; return 8; }
-    for (size_t a = 0; a < en.size(); ++a) {
-      const int da = s.node_dn[en[a]];
-      adj[da].push_back(e * 32 + (int)a);
-      for (size_t b = 0; b < en.size(); ++b) nb[da].push_back(s.node_dn[en[b]]);
+  auto elem_node = [&](int e, int a) {
+    const int c = s.cut_of[e];
+    return c < 0 ? s.conn[(size_t)e * s.npe + a] : s.cut_nodes[s.cut_node_off[c] + a];
+  };
+  for (int e = 0; e < s.ne; ++e)
+    if (elem_n(e) > 32) { s.error = "element with more than 32 nodes"; return 8; }
+  const int nt = setup_threads();
+  std::vector<std::vector<long long>> cadj(nt, std::vector<long long>(s.n_dn, 0)), cnb(nt, std::vector<long long>(s.n_dn, 0));
+  chunked(s.ne, nt, [&](int k, int e0, int e1) {
+    for (int e = e0; e < e1; ++e) {
+      const int m = elem_n(e);
+      for (int a = 0; a < m; ++a) {
+        const int da = s.node_dn[elem_node(e, a)];
+        cadj[k][da] += 1;
+        cnb[k][da] += m;
+      }
     }
-  }
-  s.dn_adj_off.assign(1, 0);
-  s.dn_nbr_off.assign(1, 0);
+  });
+  std::vector<long long> adj_off(s.n_dn + 1, 0), nb_off(s.n_dn + 1, 0);
   for (int a = 0; a < s.n_dn; ++a) {
-    std::sort(nb[a].begin(), nb[a].end());
-    nb[a].erase(std::unique(nb[a].begin(), nb[a].end()), nb[a].end());
-    for (int v : adj[a]) s.dn_adj.push_back(v);
-    s.dn_adj_off.push_back((int)s.dn_adj.size());
-    for (int v : nb[a]) s.dn_nbr.push_back(v);
-    s.dn_nbr_off.push_back((int)s.dn_nbr.size());
+    long long ta = adj_off[a], tb = nb_off[a];
+    for (int k = 0; k < nt; ++k) {
+      const long long ca = cadj[k][a], cb = cnb[k][a];
+      cadj[k][a] = ta; cnb[k][a] = tb;   // the chunk's first place for this node
+      ta += ca; tb += cb;
+    }
+    adj_off[a + 1] = ta; nb_off[a + 1] = tb;
   }
+  if (adj_off[s.n_dn] > 2147483647LL || nb_off[s.n_dn] > 2147483647LL) { s.error = "mesh too large"; return 2; }
+  s.dn_adj.assign((size_t)adj_off[s.n_dn], 0);
+  std::vector<int> nb_all((size_t)nb_off[s.n_dn]);
+  chunked(s.ne, nt, [&](int k, int e0, int e1) {
+    for (int e = e0; e < e1; ++e) {
+      const int m = elem_n(e);
+      for (int a = 0; a < m; ++a) {
+        const int da = s.node_dn[elem_node(e, a)];
+        s.dn_adj[(size_t)cadj[k][da]++] = e * 32 + a;
+        long long& p = cnb[k][da];
+        for (int b = 0; b < m; ++b) nb_all[(size_t)p++] = s.node_dn[elem_node(e, b)];
+      }
+    }
+  });
+  s.dn_adj_off.resize(s.n_dn + 1);
+  for (int a = 0; a <= s.n_dn; ++a) s.dn_adj_off[a] = (int)adj_off[a];
+  std::vector<int> nb_cnt(s.n_dn);
+  chunked(s.n_dn, nt, [&](int, int a0, int a1) {
+    for (int a = a0; a < a1; ++a) {
+      int* b = nb_all.data() + nb_off[a];
+      int* e = nb_all.data() + nb_off[a + 1];
+      std::sort(b, e);
+      nb_cnt[a] = (int)(std::unique(b, e) - b);
+    }
+  });
+  s.dn_nbr_off.assign(s.n_dn + 1, 0);
+  for (int a = 0; a < s.n_dn; ++a) s.dn_nbr_off[a + 1] = s.dn_nbr_off[a] + nb_cnt[a];
+  s.dn_nbr.resize(s.dn_nbr_off[s.n_dn]);
+  chunked(s.n_dn, nt, [&](int, int a0, int a1) {
+    for (int a = a0; a < a1; ++a)
+      std::copy(nb_all.begin() + nb_off[a], nb_all.begin() + nb_off[a] + nb_cnt[a], s.dn_nbr.begin() + s.dn_nbr_off[a]);
+  });
   // CSR of the four blocks; rows in DOF order follow DOF-node order.
   s.nrows[0] = s.n_free; s.ncols[0] = s.n_free;
   s.nrows[1] = s.n_free; s.ncols[1] = s.n_const;
   s.nrows[2] = s.n_const; s.ncols[2] = s.n_free;
   s.nrows[3] = s.n_const; s.ncols[3] = s.n_const;
   for (int b = 0; b < 4; ++b) { s.rp[b].assign(s.nrows[b] + 1, 0); s.ci[b].clear(); }
-  // row lengths
-  for (int a = 0; a < s.n_dn; ++a) {
+  // row lengths (each DOF node writes only its own rows' entries)
+  chunked(s.n_dn, nt, [&](int, int a0, int a1) {
+  for (int a = a0; a < a1; ++a) {
     const int na = s.dn_node[a];
     int cf = 0, cp = 0;
     for (int k = s.dn_nbr_off[a]; k < s.dn_nbr_off[a + 1]; ++k) {
@@ -953,9 +1099,11 @@ int build_setup(const ProblemDesc& d, Setup& s) {
       else { s.rp[2][g - s.n_free + 1] = cf; s.rp[3][g - s.n_free + 1] = cp; }
     }
   }
+  });
   for (int b = 0; b < 4; ++b) for (int r = 0; r < s.nrows[b]; ++r) s.rp[b][r + 1] += s.rp[b][r];
   for (int b = 0; b < 4; ++b) s.ci[b].assign(s.rp[b][s.nrows[b]], -1);
-  for (int a = 0; a < s.n_dn; ++a) {
+  chunked(s.n_dn, nt, [&](int, int a0, int a1) {
+  for (int a = a0; a < a1; ++a) {
     const int na = s.dn_node[a];
     for (int q = 0; q < dim; ++q) {
       const int g = s.node_dof[(size_t)na * dim + q];
@@ -973,6 +1121,7 @@ int build_setup(const ProblemDesc& d, Setup& s) {
       }
     }
   }
+  });
   return 0;
 }
 
