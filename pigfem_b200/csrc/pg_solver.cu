@@ -31,7 +31,7 @@ struct PcgArgs {
   int n, nrhs, nb;
   double rtol;
   const double* dinv;
-  double *x, *r, *z, *p, *q;
+  double *x, *r, *z, *p, *q;   // p interleaved by right-hand side: p[i * nrhs + s]; the others [s][n]
   double* part;   // [3][nrhs][nb]
   double* sc;     // [nrhs][S_NSC]
   int* flag;      // [0, nrhs) done, [nrhs, 2 nrhs) iterations, [2 nrhs] active count
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_start(PcgArgs a, const double*
       if (i < r1 && lane == 0) {
         const double ri = b[o + i] - ax;
         const double zi = a.dinv[i] * ri;
-        a.r[o + i] = ri; a.z[o + i] = zi; a.p[o + i] = zi;
+        a.r[o + i] = ri; a.z[o + i] = zi; a.p[(size_t)i * a.nrhs + s] = zi;
         rz += ri * zi; bb += b[o + i] * b[o + i]; rr += ri * ri;
       }
     }
@@ -127,26 +127,51 @@ __global__ void __launch_bounds__(kThreads) k_pcg_start_reduce(PcgArgs a) {
   }
 }
 
-// q = A p; partials of p.q
+// q = A p; partials of p.q.  The right-hand sides still iterating share one pass over the matrix
+// (up to kSpmvRhs at a time): each row's values and column indices are read once and multiplied
+// with every right-hand side's p, whose values for one column are adjacent (p is interleaved by
+// right-hand side).  Each right-hand side's sums are the ones row_dot forms (same lane-strided
+// products, same shuffle tree), so its iterates do not depend on the others.
+constexpr int kSpmvRhs = 8;
 __global__ void __launch_bounds__(kThreads) k_pcg_spmv(PcgArgs a) {
   __shared__ double sh[kThreads];
   if (a.flag[2 * a.nrhs] == 0) return;
   int r0, r1;
   block_rows(a.n, a.nb, &r0, &r1);
   const int grp = threadIdx.x / kRowGroup, lane = threadIdx.x % kRowGroup, ngrp = kThreads / kRowGroup;
-  for (int s = 0; s < a.nrhs; ++s) {
-    if (a.flag[s]) continue;
-    const size_t o = (size_t)s * a.n;
-    double pq = 0.0;
+  for (int s0 = 0; s0 < a.nrhs; s0 += kSpmvRhs) {
+    const int ns = min(kSpmvRhs, a.nrhs - s0);
+    bool act[kSpmvRhs];
+    double pq[kSpmvRhs];
+#pragma unroll
+    for (int j = 0; j < kSpmvRhs; ++j) { act[j] = j < ns && !a.flag[s0 + j]; pq[j] = 0.0; }
     for (int i0 = r0; i0 < r1; i0 += ngrp) {
       const int i = i0 + grp;
-      const double ap = row_dot(a, a.p + o, i, i < r1);
-      if (i < r1 && lane == 0) {
-        a.q[o + i] = ap;
-        pq += a.p[o + i] * ap;
+      const bool valid = i < r1;
+      double v[kSpmvRhs];
+#pragma unroll
+      for (int j = 0; j < kSpmvRhs; ++j) v[j] = 0.0;
+      const int k0 = valid ? a.rp[i] : 0, k1 = valid ? a.rp[i + 1] : 0;
+      for (int k = k0 + lane; k < k1; k += kRowGroup) {
+        const double av = a.val[k];
+        const int c = a.ci[k];
+#pragma unroll
+        for (int j = 0; j < kSpmvRhs; ++j)
+          if (act[j]) v[j] += av * a.p[(size_t)c * a.nrhs + s0 + j];
+      }
+#pragma unroll
+      for (int j = 0; j < kSpmvRhs; ++j) {
+        if (!act[j]) continue;   // uniform over the block
+#pragma unroll
+        for (int o = kRowGroup / 2; o > 0; o >>= 1) v[j] += __shfl_down_sync(0xffffffffu, v[j], o, kRowGroup);
+        if (valid && lane == 0) {
+          a.q[(size_t)(s0 + j) * a.n + i] = v[j];
+          pq[j] += a.p[(size_t)i * a.nrhs + s0 + j] * v[j];
+        }
       }
     }
-    block_sum(sh, pq, &a.part[(0 * a.nrhs + s) * a.nb + blockIdx.x]);
+    for (int j = 0; j < ns; ++j)
+      if (act[j]) block_sum(sh, pq[j], &a.part[(0 * a.nrhs + s0 + j) * a.nb + blockIdx.x]);
   }
 }
 
@@ -177,7 +202,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_update(PcgArgs a) {
     const double al = a.sc[s * S_NSC + S_ALPHA];
     double rz = 0.0, rr = 0.0;
     for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
-      a.x[o + i] += al * a.p[o + i];
+      a.x[o + i] += al * a.p[(size_t)i * a.nrhs + s];
       const double ri = a.r[o + i] - al * a.q[o + i];
       const double zi = a.dinv[i] * ri;
       a.r[o + i] = ri; a.z[o + i] = zi;
@@ -224,7 +249,10 @@ __global__ void __launch_bounds__(kThreads) k_pcg_dir(PcgArgs a) {
     if (a.flag[s]) continue;
     const size_t o = (size_t)s * a.n;
     const double be = a.sc[s * S_NSC + S_BETA];
-    for (int i = r0 + threadIdx.x; i < r1; i += kThreads) a.p[o + i] = a.z[o + i] + be * a.p[o + i];
+    for (int i = r0 + threadIdx.x; i < r1; i += kThreads) {
+      double& pi = a.p[(size_t)i * a.nrhs + s];
+      pi = a.z[o + i] + be * pi;
+    }
   }
 }
 
@@ -248,7 +276,7 @@ int pcg_reserve(pg_ctx* c, int nrhs) {
   }
   w.n = n;
   w.cap_rhs = nrhs;
-  w.nb = 2 * 148;
+  w.nb = 8 * 148;   // row ranges: enough blocks in flight to hide the matrix-vector latency
   int rc = 0;
   if (!w.dinv) rc |= pg_dalloc(c, (size_t)n, &w.dinv);
   if (!w.ci) {
