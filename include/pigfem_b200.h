@@ -112,6 +112,18 @@ int pg_assemble(pg_ctx* ctx, const double* U_node_major, double t_frac, int flag
 /* Same, on device-resident data: d_U is a 16-byte aligned device pointer (n_nodes*dim); results
  * stay in the context's device buffers (pg_device_outputs). */
 int pg_assemble_device(pg_ctx* ctx, const double* d_U, double t_frac, int flags);
+/* Residuals of several macroscale strains in one pass, for subscale problems: the load cases of a
+ * homogenization, which the reference assembles one Assembler::assemble(assembleJac = false) at a
+ * time after Assembler::assemble_new_load_step sets each case's macroscale value
+ * (src/Assembler.cpp:65-146, 394-511).  Case k's strain is eps[6k .. 6k+5] * t_frac (Voigt; the 3D
+ * entries are ignored in 2D); its residual parts go to d_Rf[k * n_free ...] and d_Rp[k * n_const
+ * ...] (device arrays; d_Rp may be NULL when n_const = 0).  Each case's values are those of a
+ * residual-only pg_assemble_device with that strain, up to the rounding of fused multiply-adds;
+ * the openings, laws and internal variables of the cohesive points are evaluated once (they
+ * depend on U only).  K and the context's own residual buffers are left as they are.
+ * 1 <= n_cases <= 6.  Asynchronous on the context's stream. */
+int pg_residual_strains(pg_ctx* ctx, const double* d_U, double t_frac, int n_cases, const double* eps,
+                        double* d_Rf, double* d_Rp);
 /* Device pointers of the outputs: K values (4 blocks), P_f, P_p. */
 int pg_device_outputs(pg_ctx* ctx, double** K_vals4, double** P_f, double** P_p);
 /* Stream the context launches on (a cudaStream_t, 0 = legacy default). */

@@ -33,7 +33,7 @@ ERRORS = {2: "PG_ERR_INPUT", 3: "PG_ERR_GEOMETRY", 4: "PG_ERR_UNSUPPORTED", 7: "
 # Every symbol include/pigfem_b200.h declares.
 EXPORTED = [
     "pg_create", "pg_create_host", "pg_upload", "pg_debug_array", "pg_destroy", "pg_last_error",
-    "pg_get_sizes", "pg_get_pattern", "pg_get_nodes", "pg_assemble", "pg_assemble_device",
+    "pg_get_sizes", "pg_get_pattern", "pg_get_nodes", "pg_assemble", "pg_assemble_device", "pg_residual_strains",
     "pg_device_outputs", "pg_set_stream", "pg_set_isv", "pg_get_isv", "pg_commit_isv",
     "pg_get_damage_zones", "pg_residual_norm", "pg_set_timing", "pg_kernel_times", "pg_set_macro_strain",
     "pg_pcg_solve", "pg_homogenize", "pg_norm2_noalloc",
@@ -91,6 +91,7 @@ def load_library(path: Optional[str] = None):
         "pg_get_nodes": (i32, [vp, p, p, p]),
         "pg_assemble": (i32, [vp, p, dbl, i32, p, p, p, p, p, p]),
         "pg_assemble_device": (i32, [vp, p, dbl, i32]),
+        "pg_residual_strains": (i32, [vp, vp, dbl, i32, p, vp, vp]),
         "pg_device_outputs": (i32, [vp, p, p, p]),
         "pg_set_stream": (i32, [vp, vp]),
         "pg_set_isv": (i32, [vp, p]),
@@ -312,6 +313,17 @@ class Problem:
         self._check(load_library().pg_pcg_solve(self.h, ctypes.c_void_p(d_b), ctypes.c_void_p(d_x), int(nrhs),
                                                 float(rtol), int(max_it), _ptr(it), _ptr(rr)))
         return it, rr
+
+    def residual_strains(self, d_U: int, eps_cases, d_Rf: int, d_Rp: int = 0, t_frac: float = 1.0):
+        """Residuals of several macroscale strains in one pass (subscale problems): eps_cases is
+        n_cases x (3 or 6) Voigt strains; case k's residual parts land in the device arrays at
+        d_Rf + k * n_free and d_Rp + k * n_const (doubles)."""
+        e = np.zeros((len(eps_cases), 6))
+        for k, ek in enumerate(eps_cases):
+            e[k, :len(ek)] = ek
+        e = np.ascontiguousarray(e)
+        self._check(load_library().pg_residual_strains(self.h, ctypes.c_void_p(d_U), float(t_frac), len(eps_cases),
+                                                       _ptr(e), ctypes.c_void_p(d_Rf), ctypes.c_void_p(d_Rp or None)))
 
     def homogenize(self, d_U: int, t_frac: float = 1.0) -> np.ndarray:
         """Volume-averaged stress (Voigt) and the integrated volume as the last entry."""

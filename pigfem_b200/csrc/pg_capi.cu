@@ -713,6 +713,46 @@ int pg_assemble_device(pg_ctx* c, const double* d_U, double t_frac, int flags) {
   return rc;
 }
 
+int pg_residual_strains(pg_ctx* c, const double* d_U, double t_frac, int n_cases, const double* eps, double* d_Rf,
+                        double* d_Rp) {
+  if (!c || !d_U || !eps || !d_Rf || n_cases < 1 || n_cases > 6) return PG_ERR_INPUT;
+  if (reinterpret_cast<uintptr_t>(d_U) % 16) return set_err(c, PG_ERR_INPUT, "the displacement array must be 16-byte aligned");
+  if (!c->s.desc.subscale) return set_err(c, PG_ERR_INPUT, "macroscale strain cases need a subscale (periodic) problem");
+  if (c->s.n_const > 0 && !d_Rp) return set_err(c, PG_ERR_INPUT, "d_Rp is required when the problem has constrained DOFs");
+  pgd::DevProblem P = c->P;
+  P.U = d_U;
+  P.flags = PG_FUNC;
+  for (int v = 0; v < 6; ++v) P.eps_macro[v] = 0.0;
+  P.n_cases = n_cases;
+  for (int k = 0; k < n_cases; ++k)
+    for (int v = 0; v < 6; ++v) P.eps_cases[k][v] = eps[k * 6 + v] * t_frac;
+  P.Pf_cases = d_Rf;
+  P.Pp_cases = d_Rp;
+  const int dim = c->s.dim;
+  // the cohesive elements once (openings, laws, internal variables, tractions: U only), then
+  // the stencil rows and the general rows for every case
+  if (P.n_coh_el > 0) {
+    const int lanes = (dim == 2) ? pgd::CohLanes<2>::CQ : pgd::CohLanes<3>::CQ;
+    const int grid = (int)(((long long)P.n_coh_el * lanes + 127) / 128);
+    if (dim == 2) pgd::k_coh_elements<2><<<grid, 128, 0, c->stream>>>(P);
+    else pgd::k_coh_elements<3><<<grid, 128, 0, c->stream>>>(P);
+  }
+  if (c->n_stencil > 0) {
+    const int grid = (c->n_stencil + 127) / 128;
+    if (dim == 2) pgd::k_rows_stencil_cases<2><<<grid, 128, 0, c->stream>>>(P, c->grid, c->stencil, c->n_stencil);
+    else pgd::k_rows_stencil_cases<3><<<grid, 128, 0, c->stream>>>(P, c->grid, c->stencil, c->n_stencil);
+  }
+  if (P.n_slow_dn > 0) {
+    constexpr int L = 8;
+    const int grid = (int)(((long long)P.n_slow_dn * L + 127) / 128);
+    if (dim == 2) pgd::k_rows_general_cases<2, L><<<grid, 128, 0, c->stream>>>(P);
+    else pgd::k_rows_general_cases<3, L><<<grid, 128, 0, c->stream>>>(P);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_err(c, PG_ERR_DEVICE, std::string("launch failed: ") + cudaGetErrorString(e));
+  return 0;
+}
+
 int pg_assemble(pg_ctx* c, const double* U, double t_frac, int flags, double* Kff, double* Kfp, double* Kpf, double* Kpp,
                 double* Pf, double* Pp) {
   if (!c || !U) return PG_ERR_INPUT;

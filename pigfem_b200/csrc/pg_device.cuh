@@ -92,6 +92,12 @@ struct DevProblem {
   double eps_macro[6];
   int flags;
   int* err;
+  // residual passes over several macroscale strains (pg_residual_strains): case k's strain and
+  // its residual parts, [k][n_free] and [k][n_const]
+  int n_cases;
+  double eps_cases[6][6];
+  double* Pf_cases;
+  double* Pp_cases;
 };
 
 // ---------------------------------------------------------------- cohesive laws (FP64)

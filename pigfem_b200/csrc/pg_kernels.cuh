@@ -442,6 +442,143 @@ __global__ void __launch_bounds__(128) k_rows_general_resid(DevProblem P) {
   if (gdof < P.n_free) P.Pf[gdof] = mine; else P.Pp[gdof - P.n_free] = mine;
 }
 
+// Residuals of the general rows for the P.n_cases macroscale strains of a multi-strain pass,
+// entry-parallel like k_rows_general_resid: an uncut element's geometry and strain of U are formed
+// once and each case adds its strain; a cut element's K_vol block row times U is formed once and
+// each case adds its macroscale-strain response and the traction.  For each case these are the
+// operations of the single-strain residual with that case as eps_macro, summed in entry order.
+template <int DIM, int L>
+__global__ void __launch_bounds__(128) k_rows_general_cases(DevProblem P) {
+  constexpr int NPE = DIM + 1;
+  constexpr int NV = (DIM == 2) ? 3 : 6;
+  constexpr int D2 = DIM * DIM;
+  constexpr int MC = 6;
+  const int nc = P.n_cases;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int node = t / L, k = t % L;
+  const bool valid = node < P.n_slow_dn;
+  const unsigned gmask = (L == 32) ? 0xffffffffu : (((1u << L) - 1u) << ((threadIdx.x & 31) / L * L));
+  if (__all_sync(0xffffffffu, !valid)) return;
+  int4 gd = make_int4(0, 0, 0, 0);
+  if (valid) gd = __ldg(&P.gdesc[node]);
+  double rs[MC][DIM];
+#pragma unroll
+  for (int c = 0; c < MC; ++c)
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) rs[c][q] = 0.0;
+  for (int e0 = 0; e0 < gd.y; e0 += L) {
+    const int ei = e0 + k;
+    double re[MC][DIM];
+#pragma unroll
+    for (int c = 0; c < MC; ++c)
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) re[c][q] = 0.0;
+    if (ei < gd.y) {
+      const int4 ad = __ldg(&P.adesc[gd.x + ei]);
+      const int4 ax = __ldg(&P.aresd[gd.x + ei]);
+      const int la = ad.y & 255, mn = ad.y >> 8;
+      if (mn == 0) {
+        const int nd[4] = {ax.x, ax.y, ax.z, ax.w};
+        const double* D = P.D[ad.w];
+        double x[NPE][DIM], g[NPE][DIM], J;
+#pragma unroll
+        for (int n = 0; n < NPE; ++n) load_node<DIM>(P.X, nd[n], x[n]);
+        simplex_geom<DIM, double>(x, g, &J);
+        const double wgt = J * ((DIM == 2) ? tri4_wsum() : tet5_wsum());
+        double ga[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) ga[d] = g[0][d];
+#pragma unroll
+        for (int n = 1; n < NPE; ++n)
+          if (la == n)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) ga[d] = g[n][d];
+        double eps[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) eps[v] = 0.0;
+#pragma unroll
+        for (int n = 0; n < NPE; ++n) {
+          double u[DIM];
+          load_node<DIM>(P.U, nd[n], u);
+          add_strain<DIM, double>(g[n], u, eps);
+        }
+#pragma unroll
+        for (int c = 0; c < MC; ++c) {
+          if (c >= nc) break;
+          double ek[NV], sig[NV];
+#pragma unroll
+          for (int v = 0; v < NV; ++v) ek[v] = eps[v] + P.eps_cases[c][v];
+          lei_stress<DIM, double>(D, ek, sig);
+#pragma unroll
+          for (int q = 0; q < DIM; ++q) re[c][q] = wgt * bt_sig<DIM, double>(ga, sig, q);
+        }
+      } else {
+        const int* cn = P.cut_nodes + ax.y;
+        const double* kr = P.ke + ad.w;             // block row la of K_vol
+        double base[DIM];
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) base[q] = 0.0;
+        for (int b = 0; b < mn; ++b) {
+          const int nb = __ldg(&cn[b]);
+          double u[DIM];
+          load_node<DIM>(P.U, nb, u);
+#pragma unroll
+          for (int q = 0; q < DIM; ++q) {
+            double s = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) s += __ldg(&kr[b * D2 + q * DIM + d]) * u[d];
+            base[q] += s;
+          }
+        }
+        const double* gm = P.gmac + __ldg(&P.re_off[ax.x]) / DIM * DIM * NV + (size_t)la * DIM * NV;
+        double tr[DIM];
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) tr[q] = 0.0;
+        const int cpa = ax.z;
+        if (cpa >= 0) {
+          const int ce = cpa >> 5, n1 = cpa & 31;
+          const int nh = __ldg(&P.coh_nh[ce]);
+          const double sgn = (n1 >= nh) ? 1.0 : -1.0;
+          const double* tp = P.kcoh + __ldg(&P.kc_off[ce]) + nh * nh * D2 + (n1 % nh) * DIM;
+#pragma unroll
+          for (int q = 0; q < DIM; ++q) tr[q] = sgn * tp[q];
+        }
+#pragma unroll
+        for (int c = 0; c < MC; ++c) {
+          if (c >= nc) break;
+#pragma unroll
+          for (int q = 0; q < DIM; ++q) {
+            double v = base[q];
+#pragma unroll
+            for (int w = 0; w < NV; ++w) v += gm[q * NV + w] * P.eps_cases[c][w];
+            if (cpa >= 0) v += tr[q];
+            re[c][q] = v;
+          }
+        }
+      }
+    }
+    const int n_here = min(L, gd.y - e0);
+    for (int jj = 0; jj < n_here; ++jj)
+#pragma unroll
+      for (int c = 0; c < MC; ++c) {
+        if (c >= nc) break;
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) rs[c][q] += __shfl_sync(gmask, re[c][q], jj, L);
+      }
+  }
+  if (!valid || k >= DIM) return;
+  const int gdof = __ldg(&P.growd[(size_t)node * 3 * DIM + k]);
+#pragma unroll
+  for (int c = 0; c < MC; ++c) {
+    if (c >= nc) break;
+    double mine = rs[c][0];
+#pragma unroll
+    for (int q = 1; q < DIM; ++q) if (k == q) mine = rs[c][q];
+    if (gdof < P.n_free) P.Pf_cases[(size_t)c * P.n_free + gdof] = mine;
+    else P.Pp_cases[(size_t)c * P.n_const + gdof - P.n_free] = mine;
+  }
+}
+
 template <int DIM, int G>
 __global__ void __launch_bounds__(128) k_rows_general(DevProblem P, int slab_slots, int max_mn) {
   constexpr int NB = 128 / G;

@@ -296,6 +296,89 @@ __global__ void __launch_bounds__(128) k_rows_stencil(DevProblem P, GridInfo gi,
   }
 }
 
+// Residuals of one stencil node (all its rows) for the P.n_cases macroscale strains of a
+// multi-strain pass: per adjacent element the geometry and the strain of U are formed once, then
+// each case adds its strain and forms its stress and B^T sigma -- for each case the operations of
+// stencil_rows with that case as eps_macro.
+template <class S, int DIM>
+__device__ __forceinline__ void stencil_resid_cases(const DevProblem& P, const GridInfo& gi, int nid, int g0) {
+  constexpr int NPE = DIM + 1;
+  constexpr int NV = (DIM == 2) ? 3 : 6;
+  constexpr int ND = (DIM == 2) ? 5 : 12;
+  constexpr int MC = 6;
+  const int nc = P.n_cases;
+  const int sx = gi.nx + 1, sxy = sx * (gi.ny + 1);
+  const int i = nid % sx, j = (nid / sx) % (gi.ny + 1), k = nid / sxy;
+  double r[MC][DIM];
+#pragma unroll
+  for (int c = 0; c < MC; ++c)
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) r[c][q] = 0.0;
+#pragma unroll
+  for (int a = 0; a < S::NADJ; ++a) {
+    const int ci = i + S::ent(a, 0), cj = j + S::ent(a, 1), ck = k + S::ent(a, 2);
+    const int e = (DIM == 2) ? 2 * (cj * gi.nx + ci) + S::ent(a, 3) : 6 * ((ck * gi.ny + cj) * gi.nx + ci) + S::ent(a, 3);
+    const int m = __ldg(&P.emat[e]);
+    double x[NPE][DIM], u[NPE][DIM], g[NPE][DIM], J;
+#pragma unroll
+    for (int n = 0; n < NPE; ++n) {
+      const int sl = S::ent(a, 5 + n);
+      const int id = nid + S::off(sl, 0) + S::off(sl, 1) * sx + S::off(sl, 2) * sxy;
+      load_node<DIM>(P.X, id, x[n]);
+      load_node<DIM>(P.U, id, u[n]);
+    }
+    simplex_geom<DIM, double>(x, g, &J);
+    const double w = J * ((DIM == 2) ? tri4_wsum() : tet5_wsum());
+    double eps[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) eps[v] = 0;
+#pragma unroll
+    for (int n = 0; n < NPE; ++n) add_strain<DIM, double>(g[n], u[n], eps);
+    double d[ND];
+    iso_from<DIM, double>(P.D[m], d);
+    const int la = S::ent(a, 4);
+    double ga[DIM];
+#pragma unroll
+    for (int dd = 0; dd < DIM; ++dd) ga[dd] = g[0][dd];
+#pragma unroll
+    for (int n = 1; n < NPE; ++n)
+      if (la == n)
+#pragma unroll
+        for (int dd = 0; dd < DIM; ++dd) ga[dd] = g[n][dd];
+#pragma unroll
+    for (int c = 0; c < MC; ++c) {
+      if (c >= nc) break;
+      double ek[NV], sig[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) ek[v] = eps[v] + P.eps_cases[c][v];
+      lei_stress_iso<DIM, double>(d, ek, sig);
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) r[c][q] += w * bt_sig<DIM, double>(ga, sig, q);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < MC; ++c) {
+    if (c >= nc) break;
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) P.Pf_cases[(size_t)c * P.n_free + g0 + q] = r[c][q];
+  }
+}
+
+// One thread per stencil node: residuals of P.n_cases macroscale strains.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_rows_stencil_cases(DevProblem P, GridInfo gi, const int4* __restrict__ st, int n) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int4 v = __ldg(&st[t]);
+  if (v.x < 0) return;   // padding entry
+  if constexpr (DIM == 2) {
+    if (v.w == 0) stencil_resid_cases<Tri3Stencil0, 2>(P, gi, v.x, v.y);
+    else stencil_resid_cases<Tri3Stencil1, 2>(P, gi, v.x, v.y);
+  } else {
+    stencil_resid_cases<Tet4Stencil0, 3>(P, gi, v.x, v.y);
+  }
+}
+
 // Host-side copies of the tables for the set-up's check.
 struct StencilView {
   int nn, nadj, npe;

@@ -143,13 +143,11 @@ def run_request(P: capi.Problem, req: Request, stream) -> Dict[str, np.ndarray]:
             n = P.n_free
             zero = torch.zeros(nn, dtype=torch.float64, device="cuda")
             rhs = torch.empty(nv * n, dtype=torch.float64, device="cuda")
-            for k in range(nv):
-                e = [0.0] * nv
-                e[k] = 1.0
-                P.set_macro_strain(e)
-                P.assemble_device(zero.data_ptr(), 1.0, capi.FUNC | (capi.JAC if k == nv - 1 else 0))
-                _, pf, _ = P.device_outputs()
-                rhs[k * n:(k + 1) * n].copy_(capi.device_view(pf, n))
+            rhs_p = torch.empty(max(1, nv * P.n_const), dtype=torch.float64, device="cuda")
+            # K once, then the residual of every unit macroscale strain in one pass
+            P.assemble_device(zero.data_ptr(), 1.0, capi.JAC)
+            P.residual_strains(zero.data_ptr(), [list(np.eye(nv)[k]) for k in range(nv)], rhs.data_ptr(),
+                               rhs_p.data_ptr() if P.n_const else 0)
             x = torch.zeros_like(rhs)
             it, rr = P.pcg_solve(rhs.data_ptr(), x.data_ptr(), nv, 1e-8, 200000)
             _, dofs, _ = P.nodes()

@@ -200,3 +200,54 @@ def test_live_oracle_larger_meshes(oracle_lib, kw):
     assert n_stencil > 0 or c["elem_type"] == 0
     R.close()
     P.close()
+
+
+@pytest.mark.parametrize("name", ["lin_tri3_subscale", "lin_tet4_subscale"])
+def test_residual_strains_equal_single_strain_assemblies(name):
+    """pg_residual_strains: the residuals of several macroscale strains from one pass equal, case
+    by case, residual-only assemblies with each strain set alone (to 1e-14: the same operations,
+    with the compiler free to fuse other multiply-adds), the case with the fixture's strain equals
+    the reference's residual, and K is left as the last K assembly wrote it."""
+    import torch
+    from pigfem_b200 import capi
+    g = load_case(name)
+    P = build(name)
+    nv = 3 if P.dim == 2 else 6
+    U = torch.from_numpy(np.ascontiguousarray(g["U_dof"][g["node_dofs"]])).cuda()
+    fixture_eps = list(CASES[name]["eps_macro"])
+    cases = [fixture_eps] + [list(np.eye(nv)[k] * (0.5 + k)) for k in range(nv - 1)]
+    P.assemble_device(U.data_ptr(), 1.0, capi.JAC)
+    torch.cuda.synchronize()
+    K4, pf, pp = P.device_outputs()
+    k_before = capi.device_view(K4[0], P.nnz[0]).cpu().numpy().copy()
+    nf, nc = P.n_free, P.n_const
+    Rf = torch.full((len(cases) * nf,), float("nan"), dtype=torch.float64, device="cuda")
+    Rp = torch.full((max(1, len(cases) * nc),), float("nan"), dtype=torch.float64, device="cuda")
+    P.residual_strains(U.data_ptr(), cases, Rf.data_ptr(), Rp.data_ptr() if nc else 0, 0.75)
+    torch.cuda.synchronize()
+    assert np.array_equal(capi.device_view(K4[0], P.nnz[0]).cpu().numpy(), k_before)
+    for k, e in enumerate(cases):
+        P.set_macro_strain(e)
+        P.assemble_device(U.data_ptr(), 0.75, capi.FUNC)
+        torch.cuda.synchronize()
+        ref_f = capi.device_view(pf, nf).cpu().numpy()
+        got_f = Rf[k * nf:(k + 1) * nf].cpu().numpy()
+        assert rel(got_f, ref_f) <= 1e-14, (k, rel(got_f, ref_f))
+        if nc:
+            assert rel(Rp[k * nc:(k + 1) * nc].cpu().numpy(), capi.device_view(pp, nc).cpu().numpy()) <= 1e-14
+    # the fixture's own strain at t_frac = 1 against the reference's residual
+    P.residual_strains(U.data_ptr(), cases[:1], Rf.data_ptr(), Rp.data_ptr() if nc else 0, 1.0)
+    torch.cuda.synchronize()
+    assert rel(Rf[:nf].cpu().numpy(), g["P_f"]) <= FP64_TOL
+    P.close()
+
+
+def test_residual_strains_need_a_subscale_problem():
+    import torch
+    from pigfem_b200 import capi
+    P = build("coh_bl")
+    U = torch.zeros(P.n_nodes * P.dim, dtype=torch.float64, device="cuda")
+    R = torch.zeros(P.n_free + P.n_const, dtype=torch.float64, device="cuda")
+    with pytest.raises(capi.PigfemError):
+        P.residual_strains(U.data_ptr(), [[0.01, 0.0, 0.0]], R.data_ptr(), R.data_ptr())
+    P.close()
