@@ -703,6 +703,7 @@ int pg_set_stream(pg_ctx* c, void* stream) {
 
 int pg_assemble_device(pg_ctx* c, const double* d_U, double t_frac, int flags) {
   if (!c || !d_U) return PG_ERR_INPUT;
+  if (!pg_resident(c)) return set_err(c, PG_ERR_STATE, "the context has no device residency (pg_upload it first)");
   if (reinterpret_cast<uintptr_t>(d_U) % 16) return set_err(c, PG_ERR_INPUT, "the displacement array must be 16-byte aligned");
   if (!(flags & (PG_FUNC | PG_JAC))) return 0;
   double* keep = c->d_U;
@@ -716,6 +717,7 @@ int pg_assemble_device(pg_ctx* c, const double* d_U, double t_frac, int flags) {
 int pg_residual_strains(pg_ctx* c, const double* d_U, double t_frac, int n_cases, const double* eps, double* d_Rf,
                         double* d_Rp) {
   if (!c || !d_U || !eps || !d_Rf || n_cases < 1 || n_cases > 6) return PG_ERR_INPUT;
+  if (!pg_resident(c)) return set_err(c, PG_ERR_STATE, "the context has no device residency (pg_upload it first)");
   if (reinterpret_cast<uintptr_t>(d_U) % 16) return set_err(c, PG_ERR_INPUT, "the displacement array must be 16-byte aligned");
   if (!c->s.desc.subscale) return set_err(c, PG_ERR_INPUT, "macroscale strain cases need a subscale (periodic) problem");
   if (c->s.n_const > 0 && !d_Rp) return set_err(c, PG_ERR_INPUT, "d_Rp is required when the problem has constrained DOFs");
@@ -756,6 +758,7 @@ int pg_residual_strains(pg_ctx* c, const double* d_U, double t_frac, int n_cases
 int pg_assemble(pg_ctx* c, const double* U, double t_frac, int flags, double* Kff, double* Kfp, double* Kpf, double* Kpp,
                 double* Pf, double* Pp) {
   if (!c || !U) return PG_ERR_INPUT;
+  if (!pg_resident(c)) return set_err(c, PG_ERR_STATE, "the context has no device residency (pg_upload it first)");
   if (!(flags & (PG_FUNC | PG_JAC))) return 0;
   const pg::Setup& s = c->s;
   const size_t nU = (size_t)(s.n_std + s.n_enr) * s.dim;
@@ -792,6 +795,7 @@ int pg_device_outputs(pg_ctx* c, double** K, double** Pf, double** Pp) {
 
 int pg_set_isv(pg_ctx* c, const double* v) {
   if (!c || (!v && c->s.n_isv)) return PG_ERR_INPUT;
+  if (!pg_resident(c)) return set_err(c, PG_ERR_STATE, "the context has no device residency (pg_upload it first)");
   if (c->s.n_isv == 0) return 0;
   cudaMemcpyAsync(c->d_isv_committed, v, (size_t)c->s.n_isv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "copy of internal variables failed");
@@ -800,6 +804,7 @@ int pg_set_isv(pg_ctx* c, const double* v) {
 
 int pg_get_isv(const pg_ctx* c, int trial, double* out) {
   if (!c || (!out && c->s.n_isv)) return PG_ERR_INPUT;
+  if (!pg_resident(c)) return PG_ERR_STATE;
   if (c->s.n_isv == 0) return 0;
   cudaStreamSynchronize(c->stream);
   cudaMemcpyAsync(out, trial ? c->d_isv_trial : c->d_isv_committed, (size_t)c->s.n_isv * sizeof(double), cudaMemcpyDeviceToHost,
@@ -810,6 +815,7 @@ int pg_get_isv(const pg_ctx* c, int trial, double* out) {
 
 int pg_commit_isv(pg_ctx* c) {
   if (!c) return PG_ERR_INPUT;
+  if (!pg_resident(c)) return set_err(c, PG_ERR_STATE, "the context has no device residency (pg_upload it first)");
   if (c->s.n_isv == 0) return 0;
   cudaMemcpyAsync(c->d_isv_committed, c->d_isv_trial, (size_t)c->s.n_isv * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
   return cudaStreamSynchronize(c->stream) == cudaSuccess ? 0 : PG_ERR_DEVICE;
@@ -817,6 +823,7 @@ int pg_commit_isv(pg_ctx* c) {
 
 int pg_get_damage_zones(const pg_ctx* c, uint8_t* z) {
   if (!c || (!z && c->n_coh_qp)) return PG_ERR_INPUT;
+  if (!pg_resident(c)) return PG_ERR_STATE;
   if (!c->n_coh_qp) return 0;
   cudaStreamSynchronize(c->stream);
   cudaMemcpyAsync(z, c->d_zone, (size_t)c->n_coh_qp, cudaMemcpyDeviceToHost, c->stream);
@@ -833,6 +840,7 @@ int pg_set_macro_strain(pg_ctx* c, const double* eps) {
 
 int pg_residual_norm(pg_ctx* c, double* out) {
   if (!c || !out) return PG_ERR_INPUT;
+  if (!pg_resident(c)) return set_err(c, PG_ERR_STATE, "the context has no device residency (pg_upload it first)");
   const int nb = 256;
   k_sumsq_partial<<<nb, 256, 0, c->stream>>>(c->P.Pf, c->s.n_free, c->d_red);
   k_sum_final<<<1, 32, 0, c->stream>>>(c->d_red, nb, c->d_red + nb);

@@ -64,6 +64,11 @@ struct pg_ctx {
   cudaStream_t up = nullptr;
 };
 
+// Whether the context's tables are on the device (pg_create, or pg_create_host then pg_upload);
+// every entry point that launches work checks it first, so a host-only context gets
+// PG_ERR_STATE instead of kernels on null pointers.
+inline bool pg_resident(const pg_ctx* c) { return c && c->P.X != nullptr && c->d_err != nullptr; }
+
 // The allocation stream of a context (created on first use).
 int pg_alloc_stream(pg_ctx* c);
 

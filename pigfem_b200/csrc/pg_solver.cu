@@ -385,6 +385,7 @@ extern "C" {
 int pg_pcg_solve(pg_ctx* c, const double* d_b, double* d_x, int nrhs, double rtol, int max_it, int* iters,
                  double* relres) {
   if (!c || !d_b || !d_x || nrhs < 1 || nrhs > 16 || !(rtol > 0.0) || max_it < 1) return PG_ERR_INPUT;
+  if (!pg_resident(c)) return pg_set_err(c, PG_ERR_STATE, "the context has no device residency (pg_upload it first)");
   if (!c->assembled) return pg_set_err(c, PG_ERR_STATE, "assemble K before solving with it");
   if (c->s.n_free == 0) return pg_set_err(c, PG_ERR_STATE, "no free degrees of freedom");
   if (int rc = pcg_reserve(c, nrhs)) return rc;
@@ -448,6 +449,7 @@ int pg_pcg_solve(pg_ctx* c, const double* d_b, double* d_x, int nrhs, double rto
 
 int pg_homogenize(pg_ctx* c, const double* d_U, double t_frac, double* out) {
   if (!c || !d_U || !out) return PG_ERR_INPUT;
+  if (!pg_resident(c)) return pg_set_err(c, PG_ERR_STATE, "the context has no device residency (pg_upload it first)");
   const int dim = c->s.dim, nv = dim == 2 ? 3 : 6;
   if (!c->d_hom && (pg_dalloc(c, (size_t)(nv + 2) * kHomBlocks + 8, &c->d_hom) || pg_alloc_sync(c))) return PG_ERR_DEVICE;
   pgd::DevProblem P = c->P;

@@ -136,3 +136,25 @@ def test_uncut_sizes():
     # left column u_x = 0 (5 dofs), right column u_x prescribed (5 dofs), node 0 also u_y = 0
     assert s["n_const"] == 11 and s["n_free"] == 39
     P.close()
+
+
+def test_device_entry_points_refuse_host_only_contexts():
+    """A context built by the host set-up alone (no pg_upload) has no device tables: every entry
+    point that launches work returns PG_ERR_STATE before touching the GPU."""
+    import ctypes
+    from pigfem_b200 import capi
+    L = capi.load_library()
+    P = host_problem("lin_tri3_subscale")
+    h = P.h
+    buf = np.zeros(64)
+    dptr = ctypes.c_void_p(4096)   # never dereferenced: the residency check comes first
+    eps = np.zeros(6)
+    out = ctypes.c_double(0.0)
+    assert L.pg_assemble_device(h, dptr, 1.0, capi.FUNC | capi.JAC) == 12
+    assert L.pg_residual_strains(h, dptr, 1.0, 1, eps.ctypes.data, dptr, dptr) == 12
+    assert L.pg_assemble(h, buf.ctypes.data, 1.0, capi.FUNC, None, None, None, None, buf.ctypes.data, buf.ctypes.data) == 12
+    assert L.pg_residual_norm(h, ctypes.byref(out)) == 12
+    assert L.pg_homogenize(h, dptr, 1.0, buf.ctypes.data) == 12
+    it = np.zeros(1, np.int32)
+    assert L.pg_pcg_solve(h, dptr, dptr, 1, 1e-8, 10, it.ctypes.data, buf.ctypes.data) == 12
+    P.close()
