@@ -175,6 +175,75 @@ __global__ void __launch_bounds__(kThreads) k_pcg_spmv(PcgArgs a) {
   }
 }
 
+// The same product for exactly NS right-hand sides (NS = nrhs <= 8, known at compile time): a
+// column's NS values of p are read as 16-byte pairs when NS is even, and every lane keeps two
+// nonzeros in flight; each right-hand side's products are still added in the lane's nonzero
+// order, so the sums are those of k_pcg_spmv.
+template <int NS>
+__device__ __forceinline__ void load_p(const double* __restrict__ p, int c, double* out) {
+  if constexpr (NS % 2 == 0) {
+    const double2* q = reinterpret_cast<const double2*>(p + (size_t)c * NS);
+#pragma unroll
+    for (int j = 0; j < NS / 2; ++j) { const double2 t = __ldg(q + j); out[2 * j] = t.x; out[2 * j + 1] = t.y; }
+  } else {
+#pragma unroll
+    for (int j = 0; j < NS; ++j) out[j] = __ldg(p + (size_t)c * NS + j);
+  }
+}
+
+template <int NS>
+__global__ void __launch_bounds__(kThreads) k_pcg_spmv_n(PcgArgs a) {
+  __shared__ double sh[kThreads];
+  if (a.flag[2 * a.nrhs] == 0) return;
+  int r0, r1;
+  block_rows(a.n, a.nb, &r0, &r1);
+  const int grp = threadIdx.x / kRowGroup, lane = threadIdx.x % kRowGroup, ngrp = kThreads / kRowGroup;
+  bool act[NS];
+  double pq[NS];
+#pragma unroll
+  for (int j = 0; j < NS; ++j) { act[j] = !a.flag[j]; pq[j] = 0.0; }
+  for (int i0 = r0; i0 < r1; i0 += ngrp) {
+    const int i = i0 + grp;
+    const bool valid = i < r1;
+    double v[NS];
+#pragma unroll
+    for (int j = 0; j < NS; ++j) v[j] = 0.0;
+    const int k0 = valid ? a.rp[i] : 0, k1 = valid ? a.rp[i + 1] : 0;
+    int k = k0 + lane;
+    for (; k + kRowGroup < k1; k += 2 * kRowGroup) {
+      const double av0 = __ldg(a.val + k), av1 = __ldg(a.val + k + kRowGroup);
+      const int c0 = __ldg(a.ci + k), c1 = __ldg(a.ci + k + kRowGroup);
+      double p0[NS], p1[NS];
+      load_p<NS>(a.p, c0, p0);
+      load_p<NS>(a.p, c1, p1);
+#pragma unroll
+      for (int j = 0; j < NS; ++j) v[j] += av0 * p0[j];
+#pragma unroll
+      for (int j = 0; j < NS; ++j) v[j] += av1 * p1[j];
+    }
+    if (k < k1) {
+      const double av0 = __ldg(a.val + k);
+      double p0[NS];
+      load_p<NS>(a.p, __ldg(a.ci + k), p0);
+#pragma unroll
+      for (int j = 0; j < NS; ++j) v[j] += av0 * p0[j];
+    }
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+      if (!act[j]) continue;   // uniform over the block
+#pragma unroll
+      for (int o = kRowGroup / 2; o > 0; o >>= 1) v[j] += __shfl_down_sync(0xffffffffu, v[j], o, kRowGroup);
+      if (valid && lane == 0) {
+        a.q[(size_t)j * a.n + i] = v[j];
+        pq[j] += a.p[(size_t)i * NS + j] * v[j];
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < NS; ++j)
+    if (act[j]) block_sum(sh, pq[j], &a.part[(0 * a.nrhs + j) * a.nb + blockIdx.x]);
+}
+
 __global__ void __launch_bounds__(kThreads) k_pcg_alpha(PcgArgs a) {
   __shared__ double sh[kThreads];
   if (a.flag[2 * a.nrhs] == 0) return;
@@ -257,7 +326,14 @@ __global__ void __launch_bounds__(kThreads) k_pcg_dir(PcgArgs a) {
 }
 
 void launch_iteration(const PcgArgs& a, cudaStream_t st) {
-  k_pcg_spmv<<<a.nb, kThreads, 0, st>>>(a);
+  switch (a.nrhs) {
+    case 1: k_pcg_spmv_n<1><<<a.nb, kThreads, 0, st>>>(a); break;
+    case 2: k_pcg_spmv_n<2><<<a.nb, kThreads, 0, st>>>(a); break;
+    case 3: k_pcg_spmv_n<3><<<a.nb, kThreads, 0, st>>>(a); break;
+    case 4: k_pcg_spmv_n<4><<<a.nb, kThreads, 0, st>>>(a); break;
+    case 6: k_pcg_spmv_n<6><<<a.nb, kThreads, 0, st>>>(a); break;
+    default: k_pcg_spmv<<<a.nb, kThreads, 0, st>>>(a); break;
+  }
   k_pcg_alpha<<<a.nrhs, kThreads, 0, st>>>(a);
   k_pcg_update<<<a.nb, kThreads, 0, st>>>(a);
   k_pcg_beta<<<a.nrhs, kThreads, 0, st>>>(a);
