@@ -461,11 +461,9 @@ __global__ void __launch_bounds__(128) k_rows_general_cases(DevProblem P) {
   if (__all_sync(0xffffffffu, !valid)) return;
   int4 gd = make_int4(0, 0, 0, 0);
   if (valid) gd = __ldg(&P.gdesc[node]);
-  double rs[MC][DIM];
+  double rs[MC];   // lane k < DIM: row k of the node, per case
 #pragma unroll
-  for (int c = 0; c < MC; ++c)
-#pragma unroll
-    for (int q = 0; q < DIM; ++q) rs[c][q] = 0.0;
+  for (int c = 0; c < MC; ++c) rs[c] = 0.0;
   for (int e0 = 0; e0 < gd.y; e0 += L) {
     const int ei = e0 + k;
     double re[MC][DIM];
@@ -563,7 +561,10 @@ __global__ void __launch_bounds__(128) k_rows_general_cases(DevProblem P) {
       for (int c = 0; c < MC; ++c) {
         if (c >= nc) break;
 #pragma unroll
-        for (int q = 0; q < DIM; ++q) rs[c][q] += __shfl_sync(gmask, re[c][q], jj, L);
+        for (int q = 0; q < DIM; ++q) {
+          const double v = __shfl_sync(gmask, re[c][q], jj, L);
+          if (k == q) rs[c] += v;
+        }
       }
   }
   if (!valid || k >= DIM) return;
@@ -571,11 +572,8 @@ __global__ void __launch_bounds__(128) k_rows_general_cases(DevProblem P) {
 #pragma unroll
   for (int c = 0; c < MC; ++c) {
     if (c >= nc) break;
-    double mine = rs[c][0];
-#pragma unroll
-    for (int q = 1; q < DIM; ++q) if (k == q) mine = rs[c][q];
-    if (gdof < P.n_free) P.Pf_cases[(size_t)c * P.n_free + gdof] = mine;
-    else P.Pp_cases[(size_t)c * P.n_const + gdof - P.n_free] = mine;
+    if (gdof < P.n_free) P.Pf_cases[(size_t)c * P.n_free + gdof] = rs[c];
+    else P.Pp_cases[(size_t)c * P.n_const + gdof - P.n_free] = rs[c];
   }
 }
 
