@@ -241,20 +241,50 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
   double* part = rs + 4;                    // per-block residual partials of one cut element
   if (valid)
     for (int i = g; i < gd.w * D2 + DIM; i += G) slab[i] = 0.0;
-  int n_ent = gd.y;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) n_ent = max(n_ent, __shfl_xor_sync(0xffffffffu, n_ent, o));
+  // 3D with G >= 8: two uncut elements per pass -- lanes 0..3 take one, lanes 4..7 the next (the
+  // entries are cut-first, so the one after an uncut entry is uncut too); the second element's
+  // blocks go into the slab after the first's and its residual is added after the first's, so
+  // every sum keeps the entry order.
+  constexpr bool PAIRS = (DIM == 3 && G >= 2 * NPE);
+  const int glead = (threadIdx.x & 31) - g;   // the group's first lane within the warp
   __syncwarp();
   // the next entry's descriptors are loaded while the current one is processed
   int4 ad_next = make_int4(0, 0, 0, 0), ax_next = make_int4(0, 0, 0, 0);
   if (valid && gd.y > 0) { ad_next = __ldg(&P.adesc[gd.x]); ax_next = __ldg(&P.aresd[gd.x]); }
-  for (int ei = 0; ei < n_ent; ++ei) {
+  int ei = 0;
+  while (__any_sync(0xffffffffu, valid && ei < gd.y)) {
     const bool have = valid && ei < gd.y;
     const int4 ad = ad_next, ax = ax_next;
     const int cc = ax.x;
-    if (valid && ei + 1 < gd.y) { ad_next = __ldg(&P.adesc[gd.x + ei + 1]); ax_next = __ldg(&P.aresd[gd.x + ei + 1]); }
     const int la = ad.y & 255, mn = ad.y >> 8;
-    if (have && mn == 0) {
+    const bool pair = PAIRS && have && mn == 0 && ei + 1 < gd.y;
+    const int step = pair ? 2 : 1;
+    if (valid && ei + step < gd.y) { ad_next = __ldg(&P.adesc[gd.x + ei + step]); ax_next = __ldg(&P.aresd[gd.x + ei + step]); }
+    if constexpr (PAIRS) {
+      const bool second = pair && g >= NPE && g < 2 * NPE;
+      const bool first = have && mn == 0 && g < NPE;
+      int4 ad2 = ad, ax2 = ax;
+      if (second) { ad2 = __ldg(&P.adesc[gd.x + ei + 1]); ax2 = __ldg(&P.aresd[gd.x + ei + 1]); }
+      double kb[DIM][DIM], rv[DIM];
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) rv[q] = 0.0;
+      const int lb = second ? g - NPE : g;
+      if (first || second)
+        simplex_block<DIM>(P, ax2, ad2.y & 255, lb, P.D[ad2.w], kb, rv, lb == 0);
+      if (first) slab_add<DIM>(slab + ((((unsigned)ad.z) >> (8 * g)) & 255) * D2, &kb[0][0]);
+      __syncwarp();
+      if (second) slab_add<DIM>(slab + ((((unsigned)ad2.z) >> (8 * lb)) & 255) * D2, &kb[0][0]);
+      double rv2[DIM];
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) rv2[q] = __shfl_sync(0xffffffffu, rv[q], glead + NPE);
+      if (have && mn == 0 && g == 0) {
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) rs[q] += rv[q];
+        if (pair)
+#pragma unroll
+          for (int q = 0; q < DIM; ++q) rs[q] += rv2[q];
+      }
+    } else if (have && mn == 0) {
       if (g < NPE) {
         double kb[DIM][DIM], rv[DIM];
         simplex_block<DIM>(P, ax, la, g, P.D[ad.w], kb, rv, g == 0);   // D from the parameter space
@@ -264,7 +294,8 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
 #pragma unroll
           for (int q = 0; q < DIM; ++q) rs[q] += rv[q];
       }
-    } else if (have) {
+    }
+    if (have && mn > 0) {
       const int base = ax.y;
       const int* cn = P.cut_nodes + base;
       const double* kr = P.ke + ad.w;                 // block row la of K_vol
@@ -332,6 +363,7 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
       for (int q = 0; q < DIM; ++q) rs[q] += r[q];
     }
     __syncwarp();
+    ei += step;
   }
   if (!valid) return;
   const int nn = gd.w;
