@@ -71,7 +71,8 @@ def _check_batch(probs, us, flags, tune=False):
 @pytest.mark.parametrize("fp32", [False, True], ids=["fp64", "fp32_mixed"])
 def test_batch_2d_bitwise_equals_alone(fp32):
     from pigfem_b200 import capi
-    probs, us = _problems(["coh_bl", "coh_xn", "lin_tri3_three_fibers", "coh_bl_polygon", "lin_tri3_subscale"], extra_2d=3)
+    probs, us = _problems(["coh_bl", "coh_xn", "lin_tri3_three_fibers", "coh_bl_polygon", "lin_tri3_subscale", "coh_stl",
+                           "coh_tlnu_compression"], extra_2d=3)
     flags = capi.FUNC | capi.JAC | (capi.FP32 if fp32 else 0)
     _check_batch(probs, us, flags)
     for P in probs:
@@ -88,7 +89,7 @@ def test_batch_autotuned_shape_keeps_results():
 
 def test_batch_3d_bitwise_equals_alone():
     from pigfem_b200 import capi
-    probs, us = _problems(["coh_tet4_bl", "coh_tet4_opaug_two_spheres", "lin_tet4_subscale", "lin_tet4_uncut"])
+    probs, us = _problems(["coh_tet4_bl", "coh_tet4_opaug_two_spheres", "lin_tet4_subscale", "lin_tet4_uncut", "coh_tet4_tl"])
     _check_batch(probs, us, capi.FUNC | capi.JAC)
     for P in probs:
         P.close()
