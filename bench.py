@@ -43,6 +43,10 @@ L2_FLUSH_BYTES = 256 << 20
 
 
 def parse():
+    return parse_from(None)
+
+
+def parse_from(argv):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=300)
@@ -59,7 +63,8 @@ def parse():
     p.add_argument("--spheres", type=int, default=50)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (default: --steps)")
-    return p.parse_args()
+    p.add_argument("--ref-procs", type=int, default=0, help="reference arm: replica processes (default: one per core)")
+    return p.parse_args(argv)
 
 
 def dist_env():
@@ -246,15 +251,33 @@ UNIT_STRAINS_3D = [tuple(1.0 if i == k else 0.0 for i in range(6)) for k in rang
 
 
 def reference_problem(R, P, U):
-    """The reference's own Problem (oracle/_ref) for the same RVE and state; returns it and the DOF
-    vector (free then constrained) of U."""
-    import dataclasses
+    """The reference's own Problem (oracle/_ref) for the same RVE and state as this library's
+    problem P; returns it and the DOF vector (free then constrained) of U."""
     from oracle import ref
-    RP = ref.RefProblem(ref.ProblemSpec(**{f.name: getattr(R.desc, f.name) for f in dataclasses.fields(R.desc)}))
+    RP = ref.RefProblem(ref_spec(R))
     _, dofs, _ = P.nodes()
     Ud = np.zeros(RP.n_free + RP.n_const)
     Ud[dofs.reshape(-1)] = U
     return RP, Ud
+
+
+def ref_spec(R):
+    import dataclasses
+    from oracle import ref
+    return ref.ProblemSpec(**{f.name: getattr(R.desc, f.name) for f in dataclasses.fields(R.desc)})
+
+
+def reference_state(args, RP):
+    """The workload's displacement state (DOF vector) built from the reference's own mesh tables:
+    the same function of the enriched mesh as build_problem's, so both arms time the same state
+    (equal to 1e-14; tests/test_config_parity_gpu.py checks it)."""
+    from pigfem_b200 import rve
+    if args.workload == "linear_3d_64":
+        return np.zeros(RP.n_free + RP.n_const)
+    U = rve.interface_state_tables(**RP.cut_tables(), seed=0)
+    Ud = np.zeros(RP.n_free + RP.n_const)
+    Ud[RP.get("node_dofs")] = U
+    return Ud
 
 
 def reference_step_seconds(args, RP, Ud, budget_s: float, max_steps: int):
@@ -280,32 +303,118 @@ def reference_step_seconds(args, RP, Ud, budget_s: float, max_steps: int):
     return float(np.mean(times)), len(times)
 
 
+def host_info() -> dict:
+    """nproc and the CPU model of this host (the cores the CPU figures ran on)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "cpu_model": model}
+
+
+def _reference_worker(job):
+    """One replica process of the reference arm: builds the reference's Problem for the workload,
+    the state from its own tables, and times assemblies for the budget.  Returns (elements,
+    seconds per step, steps, config facts)."""
+    argv, budget_s, max_steps = job
+    args = parse_from(argv)
+    from pigfem_b200 import rve
+    from oracle import ref
+    R = reference_rve(args)
+    RP = ref.RefProblem(ref_spec(R))
+    Ud = reference_state(args, RP)
+    sec, n = reference_step_seconds(args, RP, Ud, budget_s, max_steps)
+    facts = {"elements": len(RP.get("elem_cut")), "nnz": int(sum(len(RP.get(f"{b}_cols")) for b in ("K_ff", "K_fp", "K_pf", "K_pp"))),
+             "cut_elements": int(np.count_nonzero(RP.get("elem_cut"))), "cohesive_qps": int(RP.get("coh_qp_off")[-1])}
+    RP.close()
+    return facts["elements"], sec, n, facts
+
+
+def reference_rve(args):
+    """The workload's RVE description, built without this library's set-up (2D: pure numpy)."""
+    from pigfem_b200 import rve
+    if args.workload == "linear_3d_64":
+        return rve.linear_3d(n=args.grid3d, n_spheres=args.spheres, seed=1, request=0)
+    return rve.cohesive_2d(n=args.grid, n_fibers=args.fibers, seed=1, request=0)
+
+
+def reference_workers(max_procs: int, per_proc_bytes: float) -> int:
+    """Replica processes the host can hold: one per core, bounded by 80 % of the available memory."""
+    avail = None
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    avail = int(line.split()[1]) * 1024
+                    break
+    except OSError:
+        pass
+    n = os.cpu_count() or 1
+    if avail:
+        n = min(n, max(1, int(0.8 * avail / per_proc_bytes)))
+    return max(1, min(n, max_procs))
+
+
+# resident memory of one reference replica of the 512^2 cohesive workload (measured: set-up plus
+# one assembly), used to bound the replica count
+REF_PROC_BYTES = {"cohesive_2d_512": 2.5e9, "linear_3d_64": 15e9}
+
+
 def run_reference(args, ws, rank):
-    """The reference's own CPU assembly (oracle/_ref, built from its sources) on rank 0.  The
-    reference assembles serially (one MPI rank; no threads in its assembly), so it uses one core."""
+    """The reference's own CPU assembly (oracle/_ref, built from its sources) on rank 0, on all the
+    host cores it can use.  The reference assembles serially (one MPI rank, no threads in its
+    assembly) and no MPI library is available to partition the mesh, so every core runs an
+    independent replica of the workload (its own Problem, same RVE and state); the value is the
+    replicas' summed elements/s.  The state comes from the reference's own mesh tables, so this
+    arm never loads libpigfem_b200.so."""
     if rank != 0:
         return
     from oracle import ref
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libpigfem_ref.so not built (make -C oracle)"}))
         return
-    from pigfem_b200 import capi
-    R, P, U = build_problem(args, 0, device=False)
-    RP, Ud = reference_problem(R, P, U)
-    sec, n_timed = reference_step_seconds(args, RP, Ud, budget_s=90.0, max_steps=args.steps)
-    ne = P.sizes["n_elem"]
-    value = ne / sec
-    sample = (f"mean of {n_timed} timed steps (of {args.steps} requested; capped at ~90 s of CPU work) after 1 warm-up, "
-              f"each a full Assembler::assemble of the {ne}-element RVE" +
-              (" with K and 6 right-hand sides" if args.workload == "linear_3d_64" else " (K+R)"))
+    import multiprocessing as mp
+    nproc = reference_workers(args.ref_procs or 256, REF_PROC_BYTES.get(args.workload, 4e9))
+    budget = 60.0
+    job = (sys.argv[1:], budget, args.steps)
+    if nproc == 1:
+        results = [_reference_worker(job)]
+    else:
+        with mp.get_context("spawn").Pool(nproc) as pool:
+            results = pool.map(_reference_worker, [job] * nproc)
+    ne, _, _, facts = results[0]
+    rates = [e / sec for e, sec, _, _ in results]
+    value = float(sum(rates))
+    n_timed = min(n for _, _, n, _ in results)
+    sec_mean = float(np.mean([sec for _, sec, _, _ in results]))
+    sample = (f"{nproc} concurrent replica processes (one per core), each a full Assembler::assemble of the {ne}-element RVE" +
+              (" with K and 6 right-hand sides" if args.workload == "linear_3d_64" else " (K+R)") +
+              f" repeated for up to {budget:.0f} s after 1 warm-up (at least {n_timed} timed steps each); value = sum of the replicas' elements/s")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "steps_timed": n_timed,
-            "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded fiber layout)", "impl": "reference",
-            "config": {"workload": WORKLOADS[args.workload], "elements": ne, "l2": "cpu run", "parallelism": "single core"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
+            "warmup": args.warmup, "ms_per_step": 1e3 * sec_mean / nproc, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": DATA, "impl": "reference",
+            "config": bench_config(args, facts, ws),
+            "per_core": {"value": float(np.mean(rates)), "ms_per_step": 1e3 * sec_mean},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "reference", "sample": sample,
+                             **host_info()},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    RP.close()
     print(json.dumps(line))
+
+
+DATA = "synthetic (seeded fiber layout; reference publishes no data set)"
+
+
+def bench_config(args, facts: dict, ws: int) -> dict:
+    """The `config` object of both arms' lines (identical keys and values for one workload)."""
+    return {"workload": WORKLOADS[args.workload], "elements": facts["elements"], "nnz": facts["nnz"],
+            "cut_elements": facts["cut_elements"], "cohesive_qps": facts["cohesive_qps"],
+            "l2": f"GPU arm: flushed before every timed step ({L2_FLUSH_BYTES >> 20} MiB write); CPU arm: host caches",
+            "parallelism": f"replicas x{ws} (one RVE per GPU) / one replica per host core"}
 
 
 def main_batched(args, ws, rank, local):
@@ -651,14 +760,13 @@ def main():
     if rank == 0:
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
-            cpu = cpu_baseline(args, R, P, U)
+            cpu = cpu_baseline(args, R, P, U, out_np)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms64 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded fiber layout; reference publishes no data set)",
-            "config": {"workload": WORKLOADS[args.workload], "elements": ne, "nnz": int(sum(P.nnz)), "cut_elements": P.sizes["n_cut_elem"],
-                       "cohesive_qps": P.sizes["n_coh_qp"], "l2": f"flushed before every timed step ({L2_FLUSH_BYTES >> 20} MiB write)",
-                       "parallelism": f"replicas x{ws} (one RVE per GPU)"},
+            "dtype": "f64", "data": DATA,
+            "config": bench_config(args, {"elements": ne, "nnz": int(sum(P.nnz)), "cut_elements": P.sizes["n_cut_elem"],
+                                          "cohesive_qps": P.sizes["n_coh_qp"]}, ws),
             "fp32_mixed": {"value": value32, "unit": UNIT, "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": value32 / value,
                            "kernel_ms": [float(x) for x in kt32]},
             "kernel_ms": {"cohesive_elements": float(kt64[0]), "rows_stencil": float(kt64[1]),
@@ -687,18 +795,31 @@ def main():
         print(json.dumps(line))
 
 
-def cpu_baseline(args, R, P, U):
-    """The reference's assembly (oracle/_ref) on this host, one core, same RVE and state."""
+def cpu_baseline(args, R, P, U, gpu_out):
+    """The reference's assembly (oracle/_ref) on this host, one core, same RVE and state; and,
+    outside every timed region, the relative Frobenius error of this library's K and R (gpu_out,
+    the last end-to-end step's host outputs) against the reference's on that state."""
     try:
         from oracle import ref
         if not ref.available():
             return None
         RP, Ud = reference_problem(R, P, U)
         sec, n_timed = reference_step_seconds(args, RP, Ud, budget_s=20.0, max_steps=5)
+        if args.workload == "linear_3d_64":
+            RP.set_macro(UNIT_STRAINS_3D[0])
+            RP.assemble(Ud, None, 1.0)
+
+        def rel(a, b):
+            nb = float(np.linalg.norm(b))
+            return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+        errs = {f"K_{b}": rel(gpu_out[f"K_{b}"][:P.nnz[i]], RP.csr(f"K_{b}")[2]) for i, b in enumerate(("ff", "fp", "pf", "pp"))}
+        errs["P_f"] = rel(gpu_out["P_f"][:P.n_free], RP.get("P_f"))
+        errs["P_p"] = rel(gpu_out["P_p"][:P.n_const], RP.get("P_p")) if P.n_const else 0.0
         RP.close()
         ne = P.sizes["n_elem"]
         return {"value": ne / sec, "unit": UNIT, "cores": 1, "kind": "reference",
-                "sample": f"mean of {n_timed} steps (bounded at ~20 s) of Assembler::assemble on the same {ne}-element RVE and state, after 1 warm-up"}
+                "sample": f"mean of {n_timed} steps (bounded at ~20 s) of Assembler::assemble on the same {ne}-element RVE and state, after 1 warm-up",
+                **host_info(), "fp64_rel_error_vs_reference": errs}
     except Exception as e:  # the baseline is reported, never required
         return {"error": str(e)}
 

@@ -7,7 +7,7 @@
  *                                        NodalData* solution, bool assembleFunc, bool assembleJac)
  * (include/Assembler.h:46-48, src/Assembler.cpp:65-146), reached by every solver through a
  * non-virtual call.  The entry points below are what a host-side Assembler translation unit
- * forwards to; see INTEGRATION.md for the binding.  Plain pointers and sizes only; every call
+ * forwards to (pigfem_b200/drop_in/Assembler_b200.cpp).  Plain pointers and sizes only; every call
  * returns 0 on success or one of the PG_ERR_* codes (never exits, never traps), with a message
  * available from pg_last_error().
  */
@@ -199,8 +199,8 @@ void pg_batch_destroy(pg_batch* b);
 
 /* ||x||_2 of a device vector of n doubles, written to the device double *d_out, enqueued on
  * `stream` (a cudaStream_t; NULL = legacy default stream).  No counterpart in the reference.
- * It allocates nothing: the block partials and a completion counter live in a fixed 32 KiB
- * __device__ array, so n is limited to PG_NORM_NOALLOC_MAX_N (PG_ERR_CAPACITY beyond it).
+ * It allocates nothing: the block partials live in a fixed 32 KiB __device__ array (two
+ * stream-ordered launches: the partials, then their sum), so n is limited to PG_NORM_NOALLOC_MAX_N (PG_ERR_CAPACITY beyond it).
  * For callers that must not allocate device memory: a request served against a fixed device
  * memory budget (an allocation would fall outside the admitted budget, and cudaFree
  * synchronises the whole device, stalling the other requests in flight), and a caller holding

@@ -15,6 +15,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libpigfem_ref.so")
+# The same reference build with its Assembler::assemble replaced by the drop-in translation unit
+# (pigfem_b200/drop_in/Assembler_b200.cpp) and linked against libpigfem_b200.so.
+LIB_B200_PATH = os.path.join(HERE, "_ref", "libpigfem_ref_b200.so")
 
 COH_NONE, COH_BL, COH_BLNU, COH_XN, COH_XNNU, COH_OP, COH_OPNU, COH_OPAUG, COH_OPNUAUG = range(9)
 TRI3, QUAD4, TET4 = 0, 1, 2
@@ -34,19 +37,20 @@ class _Config(ctypes.Structure):
     ]
 
 
-_lib = None
+_libs = {}
 
 
-def available() -> bool:
-    return os.path.exists(LIB_PATH)
+def available(variant: str = "cpu") -> bool:
+    return os.path.exists(LIB_B200_PATH if variant == "b200" else LIB_PATH)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not available():
-            raise FileNotFoundError(f"oracle library not built: {LIB_PATH} (run `make -C oracle`)")
-        L = ctypes.CDLL(LIB_PATH)
+def lib(variant: str = "cpu"):
+    """The reference library: "cpu" (its own Assembler::assemble) or "b200" (the drop-in)."""
+    if variant not in _libs:
+        path = LIB_B200_PATH if variant == "b200" else LIB_PATH
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle library not built: {path} (run `make -C oracle`)")
+        L = ctypes.CDLL(path)
         L.pgref_create.restype = ctypes.c_void_p
         L.pgref_create.argtypes = [ctypes.POINTER(_Config)]
         L.pgref_assemble.restype = ctypes.c_double
@@ -69,8 +73,12 @@ def lib():
         L.pgref_set_macro.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.pgref_destroy.restype = None
         L.pgref_destroy.argtypes = [ctypes.c_void_p]
-        _lib = L
-    return _lib
+        L.pgref_bind_gpu.restype = ctypes.c_int
+        L.pgref_bind_gpu.argtypes = [ctypes.c_void_p]
+        L.pgref_gpu_error.restype = ctypes.c_char_p
+        L.pgref_gpu_error.argtypes = []
+        _libs[variant] = L
+    return _libs[variant]
 
 
 @dataclass
@@ -94,8 +102,9 @@ class ProblemSpec:
 
 
 class RefProblem:
-    def __init__(self, spec: ProblemSpec):
-        L = lib()
+    def __init__(self, spec: ProblemSpec, variant: str = "cpu"):
+        self.variant = variant
+        L = lib(variant)
         self.spec = spec
         dim = 3 if spec.elem_type == TET4 else 2
         self.dim = dim
@@ -127,7 +136,7 @@ class RefProblem:
     def get(self, name: str) -> np.ndarray:
         n = ctypes.c_long(0)
         p = ctypes.c_void_p(0)
-        kind = lib().pgref_get(self.h, name.encode(), ctypes.byref(n), ctypes.byref(p))
+        kind = lib(self.variant).pgref_get(self.h, name.encode(), ctypes.byref(n), ctypes.byref(p))
         if kind == 0:
             raise KeyError(name)
         if n.value == 0:
@@ -135,6 +144,23 @@ class RefProblem:
         ct = ctypes.c_int32 if kind == 1 else ctypes.c_double
         arr = np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ct)), shape=(n.value,))
         return arr.copy()
+
+    def cut_tables(self) -> dict:
+        """The enriched mesh's cut elements in the terms of pigfem_b200.rve.interface_state_tables,
+        read from the reference's own mesh (export_mesh in ref_driver.cpp): node lists of the cut
+        elements (parent nodes then enrichment nodes), their cohesive-element ranges, the cohesive
+        local node lists and the cohesive quadrature rotations."""
+        dim = self.dim
+        eoff, enodes, ecut = self.get("elem_node_off"), self.get("elem_nodes"), self.get("elem_cut")
+        ecoh = self.get("elem_coh_off")
+        cut = np.nonzero(ecut)[0]
+        lens = eoff[cut + 1] - eoff[cut]
+        cut_node_off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+        cut_nodes = np.concatenate([enodes[eoff[e]:eoff[e + 1]] for e in cut]) if len(cut) else np.zeros(0, np.int64)
+        cut_coh_off = np.concatenate([ecoh[cut], [ecoh[-1]]]) if len(cut) else np.zeros(1, np.int64)
+        return dict(dim=dim, n_nodes=len(self.get("node_dofs")) // dim, cut_node_off=cut_node_off, cut_nodes=cut_nodes,
+                    cut_coh_off=cut_coh_off, coh_local_off=self.get("coh_struct_off"), coh_local=self.get("coh_struct"),
+                    coh_qp_off=self.get("coh_qp_off"), cqp_R=self.get("coh_qp_R"))
 
     def csr(self, block: str):
         rp, ci, v = self.get(f"{block}_rowptr"), self.get(f"{block}_cols"), self.get(f"{block}_vals")
@@ -149,34 +175,42 @@ class RefProblem:
         if isv_committed is not None:
             isv_committed = np.ascontiguousarray(isv_committed, dtype=np.float64)
             iv = isv_committed.ctypes.data
-        return lib().pgref_assemble(self.h, U.ctypes.data, iv, t_frac, int(func), int(jac))
+        return lib(self.variant).pgref_assemble(self.h, U.ctypes.data, iv, t_frac, int(func), int(jac))
 
     def homogenize(self) -> np.ndarray:
-        lib().pgref_homogenize(self.h)
+        lib(self.variant).pgref_homogenize(self.h)
         return self.get("homogenized")
 
     def write_homogenization(self, filename: str, t: float, step: int):
         """The reference's WriterHomogenization::writeConsecutive on the current state."""
-        lib().pgref_write_homogenization(self.h, filename.encode(), float(t), int(step))
+        lib(self.variant).pgref_write_homogenization(self.h, filename.encode(), float(t), int(step))
 
     def set_macro(self, eps):
         e = np.zeros(6)
         e[:len(eps)] = eps
-        lib().pgref_set_macro(self.h, e.ctypes.data)
+        lib(self.variant).pgref_set_macro(self.h, e.ctypes.data)
 
     def time_assemble(self, n_rep: int) -> float:
-        return lib().pgref_time_assemble(self.h, n_rep)
+        return lib(self.variant).pgref_time_assemble(self.h, n_rep)
 
     def set_solver(self, rel_tol=1e-8, abs_tol=1e-8, max_dt=1e-2, min_dt=1e-5, T_final=1.0, max_iter=25):
-        lib().pgref_set_solver(self.h, rel_tol, abs_tol, max_dt, min_dt, T_final, max_iter)
+        lib(self.variant).pgref_set_solver(self.h, rel_tol, abs_tol, max_dt, min_dt, T_final, max_iter)
 
     def solve(self) -> str:
-        lib().pgref_solve(self.h)
+        lib(self.variant).pgref_solve(self.h)
         return bytes(self.get("log").astype(np.uint8)).decode(errors="replace")
+
+    def bind_gpu(self) -> int:
+        """Attach a B200 context through the drop-in (the "b200" variant only): from then on the
+        reference's own Assembler::assemble calls, its solvers' included, run on the device."""
+        rc = lib(self.variant).pgref_bind_gpu(self.h)
+        if rc != 0:
+            raise RuntimeError(f"pgref_bind_gpu: {rc} {lib(self.variant).pgref_gpu_error().decode()}")
+        return rc
 
     def close(self):
         if self.h:
-            lib().pgref_destroy(self.h)
+            lib(self.variant).pgref_destroy(self.h)
             self.h = None
 
     def __del__(self):

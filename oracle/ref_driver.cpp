@@ -38,6 +38,11 @@
 #include <unordered_map>
 #include <vector>
 #include <chrono>
+
+#include "../include/pigfem_b200_dropin.h"
+// Defined only when the drop-in Assembler::assemble and libpigfem_b200.so are linked in.
+extern "C" int pg_dropin_bind(void* problem, const pg_problem_desc* desc) __attribute__((weak));
+extern "C" const char* pg_dropin_last_error(void) __attribute__((weak));
 #include <sys/time.h>
 #include <unistd.h>
 
@@ -138,6 +143,8 @@ struct Handle {
   std::map<std::string, Export> out;
   std::string log_path;
   std::string err;
+  pgref_config cfg{};            // the configuration it was built from (incl points into incl_store)
+  std::vector<double> incl_store;
 };
 
 Export& put_i(Handle* h, const std::string& k) { Export& e = h->out[k]; e.is_int = true; e.i32.clear(); return e; }
@@ -330,6 +337,9 @@ extern "C" {
 
 void* pgref_create(const pgref_config* cfg) {
   Handle* h = new Handle;
+  h->cfg = *cfg;
+  h->incl_store.assign(cfg->incl, cfg->incl + (size_t)cfg->n_incl * ((cfg->elem_type == 2) ? 4 : 3));
+  h->cfg.incl = h->incl_store.data();
   char tmpl[] = "/tmp/pgref_log_XXXXXX";
   int fd = mkstemp(tmpl);
   if (fd >= 0) close(fd);
@@ -556,6 +566,35 @@ int pgref_solve(void* vh) {
   for (char c : txt) lg.i32.push_back((int)(unsigned char)c);
   return 0;
 }
+
+/*
+ * Attaches a B200 context to this problem through the drop-in Assembler::assemble
+ * (pigfem_b200/drop_in/Assembler_b200.cpp): only in the library variant linked with it
+ * (_ref/libpigfem_ref_b200.so), where every later Assembler::assemble -- the reference's own
+ * solvers included -- runs on the device.  Returns the pg_dropin_bind status, or -1 in the
+ * CPU-only library.
+ */
+int pgref_bind_gpu(void* vh) {
+  Handle* h = (Handle*)vh;
+  if (!pg_dropin_bind) return -1;
+  const pgref_config& c = h->cfg;
+  pg_problem_desc d;
+  std::memset(&d, 0, sizeof(d));
+  d.elem_type = c.elem_type;
+  d.n[0] = c.nx; d.n[1] = c.ny; d.n[2] = c.nz;
+  d.lo[0] = c.xmin; d.lo[1] = c.ymin; d.lo[2] = c.zmin;
+  d.hi[0] = c.xmax; d.hi[1] = c.ymax; d.hi[2] = c.zmax;
+  d.n_incl = c.n_incl; d.incl = c.incl;
+  d.E_matrix = c.E_matrix; d.nu_matrix = c.nu_matrix; d.E_fiber = c.E_fiber; d.nu_fiber = c.nu_fiber;
+  d.coh_law = c.coh_law;
+  for (int i = 0; i < 4; ++i) d.coh[i] = c.coh[i];
+  d.plane_strain = c.plane_strain; d.subscale = c.subscale;
+  for (int i = 0; i < 6; ++i) d.eps_macro[i] = c.eps_macro[i];
+  d.app_strain = c.app_strain;
+  return pg_dropin_bind((void*)h->prob, &d);
+}
+
+const char* pgref_gpu_error(void) { return pg_dropin_last_error ? pg_dropin_last_error() : "drop-in not linked"; }
 
 /* Named-array access: returns 1 for int32, 2 for float64, 0 if absent; *n gets the length. */
 int pgref_get(void* vh, const char* name, long* n, void** ptr) {

@@ -172,6 +172,8 @@ PetscErrorCode MatSetValues(Mat A, PetscInt m, const PetscInt idxm[], PetscInt n
 PetscErrorCode MatAssemblyBegin(Mat A, MatAssemblyType t);
 PetscErrorCode MatAssemblyEnd(Mat A, MatAssemblyType t);
 PetscErrorCode MatZeroEntries(Mat A);
+PetscErrorCode MatSeqAIJGetArray(Mat A, PetscScalar** a);
+PetscErrorCode MatSeqAIJRestoreArray(Mat A, PetscScalar** a);
 PetscErrorCode MatMult(Mat A, Vec x, Vec y);
 PetscErrorCode MatMultTranspose(Mat A, Vec x, Vec y);
 PetscErrorCode MatGetOwnershipRange(Mat A, PetscInt* m, PetscInt* n);

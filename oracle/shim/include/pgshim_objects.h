@@ -13,6 +13,7 @@ struct pg_Mat {
   std::vector<std::vector<int>> cols;     // sorted column indices per row
   std::vector<std::vector<double>> vals;  // values aligned with cols
   std::vector<double> dvals;              // dense storage (row-major) when dense
+  std::vector<double> flat;               // MatSeqAIJGetArray: the values of all rows, in row order
 };
 struct pg_Vec { std::vector<double> a; };
 struct pg_IS { std::vector<int> idx; };

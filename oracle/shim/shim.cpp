@@ -156,6 +156,24 @@ PetscErrorCode MatZeroEntries(Mat A) {
   for (auto& r : A->vals) std::fill(r.begin(), r.end(), 0.0);
   return 0;
 }
+// PETSc's SeqAIJ value array: every stored value, rows in order, columns sorted within a row; the
+// caller may overwrite it, and RestoreArray writes it back into the rows.
+PetscErrorCode MatSeqAIJGetArray(Mat A, PetscScalar** a) {
+  if (A->dense) return 56;
+  A->flat.clear();
+  for (auto& r : A->vals) A->flat.insert(A->flat.end(), r.begin(), r.end());
+  *a = A->flat.data();
+  return 0;
+}
+PetscErrorCode MatSeqAIJRestoreArray(Mat A, PetscScalar** a) {
+  if (A->dense) return 56;
+  size_t k = 0;
+  for (auto& r : A->vals)
+    for (double& v : r) v = A->flat[k++];
+  A->flat.clear();
+  if (a) *a = nullptr;
+  return 0;
+}
 PetscErrorCode MatMult(Mat A, Vec x, Vec y) {
   y->a.assign(A->m, 0.0);
   for (int i = 0; i < A->m; ++i) {

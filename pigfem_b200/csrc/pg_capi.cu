@@ -5,6 +5,7 @@
 // committed and trial internal variables and the cut-element scratch.  The caller owns its
 // host arrays; pointers are never retained across calls.
 #include "pg_ctx.h"
+#include "pg_launch.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -69,69 +70,8 @@ int launch(pg_ctx* c, double t_frac, int flags) {
   const int dim = c->s.dim;
   const bool fp32 = (flags & PG_FP32) != 0;
   const bool jac = (flags & PG_JAC) != 0;   // without it: the residual-only kernels
-  // fork: the fast rows (uncut elements only) run on the side stream, concurrently with the
-  // cut-element kernels and the general rows on the main stream
-  cudaEventRecord(c->ev[0], c->stream);
-  cudaStreamWaitEvent(c->side, c->ev[0], 0);
-  if (P.n_coh_el > 0) {
-    const int tpb = 128;
-    const int lanes = (dim == 2) ? pgd::CohLanes<2>::CQ : pgd::CohLanes<3>::CQ;
-    const int grid = (int)(((long long)P.n_coh_el * lanes + tpb - 1) / tpb);
-    if (dim == 2) pgd::k_coh_elements<2><<<grid, tpb, 0, c->stream>>>(P);
-    else pgd::k_coh_elements<3><<<grid, tpb, 0, c->stream>>>(P);
-  }
-  // 2D: the stencil rows run on the side stream, concurrently with the cohesive elements and the
-  // general rows (the cohesive kernel leaves most SMs idle).  3D: on the main stream between the
-  // two -- the 3D stencil and general kernels each fill the GPU, and run concurrently they took
-  // 1.65 ms per 64^3 assembly against 1.0 ms one after the other.
-  cudaEventRecord(c->ev[3], c->stream);
-  cudaStream_t sst = (dim == 2) ? c->side : c->stream;
-  if (c->n_stencil > 0 && !jac) {
-    const int tpb = 128;
-    const int grid = (c->n_stencil + tpb - 1) / tpb;
-    if (dim == 2) pgd::k_rows_stencil<2, double, false><<<grid, tpb, 0, sst>>>(P, c->grid, c->stencil, c->n_stencil);
-    else pgd::k_rows_stencil<3, double, false><<<grid, tpb, 0, sst>>>(P, c->grid, c->stencil, c->n_stencil);
-  } else if (c->n_stencil > 0) {
-    const int tpb = 128;
-    const int nthreads = (dim == 2) ? c->n_stencil : 3 * 32 * ((c->n_stencil + 31) / 32);
-    const int grid = (nthreads + tpb - 1) / tpb;
-    if (dim == 2) {
-      const size_t smem = pgd::stencil_stage_bytes(tpb);
-      if (fp32) pgd::k_rows_stencil<2, float><<<grid, tpb, smem, sst>>>(P, c->grid, c->stencil, c->n_stencil);
-      else pgd::k_rows_stencil<2, double><<<grid, tpb, smem, sst>>>(P, c->grid, c->stencil, c->n_stencil);
-    } else {
-      if (fp32) pgd::k_rows_stencil<3, float><<<grid, tpb, 0, sst>>>(P, c->grid, c->stencil, c->n_stencil);
-      else pgd::k_rows_stencil<3, double><<<grid, tpb, 0, sst>>>(P, c->grid, c->stencil, c->n_stencil);
-    }
-  }
-  cudaEventRecord(c->ev[1], sst);
-  if (P.n_slow_dn > 0 && !jac) {
-    // residual only: entry-parallel groups of L lanes per node
-    constexpr int L2 = 8, L3 = 8;
-    const int L = (dim == 2) ? L2 : L3;
-    const int grid = (int)(((long long)P.n_slow_dn * L + 127) / 128);
-    if (dim == 2) pgd::k_rows_general_resid<2, L2><<<grid, 128, 0, c->stream>>>(P);
-    else pgd::k_rows_general_resid<3, L3><<<grid, 128, 0, c->stream>>>(P);
-  } else if (P.n_slow_dn > 0) {
-    const int slots = P.maxnb_general;
-    if (dim == 2) {
-      constexpr int G = 4;
-      const int grid = (P.n_slow_dn + (128 / G) - 1) / (128 / G);
-      const size_t smem = (size_t)(128 / G) * pgd::general_slab_doubles(slots, 2, P.max_mn) * sizeof(double);
-      cudaFuncSetAttribute(pgd::k_rows_general<2, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      pgd::k_rows_general<2, G><<<grid, 128, smem, c->stream>>>(P, slots, P.max_mn);
-    } else {
-      constexpr int G = 8;
-      const int grid = (P.n_slow_dn + (128 / G) - 1) / (128 / G);
-      const size_t smem = (size_t)(128 / G) * pgd::general_slab_doubles(slots, 3, P.max_mn) * sizeof(double);
-      cudaFuncSetAttribute(pgd::k_rows_general<3, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      pgd::k_rows_general<3, G><<<grid, 128, smem, c->stream>>>(P, slots, P.max_mn);
-    }
-  }
-  cudaEventRecord(c->ev[4], c->stream);
-  // join
-  cudaStreamWaitEvent(c->stream, c->ev[1], 0);
-  cudaEventRecord(c->ev[5], c->stream);
+  if (dim == 2) pgl::assembly<2>(c, P, jac, fp32);
+  else pgl::assembly<3>(c, P, jac, fp32);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(c, PG_ERR_DEVICE, std::string("launch failed: ") + cudaGetErrorString(e));
   return 0;
@@ -336,7 +276,7 @@ int pg_upload(pg_ctx* c) {
     ke_off[cc + 1] = ke_off[cc] + (long long)nd * nd;
     re_off[cc + 1] = re_off[cc] + nd;
   }
-  c->cut_scratch = ke_off[s.ncut] + re_off[s.ncut];
+  c->cut_scratch = ke_off[s.ncut];
   c->n_coh_qp = (int)s.cqp_wgt.size();
 
   // descriptors of the general rows (k_rows_general)
@@ -369,9 +309,7 @@ int pg_upload(pg_ctx* c) {
         aresd.push_back(make_int4(en[0], en[1], en[2], s.npe > 3 ? en[3] : -1));
       } else {
         const int mn = s.cut_node_off[cc + 1] - s.cut_node_off[cc];
-        const long long kro = ke_off[cc] + (long long)la * mn * dim * dim;
-        if (kro > 2147483647LL) return set_err(c, PG_ERR_UNSUPPORTED, "cut-element scratch beyond 2^31 doubles");
-        adesc.push_back(make_int4(e, la | (mn << 8), slot_off[k], (int)kro));
+        adesc.push_back(make_int4(e, la | (mn << 8), slot_off[k], 0));
         // the row node's place on a cohesive element of this cut element: (element << 5 | position)
         int cpa = -1;
         for (int ce = s.cut_coh_off[cc]; ce < s.cut_coh_off[cc + 1] && cpa < 0; ++ce)
@@ -380,6 +318,11 @@ int pg_upload(pg_ctx* c) {
         aresd.push_back(make_int4(cc, s.cut_node_off[cc], cpa, 0));
       }
     }
+    // k_rows_general's 3D paired path takes the entry after an uncut one as uncut too: every
+    // node's entries must be cut-first
+    for (size_t k = (size_t)gdesc.back().x + 1; k < adesc.size(); ++k)
+      if ((adesc[k].y >> 8) != 0 && (adesc[k - 1].y >> 8) == 0)
+        return set_err(c, PG_ERR_STATE, "internal: a cut entry after an uncut one in a general row");
   }
 
   // ---- device residency
@@ -489,10 +432,10 @@ int pg_upload(pg_ctx* c) {
   PG_TRY(upload(c, s.cqp_isv, &P.cqp_isv));
   PG_TRY(upload(c, ke_off, &P.ke_off));
   PG_TRY(upload(c, re_off, &P.re_off));
-  double* dke; double* dre;
+  // the cut elements' volumetric blocks: set-up only (reduced into the static rows, then released)
+  double* dke = nullptr;
   PG_TRY(dalloc(c, (size_t)ke_off[s.ncut], &dke));
-  PG_TRY(dalloc(c, (size_t)re_off[s.ncut], &dre));
-  P.ke = dke; P.re = dre;
+  P.ke = dke;
   PG_TRY(dalloc(c, (size_t)s.n_isv, &c->d_isv_committed));
   PG_TRY(dalloc(c, (size_t)s.n_isv, &c->d_isv_trial));
   P.isv_committed = c->d_isv_committed; P.isv_trial = c->d_isv_trial;
@@ -575,24 +518,52 @@ int pg_upload(pg_ctx* c) {
   PG_TRY(dalloc(c, 1, &c->d_err));
   P.err = c->d_err;
   PG_TRY(dalloc(c, 1024, &c->d_red));
-  // state-independent volumetric blocks of the cut elements, once
-  if (s.ncut > 0) {
-    double* dg;
-    PG_TRY(dalloc(c, (size_t)re_off[s.ncut] / dim * dim * (dim == 2 ? 3 : 6), &dg));
-    P.gmac = dg;
-    for (int cls = 0; cls < 2; ++cls) {
-      const int n = c->n_cut_list[cls];
-      if (n == 0) continue;
-      const size_t smem = (size_t)pgd::cut_smem_doubles(c->cut_cls_qp[cls], c->cut_cls_nodes[cls], dim) * sizeof(double);
-      if (dim == 2) { cudaFuncSetAttribute(pgd::k_cut_volumetric<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                      pgd::k_cut_volumetric<2><<<n, 64, smem, c->up>>>(P, c->cut_list[cls], n, dg); }
-      else { cudaFuncSetAttribute(pgd::k_cut_volumetric<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-             pgd::k_cut_volumetric<3><<<n, 64, smem, c->up>>>(P, c->cut_list[cls], n, dg); }
+  // Static part of the general rows next to cut elements: the general nodes are sorted with the
+  // ones that have cut adjacent elements first, so those form the prefix [0, n_stat).  Each gets
+  // its neighbour slots' blocks (slab layout), the slot node ids and a macroscale-strain response.
+  {
+    const int nv = (dim == 2) ? 3 : 6;
+    int n_stat = 0;
+    for (size_t i = 0; i < slow.size(); ++i) {
+      const int4 gd = gdesc[i];
+      const bool has_cut = gd.y > 0 && (adesc[gd.x].y >> 8) != 0;   // entries are cut-first
+      if (has_cut && (int)i != n_stat) return set_err(c, PG_ERR_STATE, "internal: general nodes next to cut elements are not a prefix");
+      if (has_cut) ++n_stat;
     }
-    int herr = 0;
-    cudaMemcpyAsync(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->up);
-    if (cudaStreamSynchronize(c->up) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "cut-element set-up kernel failed");
-    if (herr) return set_err(c, PG_ERR_NONFINITE, "non-finite cut-element stiffness at set-up");
+    std::vector<int> stat_off(n_stat + 1, 0), stat_node;
+    for (int i = 0; i < n_stat; ++i) {
+      const int4 gd = gdesc[i];
+      stat_off[i + 1] = stat_off[i] + gd.w;
+      for (int k = gd.z; k < gd.z + gd.w; ++k) stat_node.push_back(s.dn_node[s.dn_nbr[k]]);
+    }
+    P.n_stat = n_stat;
+    PG_TRY(upload(c, stat_off, &P.stat_slot_off));
+    PG_TRY(upload(c, stat_node, &P.stat_node));
+    double* dst = nullptr;
+    double* dsg = nullptr;
+    PG_TRY(dalloc(c, (size_t)stat_off[n_stat] * dim * dim, &dst));
+    PG_TRY(dalloc(c, (size_t)n_stat * dim * nv, &dsg));
+    P.stat = dst;
+    P.stat_g = dsg;
+    c->stat_doubles = (long long)stat_off[n_stat] * dim * dim + (long long)n_stat * dim * nv;
+    if (s.ncut > 0) {
+      double* dg = nullptr;
+      PG_TRY(dalloc(c, (size_t)re_off[s.ncut] / dim * dim * nv, &dg));
+      P.gmac = dg;
+      if (dim == 2) { pgl::cut_volumetric<2>(c, P, dg); pgl::general_static<2>(c, P, dst, dsg); }
+      else { pgl::cut_volumetric<3>(c, P, dg); pgl::general_static<3>(c, P, dst, dsg); }
+      int herr = 0;
+      cudaMemcpyAsync(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->up);
+      if (cudaStreamSynchronize(c->up) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "cut-element set-up kernel failed");
+      if (herr) return set_err(c, PG_ERR_NONFINITE, "non-finite cut-element stiffness at set-up");
+      // the per-element blocks are reduced: give their memory back
+      for (double* p : {dke, dg}) {
+        c->allocs.erase(std::remove(c->allocs.begin(), c->allocs.end(), (void*)p), c->allocs.end());
+        cudaFreeAsync(p, c->up);
+      }
+      P.ke = nullptr;
+      P.gmac = nullptr;
+    }
   }
   return pg_alloc_sync(c);
 }
@@ -731,25 +702,8 @@ int pg_residual_strains(pg_ctx* c, const double* d_U, double t_frac, int n_cases
   P.Pf_cases = d_Rf;
   P.Pp_cases = d_Rp;
   const int dim = c->s.dim;
-  // the cohesive elements once (openings, laws, internal variables, tractions: U only), then
-  // the stencil rows and the general rows for every case
-  if (P.n_coh_el > 0) {
-    const int lanes = (dim == 2) ? pgd::CohLanes<2>::CQ : pgd::CohLanes<3>::CQ;
-    const int grid = (int)(((long long)P.n_coh_el * lanes + 127) / 128);
-    if (dim == 2) pgd::k_coh_elements<2><<<grid, 128, 0, c->stream>>>(P);
-    else pgd::k_coh_elements<3><<<grid, 128, 0, c->stream>>>(P);
-  }
-  if (c->n_stencil > 0) {
-    const int grid = (c->n_stencil + 127) / 128;
-    if (dim == 2) pgd::k_rows_stencil_cases<2><<<grid, 128, 0, c->stream>>>(P, c->grid, c->stencil, c->n_stencil);
-    else pgd::k_rows_stencil_cases<3><<<grid, 128, 0, c->stream>>>(P, c->grid, c->stencil, c->n_stencil);
-  }
-  if (P.n_slow_dn > 0) {
-    constexpr int L = 8;
-    const int grid = (int)(((long long)P.n_slow_dn * L + 127) / 128);
-    if (dim == 2) pgd::k_rows_general_cases<2, L><<<grid, 128, 0, c->stream>>>(P);
-    else pgd::k_rows_general_cases<3, L><<<grid, 128, 0, c->stream>>>(P);
-  }
+  if (dim == 2) pgl::residual_cases<2>(c, P);
+  else pgl::residual_cases<3>(c, P);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(c, PG_ERR_DEVICE, std::string("launch failed: ") + cudaGetErrorString(e));
   return 0;

@@ -39,7 +39,8 @@ struct pg_ctx {
   uint8_t* d_zone = nullptr;
   int* d_err = nullptr;
   double* d_red = nullptr;  // residual-norm partials
-  long long cut_scratch = 0;
+  long long cut_scratch = 0;   // doubles of the cut elements' set-up blocks (released after set-up)
+  long long stat_doubles = 0;  // doubles of the general rows' static part
   int max_nd = 0;
   int maxnb_fast = 0;
   int n_coh_qp = 0;

@@ -56,11 +56,20 @@ struct DevProblem {
   const int* cut_coh_off; const int* coh_nh; const int* coh_local_off; const int* coh_local;
   const int* coh_qp_off; const double* cqp_N; const double* cqp_R; const double* cqp_wgt; const int* cqp_isv;
   const int* cqp_noff;  // first shape value of each cohesive point in cqp_N (CohTri3 3, CohQuad4 4, CohEdge2 2)
-  const long long* ke_off;  // per cut element: offset of its element matrix in the scratch
-  const int* re_off;        // per cut element: offset of its element vector in the scratch
-  double* ke;               // cache: volumetric element matrices of the cut elements (set-up)
-  const double* gmac;       // cache: macroscale-strain response of the cut elements (set-up)
-  double* re;               // scratch: element vectors of the cut elements
+  const long long* ke_off;  // per cut element: offset of its element matrix in ke
+  const int* re_off;        // per cut element: offset of its first node's rows (nodes x dim)
+  double* ke;               // set-up only: volumetric element matrices of the cut elements
+  const double* gmac;       // set-up only: macroscale-strain response of the cut elements
+  // Static part of the general rows next to cut elements (the first n_stat general nodes): the
+  // cut elements' volumetric blocks summed per neighbour slot, in the slab layout [slot][q][d]
+  // (stat, from stat_slot_off[node] slots on), the node id of each slot (stat_node) and the
+  // summed macroscale-strain response (stat_g, dim x nvoigt per node).  The bulk laws are linear
+  // elastic, so these do not depend on the state; k_general_static forms them once at set-up.
+  int n_stat;
+  const int* stat_slot_off;
+  const int* stat_node;
+  const double* stat;
+  const double* stat_g;
   const double* isv_committed;
   double* isv_trial;
   uint8_t* zone;            // per cohesive qp: damage zone (0 compression, 1 loading, 2 softening, 3 failed)

@@ -186,10 +186,11 @@ __device__ __forceinline__ void simplex_block(const DevProblem& P, int4 nodes, i
 }
 
 // Shared-memory doubles of one lane group: slab_slots blocks of DIM x DIM, the node's residual (4
-// doubles reserved) and the per-block residual partials of one cut element (max_mn x DIM).
+// doubles reserved) and the per-slot residual partials of the static part (slab_slots x DIM).
 __host__ __device__ inline int general_slab_doubles(int slab_slots, int dim, int max_mn) {
+  (void)max_mn;
   // even (16-byte aligned groups) and 2 mod 4, so consecutive groups start on different banks
-  int n = (slab_slots * dim * dim + 4 + max_mn * dim + 1) & ~1;
+  int n = (slab_slots * dim * dim + 4 + slab_slots * dim + 1) & ~1;
   return (n % 4 == 0) ? n + 2 : n;
 }
 
@@ -207,21 +208,85 @@ __device__ __forceinline__ void slab_add(double* ak, const double* v) {
   }
 }
 
+// Static residual of a general node next to cut elements: sum over its neighbour slots (in slot
+// order) of the static block times the slot node's displacement, then the macroscale-strain
+// response.  `part` holds the per-slot products (slot-major, DIM each), written by the caller's
+// lanes; the sum runs on one lane, so it does not depend on how many lanes formed the products.
+template <int DIM>
+__device__ __forceinline__ void static_resid_sum(const DevProblem& P, int node, int nn, const double* part,
+                                                 const double* eps, double* r) {
+  constexpr int NV = (DIM == 2) ? 3 : 6;
+#pragma unroll
+  for (int q = 0; q < DIM; ++q) r[q] = 0.0;
+  for (int k = 0; k < nn; ++k)
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) r[q] += part[k * DIM + q];
+  if (P.subscale) {
+    const double* Gs = P.stat_g + (size_t)node * DIM * NV;
+#pragma unroll
+    for (int q = 0; q < DIM; ++q)
+#pragma unroll
+      for (int v = 0; v < NV; ++v) r[q] += __ldg(&Gs[q * NV + v]) * eps[v];
+  }
+}
+
+// Product of static slot k of a general node with the slot node's displacement (one slot's
+// contribution to the static residual).
+template <int DIM>
+__device__ __forceinline__ void static_slot_product(const DevProblem& P, int s0, int k, double* out) {
+  constexpr int D2 = DIM * DIM;
+  const double* S = P.stat + (size_t)(s0 + k) * D2;
+  double u[DIM];
+  load_node<DIM>(P.U, __ldg(&P.stat_node[s0 + k]), u);
+#pragma unroll
+  for (int q = 0; q < DIM; ++q) {
+    double v = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v += __ldg(&S[q * DIM + d]) * u[d];
+    out[q] = v;
+  }
+}
+
+// The cohesive element's block (n1, n2) and the traction at n1 for a row node at cohesive place
+// cpa = (element << 5 | n1): sgn * B_{n1 % nh, n2 % nh} and sgn * t_{n1 % nh}
+// (cohesiveKFast / cohesiveInternalForceFast signs).
+template <int DIM>
+__device__ __forceinline__ void coh_block_add(const DevProblem& P, int cpa, int cpb, double* blk) {
+  constexpr int D2 = DIM * DIM;
+  const int ce = cpa >> 5, n1 = cpa & 31, n2 = cpb & 31;
+  const int nh = __ldg(&P.coh_nh[ce]);
+  const double sgn = ((n1 >= nh) == (n2 >= nh)) ? 1.0 : -1.0;
+  const double* B = P.kcoh + __ldg(&P.kc_off[ce]) + ((n1 % nh) * nh + (n2 % nh)) * D2;
+#pragma unroll
+  for (int i = 0; i < D2; ++i) blk[i] = sgn * B[i];
+}
+template <int DIM>
+__device__ __forceinline__ void coh_traction(const DevProblem& P, int cpa, double* t) {
+  constexpr int D2 = DIM * DIM;
+  const int ce = cpa >> 5, n1 = cpa & 31;
+  const int nh = __ldg(&P.coh_nh[ce]);
+  const double sgn = (n1 >= nh) ? 1.0 : -1.0;
+  const double* tp = P.kcoh + __ldg(&P.kc_off[ce]) + nh * nh * D2 + (n1 % nh) * DIM;
+#pragma unroll
+  for (int q = 0; q < DIM; ++q) t[q] = sgn * tp[q];
+}
+
 // Row assembly for the DOF nodes the stencil path does not take (boundary rows, nodes of cut
-// elements, enrichment nodes): one lane group of G threads per DOF node.  The group walks the
-// node's adjacent elements in adjacency order; for each element its lanes take the element's
-// nodes (lane b: block (la, b)) and add the blocks into the node's shared-memory slab -- the blocks
-// of one element go to distinct neighbour slots, so no two lanes write the same entry -- and the
-// residual contributions are summed in a fixed order.  Every sum is therefore in adjacency order
-// and independent of G.  Uncut elements are recomputed from the node coordinates; a cut element
-// contributes its cached volumetric block row (K_vol, state independent) times the displacements,
-// its macroscale-strain response and, when the row node is on its cohesive element, the cohesive
-// blocks and traction that k_coh_elements left for it.  Finally the group writes every CSR value
+// elements, enrichment nodes): one lane group of G threads per DOF node, its rows in a
+// shared-memory slab.  The slab starts from the node's static part (the cut elements' volumetric
+// blocks summed per neighbour slot at set-up; zero for nodes without cut elements) and the
+// residual from the static blocks times the displacements plus the macroscale-strain response.
+// The group then walks the node's adjacent elements in adjacency order: an uncut element is
+// recomputed from the node coordinates, its lanes taking the element's nodes (lane b: block
+// (la, b)) and adding the blocks into the slab -- the blocks of one element go to distinct
+// neighbour slots, so no two lanes write the same entry; a cut element adds, when the row node is
+// on one of its cohesive elements, the cohesive blocks and traction that k_coh_elements left for
+// it.  Every sum runs in a fixed order independent of G.  Finally the group writes every CSR value
 // of the node's rows exactly once.
 //   gdesc[node]      int4 {adjacency begin, adjacency count, neighbour begin, neighbour count}
 //   growd[node]      3*DIM ints: global DOF of each row, first slot in the row's F block, in its C block
 //   adesc[entry]     int4 {element, local node | nodes of a cut element << 8, slots (uncut: 8 bits per
-//                    node; cut: offset into adj_slots), material (uncut) / block-row offset (cut)}
+//                    node; cut: offset into adj_slots), material (uncut)}
 //   aresd[entry]     int4: uncut {element nodes (-1 padded)}; cut {cut element, its first node in
 //                    cut_nodes, the row node's cohesive place (element << 5 | position) or -1, 0}
 //   nbr_pre[slot]    free DOFs of the node's neighbours before this one (row positions)
@@ -231,31 +296,46 @@ __device__ __forceinline__ void slab_add(double* ak, const double* v) {
 template <int DIM, int G>
 __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool valid, double* slab) {
   constexpr int NPE = DIM + 1;
-  constexpr int NV = (DIM == 2) ? 3 : 6;
   constexpr int D2 = DIM * DIM;
   static_assert(G >= NPE, "one lane per element node");
   const int g = threadIdx.x % G;
   int4 gd = make_int4(0, 0, 0, 0);
   if (valid) gd = __ldg(&P.gdesc[node]);
+  const bool stat = valid && node < P.n_stat;
   double* rs = slab + gd.w * D2;           // residual of the node's rows
-  double* part = rs + 4;                    // per-block residual partials of one cut element
-  if (valid)
-    for (int i = g; i < gd.w * D2 + DIM; i += G) slab[i] = 0.0;
+  double* part = rs + 4;                    // per-slot residual partials of the static part
+  if (stat) {
+    const int s0 = __ldg(&P.stat_slot_off[node]);
+    const double* S = P.stat + (size_t)s0 * D2;
+    for (int i = g; i < gd.w * D2; i += G) slab[i] = __ldg(&S[i]);
+    for (int k = g; k < gd.w; k += G) static_slot_product<DIM>(P, s0, k, part + k * DIM);
+  } else if (valid) {
+    for (int i = g; i < gd.w * D2; i += G) slab[i] = 0.0;
+  }
   // 3D with G >= 8: two uncut elements per pass -- lanes 0..3 take one, lanes 4..7 the next (the
-  // entries are cut-first, so the one after an uncut entry is uncut too); the second element's
-  // blocks go into the slab after the first's and its residual is added after the first's, so
-  // every sum keeps the entry order.
+  // entries are cut-first, so the one after an uncut entry is uncut too; the set-up checks it);
+  // the second element's blocks go into the slab after the first's and its residual is added
+  // after the first's, so every sum keeps the entry order.
   constexpr bool PAIRS = (DIM == 3 && G >= 2 * NPE);
   const int glead = (threadIdx.x & 31) - g;   // the group's first lane within the warp
   __syncwarp();
+  if (valid && g == 0) {
+    double r[DIM];
+    if (stat) static_resid_sum<DIM>(P, node, gd.w, part, P.eps_macro, r);
+    else
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) r[q] = 0.0;
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) rs[q] = r[q];
+  }
   // the next entry's descriptors are loaded while the current one is processed
   int4 ad_next = make_int4(0, 0, 0, 0), ax_next = make_int4(0, 0, 0, 0);
   if (valid && gd.y > 0) { ad_next = __ldg(&P.adesc[gd.x]); ax_next = __ldg(&P.aresd[gd.x]); }
   int ei = 0;
+  __syncwarp();
   while (__any_sync(0xffffffffu, valid && ei < gd.y)) {
     const bool have = valid && ei < gd.y;
     const int4 ad = ad_next, ax = ax_next;
-    const int cc = ax.x;
     const int la = ad.y & 255, mn = ad.y >> 8;
     const bool pair = PAIRS && have && mn == 0 && ei + 1 < gd.y;
     const int step = pair ? 2 : 1;
@@ -295,72 +375,25 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
           for (int q = 0; q < DIM; ++q) rs[q] += rv[q];
       }
     }
-    if (have && mn > 0) {
+    // a cut element: its volumetric part is in the static slab; the cohesive blocks of the
+    // cohesive element the row node is on, if any
+    const int cpa = ax.z;
+    if (have && mn > 0 && cpa >= 0) {
       const int base = ax.y;
-      const int* cn = P.cut_nodes + base;
-      const double* kr = P.ke + ad.w;                 // block row la of K_vol
-      const int cpa = ax.z;                           // (cohesive element << 5 | position) or -1
       for (int b = g; b < mn; b += G) {
-        double blk[D2];
-        if constexpr (DIM == 2) {   // a 2 x 2 block: 32 bytes, 32-byte aligned in the cache
-          const double2 b0 = __ldg(reinterpret_cast<const double2*>(kr + b * D2));
-          const double2 b1 = __ldg(reinterpret_cast<const double2*>(kr + b * D2) + 1);
-          blk[0] = b0.x; blk[1] = b0.y; blk[2] = b1.x; blk[3] = b1.y;
-        } else {
-#pragma unroll
-          for (int i = 0; i < D2; ++i) blk[i] = kr[b * D2 + i];
+        const int cpb = __ldg(&P.cohpos[base + b]);
+        if (cpb >= 0 && (cpb >> 5) == (cpa >> 5)) {
+          double blk[D2];
+          coh_block_add<DIM>(P, cpa, cpb, blk);
+          slab_add<DIM>(slab + __ldg(&P.adj_slots[ad.z + b]) * D2, blk);
         }
-        const int nb = __ldg(&cn[b]);
-        double u[DIM];
-        load_node<DIM>(P.U, nb, u);
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) {
-          double s = 0.0;
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) s += blk[q * DIM + d] * u[d];
-          part[b * DIM + q] = s;
-        }
-        if (cpa >= 0) {
-          const int cpb = __ldg(&P.cohpos[base + b]);
-          if (cpb >= 0 && (cpb >> 5) == (cpa >> 5)) {
-            const int ce = cpa >> 5, n1 = cpa & 31, n2 = cpb & 31;
-            const int nh = __ldg(&P.coh_nh[ce]);
-            const double sgn = ((n1 >= nh) == (n2 >= nh)) ? 1.0 : -1.0;
-            const double* B = P.kcoh + __ldg(&P.kc_off[ce]) + ((n1 % nh) * nh + (n2 % nh)) * D2;
-#pragma unroll
-            for (int i = 0; i < D2; ++i) blk[i] += sgn * B[i];
-          }
-        }
-        double* ak = slab + __ldg(&P.adj_slots[ad.z + b]) * D2;
-        slab_add<DIM>(ak, blk);
       }
-    }
-    __syncwarp();
-    if (have && mn > 0 && g == 0) {
-      double r[DIM];
+      if (g == 0) {
+        double t[DIM];
+        coh_traction<DIM>(P, cpa, t);
 #pragma unroll
-      for (int q = 0; q < DIM; ++q) r[q] = 0.0;
-      for (int b = 0; b < mn; ++b)
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) r[q] += part[b * DIM + q];
-      if (P.subscale) {
-        const double* gm = P.gmac + __ldg(&P.re_off[cc]) / DIM * DIM * NV + (size_t)la * DIM * NV;
-#pragma unroll
-        for (int q = 0; q < DIM; ++q)
-#pragma unroll
-          for (int v = 0; v < NV; ++v) r[q] += gm[q * NV + v] * P.eps_macro[v];
+        for (int q = 0; q < DIM; ++q) rs[q] += t[q];
       }
-      const int cpa = ax.z;
-      if (cpa >= 0) {
-        const int ce = cpa >> 5, n1 = cpa & 31;
-        const int nh = __ldg(&P.coh_nh[ce]);
-        const double sgn = (n1 >= nh) ? 1.0 : -1.0;
-        const double* t = P.kcoh + __ldg(&P.kc_off[ce]) + nh * nh * D2 + (n1 % nh) * DIM;
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) r[q] += sgn * t[q];
-      }
-#pragma unroll
-      for (int q = 0; q < DIM; ++q) rs[q] += r[q];
     }
     __syncwarp();
     ei += step;
@@ -394,17 +427,36 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
   }
 }
 
-// Residual-only rows of the general nodes, entry-parallel: L lanes per DOF node, lane k takes the
-// node's entries k, k + L, ... and forms each entry's whole contribution to the node's residual
-// (an uncut element's w B^T sigma; a cut element's block row of K_vol times the displacements in
-// block order, its macroscale-strain response and the cohesive traction at the node) -- the same
-// operations general_rows performs for that entry -- and the group adds the contributions in
-// entry (adjacency) order with shuffles.  Every entry's loads are in flight at once instead of
-// one entry after the other.  L divides 32.
+// Static residual of a general node for a group of L lanes (lane k of the group): the per-slot
+// products of static_slot_product summed in slot order with shuffles, as static_resid_sum sums
+// them, without the macroscale-strain response.  Every lane of the group gets the sum.
+template <int DIM, int L>
+__device__ __forceinline__ void static_resid_group(const DevProblem& P, int node, int nn, int k, unsigned gmask,
+                                                   double* r) {
+#pragma unroll
+  for (int q = 0; q < DIM; ++q) r[q] = 0.0;
+  const int s0 = __ldg(&P.stat_slot_off[node]);
+  for (int k0 = 0; k0 < nn; k0 += L) {           // nn is uniform over the group
+    double pk[DIM];
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) pk[q] = 0.0;
+    if (k0 + k < nn) static_slot_product<DIM>(P, s0, k0 + k, pk);
+    const int n_here = min(L, nn - k0);
+    for (int j = 0; j < n_here; ++j)
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) r[q] += __shfl_sync(gmask, pk[q], j, L);
+  }
+}
+
+// Residual-only rows of the general nodes, entry-parallel: L lanes per DOF node.  The node's
+// static residual first (static blocks times displacements in slot order, then the macroscale-
+// strain response), then lane k takes the node's entries k, k + L, ... and forms each entry's
+// contribution (an uncut element's w B^T sigma; the cohesive traction at the node for a cut
+// element the node is on a cohesive element of) -- the same operations general_rows performs --
+// and the group adds the contributions in entry (adjacency) order with shuffles.  L divides 32.
 template <int DIM, int L>
 __global__ void __launch_bounds__(128) k_rows_general_resid(DevProblem P) {
   constexpr int NV = (DIM == 2) ? 3 : 6;
-  constexpr int D2 = DIM * DIM;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int node = t / L, k = t % L;
   const bool valid = node < P.n_slow_dn;   // uniform over each group of L lanes
@@ -415,6 +467,16 @@ __global__ void __launch_bounds__(128) k_rows_general_resid(DevProblem P) {
   double rs[DIM];
 #pragma unroll
   for (int q = 0; q < DIM; ++q) rs[q] = 0.0;
+  if (valid && node < P.n_stat) {                // uniform over the group
+    static_resid_group<DIM, L>(P, node, gd.w, k, gmask, rs);
+    if (P.subscale) {
+      const double* Gs = P.stat_g + (size_t)node * DIM * NV;
+#pragma unroll
+      for (int q = 0; q < DIM; ++q)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) rs[q] += __ldg(&Gs[q * NV + v]) * P.eps_macro[v];
+    }
+  }
   for (int e0 = 0; e0 < gd.y; e0 += L) {          // gd.y is uniform over the group
     const int ei = e0 + k;
     double re[DIM];
@@ -427,37 +489,8 @@ __global__ void __launch_bounds__(128) k_rows_general_resid(DevProblem P) {
       if (mn == 0) {
         double kb[DIM][DIM];
         simplex_block<DIM, false>(P, ax, la, 0, P.D[ad.w], kb, re, true);
-      } else {
-        const int* cn = P.cut_nodes + ax.y;
-        const double* kr = P.ke + ad.w;             // block row la of K_vol
-        for (int b = 0; b < mn; ++b) {
-          const int nb = __ldg(&cn[b]);
-          double u[DIM];
-          load_node<DIM>(P.U, nb, u);
-#pragma unroll
-          for (int q = 0; q < DIM; ++q) {
-            double s = 0.0;
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) s += __ldg(&kr[b * D2 + q * DIM + d]) * u[d];
-            re[q] += s;
-          }
-        }
-        if (P.subscale) {
-          const double* gm = P.gmac + __ldg(&P.re_off[ax.x]) / DIM * DIM * NV + (size_t)la * DIM * NV;
-#pragma unroll
-          for (int q = 0; q < DIM; ++q)
-#pragma unroll
-            for (int v = 0; v < NV; ++v) re[q] += gm[q * NV + v] * P.eps_macro[v];
-        }
-        const int cpa = ax.z;
-        if (cpa >= 0) {
-          const int ce = cpa >> 5, n1 = cpa & 31;
-          const int nh = __ldg(&P.coh_nh[ce]);
-          const double sgn = (n1 >= nh) ? 1.0 : -1.0;
-          const double* tr = P.kcoh + __ldg(&P.kc_off[ce]) + nh * nh * D2 + (n1 % nh) * DIM;
-#pragma unroll
-          for (int q = 0; q < DIM; ++q) re[q] += sgn * tr[q];
-        }
+      } else if (ax.z >= 0) {
+        coh_traction<DIM>(P, ax.z, re);
       }
     }
     // the node's sum in entry order
@@ -475,15 +508,15 @@ __global__ void __launch_bounds__(128) k_rows_general_resid(DevProblem P) {
 }
 
 // Residuals of the general rows for the P.n_cases macroscale strains of a multi-strain pass,
-// entry-parallel like k_rows_general_resid: an uncut element's geometry and strain of U are formed
-// once and each case adds its strain; a cut element's K_vol block row times U is formed once and
-// each case adds its macroscale-strain response and the traction.  For each case these are the
-// operations of the single-strain residual with that case as eps_macro, summed in entry order.
+// entry-parallel like k_rows_general_resid: the static residual is formed once and each case
+// adds its macroscale-strain response; an uncut element's geometry and strain of U are formed
+// once and each case adds its strain; a cut element adds the cohesive traction (the same for every
+// case).  For each case these are the operations of the single-strain residual with that case as
+// eps_macro, summed in the same order.
 template <int DIM, int L>
 __global__ void __launch_bounds__(128) k_rows_general_cases(DevProblem P) {
   constexpr int NPE = DIM + 1;
   constexpr int NV = (DIM == 2) ? 3 : 6;
-  constexpr int D2 = DIM * DIM;
   constexpr int MC = 6;
   const int nc = P.n_cases;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -493,9 +526,27 @@ __global__ void __launch_bounds__(128) k_rows_general_cases(DevProblem P) {
   if (__all_sync(0xffffffffu, !valid)) return;
   int4 gd = make_int4(0, 0, 0, 0);
   if (valid) gd = __ldg(&P.gdesc[node]);
-  double rs[MC];   // lane k < DIM: row k of the node, per case
+  double rs[MC][DIM];   // per case, every lane of the group
 #pragma unroll
-  for (int c = 0; c < MC; ++c) rs[c] = 0.0;
+  for (int c = 0; c < MC; ++c)
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) rs[c][q] = 0.0;
+  if (valid && node < P.n_stat) {
+    double su[DIM];
+    static_resid_group<DIM, L>(P, node, gd.w, k, gmask, su);
+    const double* Gs = P.stat_g + (size_t)node * DIM * NV;
+#pragma unroll
+    for (int c = 0; c < MC; ++c) {
+      if (c >= nc) break;
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) {
+        double v = su[q];
+#pragma unroll
+        for (int w = 0; w < NV; ++w) v += __ldg(&Gs[q * NV + w]) * P.eps_cases[c][w];
+        rs[c][q] = v;
+      }
+    }
+  }
   for (int e0 = 0; e0 < gd.y; e0 += L) {
     const int ei = e0 + k;
     double re[MC][DIM];
@@ -542,48 +593,14 @@ __global__ void __launch_bounds__(128) k_rows_general_cases(DevProblem P) {
 #pragma unroll
           for (int q = 0; q < DIM; ++q) re[c][q] = wgt * bt_sig<DIM, double>(ga, sig, q);
         }
-      } else {
-        const int* cn = P.cut_nodes + ax.y;
-        const double* kr = P.ke + ad.w;             // block row la of K_vol
-        double base[DIM];
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) base[q] = 0.0;
-        for (int b = 0; b < mn; ++b) {
-          const int nb = __ldg(&cn[b]);
-          double u[DIM];
-          load_node<DIM>(P.U, nb, u);
-#pragma unroll
-          for (int q = 0; q < DIM; ++q) {
-            double s = 0.0;
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) s += __ldg(&kr[b * D2 + q * DIM + d]) * u[d];
-            base[q] += s;
-          }
-        }
-        const double* gm = P.gmac + __ldg(&P.re_off[ax.x]) / DIM * DIM * NV + (size_t)la * DIM * NV;
+      } else if (ax.z >= 0) {
         double tr[DIM];
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) tr[q] = 0.0;
-        const int cpa = ax.z;
-        if (cpa >= 0) {
-          const int ce = cpa >> 5, n1 = cpa & 31;
-          const int nh = __ldg(&P.coh_nh[ce]);
-          const double sgn = (n1 >= nh) ? 1.0 : -1.0;
-          const double* tp = P.kcoh + __ldg(&P.kc_off[ce]) + nh * nh * D2 + (n1 % nh) * DIM;
-#pragma unroll
-          for (int q = 0; q < DIM; ++q) tr[q] = sgn * tp[q];
-        }
+        coh_traction<DIM>(P, ax.z, tr);
 #pragma unroll
         for (int c = 0; c < MC; ++c) {
           if (c >= nc) break;
 #pragma unroll
-          for (int q = 0; q < DIM; ++q) {
-            double v = base[q];
-#pragma unroll
-            for (int w = 0; w < NV; ++w) v += gm[q * NV + w] * P.eps_cases[c][w];
-            if (cpa >= 0) v += tr[q];
-            re[c][q] = v;
-          }
+          for (int q = 0; q < DIM; ++q) re[c][q] = tr[q];
         }
       }
     }
@@ -593,10 +610,7 @@ __global__ void __launch_bounds__(128) k_rows_general_cases(DevProblem P) {
       for (int c = 0; c < MC; ++c) {
         if (c >= nc) break;
 #pragma unroll
-        for (int q = 0; q < DIM; ++q) {
-          const double v = __shfl_sync(gmask, re[c][q], jj, L);
-          if (k == q) rs[c] += v;
-        }
+        for (int q = 0; q < DIM; ++q) rs[c][q] += __shfl_sync(gmask, re[c][q], jj, L);
       }
   }
   if (!valid || k >= DIM) return;
@@ -604,9 +618,46 @@ __global__ void __launch_bounds__(128) k_rows_general_cases(DevProblem P) {
 #pragma unroll
   for (int c = 0; c < MC; ++c) {
     if (c >= nc) break;
-    if (gdof < P.n_free) P.Pf_cases[(size_t)c * P.n_free + gdof] = rs[c];
-    else P.Pp_cases[(size_t)c * P.n_const + gdof - P.n_free] = rs[c];
+    double mine = rs[c][0];
+#pragma unroll
+    for (int q = 1; q < DIM; ++q) if (k == q) mine = rs[c][q];
+    if (gdof < P.n_free) P.Pf_cases[(size_t)c * P.n_free + gdof] = mine;
+    else P.Pp_cases[(size_t)c * P.n_const + gdof - P.n_free] = mine;
   }
+}
+
+// Set-up: the static part of the general rows next to cut elements (one thread per such node):
+// each cut entry's volumetric block row (K_vol, from k_cut_volumetric) added into the node's
+// neighbour slots and its macroscale-strain response into the node's sum, in entry order.  The
+// entries are cut-first, so the walk stops at the first uncut one.  stat and stat_g start at zero.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_general_static(DevProblem P, double* stat, double* stat_g) {
+  constexpr int NV = (DIM == 2) ? 3 : 6;
+  constexpr int D2 = DIM * DIM;
+  const int node = blockIdx.x * blockDim.x + threadIdx.x;
+  if (node >= P.n_stat) return;
+  const int4 gd = __ldg(&P.gdesc[node]);
+  double* S = stat + (size_t)__ldg(&P.stat_slot_off[node]) * D2;
+  double* Gs = stat_g + (size_t)node * DIM * NV;
+  bool bad = false;
+  for (int e = 0; e < gd.y; ++e) {
+    const int4 ad = __ldg(&P.adesc[gd.x + e]);
+    const int4 ax = __ldg(&P.aresd[gd.x + e]);
+    const int la = ad.y & 255, mn = ad.y >> 8;
+    if (mn == 0) break;
+    const int cc = ax.x;
+    const double* kr = P.ke + __ldg(&P.ke_off[cc]) + (size_t)la * mn * D2;   // block row la of K_vol
+    for (int b = 0; b < mn; ++b) {
+      double* o = S + (size_t)__ldg(&P.adj_slots[ad.z + b]) * D2;
+#pragma unroll
+      for (int i = 0; i < D2; ++i) o[i] += kr[b * D2 + i];
+    }
+    const double* gm = P.gmac + (size_t)__ldg(&P.re_off[cc]) / DIM * DIM * NV + (size_t)la * DIM * NV;
+#pragma unroll
+    for (int i = 0; i < DIM * NV; ++i) Gs[i] += gm[i];
+  }
+  for (int i = 0; i < gd.w * D2; ++i) bad |= !isfinite(S[i]);
+  if (bad) atomicOr(P.err, ERR_NONFINITE);
 }
 
 template <int DIM, int G>

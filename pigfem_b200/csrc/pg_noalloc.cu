@@ -1,8 +1,10 @@
 // pg_noalloc.cu -- a residual norm that allocates nothing (pg_norm2_noalloc).
 //
-// The norm's block partials and its completion counter live in one file-scope __device__ array
-// of fixed size, so a call makes no device allocation at all.  Its address is looked up once
-// per device with cudaGetSymbolAddress and then passed to the kernel as a plain pointer.
+// The norm's block partials live in one file-scope __device__ array of fixed size, so a call
+// makes no device allocation at all.  Its address is looked up once per device with
+// cudaGetSymbolAddress and then passed to the kernels as a plain pointer.  Two launches on the
+// caller's stream: the block partials, then one block that sums them.  Stream order separates
+// the two, so no completion counter (and no state that could outlive a call) is needed.
 #include "../../include/pigfem_b200.h"
 
 #include <cuda_runtime.h>
@@ -17,22 +19,18 @@ constexpr long long kPerBlock = (long long)kThreads * kPerThread;  // 8192 value
 constexpr int kMaxBlocks = PG_NORM_NOALLOC_MAX_N / kPerBlock;      // 4096 partials (32 KiB)
 static_assert((long long)kMaxBlocks * kPerBlock == PG_NORM_NOALLOC_MAX_N, "max size is whole blocks");
 
-// [0, kMaxBlocks): one partial sum of squares per block.  [kMaxBlocks]: the completion counter,
-// read as an unsigned int.  The counter must be zero when a call starts: the array is zero at
-// module load and the last block of every call puts the counter back to zero.
-__device__ __align__(256) double pg_norm_scratch[kMaxBlocks + 32];
+// One partial sum of squares per block of the first launch.  Every call writes the partials it
+// reads, so nothing has to start at zero.
+__device__ __align__(256) double pg_norm_scratch[kMaxBlocks];
 
 constexpr int kMaxDevices = 64;
 double* g_scratch[kMaxDevices] = {};
 std::mutex g_scratch_mu;
 
 // Sum of squares in a fixed order: block b reduces values [b*8192, (b+1)*8192) with a fixed
-// per-thread stride and a fixed tree; the last block to finish sums the partials in a fixed
-// tree order.  The result depends on n and the data only, never on block scheduling.
-__global__ void __launch_bounds__(kThreads) k_norm2_noalloc(const double* __restrict__ x, long long n,
-                                                           double* scratch, double* out) {
+// per-thread stride and a fixed tree into part[b].
+__global__ void __launch_bounds__(kThreads) k_norm2_partials(const double* __restrict__ x, long long n, double* part) {
   __shared__ double sh[kThreads];
-  __shared__ bool last;
   const long long b0 = (long long)blockIdx.x * kPerBlock;
   const long long b1 = b0 + kPerBlock < n ? b0 + kPerBlock : n;
   double s = 0.0;
@@ -43,28 +41,22 @@ __global__ void __launch_bounds__(kThreads) k_norm2_noalloc(const double* __rest
     if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
     __syncthreads();
   }
-  unsigned int* done = reinterpret_cast<unsigned int*>(scratch + kMaxBlocks);
-  if (threadIdx.x == 0) {
-    scratch[blockIdx.x] = sh[0];
-    __threadfence();
-    last = (atomicAdd(done, 1u) == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  const volatile double* part = scratch;
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+// One block: the partials summed in a fixed tree order, then the square root.  The result
+// depends on n and the data only, never on block scheduling.
+__global__ void __launch_bounds__(kThreads) k_norm2_final(const double* __restrict__ part, int nb, double* out) {
+  __shared__ double sh[kThreads];
   double t = 0.0;
-  for (int i = threadIdx.x; i < (int)gridDim.x; i += kThreads) t += part[i];
+  for (int i = threadIdx.x; i < nb; i += kThreads) t += part[i];
   sh[threadIdx.x] = t;
   __syncthreads();
   for (int w = kThreads / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    *out = sqrt(sh[0]);
-    *done = 0u;
-  }
+  if (threadIdx.x == 0) *out = sqrt(sh[0]);
 }
 
 // Per-device set-up: the scratch address of the current device, looked up on the first call.
@@ -89,6 +81,8 @@ extern "C" int pg_norm2_noalloc(const double* d_x, int64_t n, double* d_out, voi
   double* scratch = nullptr;
   if (int rc = scratch_for_current_device(&scratch)) return rc;
   const int blocks = n == 0 ? 1 : (int)((n + kPerBlock - 1) / kPerBlock);
-  k_norm2_noalloc<<<blocks, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(d_x, (long long)n, scratch, d_out);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_norm2_partials<<<blocks, kThreads, 0, st>>>(d_x, (long long)n, scratch);
+  k_norm2_final<<<1, kThreads, 0, st>>>(scratch, blocks, d_out);
   return cudaGetLastError() == cudaSuccess ? PG_OK : PG_ERR_DEVICE;
 }

@@ -4,6 +4,9 @@ The reference reads fiber layouts from CSV files (Tests/Main.cpp:744-860) and pu
 set; the workloads here are seeded synthetic layouts with the sizes and distributions of the
 benchmark configurations:
 
+* ``linear_2d``: unit square, 64 x 64 quads split into 8,192 tri3, ten fibers with radius
+  ~ U[0.03, 0.06] and a minimum gap of 0.01, linear elastic, 1 % uniaxial strain prescribed on the
+  right edge (Tests/Main.cpp:563-571): one K and R assembly.
 * ``cohesive_2d``: unit square, N x N quads split into 2 N^2 tri3 (Mesh::generate_mesh), fibers
   placed by rejection sampling with radius ~ U[r_lo, r_hi], centre ~ U[r, 1-r]^2 and a minimum
   surface gap; bilinear cohesive law on every interface.
@@ -23,7 +26,7 @@ from typing import Optional
 
 import numpy as np
 
-from .capi import COH_BL, TET4, TRI3, ProblemDesc
+from .capi import COH_BL, COH_NONE, TET4, TRI3, ProblemDesc
 
 E_MATRIX, NU_MATRIX = 3.5e3, 0.35   # MPa
 E_FIBER, NU_FIBER = 72e3, 0.22
@@ -120,6 +123,15 @@ def cohesive_2d(n: int = 512, n_fibers: int = 200, r_lo: float = 0.008, r_hi: fl
     return RVE(desc, fib, vf)
 
 
+def linear_2d(n: int = 64, n_fibers: int = 10, r_lo: float = 0.03, r_hi: float = 0.06, gap: float = 0.01,
+              seed: int = 1, request: int = 0, workload: int = 0, app_strain: float = 0.01) -> RVE:
+    """The 2D linear-elastic RVE: n x n quads split into tri3, seeded non-overlapping circular
+    fibers, matrix / fiber isotropic linear elasticity (plane strain), no cohesive interfaces,
+    u_x = app_strain * L on the right edge, u_x = 0 on the left, node 0 pinned."""
+    return cohesive_2d(n=n, n_fibers=n_fibers, r_lo=r_lo, r_hi=r_hi, gap=gap, seed=seed, request=request,
+                       workload=workload, app_strain=app_strain, coh_law=COH_NONE, coh=(0.0, 0.0, 0.0, 0.0))
+
+
 def linear_3d(n: int = 64, n_spheres: int = 50, r_lo: float = 0.04, r_hi: float = 0.08, gap: float = 0.01,
               seed: int = 1, request: int = 0, workload: int = 3, max_redraws: int = 50) -> RVE:
     """Unit cube, n^3 hexes split into 6 tet4, seeded non-overlapping spheres, periodic subscale
@@ -175,26 +187,39 @@ def cohesive_batch(count: int = 256, seed: int = 1, n_lo: int = 32, n_hi: int = 
 
 
 def interface_state(problem, seed: int = 0, open_lo: float = 1e-7, open_hi: float = 6e-3, u_scale: float = 1e-6):
+    """A displacement field (node-major) with seeded tensile openings at every cohesive interface
+    of `problem` (a :class:`capi.Problem`): :func:`interface_state_tables` on its set-up tables."""
+    return interface_state_tables(
+        problem.dim, problem.n_nodes, problem.debug("cut_node_off"), problem.debug("cut_nodes"),
+        problem.debug("cut_coh_off"), problem.debug("coh_local_off"), problem.debug("coh_local"),
+        problem.debug("coh_qp_off"), problem.debug("cqp_R"), seed=seed, open_lo=open_lo, open_hi=open_hi,
+        u_scale=u_scale)
+
+
+def interface_state_tables(dim: int, n_nodes: int, cut_node_off, cut_nodes, cut_coh_off, coh_local_off, coh_local,
+                           coh_qp_off, cqp_R, seed: int = 0, open_lo: float = 1e-7, open_hi: float = 6e-3,
+                           u_scale: float = 1e-6):
     """A displacement field (node-major) with seeded tensile openings at every cohesive interface:
     each '+' enrichment node is displaced from its '-' partner along the mean normal of the
     cohesive elements that hold the pair, by a log-uniform opening in [open_lo, open_hi] plus a
     tangential slip of up to 0.3 of it, so the bilinear law runs through its loading, softening
     and failed branches while every cohesive point stays in tension.  Bulk displacements are small
-    random values."""
+    random values.
+
+    The tables describe the enriched mesh in the reference's own terms, so the same state can be
+    built from this library's set-up or from the reference's mesh: the cut elements' node lists
+    (parent nodes, then enrichment nodes; node ids standard first, then enrichment), the range of
+    cohesive elements of each cut element, each cohesive element's local node list ('-' half, then
+    '+' half, indices into its cut element's node list), and the rotation of every cohesive
+    quadrature point (dim x dim, last row the normal)."""
+    cut_node_off, cut_nodes, cut_coh_off = (np.asarray(a) for a in (cut_node_off, cut_nodes, cut_coh_off))
+    coh_local_off, coh_local, coh_qp_off = (np.asarray(a) for a in (coh_local_off, coh_local, coh_qp_off))
     rng = np.random.default_rng(seed)
-    dim = problem.dim
-    n_nodes = problem.n_nodes
     U = rng.uniform(-u_scale, u_scale, n_nodes * dim).reshape(-1, dim)
-    cut_node_off = problem.debug("cut_node_off")
-    cut_nodes = problem.debug("cut_nodes")
-    cut_coh_off = problem.debug("cut_coh_off")
-    coh_local_off = problem.debug("coh_local_off")
-    coh_local = problem.debug("coh_local")
-    coh_qp_off = problem.debug("coh_qp_off")
     n_ce = len(coh_local_off) - 1
     if n_ce <= 0:
         return np.ascontiguousarray(U.reshape(-1))
-    R = problem.debug("cqp_R").reshape(-1, dim, dim)
+    R = np.asarray(cqp_R, dtype=np.float64).reshape(-1, dim, dim)
     ce_cut = np.repeat(np.arange(len(cut_coh_off) - 1), np.diff(cut_coh_off))
     Rm = np.add.reduceat(R, coh_qp_off[:-1], axis=0) / np.diff(coh_qp_off)[:, None, None]
     nh = np.diff(coh_local_off) // 2

@@ -21,10 +21,11 @@ from tests.golden.cases import CASES, spec_kwargs
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 HEADER = os.path.join(ROOT, "include", "pigfem_b200.h")
+DROPIN_HEADER = os.path.join(ROOT, "include", "pigfem_b200_dropin.h")
 
 
-def header_functions():
-    txt = open(HEADER).read()
+def header_functions(path=HEADER):
+    txt = open(path).read()
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
     return sorted(set(re.findall(r"^\s*(?:const\s+)?(?:int|void|char\s*\*|const char\s*\*)\s*\*?\s*(pg_\w+)\s*\(", txt, flags=re.M)))
 
@@ -42,6 +43,19 @@ def test_library_exports_every_declared_function():
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
     assert set(capi.EXPORTED) <= set(names)
+
+
+def test_dropin_build_exports_its_binding_calls():
+    """The reference built with the drop-in Assembler::assemble (oracle/_ref/libpigfem_ref_b200.so)
+    exports every call include/pigfem_b200_dropin.h declares, and its Assembler::assemble is the
+    drop-in's (the reference's own definition is weak in that build)."""
+    from oracle import ref
+    if not ref.available("b200"):
+        pytest.skip("drop-in variant of the oracle not built")
+    L = ctypes.CDLL(ref.LIB_B200_PATH)
+    names = header_functions(DROPIN_HEADER)
+    assert names == ["pg_dropin_bind", "pg_dropin_last_error", "pg_dropin_unbind"], names
+    assert all(hasattr(L, n) for n in names)
 
 
 @pytest.mark.parametrize("name", sorted(CASES))

@@ -2,7 +2,7 @@
 
 Called through the C ABI on the internal-force vector P_f of an assembled cohesive problem and
 compared with pg_residual_norm (the context-scratch norm) on two calls in a row; the second
-call checks that the completion counter was put back to zero.  Also: a multi-block vector
+call reads the partials the first one left behind and must overwrite them all.  Also: a multi-block vector
 against torch's FP64 norm, the empty vector, and the size limit.
 """
 import ctypes
