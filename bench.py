@@ -58,10 +58,13 @@ def parse_from(argv):
                    default="cohesive_2d_512")
     p.add_argument("--requests", type=int, default=48, help="serving: requests per swept rate")
     p.add_argument("--rates", type=str, default="2,4,8", help="serving: Poisson arrival rates (requests/s)")
+    p.add_argument("--session-steps", type=int, default=3,
+                   help="serving: load steps per cohesive session (1: every cohesive request stands alone)")
     p.add_argument("--batch", type=int, default=256)
     p.add_argument("--grid3d", type=int, default=64)
     p.add_argument("--spheres", type=int, default=50)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-batched", action="store_true", help="leave the batched sub-object out of the default line")
     p.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (default: --steps)")
     p.add_argument("--ref-procs", type=int, default=0, help="reference arm: replica processes (default: one per core)")
     return p.parse_args(argv)
@@ -229,7 +232,7 @@ def measured_peak_hbm():
 WORKLOADS = {
     "cohesive_2d_512": "cohesive_2d_512: 512x512 tri3 split (524,288 tri3), 200 circular fibers, bilinear cohesive interfaces",
     "linear_3d_64": "linear_3d_64: 64^3 hexes split into 6 tet4 (1,572,864 tet4), 50 spheres, periodic, one K and six unit-strain right-hand sides",
-    "serving": "serving: Poisson RVE requests (70% 2D 32^2-512^2 with 5-300 fibers, 30% 3D tet4 16^3-64^3 with 5-60 spheres; 60% homogenization by device PCG to 1e-8, 40% cohesive load-step tangent/residual)",
+    "serving": "serving: Poisson RVE requests (70% 2D 32^2-512^2 with 5-300 fibers, 30% 3D tet4 16^3-64^3 with 5-60 spheres; 60% homogenization by device PCG to 1e-8, 40% cohesive load-step tangent/residual, each opening a session of --session-steps load steps on a device-resident context)",
     "batched_2d_256": "batched_2d_256: 256 independent 2D cohesive RVEs (grid side log-uniform 32-256, 5-120 fibers, volume fraction 0.2-0.5), one batched assembly of all",
 }
 
@@ -547,6 +550,85 @@ def main_batched(args, ws, rank, local):
     print(json.dumps(line))
 
 
+def batched_summary(args, ws, rank, steps: int = 10, warmup: int = 3) -> dict:
+    """The batched workload (256 independent 2D cohesive RVEs, grid side log-uniform 32-256, 5-120
+    fibers, volume fraction 0.2-0.5) as a compact sub-object of the default line: one batched
+    FP32-mixed and one batched FP64 assembly of every RVE per step (persistent kernels replayed
+    from a CUDA graph, autotuned shape), beside the plain path (one pg_assemble_device call per
+    RVE, FP64), device-resident inputs, L2 flushed before every step.  Every rank runs its own batch
+    (the same collective calls in the same order on every rank)."""
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+    from pigfem_b200 import capi, rve
+    t0 = time.time()
+    rves = rve.cohesive_batch(count=args.batch, seed=1 + 1000 * rank)
+    with ThreadPoolExecutor(max(1, min(16, os.cpu_count() or 1))) as ex:
+        probs = list(ex.map(lambda r: capi.Problem(r.desc, device=False), rves))
+    for P in probs:
+        P.upload()
+    dUs = [torch.from_numpy(rve.interface_state(P, seed=i)).cuda() for i, P in enumerate(probs)]
+    ptrs = [u.data_ptr() for u in dUs]
+    B = capi.Batch(probs)
+    setup_s = time.time() - t0
+    ne = sum(P.sizes["n_elem"] for P in probs)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    f64, f32 = capi.FUNC | capi.JAC, capi.FUNC | capi.JAC | capi.FP32
+    B.tune(ptrs, f32, reps=3)
+    info = B.info()
+
+    def batch_ms(flags):
+        for _ in range(warmup):
+            B.assemble(ptrs, flags)
+            B.wait()
+        total = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            B.assemble(ptrs, flags)
+            total += B.wait()
+        return total
+
+    def plain_ms(flags):
+        for P in probs:
+            P.set_stream(stream.cuda_stream)
+        for _ in range(warmup):
+            for P, pu in zip(probs, ptrs):
+                P.assemble_device(pu, 1.0, flags)
+        torch.cuda.synchronize()
+        total = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for P, pu in zip(probs, ptrs):
+                P.assemble_device(pu, 1.0, flags)
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        return total
+
+    ms32, ms64, ms_plain = replicas.max_over_ranks([batch_ms(f32), batch_ms(f64), plain_ms(f64)], "cuda")
+    alg32 = sum(algorithmic_bytes(P, True)["total"] for P in probs)
+    alg64 = sum(algorithmic_bytes(P, False)["total"] for P in probs)
+    peak, peak_kind = measured_peak_hbm()
+    v32 = ws * ne * steps / (ms32 * 1e-3)
+    v64 = ws * ne * steps / (ms64 * 1e-3)
+    vplain = ws * ne * steps / (ms_plain * 1e-3)
+    B.close()
+    for P in probs:
+        P.close()
+    return {"workload": WORKLOADS["batched_2d_256"], "rves": len(probs), "elements": ne, "steps": steps,
+            "fp32_mixed": {"value": v32, "unit": UNIT, "ms_per_step": ms32 / steps,
+                           "hbm_frac": alg32 / (ms32 / steps * 1e-3) / 1e9 / peak},
+            "fp64": {"value": v64, "unit": UNIT, "ms_per_step": ms64 / steps,
+                     "hbm_frac": alg64 / (ms64 / steps * 1e-3) / 1e9 / peak},
+            "plain_fp64_per_rve_calls": {"value": vplain, "unit": UNIT, "ms_per_step": ms_plain / steps},
+            "fp32_batched_over_plain_fp64": v32 / vplain, "fp32_over_fp64_batched": v32 / v64,
+            "peak": peak, "peak_kind": peak_kind, "autotuned_shape": info, "setup_s": setup_s,
+            "l2": f"flushed before every timed step ({L2_FLUSH_BYTES >> 20} MiB write)"}
+
+
 def main_serving(args, ws, rank, local):
     """The request loop at swept arrival rates, beside the same requests run one at a time."""
     import torch
@@ -555,17 +637,23 @@ def main_serving(args, ws, rank, local):
     free, total = torch.cuda.mem_get_info()
     budget = int(0.5 * free)
     rates = [float(x) for x in args.rates.split(",")]
-    # one-at-a-time plain FP64 calls (closed loop): the baseline
-    base_reqs = serving.poisson_stream(args.requests, rates[0], seed=11 + rank)
-    serving.run_alone(base_reqs[0])      # warm-up (module loading, pools)
+    # one-at-a-time plain FP64 calls (closed loop): the baseline; a session's steps run on one
+    # context, one after the other
+    base_reqs = serving.poisson_stream(args.requests, rates[0], seed=11 + rank, session_steps=args.session_steps)
+    serving.run_alone(next(q for q in base_reqs if q.session < 0))      # warm-up (module loading, pools)
     t0 = time.perf_counter()
-    alone = [serving.run_alone(r) for r in base_reqs]
+    alone = []
+    for q in base_reqs:
+        if q.session < 0:
+            alone.append(serving.run_alone(q))
+        elif q.step == 0:
+            alone += serving.run_session_alone([r for r in base_reqs if r.session == q.session])
     wall_alone = time.perf_counter() - t0
     lat_alone = np.array([a.done for a in alone])
     sweep = []
     clk = Clocks(local).__enter__()
     for rate in rates:
-        reqs = serving.poisson_stream(args.requests, rate, seed=11 + rank)
+        reqs = serving.poisson_stream(args.requests, rate, seed=11 + rank, session_steps=args.session_steps)
         eng = serving.ServingEngine(memory_budget=budget, max_inflight=8, setup_workers=min(16, os.cpu_count() or 1))
         t0 = time.perf_counter()
         res = eng.run(reqs, realtime=True)
@@ -576,6 +664,9 @@ def main_serving(args, ws, rank, local):
         summ["mean_setup_s"] = float(np.mean([r.setup_done - r.arrival for r in res]))
         summ["mean_queue_s"] = float(np.mean([r.admitted - r.setup_done for r in res]))
         summ["mean_gpu_s"] = float(np.mean([r.done - r.admitted for r in res]))
+        summ["session_steps"] = sum(1 for q in reqs if q.session >= 0)
+        summ["bytes_calibration"] = eng.calibration
+        summ["peak_ledger_bytes"] = eng.peak_charged
         sweep.append(summ)
     clk.__exit__(None, None, None)
     # whole-job request rates: each rank serves its own stream
@@ -589,7 +680,8 @@ def main_serving(args, ws, rank, local):
         "warmup": 1, "ms_per_step": 1e3 / best["req_per_s"] if best["req_per_s"] else None, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded request geometries)",
         "config": {"workload": WORKLOADS["serving"], "requests_per_rate": args.requests, "rates": rates,
-                   "memory_budget_bytes": budget, "max_inflight": 8, "l2": "n/a (request stream)",
+                   "memory_budget_bytes": budget, "max_inflight": 8, "session_steps": args.session_steps,
+                   "l2": "n/a (request stream)",
                    "parallelism": f"replicas x{ws}"},
         "p50_s": best["p50_s"], "p99_s": best["p99_s"], "sweep": sweep,
         "one_at_a_time_fp64": {"req_per_s": len(alone) / wall_alone, "p50_s": float(np.percentile(lat_alone, 50)),
@@ -739,6 +831,9 @@ def main():
     h2d = U.nbytes
     d2h = 8 * (sum(P.nnz) + n_rhs * (P.n_free + P.n_const))
 
+    batched = None
+    if args.workload == "cohesive_2d_512" and not args.no_batched:
+        batched = batched_summary(args, ws, rank)
     # roofline of the dominant kernel (the fast row kernel), from the live per-kernel events
     peak, peak_kind = measured_peak_hbm()
     fk_bytes = fast_kernel_bytes(P, False)
@@ -750,8 +845,8 @@ def main():
         # the five extra right-hand sides write their residuals (one pass reads the nodes once)
         extra = 5 * 8 * (P.n_free + P.n_const)
         alg["total"] += extra
-    stencil_name = f"k_rows_stencil<{P.dim},double>"
-    general_name = f"k_rows_general<{P.dim},{4 if P.dim == 2 else 8}>"
+    stencil_name = f"k_rows_tile{P.dim}<double,1>"
+    general_name = f"k_gen_rows<{P.dim}>"
     gk_bytes = general_kernel_bytes(P, False)
     gk_ms = float(kt64[2])
     g_achieved = gk_bytes / (gk_ms * 1e-3) / 1e9 if gk_ms > 0 else None
@@ -769,17 +864,17 @@ def main():
                                           "cohesive_qps": P.sizes["n_coh_qp"]}, ws),
             "fp32_mixed": {"value": value32, "unit": UNIT, "ms_per_step": ms32 / args.steps, "speedup_vs_fp64": value32 / value,
                            "kernel_ms": [float(x) for x in kt32]},
-            "kernel_ms": {"cohesive_elements": float(kt64[0]), "rows_stencil": float(kt64[1]),
+            "kernel_ms": {"cohesive_elements_and_records": float(kt64[0]), "rows_stencil": float(kt64[1]),
                           "rows_general": float(kt64[2]), "assembly": float(kt64[3])},
             "algorithmic_bytes_per_step": alg["total"], "algorithmic_bytes_per_element": alg["total"] / ne,
             "algorithmic_gbs": alg["total"] / (ms64 / args.steps * 1e-3) / 1e9,
-            "roofline": {"bound": "hbm", "kernel": f"{stencil_name} " + ("(side stream, concurrent with the cohesive and general-row kernels)" if P.dim == 2 else "(main stream, alone)"),
+            "roofline": {"bound": "hbm", "kernel": f"{stencil_name} " + ("(low-priority stream, concurrent with the cohesive and general-row kernels)" if P.dim == 2 else "(main stream, alone)"),
                          "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": profiled_traffic(stencil_name), "bytes_per_launch": fk_bytes,
                          "traffic_note": "ncu dram read+write per launch, cold cache; row writes still in L2 at kernel end are not counted"},
             # the longest-running kernel (the stencil kernel above moves most of the bytes)
-            "roofline_general": {"bound": "hbm", "kernel": f"{general_name} " + ("(main stream, after the cohesive elements, sharing the SMs with the stencil rows)" if P.dim == 2 else "(main stream, after the stencil rows, alone)"),
+            "roofline_general": {"bound": "hbm", "kernel": f"{general_name} " + ("(high-priority stream, after the cohesive elements and records, sharing the SMs with the stencil rows)" if P.dim == 2 else "(main stream, after the stencil rows, alone)"),
                                  "achieved": g_achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                                  "frac": (g_achieved / peak) if g_achieved else None,
                                  "traffic": profiled_traffic(general_name), "bytes_per_launch": gk_bytes},
@@ -789,6 +884,7 @@ def main():
             "gpu_launches": launches_per_step(P) * (2 if three_d else 1) * args.steps,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "batched": batched,
         }
     replicas.finish()
     if line is not None:

@@ -73,6 +73,14 @@ typedef struct {
   int32_t subscale;             /* 1: periodic mesh, macroscale strain eps_macro, node 0 pinned */
   double eps_macro[6];          /* Voigt (xx, yy, xy) or (xx, yy, zz, yz, xz, xy), engineering shear */
   double app_strain;            /* Dirichlet mode: u_x = app_strain * (hi[0]-lo[0]) on the right, 0 on the left, node 0 pinned */
+  /* Bounding plies (Tests/Main.cpp:262-289, 343-360): the elements whose nodes all lie within
+   * ply_frac * (hi[1]-lo[1]) of the top or of the bottom take a transversely isotropic material
+   * (LinearElasticTransverselyIsotropicMaterial, src/material_leti.cpp; fibers along x) with
+   * ply = {E1, E2, G12, G23, nu12}.  0: no plies.  As in the reference's Mesh::detection, an
+   * element wholly inside an inclusion takes the fiber material even within a ply, and the
+   * matrix-side sub-elements of a cut ply element take the ply material. */
+  double ply_frac;
+  double ply[5];
 } pg_problem_desc;
 
 typedef struct {
@@ -95,6 +103,11 @@ int pg_debug_array(const pg_ctx* ctx, const char* name, int64_t* n, const void**
 void pg_destroy(pg_ctx* ctx);
 const char* pg_last_error(const pg_ctx* ctx);
 int pg_get_sizes(const pg_ctx* ctx, pg_sizes* out);
+/* Device memory the context holds now and the most it has held at once, in bytes: every
+ * allocation of pg_upload, the solver workspaces and the homogenization partials, counted as
+ * requested from the stream-ordered pool (0 for a host-only context).  Either pointer may be
+ * NULL. */
+int pg_device_bytes(const pg_ctx* ctx, int64_t* now, int64_t* peak);
 
 /* CSR pattern of block b (0 ff, 1 fp, 2 pf, 3 pp): rowptr[nrows+1], cols[nnz]. */
 int pg_get_pattern(const pg_ctx* ctx, int block, int32_t* rowptr, int32_t* cols);
@@ -112,7 +125,8 @@ int pg_assemble(pg_ctx* ctx, const double* U_node_major, double t_frac, int flag
 /* Same, on device-resident data: d_U is a 16-byte aligned device pointer (n_nodes*dim); results
  * stay in the context's device buffers (pg_device_outputs). */
 int pg_assemble_device(pg_ctx* ctx, const double* d_U, double t_frac, int flags);
-/* Residuals of several macroscale strains in one pass, for subscale problems: the load cases of a
+/* Residuals of several macroscale strains in one pass, for subscale tri3 / tet4 problems
+ * (PG_ERR_UNSUPPORTED for quad4): the load cases of a
  * homogenization, which the reference assembles one Assembler::assemble(assembleJac = false) at a
  * time after Assembler::assemble_new_load_step sets each case's macroscale value
  * (src/Assembler.cpp:65-146, 394-511).  Case k's strain is eps[6k .. 6k+5] * t_frac (Voigt; the 3D
@@ -131,8 +145,9 @@ int pg_set_stream(pg_ctx* ctx, void* stream);
 
 /* Device timing of the last assembly from CUDA events the context records on its streams:
  * ms[0] cohesive elements, ms[1] stencil rows (2D: side stream, concurrent with ms[0] and ms[2];
- * 3D: after ms[0]), ms[2] general rows (2D: after ms[0]; 3D: after ms[1]), ms[3] the whole
- * assembly (fork to join).  pg_set_timing is kept for callers
+ * 3D: after ms[0]), ms[2] general rows (2D: the longer of the rows on cohesive elements, after
+ * ms[0], and the other general rows, on their own stream from the start; 3D: after ms[1]),
+ * ms[3] the whole assembly (fork to join).  pg_set_timing is kept for callers
  * that toggle it; the events are always recorded. */
 int pg_set_timing(pg_ctx* ctx, int on);
 int pg_kernel_times(pg_ctx* ctx, float* ms);
@@ -187,12 +202,13 @@ int pg_batch_create(pg_ctx* const* ctxs, int n, pg_batch** out);
 int pg_batch_assemble(pg_batch* b, const double* const* d_U, const double* t_frac, int flags);
 /* Waits for the last pg_batch_assemble; ms (may be NULL) gets its device time. */
 int pg_batch_wait(pg_batch* b, float* ms);
-/* Autotuner: times every candidate launch shape (stencil nodes per block, general-row lanes per
- * node, persistent blocks per SM) over `reps` assemblies of this batch and keeps the fastest;
- * best[3] (may be NULL) gets {nodes per stencil block, lanes per general node, blocks per SM}. */
+/* Autotuner: times every candidate launch shape (persistent blocks per SM; the stencil rows run
+ * as fixed tiles, the general rows a thread per row block) over `reps` assemblies of this batch
+ * and keeps the fastest; best[3] (may be NULL) gets {threads per stencil tile, 1, blocks per SM}.
+ * Contexts must be tri3 or tet4 (PG_ERR_UNSUPPORTED for quad4). */
 int pg_batch_tune(pg_batch* b, const double* const* d_U, int flags, int reps, int* best);
-/* info[8]: contexts, elements, nodes per stencil block, lanes per general node, blocks per SM,
- * cohesive-point chunks, stencil chunks, general chunks. */
+/* info[8]: contexts, elements, threads per stencil tile, 1, blocks per SM, cohesive-point chunks,
+ * stencil chunks, general-row chunks. */
 int pg_batch_info(const pg_batch* b, int64_t* info);
 const char* pg_batch_last_error(const pg_batch* b);
 void pg_batch_destroy(pg_batch* b);

@@ -34,6 +34,7 @@ class _Config(ctypes.Structure):
         ("coh_law", ctypes.c_int), ("coh", ctypes.c_double * 4),
         ("plane_strain", ctypes.c_int), ("subscale", ctypes.c_int),
         ("eps_macro", ctypes.c_double * 6), ("app_strain", ctypes.c_double),
+        ("ply_frac", ctypes.c_double), ("ply", ctypes.c_double * 5),
     ]
 
 
@@ -99,6 +100,8 @@ class ProblemSpec:
     subscale: bool = False
     eps_macro: Sequence[float] = (0.0,) * 6
     app_strain: float = 0.01
+    ply_frac: float = 0.0
+    ply: Sequence[float] = (0.0,) * 5
 
 
 class RefProblem:
@@ -128,6 +131,9 @@ class RefProblem:
         for i, v in enumerate(spec.eps_macro):
             c.eps_macro[i] = v
         c.app_strain = spec.app_strain
+        c.ply_frac = spec.ply_frac
+        for i, v in enumerate(spec.ply):
+            c.ply[i] = v
         self._cfg = c
         self.h = L.pgref_create(ctypes.byref(c))
         nfc = self.get("n_free_const")

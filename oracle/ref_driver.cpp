@@ -61,6 +61,7 @@ extern "C" const char* pg_dropin_last_error(void) __attribute__((weak));
 #include "elem.h"
 #include "CohesiveElem.h"
 #include "material_lei.h"
+#include "material_leti.h"
 #include "Material_BilinearCohesive.h"
 #include "Material_BilinearCohesiveNU.h"
 #include "Material_XNCohesive.h"
@@ -118,6 +119,8 @@ typedef struct {
   int subscale;               /* 1: periodic mesh + macroscale strain eps_macro, node 0 pinned */
   double eps_macro[6];
   double app_strain;          /* Dirichlet mode: right x = app_strain*(xmax-xmin), left x = 0, node 0 pinned */
+  double ply_frac;            /* bounding plies: top / bottom fraction of the height (0: none) */
+  double ply[5];              /* ply material E1, E2, G12, G23, nu12 */
 } pgref_config;
 
 }  // extern "C"
@@ -313,9 +316,12 @@ void export_mesh(Handle* h) {
     coff.i32.push_back((int)cmat.i32.size());
   }
   (void)esub_nodes; (void)esub_nodes_off;
-  Export& mats = put_d(h, "materials");  // per material: kind (0 lei, 1 cohesive), E, nu
+  Export& mats = put_d(h, "materials");  // per material: kind (0 lei, 1 cohesive, 2 leti), E (E1), nu (nu12)
   for (Material* m : mesh->_materials) {
     if (m->is_cohesive()) { mats.f64.push_back(1); mats.f64.push_back(0); mats.f64.push_back(0); }
+    else if (dynamic_cast<LinearElasticTransverselyIsotropicMaterial*>(m)) {
+      mats.f64.push_back(2); mats.f64.push_back(m->get_parameter("E1")); mats.f64.push_back(m->get_parameter("NU12"));
+    }
     else { mats.f64.push_back(0); mats.f64.push_back(m->get_parameter("E")); mats.f64.push_back(m->get_parameter("nu")); }
   }
   // internal-variable layout: per element, per qp, count
@@ -392,6 +398,37 @@ void* pgref_create(const pgref_config* cfg) {
   matrix.set_name("Matrix");
   mesh.add_material(&matrix);
   mesh.set_material("Matrix");
+  if (cfg->ply_frac > 0.0) {
+    // bounding plies as Tests/Main.cpp:262-289 and 343-360 build them: element sets of the
+    // elements whose nodes all lie in the top / bottom fraction of the height, given a linear
+    // elastic transversely isotropic material
+    std::set<id_type> top_ply, bottom_ply;
+    const double y_lims = cfg->ymax - cfg->ymin;
+    const double top_limit = cfg->ymax - y_lims * cfg->ply_frac;
+    const double bottom_limit = cfg->ymin + y_lims * cfg->ply_frac;
+    for (Mesh::element_iterator it = mesh.active_elements_begin(), end = mesh.active_elements_end(); it != end; ++it) {
+      bool in_top_ply = true, in_bottom_ply = true;
+      for (id_type n = 0; n < (*it)->n_nodes(); ++n) {
+        std::vector<double> coords = (*it)->get_node(n)->get_coords();
+        if (coords[1] < top_limit) in_top_ply = false;
+        if (coords[1] > bottom_limit) in_bottom_ply = false;
+      }
+      if (in_top_ply) top_ply.insert((*it)->get_id());
+      if (in_bottom_ply) bottom_ply.insert((*it)->get_id());
+    }
+    mesh.add_elemset("top_ply", top_ply);
+    mesh.add_elemset("bottom_ply", bottom_ply);
+    LinearElasticTransverselyIsotropicMaterial bounds;
+    bounds.set_parameter("E1", cfg->ply[0]);
+    bounds.set_parameter("E2", cfg->ply[1]);
+    bounds.set_parameter("G12", cfg->ply[2]);
+    bounds.set_parameter("G23", cfg->ply[3]);
+    bounds.set_parameter("NU12", cfg->ply[4]);
+    bounds.set_name("0_degree_plies");
+    mesh.add_material(&bounds);
+    mesh.set_material_from_elemset("0_degree_plies", "top_ply");
+    mesh.set_material_from_elemset("0_degree_plies", "bottom_ply");
+  }
   if (h->nonlinear) {
     Material* coh = make_cohesive(cfg->coh_law, cfg->coh);
     mesh.add_material(coh);
@@ -591,6 +628,8 @@ int pgref_bind_gpu(void* vh) {
   d.plane_strain = c.plane_strain; d.subscale = c.subscale;
   for (int i = 0; i < 6; ++i) d.eps_macro[i] = c.eps_macro[i];
   d.app_strain = c.app_strain;
+  d.ply_frac = c.ply_frac;
+  for (int i = 0; i < 5; ++i) d.ply[i] = c.ply[i];
   return pg_dropin_bind((void*)h->prob, &d);
 }
 

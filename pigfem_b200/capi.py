@@ -33,7 +33,7 @@ ERRORS = {2: "PG_ERR_INPUT", 3: "PG_ERR_GEOMETRY", 4: "PG_ERR_UNSUPPORTED", 7: "
 # Every symbol include/pigfem_b200.h declares.
 EXPORTED = [
     "pg_create", "pg_create_host", "pg_upload", "pg_debug_array", "pg_destroy", "pg_last_error",
-    "pg_get_sizes", "pg_get_pattern", "pg_get_nodes", "pg_assemble", "pg_assemble_device", "pg_residual_strains",
+    "pg_get_sizes", "pg_device_bytes", "pg_get_pattern", "pg_get_nodes", "pg_assemble", "pg_assemble_device", "pg_residual_strains",
     "pg_device_outputs", "pg_set_stream", "pg_set_isv", "pg_get_isv", "pg_commit_isv",
     "pg_get_damage_zones", "pg_residual_norm", "pg_set_timing", "pg_kernel_times", "pg_set_macro_strain",
     "pg_pcg_solve", "pg_homogenize", "pg_norm2_noalloc",
@@ -55,7 +55,7 @@ class _Desc(ctypes.Structure):
         ("E_matrix", ctypes.c_double), ("nu_matrix", ctypes.c_double), ("E_fiber", ctypes.c_double),
         ("nu_fiber", ctypes.c_double), ("coh_law", ctypes.c_int32), ("coh", ctypes.c_double * 4),
         ("plane_strain", ctypes.c_int32), ("subscale", ctypes.c_int32), ("eps_macro", ctypes.c_double * 6),
-        ("app_strain", ctypes.c_double),
+        ("app_strain", ctypes.c_double), ("ply_frac", ctypes.c_double), ("ply", ctypes.c_double * 5),
     ]
 
 
@@ -87,6 +87,7 @@ def load_library(path: Optional[str] = None):
         "pg_destroy": (None, [vp]),
         "pg_last_error": (ctypes.c_char_p, [vp]),
         "pg_get_sizes": (i32, [vp, ctypes.POINTER(_Sizes)]),
+        "pg_device_bytes": (i32, [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
         "pg_get_pattern": (i32, [vp, i32, p, p]),
         "pg_get_nodes": (i32, [vp, p, p, p]),
         "pg_assemble": (i32, [vp, p, dbl, i32, p, p, p, p, p, p]),
@@ -154,6 +155,8 @@ class ProblemDesc:
     subscale: bool = False
     eps_macro: Sequence[float] = (0.0,) * 6
     app_strain: float = 0.01
+    ply_frac: float = 0.0                       # bounding plies (0: none)
+    ply: Sequence[float] = (0.0,) * 5           # E1, E2, G12, G23, nu12
 
     @property
     def dim(self) -> int:
@@ -185,6 +188,9 @@ class Problem:
         for i, v in enumerate(desc.eps_macro):
             d.eps_macro[i] = v
         d.app_strain = desc.app_strain
+        d.ply_frac = desc.ply_frac
+        for i, v in enumerate(desc.ply):
+            d.ply[i] = v
         self._d = d
         h = ctypes.c_void_p(0)
         rc = L.pg_create_host(ctypes.byref(d), ctypes.byref(h))
@@ -216,6 +222,12 @@ class Problem:
         self.dim = s.dim
         self.n_nodes, self.n_free, self.n_const, self.n_isv = s.n_nodes, s.n_free, s.n_const, s.n_isv
         self.nnz = self.sizes["nnz"]
+
+    def device_bytes(self):
+        """(bytes held now, most bytes held at once) of this context's device allocations."""
+        now, peak = ctypes.c_int64(0), ctypes.c_int64(0)
+        self._check(load_library().pg_device_bytes(self.h, ctypes.byref(now), ctypes.byref(peak)))
+        return int(now.value), int(peak.value)
 
     def pattern(self, block: int):
         nrows = [self.n_free, self.n_free, self.n_const, self.n_const][block]
@@ -405,7 +417,7 @@ class Batch:
     def info(self) -> dict:
         v = np.zeros(8, np.int64)
         self._check(load_library().pg_batch_info(self.h, _ptr(v)))
-        keys = ("contexts", "elements", "stencil_nodes_per_block", "general_lanes_per_node", "blocks_per_sm",
+        keys = ("contexts", "elements", "stencil_tile_threads", "general_threads_per_block", "blocks_per_sm",
                 "coh_chunks", "stencil_chunks", "general_chunks")
         return {k: int(x) for k, x in zip(keys, v)}
 

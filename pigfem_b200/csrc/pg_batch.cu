@@ -14,6 +14,8 @@
 // the fastest: stencil nodes per block (64 / 128 / 256), general-row lanes per node (2D: 4 / 8 / 16,
 // 3D: 8 / 16 / 32) and the persistent grid (2 / 4 / 8 blocks per SM).
 #include "pg_ctx.h"
+#include "pg_tile.cuh"
+#include "pg_general.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -27,6 +29,9 @@ struct BatchItem {
   pgd::GridInfo gi;
   const int4* stencil;
   int n_stencil;
+  const int4* tiles;    // 2D: the context's stencil tiles (pg_tile.cuh)
+  const int4* tnodes;
+  const int4* tsegs;
 };
 
 struct BatchCall {
@@ -66,8 +71,8 @@ __global__ void __launch_bounds__(128) k_batch_coh(const BatchItem* __restrict__
   }
 }
 
-// 2D: one thread per stencil node, chunk = blockDim nodes.  3D: 96 threads per block, a warp per
-// row of 32 nodes (chunk = 32 nodes).
+// One CTA per stencil tile (chunk = one tile): 2D the body of k_rows_tile2 (256 threads), 3D that
+// of k_rows_tile3 (192 threads).
 template <int DIM, typename T>
 __global__ void __launch_bounds__(256) k_batch_stencil(const BatchItem* __restrict__ items, const int4* __restrict__ chunks,
                                                        int n_chunks) {
@@ -76,35 +81,35 @@ __global__ void __launch_bounds__(256) k_batch_stencil(const BatchItem* __restri
     const int4 ch = chunks[c];
     const BatchItem& it = items[ch.x];
     if (DIM == 2) {
-      // chunks start at multiples of 32 of the padded list, so every warp has one class
-      if ((int)(threadIdx.x & ~31u) >= ch.z) continue;
-      const bool in = (int)threadIdx.x < ch.z;
-      const int4 v = in ? __ldg(&it.stencil[ch.y + threadIdx.x]) : make_int4(-1, 0, 0, 0);
-      const int cls = __shfl_sync(0xffffffffu, v.w, 0);
-      if (cls == 0) pgd::stencil_rows_staged<pgd::Tri3Stencil0, T>(it.P, it.gi, v, v.x >= 0, stage);
-      else pgd::stencil_rows_staged<pgd::Tri3Stencil1, T>(it.P, it.gi, v, v.x >= 0, stage);
+      pgd::stencil_tile2<T, true>(it.P, it.gi, __ldg(&it.tiles[ch.y]), it.tnodes + (size_t)ch.y * pgd::kTileOwn,
+                                  it.tsegs, stage);
+      __syncthreads();
     } else {
-      const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-      if (lane >= ch.z || w > 2) continue;
-      const int4 v = __ldg(&it.stencil[ch.y + lane]);
-      if (v.x < 0) continue;
-      if (w == 0) pgd::stencil_rows<pgd::Tet4Stencil0, 3, T, 0>(it.P, it.gi, v.x, v.y, v.z);
-      else if (w == 1) pgd::stencil_rows<pgd::Tet4Stencil0, 3, T, 1>(it.P, it.gi, v.x, v.y, v.z);
-      else pgd::stencil_rows<pgd::Tet4Stencil0, 3, T, 2>(it.P, it.gi, v.x, v.y, v.z);
+      pgd::stencil_tile3<T, true>(it.P, it.gi, __ldg(&it.tiles[2 * ch.y]), __ldg(&it.tiles[2 * ch.y + 1]),
+                                  it.tnodes + (size_t)ch.y * pgd::kT3Nodes, it.tsegs, stage);
+      __syncthreads();
     }
   }
 }
 
-template <int DIM, int G>
-__global__ void __launch_bounds__(128) k_batch_general(const BatchItem* __restrict__ items, const int4* __restrict__ chunks,
-                                                       int n_chunks, int slab_slots, int max_mn) {
-  extern __shared__ double smem[];
-  const int grp = threadIdx.x / G;
-  double* slab = smem + (size_t)grp * pgd::general_slab_doubles(slab_slots, DIM, max_mn);
+// The block-parallel general rows (pg_general.cuh) of every context: chunk = {context, first
+// item, count <= 128, pass} with pass 0 records, 1 blocks, 2 residuals; the passes are three
+// launches in that order.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_batch_gen(const BatchItem* __restrict__ items, const int4* __restrict__ chunks,
+                                                  int n_chunks) {
   for (int c = blockIdx.x; c < n_chunks; c += gridDim.x) {
     const int4 ch = chunks[c];
-    pgd::general_rows<DIM, G>(items[ch.x].P, ch.y + grp, grp < ch.z, slab);
-    __syncthreads();
+    const pgd::DevProblem& P = items[ch.x].P;
+    if (ch.w == 2) {   // residuals: a group of kGenResidLanes lanes per node, 128 / lanes nodes per chunk
+      const int grp = threadIdx.x / pgd::kGenResidLanes;
+      if (P.flags & pgd::FLAG_FUNC) pgd::gen_resid<DIM, pgd::kGenResidLanes>(P, ch.y + grp, grp < ch.z);
+      continue;
+    }
+    if ((int)threadIdx.x >= ch.z) continue;
+    const int k = ch.y + threadIdx.x;
+    if (ch.w == 0) pgd::gen_record<DIM>(P, k);
+    else if (P.flags & pgd::FLAG_JAC) pgd::gen_block<DIM>(P, k);
   }
 }
 
@@ -116,12 +121,11 @@ struct pg_batch {
   BatchItem* d_items = nullptr;
   BatchCall* d_call = nullptr;
   BatchCall* h_call = nullptr;
-  int4 *d_coh = nullptr, *d_sten = nullptr, *d_gen = nullptr;
+  int4 *d_coh = nullptr, *d_sten = nullptr, *d_gen[3] = {nullptr, nullptr, nullptr};
   int* d_err = nullptr;   // OR of the contexts' device error words of the last call
-  int n_coh = 0, n_sten = 0, n_gen = 0;
-  int slab_slots = 1;
+  int n_coh = 0, n_sten = 0, n_gen[3] = {0, 0, 0};   // general rows: records, blocks, residuals
   int max_mn = 1;
-  int tpb = 128, G = 4, mult = 4;   // launch shape (autotuned)
+  int mult = 4;   // launch shape (autotuned): persistent blocks per SM
   cudaStream_t stream = nullptr, side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr, t0 = nullptr, t1 = nullptr;
   cudaGraphExec_t exec[2] = {nullptr, nullptr};   // FP64, FP32-mixed
@@ -140,8 +144,8 @@ int berr(pg_batch* b, int code, const std::string& m) {
 void free_chunks(pg_batch* b) {
   if (b->d_coh) cudaFree(b->d_coh);
   if (b->d_sten) cudaFree(b->d_sten);
-  if (b->d_gen) cudaFree(b->d_gen);
-  b->d_coh = b->d_sten = b->d_gen = nullptr;
+  for (int k = 0; k < 3; ++k) { if (b->d_gen[k]) cudaFree(b->d_gen[k]); b->d_gen[k] = nullptr; }
+  b->d_coh = b->d_sten = nullptr;
 }
 
 void drop_graphs(pg_batch* b) {
@@ -159,56 +163,41 @@ int upload_vec(pg_batch* b, const std::vector<T>& h, T** d) {
   return 0;
 }
 
-template <int DIM, int G>
-size_t general_smem(const pg_batch* b) {
-  return (size_t)(128 / G) * pgd::general_slab_doubles(b->slab_slots, DIM, b->max_mn) * sizeof(double);
-}
-
-template <int DIM, int G>
-void general_attr(const pg_batch* b) {
-  cudaFuncSetAttribute(k_batch_general<DIM, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)general_smem<DIM, G>(b));
-}
-
 // set before any capture: the dynamic shared memory of the kernels of the current shape
 void set_attributes(const pg_batch* b) {
-  cudaFuncSetAttribute(k_batch_stencil<2, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pgd::stencil_stage_bytes(256));
-  cudaFuncSetAttribute(k_batch_stencil<2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pgd::stencil_stage_bytes(256));
-  if (b->dim == 2) { if (b->G == 4) general_attr<2, 4>(b); else if (b->G == 8) general_attr<2, 8>(b); else general_attr<2, 16>(b); }
-  else { if (b->G == 8) general_attr<3, 8>(b); else if (b->G == 16) general_attr<3, 16>(b); else general_attr<3, 32>(b); }
+  cudaFuncSetAttribute(k_batch_stencil<2, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pgd::tile2_smem_bytes());
+  cudaFuncSetAttribute(k_batch_stencil<2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pgd::tile2_smem_bytes());
+  cudaFuncSetAttribute(k_batch_stencil<3, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pgd::tile3_smem_bytes());
+  cudaFuncSetAttribute(k_batch_stencil<3, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pgd::tile3_smem_bytes());
 }
 
 // Chunk lists for the current launch shape.
 int build_chunks(pg_batch* b) {
   free_chunks(b);
   drop_graphs(b);
-  std::vector<int4> coh, sten, gen;
-  const int sten_chunk = (b->dim == 2) ? b->tpb : 32;
-  const int gen_chunk = 128 / b->G;
+  std::vector<int4> coh, sten, gen[3];
+
   for (int i = 0; i < (int)b->ctx.size(); ++i) {
     const pg_ctx* c = b->ctx[i];
     const int coh_chunk = 128 / ((b->dim == 2) ? pgd::CohLanes<2>::CQ : pgd::CohLanes<3>::CQ);
     for (int f = 0; f < c->P.n_coh_el; f += coh_chunk)
       coh.push_back(make_int4(i, f, std::min(coh_chunk, c->P.n_coh_el - f), 0));
-    for (int f = 0; f < c->n_stencil; f += sten_chunk)
-      sten.push_back(make_int4(i, f, std::min(sten_chunk, c->n_stencil - f), 0));
-    for (int f = 0; f < c->P.n_slow_dn; f += gen_chunk)
-      gen.push_back(make_int4(i, f, std::min(gen_chunk, c->P.n_slow_dn - f), 0));
+    for (int tl = 0; tl < c->n_tiles; ++tl) sten.push_back(make_int4(i, tl, 1, 0));
+    const int ng[3] = {c->P.n_grec, c->P.n_gblk, c->P.n_slow_dn};
+    for (int pass = 0; pass < 3; ++pass)
+      for (int f = 0, per = (pass == 2) ? 128 / pgd::kGenResidLanes : 128; f < ng[pass]; f += per)
+        gen[pass].push_back(make_int4(i, f, std::min(per, ng[pass] - f), pass));
   }
   b->n_coh = (int)coh.size();
   b->n_sten = (int)sten.size();
-  b->n_gen = (int)gen.size();
+  for (int k = 0; k < 3; ++k) b->n_gen[k] = (int)gen[k].size();
   int rc = upload_vec(b, coh, &b->d_coh);
   rc = rc ? rc : upload_vec(b, sten, &b->d_sten);
-  rc = rc ? rc : upload_vec(b, gen, &b->d_gen);
+  for (int k = 0; k < 3; ++k) rc = rc ? rc : upload_vec(b, gen[k], &b->d_gen[k]);
   if (!rc) set_attributes(b);
   return rc;
 }
 
-template <int DIM, int G>
-void launch_general(pg_batch* b, cudaStream_t st, int grid) {
-  k_batch_general<DIM, G><<<grid, 128, general_smem<DIM, G>(b), st>>>(b->d_items, b->d_gen, b->n_gen, b->slab_slots,
-                                                                     b->max_mn);
-}
 
 void enqueue(pg_batch* b, bool fp32) {
   const int nb = (int)b->ctx.size();
@@ -227,25 +216,20 @@ void enqueue(pg_batch* b, bool fp32) {
   if (b->n_sten) {
     const int grid = std::min(b->n_sten, cap);
     if (b->dim == 2) {
-      const size_t smem = pgd::stencil_stage_bytes(b->tpb);
-      if (fp32) k_batch_stencil<2, float><<<grid, b->tpb, smem, b->side>>>(b->d_items, b->d_sten, b->n_sten);
-      else k_batch_stencil<2, double><<<grid, b->tpb, smem, b->side>>>(b->d_items, b->d_sten, b->n_sten);
+      const size_t smem = pgd::tile2_smem_bytes();
+      if (fp32) k_batch_stencil<2, float><<<grid, pgd::kTileThreads, smem, b->side>>>(b->d_items, b->d_sten, b->n_sten);
+      else k_batch_stencil<2, double><<<grid, pgd::kTileThreads, smem, b->side>>>(b->d_items, b->d_sten, b->n_sten);
     } else {
-      if (fp32) k_batch_stencil<3, float><<<grid, 96, 0, b->side>>>(b->d_items, b->d_sten, b->n_sten);
-      else k_batch_stencil<3, double><<<grid, 96, 0, b->side>>>(b->d_items, b->d_sten, b->n_sten);
+      const size_t smem = pgd::tile3_smem_bytes();
+      if (fp32) k_batch_stencil<3, float><<<grid, pgd::kT3Threads, smem, b->side>>>(b->d_items, b->d_sten, b->n_sten);
+      else k_batch_stencil<3, double><<<grid, pgd::kT3Threads, smem, b->side>>>(b->d_items, b->d_sten, b->n_sten);
     }
   }
-  if (b->n_gen) {
-    const int grid = std::min(b->n_gen, cap);
-    if (b->dim == 2) {
-      if (b->G == 4) launch_general<2, 4>(b, st, grid);
-      else if (b->G == 8) launch_general<2, 8>(b, st, grid);
-      else launch_general<2, 16>(b, st, grid);
-    } else {
-      if (b->G == 8) launch_general<3, 8>(b, st, grid);
-      else if (b->G == 16) launch_general<3, 16>(b, st, grid);
-      else launch_general<3, 32>(b, st, grid);
-    }
+  for (int pass = 0; pass < 3; ++pass) {
+    if (!b->n_gen[pass]) continue;
+    const int grid = std::min(b->n_gen[pass], cap);
+    if (b->dim == 2) k_batch_gen<2><<<grid, 128, 0, st>>>(b->d_items, b->d_gen[pass], b->n_gen[pass]);
+    else k_batch_gen<3><<<grid, 128, 0, st>>>(b->d_items, b->d_gen[pass], b->n_gen[pass]);
   }
   cudaEventRecord(b->join, b->side);
   cudaStreamWaitEvent(st, b->join, 0);
@@ -293,12 +277,15 @@ int pg_batch_create(pg_ctx* const* ctxs, int n, pg_batch** out) {
     pg_ctx* c = ctxs[i];
     if (!c || !c->P.X) return berr(b, PG_ERR_INPUT, "every context must be uploaded (pg_create or pg_upload)");
     if (c->s.dim != b->dim) return berr(b, PG_ERR_INPUT, "a batch holds contexts of one dimension");
+    if (c->s.etype == pg::QUAD4) return berr(b, PG_ERR_UNSUPPORTED, "batches take tri3 / tet4 contexts");
     b->ctx.push_back(c);
     items[i].P = c->P;
     items[i].gi = c->grid;
     items[i].stencil = c->stencil;
     items[i].n_stencil = c->n_stencil;
-    b->slab_slots = std::max(b->slab_slots, c->P.maxnb_general);
+    items[i].tiles = c->tiles;
+    items[i].tnodes = c->tnodes;
+    items[i].tsegs = c->tsegs;
     b->max_mn = std::max(b->max_mn, c->P.max_mn);
     b->n_elem += c->s.ne;
   }
@@ -315,7 +302,6 @@ int pg_batch_create(pg_ctx* const* ctxs, int n, pg_batch** out) {
   cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming);
   cudaEventCreate(&b->t0);
   cudaEventCreate(&b->t1);
-  b->G = (b->dim == 2) ? 4 : 32;
   return build_chunks(b);
 }
 
@@ -351,29 +337,23 @@ int pg_batch_wait(pg_batch* b, float* ms) {
 
 int pg_batch_tune(pg_batch* b, const double* const* d_U, int flags, int reps, int* best) {
   if (!b || !d_U || reps < 1) return PG_ERR_INPUT;
-  const int tpbs[3] = {64, 128, 256};
-  const int gs2[3] = {4, 8, 16}, gs3[3] = {8, 16, 32};   // at least one lane per element node
-  const int mults[3] = {2, 4, 8};
+  const int mults[4] = {2, 4, 8, 16};
   float best_ms = 1e30f;
-  int bt = b->tpb, bg = b->G, bm = b->mult;
-  for (int ti = 0; ti < (b->dim == 2 ? 3 : 1); ++ti)
-    for (int gi = 0; gi < 3; ++gi)
-      for (int mi = 0; mi < 3; ++mi) {
-        b->tpb = tpbs[ti];
-        b->G = (b->dim == 2) ? gs2[gi] : gs3[gi];
-        b->mult = mults[mi];
-        if (int rc = build_chunks(b)) return rc;
-        float total = 0.0f;
-        for (int r = 0; r < reps + 2; ++r) {
-          if (int rc = pg_batch_assemble(b, d_U, nullptr, flags)) return rc;
-          float ms = 0.0f;
-          if (int rc = pg_batch_wait(b, &ms)) return rc;
-          if (r >= 2) total += ms;
-        }
-        if (total < best_ms) { best_ms = total; bt = b->tpb; bg = b->G; bm = b->mult; }
-      }
-  b->tpb = bt; b->G = bg; b->mult = bm;
-  if (best) { best[0] = bt; best[1] = bg; best[2] = bm; }
+  int bm = b->mult;
+  for (int mi = 0; mi < 4; ++mi) {
+    b->mult = mults[mi];
+    if (int rc = build_chunks(b)) return rc;
+    float total = 0.0f;
+    for (int r = 0; r < reps + 2; ++r) {
+      if (int rc = pg_batch_assemble(b, d_U, nullptr, flags)) return rc;
+      float ms = 0.0f;
+      if (int rc = pg_batch_wait(b, &ms)) return rc;
+      if (r >= 2) total += ms;
+    }
+    if (total < best_ms) { best_ms = total; bm = b->mult; }
+  }
+  b->mult = bm;
+  if (best) { best[0] = (b->dim == 2) ? pgd::kTileThreads : pgd::kT3Threads; best[1] = 1; best[2] = bm; }
   return build_chunks(b);
 }
 
@@ -381,8 +361,8 @@ int pg_batch_info(const pg_batch* b, int64_t* info) {
   if (!b || !info) return PG_ERR_INPUT;
   info[0] = (int64_t)b->ctx.size();
   info[1] = b->n_elem;
-  info[2] = b->tpb; info[3] = b->G; info[4] = b->mult;
-  info[5] = b->n_coh; info[6] = b->n_sten; info[7] = b->n_gen;
+  info[2] = (b->dim == 2) ? pgd::kTileThreads : pgd::kT3Threads; info[3] = 1; info[4] = b->mult;
+  info[5] = b->n_coh; info[6] = b->n_sten; info[7] = b->n_gen[0] + b->n_gen[1] + b->n_gen[2];
   return 0;
 }
 

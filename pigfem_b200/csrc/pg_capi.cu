@@ -6,6 +6,7 @@
 // host arrays; pointers are never retained across calls.
 #include "pg_ctx.h"
 #include "pg_launch.cuh"
+#include "pg_tile.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -24,7 +25,7 @@ int upload(pg_ctx* c, const std::vector<T>& h, const T** out) {
   if (int rc = pg_alloc_stream(c)) return rc;
   void* p = nullptr;
   if (cudaMallocAsync(&p, h.size() * sizeof(T), c->up) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "device allocation failed");
-  c->allocs.push_back(p);
+  pg_track_alloc(c, p, h.size() * sizeof(T));
   // pageable source: the call returns once the data is staged, so `h` may go away afterwards
   if (cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, c->up) != cudaSuccess)
     return set_err(c, PG_ERR_DEVICE, "host-to-device copy failed");
@@ -125,7 +126,8 @@ int pg_create_host(const pg_problem_desc* d, pg_ctx** out) {
   pd.plane_strain = d->plane_strain; pd.subscale = d->subscale;
   for (int i = 0; i < 6; ++i) pd.eps_macro[i] = d->eps_macro[i];
   pd.app_strain = d->app_strain;
-  if (d->elem_type == PG_QUAD4) { c->err = "quad4 background elements are not on the device path"; *out = c; return PG_ERR_UNSUPPORTED; }
+  pd.ply_frac = d->ply_frac;
+  for (int i = 0; i < 5; ++i) pd.ply[i] = d->ply[i];
   int rc = pg::build_setup(pd, c->s);
   if (rc) { c->err = c->s.error; *out = c; return rc == 2 ? PG_ERR_INPUT : (rc == 4 ? PG_ERR_UNSUPPORTED : (rc == 7 ? PG_ERR_JACOBIAN : PG_ERR_GEOMETRY)); }
   c->n_coh_qp = (int)c->s.cqp_wgt.size();
@@ -246,6 +248,110 @@ int pg_upload(pg_ctx* c) {
       stencil.insert(stencil.end(), v.begin(), v.end());
       while (stencil.size() % 32) stencil.push_back(make_int4(-1, 0, 0, cls));
     }
+    // 2D tiles of 16 x 8 grid nodes (pg_tile.cuh): per tile 64 class-0 then 64 class-1 node
+    // entries in row-major order, each with its run's offset in the tile's stage (a tile row of
+    // nodes is 8 runs of 36 and 8 of 20 values), and the contiguous CSR segments of each tile row
+    if (dim == 2 && grid_ok) {
+      std::vector<int4> st_of(s.n_std, make_int4(-1, 0, 0, 0));
+      for (int cls = 0; cls < 2; ++cls)
+        for (const int4& v : by_class[cls]) st_of[v.x] = v;
+      const int runlen[2] = {2 * pgd::Tri3Stencil0::NN * 2, 2 * pgd::Tri3Stencil1::NN * 2};
+      std::vector<int4> tiles, tnodes, segs;
+      for (int j0 = 0; j0 <= Ny; j0 += pgd::kTileY)
+        for (int i0 = 0; i0 <= Nx; i0 += pgd::kTileX) {
+          std::vector<int4> ent[2];
+          std::vector<int4> tsg;
+          bool any = false;
+          for (int r = 0; r < pgd::kTileY; ++r) {
+            int off = r * pgd::kTileRowStage;
+            int4 seg = make_int4(-1, 0, 0, 0);
+            int seg_next = -1;   // CSR slot that continues the open segment
+            for (int cc = 0; cc < pgd::kTileX; ++cc) {
+              const int i = i0 + cc, j = j0 + r;
+              const int cls = (i + j) % 2;
+              int4 e = make_int4(-1, 0, 0, 0);
+              if (i <= Nx && j <= Ny && st_of[j * sx + i].x >= 0) {
+                const int4 v = st_of[j * sx + i];
+                e = make_int4(v.x, v.y, v.z, off);
+                any = true;
+                if (seg.x >= 0 && v.z == seg_next) {
+                  seg.z += runlen[cls];
+                } else {
+                  if (seg.x >= 0) tsg.push_back(seg);
+                  seg = make_int4(off, v.z, runlen[cls], 0);
+                }
+                seg_next = v.z + runlen[cls];
+              } else if (seg.x >= 0) {
+                tsg.push_back(seg);
+                seg = make_int4(-1, 0, 0, 0);
+              }
+              ent[cls].push_back(e);
+              off += runlen[cls];
+            }
+            if (seg.x >= 0) tsg.push_back(seg);
+          }
+          if (!any) continue;
+          if (ent[0].size() != 64 || ent[1].size() != 64) return set_err(c, PG_ERR_STATE, "internal: tile classes");
+          tiles.push_back(make_int4(i0, j0, (int)segs.size(), (int)tsg.size()));
+          tnodes.insert(tnodes.end(), ent[0].begin(), ent[0].end());
+          tnodes.insert(tnodes.end(), ent[1].begin(), ent[1].end());
+          segs.insert(segs.end(), tsg.begin(), tsg.end());
+        }
+      PG_TRY(upload(c, tiles, &c->tiles));
+      PG_TRY(upload(c, tnodes, &c->tnodes));
+      PG_TRY(upload(c, segs, &c->tsegs));
+      c->n_tiles = (int)tiles.size();
+    }
+    // 3D tiles of 4 x 4 x 4 grid nodes (pg_tile.cuh): per tile {i0, j0, k0, 0} and {first
+    // segment, segments, 0, 0}; 64 node entries (x fastest) with their run's stage offset (a
+    // node's three rows are one run of 135 values); the contiguous CSR segments of each x-row
+    if (dim == 3 && grid_ok) {
+      std::vector<int4> st_of(s.n_std, make_int4(-1, 0, 0, 0));
+      for (const int4& v : by_class[0]) st_of[v.x] = v;
+      constexpr int T3 = pgd::kT3, RUN = pgd::kT3Run;
+      std::vector<int4> tiles, tnodes, segs;
+      for (int k0 = 0; k0 <= Nz; k0 += T3)
+        for (int j0 = 0; j0 <= Ny; j0 += T3)
+          for (int i0 = 0; i0 <= Nx; i0 += T3) {
+            std::vector<int4> ent, tsg;
+            bool any = false;
+            for (int lk = 0; lk < T3; ++lk)
+              for (int lj = 0; lj < T3; ++lj) {
+                int4 seg = make_int4(-1, 0, 0, 0);
+                int seg_next = -1;
+                for (int li = 0; li < T3; ++li) {
+                  const int i = i0 + li, j = j0 + lj, k = k0 + lk;
+                  const int off = ((lk * T3 + lj) * T3 + li) * RUN;
+                  int4 e = make_int4(-1, 0, 0, 0);
+                  if (i <= Nx && j <= Ny && k <= Nz && st_of[k * sxy + j * sx + i].x >= 0) {
+                    const int4 v = st_of[k * sxy + j * sx + i];
+                    e = make_int4(v.x, v.y, v.z, off);
+                    any = true;
+                    if (seg.x >= 0 && v.z == seg_next) seg.z += RUN;
+                    else {
+                      if (seg.x >= 0) tsg.push_back(seg);
+                      seg = make_int4(off, v.z, RUN, 0);
+                    }
+                    seg_next = v.z + RUN;
+                  } else if (seg.x >= 0) {
+                    tsg.push_back(seg);
+                    seg = make_int4(-1, 0, 0, 0);
+                  }
+                  ent.push_back(e);
+                }
+                if (seg.x >= 0) tsg.push_back(seg);
+              }
+            if (!any) continue;
+            tiles.push_back(make_int4(i0, j0, k0, 0));
+            tiles.push_back(make_int4((int)segs.size(), (int)tsg.size(), 0, 0));
+            tnodes.insert(tnodes.end(), ent.begin(), ent.end());
+            segs.insert(segs.end(), tsg.begin(), tsg.end());
+          }
+      PG_TRY(upload(c, tiles, &c->tiles));
+      PG_TRY(upload(c, tnodes, &c->tnodes));
+      PG_TRY(upload(c, segs, &c->tsegs));
+      c->n_tiles = (int)tiles.size() / 2;
+    }
     std::vector<int> rest;
     maxnb_general = 1;
     for (int a = 0; a < s.n_dn; ++a)
@@ -318,8 +424,8 @@ int pg_upload(pg_ctx* c) {
         aresd.push_back(make_int4(cc, s.cut_node_off[cc], cpa, 0));
       }
     }
-    // k_rows_general's 3D paired path takes the entry after an uncut one as uncut too: every
-    // node's entries must be cut-first
+    // k_rows_general walks a node's cut entries until the first uncut one: every node's entries
+    // must be cut-first
     for (size_t k = (size_t)gdesc.back().x + 1; k < adesc.size(); ++k)
       if ((adesc[k].y >> 8) != 0 && (adesc[k - 1].y >> 8) == 0)
         return set_err(c, PG_ERR_STATE, "internal: a cut entry after an uncut one in a general row");
@@ -330,14 +436,14 @@ int pg_upload(pg_ctx* c) {
   P.dim = dim; P.npe = s.npe; P.nvoigt = s.nvoigt;
   P.n_nodes = n_nodes; P.ne = s.ne; P.ncut = s.ncut; P.n_dn = s.n_dn;
   P.n_free = s.n_free; P.n_const = s.n_const; P.subscale = s.desc.subscale;
-  for (int m = 0; m < 2; ++m) for (int i = 0; i < 36; ++i) { P.D[m][i] = s.D[m][i]; P.Df[m][i] = (float)s.D[m][i]; }
+  for (int m = 0; m < 3; ++m) for (int i = 0; i < 36; ++i) { P.D[m][i] = s.D[m][i]; P.Df[m][i] = (float)s.D[m][i]; }
   P.coh.law = s.coh.law; P.coh.nvar = s.coh.nvar; P.coh.sigma_c = s.coh.sigma_c; P.coh.delta_c1 = s.coh.delta_c1;
   P.coh.delta_c2 = s.coh.delta_c2; P.coh.delta_cn = s.coh.delta_cn; P.coh.delta_ct = s.coh.delta_ct; P.coh.q = s.coh.q;
   P.coh.delta_c = s.coh.delta_c; P.coh.beta2 = s.coh.beta2; P.coh.alpha = s.coh.alpha; P.coh.delta_c3 = s.coh.delta_c3;
   {
-    std::vector<double> Dh(72);
-    std::vector<float> Dfh(72);
-    for (int m = 0; m < 2; ++m) for (int i = 0; i < 36; ++i) { Dh[m * 36 + i] = s.D[m][i]; Dfh[m * 36 + i] = (float)s.D[m][i]; }
+    std::vector<double> Dh(108);
+    std::vector<float> Dfh(108);
+    for (int m = 0; m < 3; ++m) for (int i = 0; i < 36; ++i) { Dh[m * 36 + i] = s.D[m][i]; Dfh[m * 36 + i] = (float)s.D[m][i]; }
     PG_TRY(upload(c, Dh, &P.Dd));
     PG_TRY(upload(c, Dfh, &P.Dfd));
   }
@@ -468,6 +574,7 @@ int pg_upload(pg_ctx* c) {
   PG_TRY(upload(c, aresd, &P.aresd));
   // cohesive elements: owning cut element, scratch offsets of their blocks, and the cohesive
   // position of every cut-element local node (a node is on at most one cohesive element)
+  std::vector<int> kc_off_h, cohpos_h;
   {
     const int n_ce = (int)s.coh_nh.size();
     if ((long long)n_ce * 32 > 2147483647LL) return set_err(c, PG_ERR_UNSUPPORTED, "too many cohesive elements");
@@ -486,8 +593,18 @@ int pg_upload(pg_ctx* c) {
         }
       }
     PG_TRY(upload(c, ce_cut, &P.ce_cut));
+    {
+      // node ids of the cohesive elements' local nodes, laid out like coh_local
+      std::vector<int> gnode(s.coh_local.size());
+      for (int ce = 0; ce < n_ce; ++ce)
+        for (int k = s.coh_local_off[ce]; k < s.coh_local_off[ce + 1]; ++k)
+          gnode[k] = s.cut_nodes[s.cut_node_off[ce_cut[ce]] + s.coh_local[k]];
+      PG_TRY(upload(c, gnode, &P.coh_gnode));
+    }
     PG_TRY(upload(c, kc_off, &P.kc_off));
     PG_TRY(upload(c, cohpos, &P.cohpos));
+    kc_off_h = kc_off;
+    cohpos_h = cohpos;
     double* dk;
     PG_TRY(dalloc(c, (size_t)kc_off[n_ce], &dk));
     P.kcoh = dk;
@@ -506,8 +623,14 @@ int pg_upload(pg_ctx* c) {
     }
     PG_TRY(upload(c, pre, &P.nbr_pre));
   }
-  if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess)
-    return set_err(c, PG_ERR_DEVICE, "stream creation failed");
+  // side: the structured tiles at the lowest priority; side2: the general chain at the highest
+  {
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, least) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&c->side2, cudaStreamNonBlocking, greatest) != cudaSuccess)
+      return set_err(c, PG_ERR_DEVICE, "stream creation failed");
+  }
   for (int b = 0; b < 4; ++b) {
     PG_TRY(upload(c, s.rp[b], &P.rp[b]));
     PG_TRY(dalloc(c, s.ci[b].size(), &P.val[b]));
@@ -545,6 +668,79 @@ int pg_upload(pg_ctx* c) {
     PG_TRY(dalloc(c, (size_t)n_stat * dim * nv, &dsg));
     P.stat = dst;
     P.stat_g = dsg;
+    // Block-parallel general rows (pg_general.cuh; tri3 / tet4): the records of the uncut
+    // elements adjacent to general nodes, one block per (general node, neighbour slot) with its
+    // static index and its cohesive and uncut contributions in adjacency order, and per node the
+    // residual lists
+    if (s.etype != pg::QUAD4) {
+      const int D2 = dim * dim;
+      std::vector<int> rec_of(s.ne, -1);
+      std::vector<int4> grec_nodes;
+      std::vector<int> grec_mat;
+      std::vector<int4> gblk;
+      std::vector<int> gblk_cl(1, 0), gcl, gul, tl_off(1, 0), tl, ul_off(1, 0), ulist;
+      std::vector<std::vector<int>> bcl, bul;
+      for (size_t i = 0; i < slow.size(); ++i) {
+        const int4 gd = gdesc[i];
+        bcl.assign(gd.w, std::vector<int>());
+        bul.assign(gd.w, std::vector<int>());
+        for (int k = gd.x; k < gd.x + gd.y; ++k) {
+          const int4 ad = adesc[k], ax = aresd[k];
+          const int la = ad.y & 255, mn = ad.y >> 8;
+          if (mn > 0) {
+            const int cpa = ax.z;
+            if (cpa < 0) continue;
+            const int ce = cpa >> 5, n1 = cpa & 31, nh = s.coh_nh[ce];
+            for (int b = 0; b < mn; ++b) {
+              const int cpb = cohpos_h[ax.y + b];
+              if (cpb < 0 || (cpb >> 5) != ce) continue;
+              const int n2 = cpb & 31;
+              const int off = kc_off_h[ce] + ((n1 % nh) * nh + (n2 % nh)) * D2;
+              const int neg = ((n1 >= nh) == (n2 >= nh)) ? 0 : 1;
+              bcl[slots[ad.z + b]].push_back(off * 2 + neg);
+            }
+            const int toff = kc_off_h[ce] + nh * nh * D2 + (n1 % nh) * dim;
+            tl.push_back(toff * 2 + ((n1 >= nh) ? 0 : 1));
+          } else {
+            const int e = ad.x;
+            if (rec_of[e] < 0) {
+              rec_of[e] = (int)grec_nodes.size();
+              grec_nodes.push_back(ax);
+              grec_mat.push_back(ad.w);
+            }
+            const int r = rec_of[e];
+            if (r >= (1 << 26)) return set_err(c, PG_ERR_UNSUPPORTED, "too many general-row elements");
+            for (int b = 0; b < s.npe; ++b) bul[(ad.z >> (8 * b)) & 255].push_back(r * 16 + la * 4 + b);
+            ulist.push_back(r * 4 + la);
+          }
+        }
+        for (int k = 0; k < gd.w; ++k) {
+          const int stat_idx = (int)i < n_stat ? stat_off[i] + k : -1;
+          gblk.push_back(make_int4((int)i, k, stat_idx, (int)gul.size()));
+          gcl.insert(gcl.end(), bcl[k].begin(), bcl[k].end());
+          gul.insert(gul.end(), bul[k].begin(), bul[k].end());
+          gblk_cl.push_back((int)gcl.size());
+        }
+        tl_off.push_back((int)tl.size());
+        ul_off.push_back((int)ulist.size());
+      }
+      gblk.push_back(make_int4(-1, 0, -1, (int)gul.size()));   // sentinel: the end of the last block's list
+      P.n_grec = (int)grec_nodes.size();
+      P.n_gblk = (int)gblk.size() - 1;
+      PG_TRY(upload(c, grec_nodes, &P.grec_nodes));
+      PG_TRY(upload(c, grec_mat, &P.grec_mat));
+      double* dgr = nullptr;
+      PG_TRY(dalloc(c, (size_t)P.n_grec * (size_t)(dim == 2 ? pgd::gen_fields<2>() : pgd::gen_fields<3>()), &dgr));
+      P.grec = dgr;
+      PG_TRY(upload(c, gblk, &P.gblk));
+      PG_TRY(upload(c, gblk_cl, &P.gblk_cl));
+      PG_TRY(upload(c, gcl, &P.gcl));
+      PG_TRY(upload(c, gul, &P.gul));
+      PG_TRY(upload(c, tl_off, &P.gnode_tl_off));
+      PG_TRY(upload(c, tl, &P.gnode_tl));
+      PG_TRY(upload(c, ul_off, &P.gnode_ul_off));
+      PG_TRY(upload(c, ulist, &P.gnode_ul));
+    }
     c->stat_doubles = (long long)stat_off[n_stat] * dim * dim + (long long)n_stat * dim * nv;
     if (s.ncut > 0) {
       double* dg = nullptr;
@@ -557,10 +753,7 @@ int pg_upload(pg_ctx* c) {
       if (cudaStreamSynchronize(c->up) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "cut-element set-up kernel failed");
       if (herr) return set_err(c, PG_ERR_NONFINITE, "non-finite cut-element stiffness at set-up");
       // the per-element blocks are reduced: give their memory back
-      for (double* p : {dke, dg}) {
-        c->allocs.erase(std::remove(c->allocs.begin(), c->allocs.end(), (void*)p), c->allocs.end());
-        cudaFreeAsync(p, c->up);
-      }
+      for (double* p : {dke, dg}) pg_untrack_free(c, p);
       P.ke = nullptr;
       P.gmac = nullptr;
     }
@@ -611,9 +804,9 @@ int pg_set_timing(pg_ctx* c, int on) {
 int pg_kernel_times(pg_ctx* c, float* ms) {
   if (!c || !ms || !c->ev[0]) return set_err(c, PG_ERR_STATE, "nothing was launched");
   if (cudaEventSynchronize(c->ev[5]) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "event wait failed");
-  // [0] cohesive elements, [1] stencil rows (2D: from the start, on the side stream, concurrent
-  // with [0] and [2]; 3D: after [0]), [2] general rows (2D: after [0]; 3D: after [1]), [3] whole
-  // assembly
+  // [0] cohesive elements and element records, [1] stencil rows (2D: from the start, on their
+  // own stream, concurrent with [0] and [2]; 3D: after [0]), [2] general rows (after [0] in 2D,
+  // after [1] in 3D), [3] whole assembly
   const bool seq = c->s.dim == 3;
   cudaEventElapsedTime(&ms[0], c->ev[0], c->ev[3]);
   cudaEventElapsedTime(&ms[1], seq ? c->ev[3] : c->ev[0], c->ev[1]);
@@ -627,18 +820,27 @@ void pg_destroy(pg_ctx* c) {
   // work of this context still in flight finishes before its memory goes back to the pool
   cudaStreamSynchronize(c->stream);
   if (c->side) cudaStreamSynchronize(c->side);
+  if (c->side2) cudaStreamSynchronize(c->side2);
   if (c->pcg.stream) cudaStreamSynchronize(c->pcg.stream);
   if (c->pcg.stream) cudaStreamDestroy(c->pcg.stream);
   if (c->pcg.ev) cudaEventDestroy(c->pcg.ev);
   if (c->pcg.hflag) cudaFreeHost(c->pcg.hflag);
   for (int i = 0; i < 6; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
   if (c->side) cudaStreamDestroy(c->side);
+  if (c->side2) cudaStreamDestroy(c->side2);
   for (void* p : c->allocs) cudaFreeAsync(p, c->up);
   if (c->up) cudaStreamDestroy(c->up);   // released once the frees have run
   delete c;
 }
 
 const char* pg_last_error(const pg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int pg_device_bytes(const pg_ctx* c, int64_t* now, int64_t* peak) {
+  if (!c) return PG_ERR_INPUT;
+  if (now) *now = (int64_t)c->dev_bytes;
+  if (peak) *peak = (int64_t)c->dev_bytes_peak;
+  return 0;
+}
 
 int pg_get_sizes(const pg_ctx* c, pg_sizes* o) {
   if (!c || !o) return PG_ERR_INPUT;
@@ -691,6 +893,7 @@ int pg_residual_strains(pg_ctx* c, const double* d_U, double t_frac, int n_cases
   if (!pg_resident(c)) return set_err(c, PG_ERR_STATE, "the context has no device residency (pg_upload it first)");
   if (reinterpret_cast<uintptr_t>(d_U) % 16) return set_err(c, PG_ERR_INPUT, "the displacement array must be 16-byte aligned");
   if (!c->s.desc.subscale) return set_err(c, PG_ERR_INPUT, "macroscale strain cases need a subscale (periodic) problem");
+  if (c->s.etype == pg::QUAD4) return set_err(c, PG_ERR_UNSUPPORTED, "the multi-strain pass takes tri3 / tet4 meshes (quad4: one residual-only assembly per strain)");
   if (c->s.n_const > 0 && !d_Rp) return set_err(c, PG_ERR_INPUT, "d_Rp is required when the problem has constrained DOFs");
   pgd::DevProblem P = c->P;
   P.U = d_U;

@@ -32,6 +32,8 @@ struct pg_ctx {
   std::string err;
   cudaStream_t stream = 0;
   std::vector<void*> allocs;
+  std::vector<size_t> alloc_bytes;   // bytes of allocs[i]
+  size_t dev_bytes = 0, dev_bytes_peak = 0;   // held now / most held at once (pg_device_bytes)
   pgd::DevProblem P{};
   double* d_U = nullptr;
   double* d_isv_committed = nullptr;
@@ -53,9 +55,17 @@ struct pg_ctx {
   int cut_cls_qp[2] = {1, 1}, cut_cls_nodes[2] = {1, 1};
   const int4* stencil = nullptr;
   int n_stencil = 0;
+  // 2D tiles of the stencil rows (pg_tile.cuh): per tile {i0, j0, first segment, segments}, per
+  // tile 128 node entries {node, first DOF, first CSR slot, stage offset}, the store segments
+  const int4* tiles = nullptr;
+  const int4* tnodes = nullptr;
+  const int4* tsegs = nullptr;
+  int n_tiles = 0;
   pgd::GridInfo grid{0, 0, 0};
   bool timing = false;
-  cudaStream_t side = nullptr;
+  cudaStream_t side = nullptr;    // 2D: the structured tiles (lowest stream priority)
+  cudaStream_t side2 = nullptr;   // 2D: cohesive elements, records and general rows (highest priority)
+  // fork, tiles done, (unused), first kernel done, general rows done, join
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   PcgWork pcg;
   double* d_hom = nullptr;  // homogenization partials
@@ -75,6 +85,25 @@ int pg_alloc_stream(pg_ctx* c);
 
 // Shared helpers of the translation units of the library.
 int pg_set_err(pg_ctx* c, int code, const std::string& m);
+// Record a device allocation of the context (freed by pg_destroy, or earlier by pg_untrack_free).
+inline void pg_track_alloc(pg_ctx* c, void* p, size_t bytes) {
+  c->allocs.push_back(p);
+  c->alloc_bytes.push_back(bytes);
+  c->dev_bytes += bytes;
+  if (c->dev_bytes > c->dev_bytes_peak) c->dev_bytes_peak = c->dev_bytes;
+}
+// Free one tracked allocation early (stream-ordered on the allocation stream).
+inline void pg_untrack_free(pg_ctx* c, void* p) {
+  for (size_t i = 0; i < c->allocs.size(); ++i)
+    if (c->allocs[i] == p) {
+      c->dev_bytes -= c->alloc_bytes[i];
+      c->allocs.erase(c->allocs.begin() + i);
+      c->alloc_bytes.erase(c->alloc_bytes.begin() + i);
+      cudaFreeAsync(p, c->up);
+      return;
+    }
+}
+
 // Zero-filled device array of n T on the context's allocation stream; ready for other streams
 // after pg_alloc_sync(c).
 template <typename T>
@@ -84,7 +113,7 @@ int pg_dalloc(pg_ctx* c, size_t n, T** out) {
   if (int rc = pg_alloc_stream(c)) return rc;
   void* p = nullptr;
   if (cudaMallocAsync(&p, n * sizeof(T), c->up) != cudaSuccess) return pg_set_err(c, PG_ERR_DEVICE, "device allocation failed");
-  c->allocs.push_back(p);
+  pg_track_alloc(c, p, n * sizeof(T));
   cudaMemsetAsync(p, 0, n * sizeof(T), c->up);
   *out = (T*)p;
   return 0;

@@ -36,9 +36,9 @@ struct DevProblem {
   int n_nodes, ne, ncut, n_dn;
   int n_free, n_const;
   int subscale;
-  double D[2][36];
-  float Df[2][36];
-  const double* Dd;   // D of the two bulk materials in device memory (2 x 36), read through the L1
+  double D[3][36];    // bulk materials: 0 matrix, 1 fiber, 2 bounding plies
+  float Df[3][36];
+  const double* Dd;   // D of the three bulk materials in device memory (3 x 36), read through the L1
   const float* Dfd;
   CohConst coh;
   // geometry / state
@@ -82,12 +82,25 @@ struct DevProblem {
   const int* tile_elem_off; const int* tile_elems; int tile_max_elems;  // elements each tile of fast nodes touches
   const uint16_t* adj_local;                     // tile-local index of each adjacency entry's element
   const int* slow_dn; int n_slow_dn;             // the remaining DOF nodes
+  // Block-parallel general rows (pg_general.cuh; tri3 / tet4 meshes).  Records: the uncut elements
+  // adjacent to general nodes, formed once per assembly (record r at grec[r * GenRec::STRIDE]:
+  // the NPE x DIM gradients, J W, the NV stresses, the material).  Blocks: one per (general node,
+  // neighbour slot), node-major: {node, slot, static index or -1, first uncut contribution}; its
+  // cohesive contributions [gblk_cl[b], gblk_cl[b + 1]) as (kcoh offset << 1 | negative), its
+  // uncut contributions [gblk[b].w, gblk[b + 1].w) as (record << 4 | la << 2 | lb), both in
+  // adjacency order.  Per general node the residual lists: tractions (kcoh offset << 1 | negative)
+  // and uncut entries (record << 2 | la), in adjacency order.
+  int n_grec, n_gblk;
+  const int4* grec_nodes; const int* grec_mat; double* grec;
+  const int4* gblk; const int* gblk_cl; const int* gcl; const int* gul;
+  const int* gnode_tl_off; const int* gnode_tl; const int* gnode_ul_off; const int* gnode_ul;
   int maxnb_general;                             // slab slots per node in k_rows_general
   const int4* gdesc; const int* growd; const int4* adesc; const int4* aresd;  // k_rows_general descriptors
   // cohesive points
   int n_coh_qp;
   int n_coh_el;                                  // cohesive elements
   const int* ce_cut;                             // cut element of each cohesive element
+  const int* coh_gnode;                          // node id of every cohesive element's local node ('-' then '+', at coh_local_off)
   const int* kc_off;                             // per cohesive element: offset of its blocks in kcoh
   double* kcoh;                                  // per call: cohesive blocks B_ab and tractions t_a
   const int* cohpos;                             // per cut-element local node: (cohesive element << 5 | position) or -1

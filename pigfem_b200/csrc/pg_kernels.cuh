@@ -185,12 +185,17 @@ __device__ __forceinline__ void simplex_block(const DevProblem& P, int4 nodes, i
   }
 }
 
-// Shared-memory doubles of one lane group: slab_slots blocks of DIM x DIM, the node's residual (4
-// doubles reserved) and the per-slot residual partials of the static part (slab_slots x DIM).
-__host__ __device__ inline int general_slab_doubles(int slab_slots, int dim, int max_mn) {
-  (void)max_mn;
+// Shared memory of one lane group of general_rows: slab_slots blocks of DIM x DIM, the node's
+// residual (4 doubles reserved), the per-slot residual partials of the static part
+// (slab_slots x DIM), then one scratch record per lane (general_lane_doubles).
+__host__ __device__ constexpr int general_lane_doubles(int dim, int npe) { return npe * dim * dim + dim + 2; }
+__host__ __device__ inline int general_scratch_offset(int slab_slots, int dim) {
+  return (slab_slots * dim * dim + 4 + slab_slots * dim + 1) & ~1;   // even: 16-byte aligned
+}
+__host__ __device__ inline int general_slab_doubles(int slab_slots, int dim, int lanes, int npe = 0) {
   // even (16-byte aligned groups) and 2 mod 4, so consecutive groups start on different banks
-  int n = (slab_slots * dim * dim + 4 + slab_slots * dim + 1) & ~1;
+  if (npe == 0) npe = dim + 1;
+  int n = (general_scratch_offset(slab_slots, dim) + lanes * general_lane_doubles(dim, npe) + 1) & ~1;
   return (n % 4 == 0) ? n + 2 : n;
 }
 
@@ -205,6 +210,131 @@ __device__ __forceinline__ void slab_add(double* ak, const double* v) {
   } else {
 #pragma unroll
     for (int i = 0; i < DIM * DIM; ++i) ak[i] += v[i];
+  }
+}
+
+// Point qp of the quad4 2 x 2 Gauss rule (src/quad4.cpp:108-127: the edge points -+1/sqrt(3),
+// qp -> (qp % 2, qp / 2), weights 1 x 1) on the bilinear map of the nodes x: the physical
+// gradients g of the four shape functions (Jacobian J(a, i) = sum_k dN_k/dr_a x_k[i], its
+// inverse by the adjugate, Elem::transform_gradients, src/elem.cpp:115-139) and the weight J W.
+__device__ __forceinline__ void quad4_point(const double (*x)[2], int qp, double (*g)[2], double* w) {
+  const double kG = 0.57735026918962576450914878050196;
+  const double r = (qp % 2) ? kG : -kG, s = (qp / 2) ? kG : -kG;
+  const double dN[4][2] = {{-0.25 * (1.0 - s), -0.25 * (1.0 - r)}, {0.25 * (1.0 - s), -0.25 * (1.0 + r)},
+                           {0.25 * (1.0 + s), 0.25 * (1.0 + r)}, {-0.25 * (1.0 + s), 0.25 * (1.0 - r)}};
+  double J[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) J[a][i] += dN[k][a] * x[k][i];
+  const double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+  const double sc = 1.0 / det;
+  const double R[2][2] = {{J[1][1] * sc, (-1.0 * J[0][1]) * sc}, {(-1.0 * J[1][0]) * sc, J[0][0] * sc}};
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int i = 0; i < 2; ++i) g[k][i] = R[i][0] * dN[k][0] + R[i][1] * dN[k][1];
+  *w = det * (1.0 * 1.0);
+}
+
+// Block row la of an uncut element with the given nodes: blk[b] = sum over its points of
+// w (B_la^T D B_b) for every element node b (NPE blocks of DIM x DIM, row-major), and its
+// residual rv = sum w (B_la^T sigma).  Simplices (NPE = DIM + 1) have constant gradients, so
+// their order-3 points are summed into one weight (the products of simplex_block); quad4
+// (DIM = 2, NPE = 4) sums its four Gauss points.  Geometry from the node coordinates, stress
+// from U (+ eps_macro).
+template <int DIM, int NPE = DIM + 1>
+__device__ __forceinline__ void uncut_block_row(const DevProblem& P, int4 nodes, int la, const double* D, double* blk,
+                                                double* rv) {
+  constexpr int NV = (DIM == 2) ? 3 : 6;
+  constexpr int D2 = DIM * DIM;
+  const int nd[4] = {nodes.x, nodes.y, nodes.z, nodes.w};
+  if constexpr (DIM == 2 && NPE == 4) {
+    double x[4][2], u[4][2];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) { load_node<2>(P.X, nd[n], x[n]); load_node<2>(P.U, nd[n], u[n]); }
+    double kb[4][4], r[2] = {0.0, 0.0};
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) kb[b][i] = 0.0;
+#pragma unroll
+    for (int qp = 0; qp < 4; ++qp) {
+      double g[4][2], w;
+      quad4_point(x, qp, g, &w);
+      double ga[2] = {g[0][0], g[0][1]};
+#pragma unroll
+      for (int n = 1; n < 4; ++n)
+        if (la == n) { ga[0] = g[n][0]; ga[1] = g[n][1]; }
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        double part[3];
+        bt_d_row<2, double>(D, ga, q, part);
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+          for (int q2 = 0; q2 < 2; ++q2) kb[b][q * 2 + q2] += w * part_b<2, double>(part, g[b], q2);
+      }
+      double eps[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int n = 0; n < 4; ++n) add_strain<2, double>(g[n], u[n], eps);
+      if (P.subscale) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) eps[v] += P.eps_macro[v];
+      }
+      double sig[3];
+      lei_stress<2, double>(D, eps, sig);
+#pragma unroll
+      for (int q = 0; q < 2; ++q) r[q] += w * bt_sig<2, double>(ga, sig, q);
+    }
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) blk[b * D2 + i] = kb[b][i];
+    rv[0] = r[0];
+    rv[1] = r[1];
+  } else {
+    double x[NPE][DIM], g[NPE][DIM], J;
+#pragma unroll
+    for (int n = 0; n < NPE; ++n) load_node<DIM>(P.X, nd[n], x[n]);
+    simplex_geom<DIM, double>(x, g, &J);
+    const double wgt = J * ((DIM == 2) ? tri4_wsum() : tet5_wsum());
+    double ga[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) ga[d] = g[0][d];
+#pragma unroll
+    for (int n = 1; n < NPE; ++n)
+      if (la == n)
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) ga[d] = g[n][d];
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) {
+      double part[NV];
+      bt_d_row<DIM, double>(D, ga, q, part);
+#pragma unroll
+      for (int b = 0; b < NPE; ++b)
+#pragma unroll
+        for (int q2 = 0; q2 < DIM; ++q2) blk[b * D2 + q * DIM + q2] = wgt * part_b<DIM, double>(part, g[b], q2);
+    }
+    double eps[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) eps[v] = 0.0;
+#pragma unroll
+    for (int n = 0; n < NPE; ++n) {
+      double u[DIM];
+      load_node<DIM>(P.U, nd[n], u);
+      add_strain<DIM, double>(g[n], u, eps);
+    }
+    if (P.subscale) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) eps[v] += P.eps_macro[v];
+    }
+    double sig[NV];
+    lei_stress<DIM, double>(D, eps, sig);
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) rv[q] = wgt * bt_sig<DIM, double>(ga, sig, q);
   }
 }
 
@@ -272,17 +402,19 @@ __device__ __forceinline__ void coh_traction(const DevProblem& P, int cpa, doubl
 }
 
 // Row assembly for the DOF nodes the stencil path does not take (boundary rows, nodes of cut
-// elements, enrichment nodes): one lane group of G threads per DOF node, its rows in a
+// elements, enrichment nodes): one lane group of L threads per DOF node, its rows in a
 // shared-memory slab.  The slab starts from the node's static part (the cut elements' volumetric
 // blocks summed per neighbour slot at set-up; zero for nodes without cut elements) and the
 // residual from the static blocks times the displacements plus the macroscale-strain response.
-// The group then walks the node's adjacent elements in adjacency order: an uncut element is
-// recomputed from the node coordinates, its lanes taking the element's nodes (lane b: block
-// (la, b)) and adding the blocks into the slab -- the blocks of one element go to distinct
-// neighbour slots, so no two lanes write the same entry; a cut element adds, when the row node is
-// on one of its cohesive elements, the cohesive blocks and traction that k_coh_elements left for
-// it.  Every sum runs in a fixed order independent of G.  Finally the group writes every CSR value
-// of the node's rows exactly once.
+// The node's adjacent elements then follow in adjacency order (cut elements first):
+//   * a cut element the row node is on a cohesive element of adds that cohesive element's blocks
+//     and traction (k_coh_elements left them in kcoh), its lanes taking the element's nodes;
+//   * the uncut elements are taken L at a time: lane k recomputes element e0 + k from the node
+//     coordinates and writes its whole block row and residual to its scratch record, then the
+//     lanes add the records into the slab in entry order, each lane owning the slots s = k,
+//     k + L, ... (an element's nodes have distinct slots), and lane 0 adds the residuals.
+// Every sum therefore runs in a fixed order that does not depend on L.  Finally the group writes
+// every CSR value of the node's rows exactly once.
 //   gdesc[node]      int4 {adjacency begin, adjacency count, neighbour begin, neighbour count}
 //   growd[node]      3*DIM ints: global DOF of each row, first slot in the row's F block, in its C block
 //   adesc[entry]     int4 {element, local node | nodes of a cut element << 8, slots (uncut: 8 bits per
@@ -290,116 +422,101 @@ __device__ __forceinline__ void coh_traction(const DevProblem& P, int cpa, doubl
 //   aresd[entry]     int4: uncut {element nodes (-1 padded)}; cut {cut element, its first node in
 //                    cut_nodes, the row node's cohesive place (element << 5 | position) or -1, 0}
 //   nbr_pre[slot]    free DOFs of the node's neighbours before this one (row positions)
-// Every lane of the warp must call it (valid = false for lanes without a node): the entry loop and
-// its warp synchronisations are warp-uniform.  G >= DIM + 1.  (Residual-only assemblies use
+// `valid` is uniform over the group, and the group synchronises only its own lanes.  `slab` is the
+// group's general_slab_doubles(slab_slots, DIM, L) doubles.  (Residual-only assemblies use
 // k_rows_general_resid.)
-template <int DIM, int G>
-__device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool valid, double* slab) {
-  constexpr int NPE = DIM + 1;
+template <int DIM, int L, int NPE = DIM + 1>
+__device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool valid, double* slab, int slab_slots) {
   constexpr int D2 = DIM * DIM;
-  static_assert(G >= NPE, "one lane per element node");
-  const int g = threadIdx.x % G;
-  int4 gd = make_int4(0, 0, 0, 0);
-  if (valid) gd = __ldg(&P.gdesc[node]);
-  const bool stat = valid && node < P.n_stat;
-  double* rs = slab + gd.w * D2;           // residual of the node's rows
-  double* part = rs + 4;                    // per-slot residual partials of the static part
+  constexpr int LD = general_lane_doubles(DIM, NPE);
+  if (!valid) return;
+  const int g = threadIdx.x % L;
+  const unsigned gmask = (L >= 32) ? 0xffffffffu : (((1u << L) - 1u) << ((threadIdx.x & 31) / L * L));
+  const int4 gd = __ldg(&P.gdesc[node]);
+  const int nn = gd.w;
+  const bool stat = node < P.n_stat;
+  double* rs = slab + nn * D2;             // residual of the node's rows
+  double* part = rs + 4;                   // per-slot residual partials of the static part
+  double* scr = slab + general_scratch_offset(slab_slots, DIM);
   if (stat) {
     const int s0 = __ldg(&P.stat_slot_off[node]);
     const double* S = P.stat + (size_t)s0 * D2;
-    for (int i = g; i < gd.w * D2; i += G) slab[i] = __ldg(&S[i]);
-    for (int k = g; k < gd.w; k += G) static_slot_product<DIM>(P, s0, k, part + k * DIM);
-  } else if (valid) {
-    for (int i = g; i < gd.w * D2; i += G) slab[i] = 0.0;
+    for (int i = g; i < nn * D2; i += L) slab[i] = __ldg(&S[i]);
+    for (int k = g; k < nn; k += L) static_slot_product<DIM>(P, s0, k, part + k * DIM);
+  } else {
+    for (int i = g; i < nn * D2; i += L) slab[i] = 0.0;
   }
-  // 3D with G >= 8: two uncut elements per pass -- lanes 0..3 take one, lanes 4..7 the next (the
-  // entries are cut-first, so the one after an uncut entry is uncut too; the set-up checks it);
-  // the second element's blocks go into the slab after the first's and its residual is added
-  // after the first's, so every sum keeps the entry order.
-  constexpr bool PAIRS = (DIM == 3 && G >= 2 * NPE);
-  const int glead = (threadIdx.x & 31) - g;   // the group's first lane within the warp
-  __syncwarp();
-  if (valid && g == 0) {
+  __syncwarp(gmask);
+  if (g == 0) {
     double r[DIM];
-    if (stat) static_resid_sum<DIM>(P, node, gd.w, part, P.eps_macro, r);
+    if (stat) static_resid_sum<DIM>(P, node, nn, part, P.eps_macro, r);
     else
 #pragma unroll
       for (int q = 0; q < DIM; ++q) r[q] = 0.0;
 #pragma unroll
     for (int q = 0; q < DIM; ++q) rs[q] = r[q];
   }
-  // the next entry's descriptors are loaded while the current one is processed
-  int4 ad_next = make_int4(0, 0, 0, 0), ax_next = make_int4(0, 0, 0, 0);
-  if (valid && gd.y > 0) { ad_next = __ldg(&P.adesc[gd.x]); ax_next = __ldg(&P.aresd[gd.x]); }
-  int ei = 0;
-  __syncwarp();
-  while (__any_sync(0xffffffffu, valid && ei < gd.y)) {
-    const bool have = valid && ei < gd.y;
-    const int4 ad = ad_next, ax = ax_next;
-    const int la = ad.y & 255, mn = ad.y >> 8;
-    const bool pair = PAIRS && have && mn == 0 && ei + 1 < gd.y;
-    const int step = pair ? 2 : 1;
-    if (valid && ei + step < gd.y) { ad_next = __ldg(&P.adesc[gd.x + ei + step]); ax_next = __ldg(&P.aresd[gd.x + ei + step]); }
-    if constexpr (PAIRS) {
-      const bool second = pair && g >= NPE && g < 2 * NPE;
-      const bool first = have && mn == 0 && g < NPE;
-      int4 ad2 = ad, ax2 = ax;
-      if (second) { ad2 = __ldg(&P.adesc[gd.x + ei + 1]); ax2 = __ldg(&P.aresd[gd.x + ei + 1]); }
-      double kb[DIM][DIM], rv[DIM];
-#pragma unroll
-      for (int q = 0; q < DIM; ++q) rv[q] = 0.0;
-      const int lb = second ? g - NPE : g;
-      if (first || second)
-        simplex_block<DIM>(P, ax2, ad2.y & 255, lb, P.D[ad2.w], kb, rv, lb == 0);
-      if (first) slab_add<DIM>(slab + ((((unsigned)ad.z) >> (8 * g)) & 255) * D2, &kb[0][0]);
-      __syncwarp();
-      if (second) slab_add<DIM>(slab + ((((unsigned)ad2.z) >> (8 * lb)) & 255) * D2, &kb[0][0]);
-      double rv2[DIM];
-#pragma unroll
-      for (int q = 0; q < DIM; ++q) rv2[q] = __shfl_sync(0xffffffffu, rv[q], glead + NPE);
-      if (have && mn == 0 && g == 0) {
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) rs[q] += rv[q];
-        if (pair)
-#pragma unroll
-          for (int q = 0; q < DIM; ++q) rs[q] += rv2[q];
-      }
-    } else if (have && mn == 0) {
-      if (g < NPE) {
-        double kb[DIM][DIM], rv[DIM];
-        simplex_block<DIM>(P, ax, la, g, P.D[ad.w], kb, rv, g == 0);   // D from the parameter space
-        double* ak = slab + ((((unsigned)ad.z) >> (8 * g)) & 255) * D2;
-        slab_add<DIM>(ak, &kb[0][0]);
-        if (g == 0)
-#pragma unroll
-          for (int q = 0; q < DIM; ++q) rs[q] += rv[q];
-      }
-    }
-    // a cut element: its volumetric part is in the static slab; the cohesive blocks of the
-    // cohesive element the row node is on, if any
+  __syncwarp(gmask);
+  // cut entries (first in the adjacency order): the cohesive element the row node is on
+  int e = 0;
+  for (; e < gd.y; ++e) {
+    const int4 ad = __ldg(&P.adesc[gd.x + e]);
+    const int mn = ad.y >> 8;
+    if (mn == 0) break;
+    const int4 ax = __ldg(&P.aresd[gd.x + e]);
     const int cpa = ax.z;
-    if (have && mn > 0 && cpa >= 0) {
-      const int base = ax.y;
-      for (int b = g; b < mn; b += G) {
-        const int cpb = __ldg(&P.cohpos[base + b]);
-        if (cpb >= 0 && (cpb >> 5) == (cpa >> 5)) {
-          double blk[D2];
-          coh_block_add<DIM>(P, cpa, cpb, blk);
-          slab_add<DIM>(slab + __ldg(&P.adj_slots[ad.z + b]) * D2, blk);
-        }
-      }
-      if (g == 0) {
-        double t[DIM];
-        coh_traction<DIM>(P, cpa, t);
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) rs[q] += t[q];
+    if (cpa < 0) continue;
+    for (int b = g; b < mn; b += L) {
+      const int cpb = __ldg(&P.cohpos[ax.y + b]);
+      if (cpb >= 0 && (cpb >> 5) == (cpa >> 5)) {
+        double blk[D2];
+        coh_block_add<DIM>(P, cpa, cpb, blk);
+        slab_add<DIM>(slab + __ldg(&P.adj_slots[ad.z + b]) * D2, blk);
       }
     }
-    __syncwarp();
-    ei += step;
+    if (g == 0) {
+      double t[DIM];
+      coh_traction<DIM>(P, cpa, t);
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) rs[q] += t[q];
+    }
+    __syncwarp(gmask);
   }
-  if (!valid) return;
-  const int nn = gd.w;
+  // uncut entries, L at a time
+  for (int e0 = e; e0 < gd.y; e0 += L) {
+    double* my = scr + g * LD;
+    unsigned z = 0u;
+    if (e0 + g < gd.y) {
+      const int4 ad = __ldg(&P.adesc[gd.x + e0 + g]);
+      const int4 ax = __ldg(&P.aresd[gd.x + e0 + g]);
+      uncut_block_row<DIM, NPE>(P, ax, ad.y & 255, P.D[ad.w], my, my + NPE * D2);
+      z = (unsigned)ad.z;
+    }
+    reinterpret_cast<unsigned*>(my + NPE * D2 + DIM)[0] = z;
+    __syncwarp(gmask);
+    const int n_here = min(L, gd.y - e0);
+    for (int s = g; s < nn; s += L) {
+      double acc[D2];
+#pragma unroll
+      for (int i = 0; i < D2; ++i) acc[i] = slab[s * D2 + i];
+      for (int j = 0; j < n_here; ++j) {
+        const double* oj = scr + j * LD;
+        const unsigned zj = reinterpret_cast<const unsigned*>(oj + NPE * D2 + DIM)[0];
+#pragma unroll
+        for (int b = 0; b < NPE; ++b)
+          if (((zj >> (8 * b)) & 255u) == (unsigned)s)
+#pragma unroll
+            for (int i = 0; i < D2; ++i) acc[i] += oj[b * D2 + i];
+      }
+#pragma unroll
+      for (int i = 0; i < D2; ++i) slab[s * D2 + i] = acc[i];
+    }
+    if (g == 0)
+      for (int j = 0; j < n_here; ++j)
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) rs[q] += scr[j * LD + NPE * D2 + q];
+    __syncwarp(gmask);
+  }
   const uint8_t* masks = P.dn_nbr_mask + gd.z;
   const int* pre = P.nbr_pre + gd.z;
   const int* rd = P.growd + (size_t)node * 3 * DIM;
@@ -410,7 +527,7 @@ __device__ __forceinline__ void general_rows(const DevProblem& P, int node, bool
     if (P.flags & FLAG_JAC) {
       double* vF = P.val[rf ? 0 : 2] + __ldg(&rd[DIM + q]);
       double* vC = P.val[rf ? 1 : 3] + __ldg(&rd[2 * DIM + q]);
-      for (int k = g; k < nn; k += G) {
+      for (int k = g; k < nn; k += L) {
         int pf = __ldg(&pre[k]);
         int pc = k * DIM - pf;
         const int mk = __ldg(&masks[k]);
@@ -454,9 +571,10 @@ __device__ __forceinline__ void static_resid_group(const DevProblem& P, int node
 // contribution (an uncut element's w B^T sigma; the cohesive traction at the node for a cut
 // element the node is on a cohesive element of) -- the same operations general_rows performs --
 // and the group adds the contributions in entry (adjacency) order with shuffles.  L divides 32.
-template <int DIM, int L>
+template <int DIM, int L, int NPE = DIM + 1>
 __global__ void __launch_bounds__(128) k_rows_general_resid(DevProblem P) {
   constexpr int NV = (DIM == 2) ? 3 : 6;
+  constexpr int D2 = DIM * DIM;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int node = t / L, k = t % L;
   const bool valid = node < P.n_slow_dn;   // uniform over each group of L lanes
@@ -487,8 +605,8 @@ __global__ void __launch_bounds__(128) k_rows_general_resid(DevProblem P) {
       const int4 ax = __ldg(&P.aresd[gd.x + ei]);
       const int la = ad.y & 255, mn = ad.y >> 8;
       if (mn == 0) {
-        double kb[DIM][DIM];
-        simplex_block<DIM, false>(P, ax, la, 0, P.D[ad.w], kb, re, true);
+        double blk[NPE * D2];   // unused: the stiffness products are left to the compiler to drop
+        uncut_block_row<DIM, NPE>(P, ax, la, P.D[ad.w], blk, re);
       } else if (ax.z >= 0) {
         coh_traction<DIM>(P, ax.z, re);
       }
@@ -660,13 +778,15 @@ __global__ void __launch_bounds__(128) k_general_static(DevProblem P, double* st
   if (bad) atomicOr(P.err, ERR_NONFINITE);
 }
 
-template <int DIM, int G>
-__global__ void __launch_bounds__(128) k_rows_general(DevProblem P, int slab_slots, int max_mn) {
-  constexpr int NB = 128 / G;
+// General rows of the nodes [node0, node1) of the general list.
+template <int DIM, int L, int NPE = DIM + 1>
+__global__ void __launch_bounds__(128) k_rows_general(DevProblem P, int slab_slots, int node0, int node1) {
+  constexpr int NB = 128 / L;
   extern __shared__ double smem[];
-  const int grp = threadIdx.x / G;
-  const int node = blockIdx.x * NB + grp;
-  general_rows<DIM, G>(P, node, node < P.n_slow_dn, smem + (size_t)grp * general_slab_doubles(slab_slots, DIM, max_mn));
+  const int grp = threadIdx.x / L;
+  const int node = node0 + blockIdx.x * NB + grp;
+  general_rows<DIM, L, NPE>(P, node, node < node1,
+                            smem + (size_t)grp * general_slab_doubles(slab_slots, DIM, L, NPE), slab_slots);
 }
 
 // Cohesive elements, one lane per quadrature point (CQ lanes per element: 2 in 2D for CohEdge2, 4
@@ -687,9 +807,8 @@ __device__ __forceinline__ void coh_element(const DevProblem& P, int ce, int qi,
   constexpr int D2 = DIM * DIM;
   constexpr int CQ = CohLanes<DIM>::CQ;
   const int lane = threadIdx.x & 31, base_lane = lane & ~(CQ - 1);
-  int c = 0, nh = 0, q0 = 0, nq = 0;
+  int nh = 0, q0 = 0, nq = 0;
   if (valid) {
-    c = __ldg(&P.ce_cut[ce]);
     nh = __ldg(&P.coh_nh[ce]);
     q0 = __ldg(&P.coh_qp_off[ce]);
     nq = min(CQ, __ldg(&P.coh_qp_off[ce + 1]) - q0);
@@ -701,8 +820,7 @@ __device__ __forceinline__ void coh_element(const DevProblem& P, int ce, int qi,
   for (int i = 0; i < DIM; ++i) Tr[i] = 0.0;
   bool bad = false;
   if (valid && qi < nq) {
-    const int* cl = P.coh_local + __ldg(&P.coh_local_off[ce]);
-    const int* nodes = P.cut_nodes + __ldg(&P.cut_node_off[c]);
+    const int* gn = P.coh_gnode + __ldg(&P.coh_local_off[ce]);   // the element's node ids
     const int cq = q0 + qi;
     const double* N = P.cqp_N + __ldg(&P.cqp_noff[cq]);
     const double* R = P.cqp_R + (size_t)cq * D2;
@@ -711,7 +829,7 @@ __device__ __forceinline__ void coh_element(const DevProblem& P, int ce, int qi,
     for (int d = 0; d < DIM; ++d) {
       double s = 0.0;
       for (int n = 0; n < nh; ++n) {
-        const int np = __ldg(&nodes[__ldg(&cl[n + nh])]), nm = __ldg(&nodes[__ldg(&cl[n])]);
+        const int np = __ldg(&gn[n + nh]), nm = __ldg(&gn[n]);
         s += N[n] * (P.U[(size_t)np * DIM + d] - P.U[(size_t)nm * DIM + d]);
       }
       d0[d] = s;
@@ -820,7 +938,7 @@ __global__ void __launch_bounds__(128) k_coh_elements(DevProblem P) {
 // G_i eps_macro).  One block per cut element, one thread per node pair; the element's gradients,
 // weights and materials are staged in shared memory.  Blocks go to the cache in (i, j) block
 // order so a block row is contiguous.  FP64.
-__host__ __device__ inline int cut_smem_doubles(int nq, int mn, int dim) { return nq * mn * dim + 2 * nq + 2 * 36 + 8; }
+__host__ __device__ inline int cut_smem_doubles(int nq, int mn, int dim) { return nq * mn * dim + 2 * nq + 3 * 36 + 8; }
 template <int DIM>
 __global__ void __launch_bounds__(64) k_cut_volumetric(DevProblem P, const int* __restrict__ list, int n_list, double* gmac) {
   constexpr int NV = (DIM == 2) ? 3 : 6;
@@ -837,7 +955,7 @@ __global__ void __launch_bounds__(64) k_cut_volumetric(DevProblem P, const int* 
   const int gbase = __ldg(&P.qp_grad_off[q0]);
   for (int i = threadIdx.x; i < nq * mn * DIM; i += blockDim.x) sg[i] = __ldg(&P.qp_grad[gbase + i]);
   for (int i = threadIdx.x; i < nq; i += blockDim.x) { sw[i] = __ldg(&P.qp_wgt[q0 + i]); smat[i] = (double)__ldg(&P.qp_mat[q0 + i]); }
-  for (int i = threadIdx.x; i < 72; i += blockDim.x) sD[i] = __ldg(&P.Dd[i]);
+  for (int i = threadIdx.x; i < 108; i += blockDim.x) sD[i] = __ldg(&P.Dd[i]);
   __syncthreads();
   double* kout = P.ke + __ldg(&P.ke_off[c]);
   bool bad = false;

@@ -5,6 +5,8 @@
 #pragma once
 
 #include "pg_ctx.h"
+#include "pg_tile.cuh"
+#include "pg_general.cuh"
 
 namespace pgl {
 
@@ -27,23 +29,45 @@ void residual_cases(pg_ctx* c, const pgd::DevProblem& P);
 #ifdef PG_LAUNCH_IMPL
 template <int DIM>
 void assembly(pg_ctx* c, const pgd::DevProblem& P, bool jac, bool fp32) {
-  // fork: the fast rows (uncut elements only) run on the side stream, concurrently with the
-  // cut-element kernels and the general rows on the main stream
+  const bool func = (P.flags & PG_FUNC) != 0;
+  auto blocks_of = [](long long n) { return (int)((n + 127) / 128); };
+  const bool simplex_general = P.n_slow_dn > 0 && P.npe == DIM + 1;
+  // 2D: the general chain (cohesive elements, element records, general rows) runs on the
+  // high-priority stream side2 and the structured tiles on the low-priority stream side, both
+  // from the fork: the block scheduler dispatches the chain's blocks first, and the tiles fill
+  // the rest of the GPU.  3D: all on the main stream, cohesive elements and records, the tiles,
+  // then the general rows (the 3D tile and general kernels each fill the GPU).
   cudaEventRecord(c->ev[0], c->stream);
   cudaStreamWaitEvent(c->side, c->ev[0], 0);
-  if (P.n_coh_el > 0) {
-    const int tpb = 128;
-    const int lanes = pgd::CohLanes<DIM>::CQ;
-    const int grid = (int)(((long long)P.n_coh_el * lanes + tpb - 1) / tpb);
-    pgd::k_coh_elements<DIM><<<grid, tpb, 0, c->stream>>>(P);
-  }
-  // 2D: the stencil rows run on the side stream, concurrently with the cohesive elements and the
-  // general rows (the cohesive kernel leaves most SMs idle).  3D: on the main stream between the
-  // two -- the 3D stencil and general kernels each fill the GPU, and run concurrently they took
-  // 1.65 ms per 64^3 assembly against 1.0 ms one after the other.
-  cudaEventRecord(c->ev[3], c->stream);
+  cudaStreamWaitEvent(c->side2, c->ev[0], 0);
+  cudaStream_t gst = (DIM == 2) ? c->side2 : c->stream;
   cudaStream_t sst = (DIM == 2) ? c->side : c->stream;
-  if (c->n_stencil > 0 && !jac) {
+  {
+    const int coh_blocks = (P.n_coh_el > 0) ? blocks_of((long long)P.n_coh_el * pgd::CohLanes<DIM>::CQ) : 0;
+    const int rec_blocks = (simplex_general && P.n_grec > 0) ? blocks_of(P.n_grec) : 0;
+    if (coh_blocks + rec_blocks > 0) pgd::k_gen_first<DIM><<<coh_blocks + rec_blocks, 128, 0, gst>>>(P, coh_blocks);
+  }
+  cudaEventRecord(c->ev[3], gst);
+  if (DIM == 2 && c->n_tiles > 0) {
+    // 2D: one CTA per 16 x 8 tile of grid nodes, each element formed once (pg_tile.cuh)
+    const size_t smem = pgd::tile2_smem_bytes();
+    if (!jac) pgd::k_rows_tile2<double, false><<<c->n_tiles, pgd::kTileThreads, smem, sst>>>(P, c->grid, c->tiles, c->tnodes, c->tsegs);
+    else if (fp32) pgd::k_rows_tile2<float, true><<<c->n_tiles, pgd::kTileThreads, smem, sst>>>(P, c->grid, c->tiles, c->tnodes, c->tsegs);
+    else pgd::k_rows_tile2<double, true><<<c->n_tiles, pgd::kTileThreads, smem, sst>>>(P, c->grid, c->tiles, c->tnodes, c->tsegs);
+  } else if (DIM == 3 && c->n_tiles > 0) {
+    // 3D: one CTA per 4 x 4 x 4 tile of grid nodes, each tet formed once (pg_tile.cuh)
+    const size_t smem = pgd::tile3_smem_bytes();
+    if (!jac) {
+      cudaFuncSetAttribute(pgd::k_rows_tile3<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      pgd::k_rows_tile3<double, false><<<c->n_tiles, pgd::kT3Threads, smem, sst>>>(P, c->grid, c->tiles, c->tnodes, c->tsegs);
+    } else if (fp32) {
+      cudaFuncSetAttribute(pgd::k_rows_tile3<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      pgd::k_rows_tile3<float, true><<<c->n_tiles, pgd::kT3Threads, smem, sst>>>(P, c->grid, c->tiles, c->tnodes, c->tsegs);
+    } else {
+      cudaFuncSetAttribute(pgd::k_rows_tile3<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      pgd::k_rows_tile3<double, true><<<c->n_tiles, pgd::kT3Threads, smem, sst>>>(P, c->grid, c->tiles, c->tnodes, c->tsegs);
+    }
+  } else if (c->n_stencil > 0 && !jac) {
     const int tpb = 128;
     const int grid = (c->n_stencil + tpb - 1) / tpb;
     pgd::k_rows_stencil<DIM, double, false><<<grid, tpb, 0, sst>>>(P, c->grid, c->stencil, c->n_stencil);
@@ -56,22 +80,30 @@ void assembly(pg_ctx* c, const pgd::DevProblem& P, bool jac, bool fp32) {
     else pgd::k_rows_stencil<DIM, double><<<grid, tpb, smem, sst>>>(P, c->grid, c->stencil, c->n_stencil);
   }
   cudaEventRecord(c->ev[1], sst);
-  if (P.n_slow_dn > 0 && !jac) {
-    // residual only: entry-parallel groups of L lanes per node
+  if (simplex_general) {
+    // block-parallel general rows (pg_general.cuh): residual lane groups and blocks in one launch
+    const int res_blocks = func ? blocks_of((long long)P.n_slow_dn * pgd::kGenResidLanes) : 0;
+    const int blk_blocks = jac ? blocks_of(P.n_gblk) : 0;
+    if (res_blocks + blk_blocks > 0)
+      pgd::k_gen_rows<DIM><<<res_blocks + blk_blocks, 128, 0, gst>>>(P, 0, P.n_slow_dn, res_blocks, 0, P.n_gblk);
+  } else if (P.n_slow_dn > 0 && !jac) {
+    // quad4 meshes, residual only: entry-parallel groups of L lanes per node
     constexpr int L = 8;
     const int grid = (int)(((long long)P.n_slow_dn * L + 127) / 128);
-    pgd::k_rows_general_resid<DIM, L><<<grid, 128, 0, c->stream>>>(P);
-  } else if (P.n_slow_dn > 0) {
+    pgd::k_rows_general_resid<DIM, L, (DIM == 2) ? 4 : DIM + 1><<<grid, 128, 0, gst>>>(P);
+  } else if (P.n_slow_dn > 0 && DIM == 2) {
+    // quad4 meshes: a lane group per general node (every node is one)
     const int slots = P.maxnb_general;
-    constexpr int G = (DIM == 2) ? 4 : 8;
-    const int grid = (P.n_slow_dn + (128 / G) - 1) / (128 / G);
-    const size_t smem = (size_t)(128 / G) * pgd::general_slab_doubles(slots, DIM, P.max_mn) * sizeof(double);
-    cudaFuncSetAttribute(pgd::k_rows_general<DIM, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    pgd::k_rows_general<DIM, G><<<grid, 128, smem, c->stream>>>(P, slots, P.max_mn);
+    constexpr int L = 8;
+    const int grid = (P.n_slow_dn + (128 / L) - 1) / (128 / L);
+    const size_t smem = (size_t)(128 / L) * pgd::general_slab_doubles(slots, DIM, L, 4) * sizeof(double);
+    cudaFuncSetAttribute(pgd::k_rows_general<DIM, L, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    pgd::k_rows_general<DIM, L, 4><<<grid, 128, smem, gst>>>(P, slots, 0, P.n_slow_dn);
   }
-  cudaEventRecord(c->ev[4], c->stream);
+  cudaEventRecord(c->ev[4], gst);
   // join
   cudaStreamWaitEvent(c->stream, c->ev[1], 0);
+  cudaStreamWaitEvent(c->stream, c->ev[4], 0);
   cudaEventRecord(c->ev[5], c->stream);
 }
 

@@ -134,6 +134,36 @@ void quad4_shape(double r, double s, double* N, double* dN) {
   dN[4] = 0.25 * (1.0 + s);  dN[5] = 0.25 * (1.0 + r);
   dN[6] = -0.25 * (1.0 + s); dN[7] = 0.25 * (1.0 - r);
 }
+// Elem::inverse_map for a quad4 parent (src/elem.cpp:697-765): the parent coordinates of the
+// global point g, by Newton steps on x(r, s) = sum_a N_a(r, s) x_a - g from (0, 0), each step
+// followed by the reference's residual test (|x - g| < 1e-12 per component, at most 1000 steps).
+// On the structured grid's rectangles x is affine in (r, s), so the first step lands on the
+// point.  Returns false when the point is outside the parent (Quad4::coords_inside, tolerance
+// 1e-12 on the reference square).
+bool quad4_inverse(const double* xs, const double* g, double* rs) {
+  double r = 0.0, t = 0.0;
+  for (int it = 0; it < 1000; ++it) {
+    double N[4], dN[8], f[2] = {-g[0], -g[1]}, J[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    quad4_shape(r, t, N, dN);
+    for (int n = 0; n < 4; ++n)
+      for (int i = 0; i < 2; ++i) {
+        f[i] += N[n] * xs[n * 2 + i];
+        for (int a = 0; a < 2; ++a) J[i][a] += dN[n * 2 + a] * xs[n * 2 + i];
+      }
+    const double det = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    if (det == 0.0) return false;
+    r -= (J[1][1] * f[0] - J[0][1] * f[1]) / det;
+    t -= (-J[1][0] * f[0] + J[0][0] * f[1]) / det;
+    quad4_shape(r, t, N, dN);
+    double res[2] = {-g[0], -g[1]};
+    for (int n = 0; n < 4; ++n) for (int i = 0; i < 2; ++i) res[i] += N[n] * xs[n * 2 + i];
+    if (std::fabs(res[0]) < 1e-12 && std::fabs(res[1]) < 1e-12) break;
+  }
+  rs[0] = r; rs[1] = t;
+  const double tol = 1e-12;
+  return r >= -1.0 - tol && r <= 1.0 + tol && t >= -1.0 - tol && t <= 1.0 + tol;
+}
+
 // Quad4 order 3: tensor product of the 2-point edge rule, qp -> (qp % 2, qp / 2) (src/quad4.cpp:108-127).
 void quad4_qp(int qp, double* r, double* s, double* w) {
   const double g[2] = {-kGauss2, kGauss2};
@@ -324,6 +354,118 @@ bool tri3_case(const int nd[3], CutCase& cc) {
   return true;
 }
 
+// Quad4::detection (src/quad4.cpp:188-497, the cases written with polygonal integration
+// elements): node detection values -> cut case (cohesive numbering: enrichment nodes 4.., their
+// mirrors after).  Returns 0 uncut, 1 cut, 4 for the layouts the reference stops on (opposite
+// nodes sharing a material: "interface highly curved").  Four inclusions on one element leave
+// the cohesive list empty, as the reference's branch does.
+int quad4_case(const int nd[4], CutCase& cc) {
+  const int n0 = nd[0], n1 = nd[1], n2 = nd[2], n3 = nd[3];
+  const bool n0e1 = n0 == n1, n0e2 = n0 == n2, n0e3 = n0 == n3, n1e2 = n1 == n2, n1e3 = n1 == n3, n2e3 = n2 == n3;
+  std::vector<int> v = {n0, n1, n2, n3};
+  std::sort(v.begin(), v.end());
+  v.erase(std::unique(v.begin(), v.end()), v.end());
+  const int nu = (int)v.size();
+  if (nu == 1) return 0;
+  const int c0 = (int)std::count(nd, nd + 4, v[0]);   // nodes holding the smallest value
+  using VV = std::vector<std::vector<int>>;
+  auto set = [&](std::vector<int> ce, std::vector<int> inc, VV sub, std::vector<int> mat) {
+    cc.cut_edge = ce; cc.incl = inc; cc.sub = sub; cc.sub_mat = mat;
+  };
+  const VV coh2 = {{4, 5, 8, 9}, {6, 7, 10, 11}};
+  const VV coh3 = {{4, 5, 10, 11}, {6, 7, 12, 13}, {8, 9, 14, 15}};
+  if (nu == 2) {
+    if (v[0] < 0) {
+      if (c0 == 1 || c0 == 3) {
+        const VV cA = {{4, 5, 6, 7}}, cB = {{5, 4, 7, 6}};
+        if (n1e2 && n1e3) {
+          cc.cut_edge = {3, 0}; cc.sub_mat = {n0, n2};
+          if (n0 < n1) { cc.sub = {{0, 5, 4}, {1, 2, 3, 6, 7}}; cc.coh = cA; } else { cc.sub = {{0, 7, 6}, {1, 2, 3, 4, 5}}; cc.coh = cB; }
+        } else if (n0e2 && n0e3) {
+          cc.cut_edge = {0, 1}; cc.sub_mat = {n1, n3};
+          if (n1 < n0) { cc.sub = {{1, 5, 4}, {2, 3, 0, 6, 7}}; cc.coh = cA; } else { cc.sub = {{1, 7, 6}, {2, 3, 0, 4, 5}}; cc.coh = cB; }
+        } else if (n0e1 && n0e3) {
+          cc.cut_edge = {1, 2}; cc.sub_mat = {n2, n0};
+          if (n2 < n0) { cc.sub = {{2, 5, 4}, {3, 0, 1, 6, 7}}; cc.coh = cA; } else { cc.sub = {{2, 7, 6}, {3, 0, 1, 4, 5}}; cc.coh = cB; }
+        } else if (n0e1 && n1e2) {
+          cc.cut_edge = {2, 3}; cc.sub_mat = {n3, n1};
+          if (n3 < n0) { cc.sub = {{3, 5, 4}, {0, 1, 2, 6, 7}}; cc.coh = cA; } else { cc.sub = {{3, 7, 6}, {0, 1, 2, 4, 5}}; cc.coh = cB; }
+        } else return 4;
+      } else if (c0 == 2) {
+        if (n0e1) {
+          cc.cut_edge = {1, 3}; cc.sub_mat = {n0, n2};
+          if (n0 < n2) { cc.sub = {{0, 1, 4, 5}, {2, 3, 7, 6}}; cc.coh = {{5, 4, 7, 6}}; }
+          else { cc.sub = {{0, 1, 6, 7}, {2, 3, 5, 4}}; cc.coh = {{4, 5, 6, 7}}; }
+        } else if (n1e2) {
+          cc.cut_edge = {2, 0}; cc.sub_mat = {n0, n1};
+          if (n0 < n1) { cc.sub = {{3, 0, 5, 4}, {1, 2, 6, 7}}; cc.coh = {{4, 5, 6, 7}}; }
+          else { cc.sub = {{3, 0, 7, 6}, {1, 2, 4, 5}}; cc.coh = {{5, 4, 7, 6}}; }
+        } else return 4;
+      } else return 4;
+      cc.incl.assign(cc.cut_edge.size(), v[1]);
+    } else {
+      if (c0 == 1 || c0 == 3) {
+        if (n1e2 && n1e3) set({0, 3, 3, 0}, {n0, n0, n2, n2}, {{0, 8, 9}, {5, 4, 7, 6}, {1, 2, 3, 10, 11}}, {n0, -1, n2});
+        else if (n0e2 && n0e3) set({1, 0, 0, 1}, {n1, n1, n3, n3}, {{1, 8, 9}, {5, 4, 7, 6}, {2, 3, 0, 10, 11}}, {n1, -1, n3});
+        else if (n0e1 && n0e3) set({2, 1, 1, 2}, {n2, n2, n0, n0}, {{2, 8, 9}, {5, 4, 7, 6}, {3, 0, 1, 10, 11}}, {n2, -1, n0});
+        else if (n0e1 && n1e2) set({3, 2, 2, 3}, {n3, n3, n1, n1}, {{3, 8, 9}, {5, 4, 7, 6}, {0, 1, 2, 10, 11}}, {n3, -1, n1});
+        else return 4;
+      } else if (c0 == 2) {
+        if (n0e1) set({1, 3, 3, 1}, {n0, n0, n2, n2}, {{0, 1, 8, 9}, {5, 4, 7, 6}, {2, 3, 10, 11}}, {n0, -1, n2});
+        else if (n1e2) set({2, 0, 0, 2}, {n1, n1, n3, n3}, {{1, 2, 8, 9}, {5, 4, 7, 6}, {3, 0, 10, 11}}, {n1, -1, n3});
+        else return 4;
+      } else return 4;
+      cc.coh = coh2;
+    }
+  } else if (nu == 3) {
+    if (v[0] < 0) {
+      if (c0 == 2) {
+        if (n0e1) set({3, 2, 2, 1}, {n3, n3, n2, n2}, {{3, 8, 9}, {2, 10, 11}, {0, 1, 7, 6, 5, 4}}, {n3, n2, -1});
+        else if (n1e2) set({0, 3, 3, 2}, {n0, n0, n3, n3}, {{0, 8, 9}, {3, 10, 11}, {1, 2, 7, 6, 5, 4}}, {n0, n3, -1});
+        else if (n2e3) set({1, 0, 0, 3}, {n1, n1, n0, n0}, {{1, 8, 9}, {0, 10, 11}, {2, 3, 7, 6, 5, 4}}, {n1, n0, -1});
+        else if (n0e3) set({2, 1, 1, 0}, {n2, n2, n1, n1}, {{2, 8, 9}, {1, 10, 11}, {3, 0, 7, 6, 5, 4}}, {n2, n1, -1});
+        else if (n0e2) set({1, 0, 3, 2}, {n1, n1, n3, n3}, {{1, 8, 9}, {3, 10, 11}, {2, 7, 6, 0, 5, 4}}, {n1, n3, -1});
+        else if (n1e3) set({0, 3, 2, 1}, {n0, n0, n2, n2}, {{0, 8, 9}, {2, 10, 11}, {1, 7, 6, 3, 5, 4}}, {n0, n2, -1});
+        else return 4;
+      } else {
+        if (n0e1 && n2 < 0) set({1, 3, 3, 2}, {n0, n0, n3, n3}, {{0, 1, 8, 9}, {3, 10, 11}, {2, 7, 6, 5, 4}}, {n0, n3, -1});
+        else if (n0e1 && n3 < 0) set({1, 3, 2, 1}, {n0, n0, n2, n2}, {{0, 1, 8, 9}, {2, 10, 11}, {3, 5, 4, 7, 6}}, {n0, n2, -1});
+        else if (n0e1) return 4;
+        else if (n1e2 && n3 < 0) set({2, 0, 0, 3}, {n1, n1, n0, n0}, {{1, 2, 8, 9}, {0, 10, 11}, {3, 7, 6, 5, 4}}, {n1, n0, -1});
+        else if (n1e2 && n0 < 0) set({2, 0, 3, 2}, {n1, n1, n3, n3}, {{1, 2, 8, 9}, {3, 10, 11}, {0, 5, 4, 7, 6}}, {n1, n3, -1});
+        else if (n1e2) return 4;
+        else if (n2e3 && n0 < 0) set({3, 1, 1, 0}, {n2, n2, n1, n1}, {{2, 3, 8, 9}, {1, 10, 11}, {0, 7, 6, 5, 4}}, {n2, n1, -1});
+        else if (n2e3 && n1 < 0) set({3, 1, 0, 3}, {n2, n2, n0, n0}, {{2, 3, 8, 9}, {0, 10, 11}, {1, 5, 4, 7, 6}}, {n2, n0, -1});
+        else if (n2e3) return 4;
+        else if (n0e3 && n1 < 0) set({0, 2, 2, 1}, {n3, n3, n2, n2}, {{3, 0, 8, 9}, {2, 10, 11}, {1, 7, 6, 5, 4}}, {n3, n2, -1});
+        else if (n0e3 && n2 < 0) set({0, 2, 1, 0}, {n3, n3, n1, n1}, {{3, 0, 8, 9}, {1, 10, 11}, {2, 5, 4, 7, 6}}, {n3, n1, -1});
+        else return 4;
+      }
+      cc.coh = coh2;
+    } else {
+      if (n0e1) set({1, 3, 3, 2, 2, 1}, {n0, n0, n3, n3, n2, n2}, {{0, 1, 10, 11}, {3, 12, 13}, {2, 14, 15}, {9, 8, 7, 6, 5, 4}}, {n0, n3, n2, -1});
+      else if (n1e2) set({2, 0, 0, 3, 3, 2}, {n1, n1, n0, n0, n3, n3}, {{1, 2, 10, 11}, {0, 12, 13}, {3, 14, 15}, {9, 8, 7, 6, 5, 4}}, {n1, n0, n3, -1});
+      else if (n2e3) set({3, 1, 1, 0, 0, 3}, {n2, n2, n1, n1, n0, n0}, {{2, 3, 10, 11}, {1, 12, 13}, {0, 14, 15}, {9, 8, 7, 6, 5, 4}}, {n2, n1, n0, -1});
+      else if (n0e3) set({0, 2, 2, 1, 1, 0}, {n3, n3, n2, n2, n1, n1}, {{3, 0, 10, 11}, {2, 12, 13}, {1, 14, 15}, {9, 8, 7, 6, 5, 4}}, {n3, n2, n1, -1});
+      else return 4;
+      cc.coh = coh3;
+    }
+  } else {
+    if (v[0] < 0) {
+      if (n0 < 0) set({3, 2, 2, 1, 1, 0}, {n3, n3, n2, n2, n1, n1}, {{3, 10, 11}, {2, 12, 13}, {1, 14, 15}, {0, 9, 8, 7, 6, 5, 4}}, {n3, n2, n1, -1});
+      else if (n1 < 0) set({0, 3, 3, 2, 2, 1}, {n0, n0, n3, n3, n2, n2}, {{0, 10, 11}, {3, 12, 13}, {2, 14, 15}, {1, 9, 8, 7, 6, 5, 4}}, {n0, n3, n2, -1});
+      else if (n2 < 0) set({1, 0, 0, 3, 3, 2}, {n1, n1, n0, n0, n3, n3}, {{1, 10, 11}, {0, 12, 13}, {3, 14, 15}, {2, 9, 8, 7, 6, 5, 4}}, {n1, n0, n3, -1});
+      else set({2, 1, 1, 0, 0, 3}, {n2, n2, n1, n1, n0, n0}, {{2, 10, 11}, {1, 12, 13}, {0, 14, 15}, {3, 9, 8, 7, 6, 5, 4}}, {n2, n1, n0, -1});
+      cc.coh = coh3;
+    } else {
+      set({3, 2, 2, 1, 1, 0, 0, 3}, {n3, n3, n2, n2, n1, n1, n0, n0},
+          {{3, 12, 13}, {2, 14, 15}, {1, 16, 17}, {0, 18, 19}, {11, 10, 9, 8, 7, 6, 5, 4}}, {n3, n2, n1, n0, -1});
+      cc.coh.clear();
+    }
+  }
+  return 1;
+}
+
 // Tet4::partitionPrism (src/tet4.cpp:776-873): a prism (l[0..2] bottom, l[3..5] top) split into
 // three tets.  g holds the global ids of the parent nodes among the prism's nodes and the local
 // ids of its enrichment nodes; bottom_known selects the rule keyed on nodes 0-2, otherwise the one
@@ -451,10 +593,6 @@ int build_setup(const ProblemDesc& d, Setup& s) {
   s.npe = (d.elem_type == TRI3) ? 3 : 4;
   s.cohesive = d.coh_law != COH_NONE;
   const int dim = s.dim;
-  if (d.elem_type == QUAD4 && !d.incl.empty()) {
-    s.error = "cut quad4 parents are not supported; use tri3 or tet4 background elements with inclusions";
-    return 2;
-  }
 
   // ---------------- materials (material_lei.cpp:52-97); D is latched per material by dimension
   s.nvoigt = (dim == 2) ? 3 : 6;
@@ -476,6 +614,41 @@ int build_setup(const ProblemDesc& d, Setup& s) {
       double coef = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
       for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) D[i * 6 + j] = coef * (i == j ? (1.0 - nu) : nu);
       for (int i = 3; i < 6; ++i) D[i * 6 + i] = coef * (1.0 - 2.0 * nu) / 2;
+    }
+  }
+
+  // ---------------- bounding plies: LinearElasticTransverselyIsotropicMaterial::computeLinearDmat
+  // (src/material_leti.cpp:52-128): fibers along x, E3 = E2, G13 = G12, nu13 = nu12,
+  // nu23 = E2 / (2 G23) - 1; the expressions and their order as the reference writes them
+  // (the plane-stress branch included).
+  {
+    double* D = s.D[2];
+    for (int i = 0; i < 36; ++i) D[i] = 0.0;
+    if (d.ply_frac > 0.0) {
+      const double E1 = d.ply[0], E2 = d.ply[1], G12 = d.ply[2], G23 = d.ply[3], nu12 = d.ply[4];
+      if (!(E1 > 0 && E2 > 0 && G12 > 0 && G23 > 0) || d.ply_frac >= 0.5) {
+        s.error = "bounding plies need E1, E2, G12, G23 > 0 and a fraction below 0.5";
+        return 2;
+      }
+      const double E3 = E2, G13 = G12, nu13 = nu12, nu23 = E2 / (2.0 * G23) - 1.0;
+      const double delta = 1.0 - 2.0 * (E3 / E1) * nu12 * nu13 * nu23 - (E3 / E1) * nu13 * nu13 - (E3 / E2) * nu23 * nu23 -
+                           (E2 / E1) * nu12 * nu12;
+      const double C11 = E1 * (1.0 - (E3 / E2) * nu23 * nu23) / delta;
+      const double C22 = E2 * (1.0 - (E3 / E1) * nu13 * nu13) / delta;
+      const double C33 = E3 * (1.0 - (E2 / E1) * nu12 * nu12) / delta;
+      const double C12 = (E2 * nu12 + E3 * nu13 * nu23) / delta;
+      const double C13 = E3 * (nu12 * nu23 + nu13) / delta;
+      const double C23 = (E3 / E1) * (E1 * nu23 + E2 * nu12 * nu13) / delta;
+      const double C44 = G23, C55 = G13, C66 = G12;
+      if (dim == 2) {
+        if (d.plane_strain) { D[0] = C11; D[1] = C12; D[3] = C12; D[4] = C22; D[8] = C66; }
+        else { D[0] = C11 - C13 / C33; D[1] = C12 - C23 / C33; D[3] = C12 - C23 / C33; D[4] = C22 - C23 / C33; D[8] = C66; }
+      } else {
+        D[0] = C11; D[1] = C12; D[2] = C13;
+        D[6] = C12; D[7] = C22; D[8] = C23;
+        D[12] = C13; D[13] = C23; D[14] = C33;
+        D[21] = C44; D[28] = C55; D[35] = C66;
+      }
     }
   }
 
@@ -630,6 +803,25 @@ int build_setup(const ProblemDesc& d, Setup& s) {
       }
   }
 
+  // ---------------- bounding plies (Tests/Main.cpp:262-289): an element whose nodes all lie at or
+  // above top = hi_y - f (hi_y - lo_y), or all at or below bottom = lo_y + f (hi_y - lo_y), takes
+  // the ply material.  This precedes detection, as in the reference (Mesh::detection reads the
+  // element's material as the one of its matrix-side sub-elements, Mesh.cpp:2988, and gives an
+  // element wholly inside an inclusion the inclusion's material, Mesh.cpp:2999-3005).
+  if (d.ply_frac > 0.0) {
+    const double span = d.hi[1] - d.lo[1];
+    const double top = d.hi[1] - span * d.ply_frac, bottom = d.lo[1] + span * d.ply_frac;
+    for (int e = 0; e < s.ne; ++e) {
+      bool in_top = true, in_bottom = true;
+      for (int q = 0; q < s.npe; ++q) {
+        const double y = X3[(size_t)s.conn[(size_t)e * s.npe + q] * 3 + 1];
+        if (y < top) in_top = false;
+        if (y > bottom) in_bottom = false;
+      }
+      if (in_top || in_bottom) s.elem_mat[e] = 2;
+    }
+  }
+
   // ---------------- element detection (Tri3::detection / Tet4::detection)
   std::vector<CutCase> cases;
   std::vector<int> cut_elems;
@@ -655,6 +847,16 @@ int build_setup(const ProblemDesc& d, Setup& s) {
         os << "element " << e << ": " << why;
         s.error = os.str();
         return rc;
+      }
+      cut = rc == 1;
+    } else if (d.elem_type == QUAD4) {
+      const int rc = quad4_case(nd, cc);
+      if (rc == 4) {
+        std::ostringstream os;
+        os << "element " << e << ": quad4 element cut in a manner the reference stops on (opposite nodes share a "
+           << "material: interface highly curved, src/quad4.cpp:333-336)";
+        s.error = os.str();
+        return 4;
       }
       cut = rc == 1;
     } else { s.error = "element type has no cut-case table here"; return 4; }
@@ -779,12 +981,16 @@ int build_setup(const ProblemDesc& d, Setup& s) {
       for (int v : enodes) A.cut_nodes.push_back(v);
       A.cut_node_off.push_back((int)A.cut_nodes.size());
 
-      // parent gradients (constant for the affine tri3 / tet4 parents)
+      // parent gradients: constant for the affine tri3 / tet4 parents; for a quad4 parent at each
+      // point, from the inverse map of the point's global coordinates (src/Mesh.cpp:1564-1580)
+      const bool quad_parent = d.elem_type == QUAD4;
       double pxs[4 * 3], pdNdr[4 * 3], pdNdx[4 * 3], pN[4], pJ;
       for (int q = 0; q < s.npe; ++q) for (int k = 0; k < dim; ++k) pxs[q * dim + k] = X3of(enodes[q])[k];
-      if (dim == 2) tri3_shape(0.0, 0.0, pN, pdNdr);
-      else tet4_shape(0.0, 0.0, 0.0, pN, pdNdr);
-      transform_gradients(dim, s.npe, pdNdr, pxs, pdNdx, &pJ);
+      if (!quad_parent) {
+        if (dim == 2) tri3_shape(0.0, 0.0, pN, pdNdr);
+        else tet4_shape(0.0, 0.0, 0.0, pN, pdNdr);
+        transform_gradients(dim, s.npe, pdNdr, pxs, pdNdx, &pJ);
+      }
 
       for (size_t ie = 0; ie < cc.sub.size(); ++ie) {
         const std::vector<int>& sub = cc.sub[ie];
@@ -817,6 +1023,13 @@ int build_setup(const ProblemDesc& d, Setup& s) {
           else { w = kTet5[qp][3]; tet4_shape(kTet5[qp][0], kTet5[qp][1], kTet5[qp][2], cN, cdN); }
           transform_gradients(dim, nsn, cdN, sx, cdNdx, &cJ);
           if (cJ < 0.0) { A.error = "negative sub-element Jacobian (src/Mesh.cpp:1561)"; A.rc = 7; return; }
+          if (quad_parent) {
+            double gx[2] = {0.0, 0.0}, rs[2];
+            for (int q = 0; q < nsn; ++q) for (int k = 0; k < 2; ++k) gx[k] += sx[q * 2 + k] * cN[q];
+            if (!quad4_inverse(pxs, gx, rs)) { A.error = "bad inverse map of a quad4 parent (src/Mesh.cpp:1572)"; A.rc = 7; return; }
+            quad4_shape(rs[0], rs[1], pN, pdNdr);
+            transform_gradients(2, 4, pdNdr, pxs, pdNdx, &pJ);
+          }
           A.qp_wgt.push_back(cJ * w);
           A.qp_mat.push_back(mat);
           // gradients over the element's nodes: parent gradients, then the child gradient of the

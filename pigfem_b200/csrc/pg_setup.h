@@ -35,6 +35,8 @@ struct ProblemDesc {
   int subscale = 0;
   double eps_macro[6] = {0, 0, 0, 0, 0, 0};
   double app_strain = 0.0;
+  double ply_frac = 0.0;     // bounding plies: fraction of the height at the top and the bottom
+  double ply[5] = {0, 0, 0, 0, 0};   // E1, E2, G12, G23, nu12 of the plies
 };
 
 // Cohesive-law constants as the reference's materials hold them after set_parameter.
@@ -55,9 +57,10 @@ struct Setup {
   int npe = 3;  // nodes per parent element
   bool cohesive = false;
   CohParams coh;
-  // materials: 0 = matrix, 1 = fiber (linear elastic isotropic); D in Voigt order, row-major
+  // materials: 0 = matrix, 1 = fiber (linear elastic isotropic), 2 = bounding plies (linear
+  // elastic transversely isotropic); D in Voigt order, row-major
   int nvoigt = 3;
-  double D[2][36];
+  double D[3][36];
 
   // nodes: standard nodes first, then enrichment nodes (cohesive mirrors after the originals)
   int n_std = 0, n_enr = 0, n_enr_initial = 0;

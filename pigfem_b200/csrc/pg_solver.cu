@@ -391,7 +391,30 @@ __global__ void __launch_bounds__(kThreads) k_homogenize(pgd::DevProblem P, cons
   for (int v = 0; v <= NV; ++v) acc[v] = 0.0;
   for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
     const int cc = P.cut_of[e];
-    if (cc < 0) {
+    if (DIM == 2 && cc < 0 && P.npe == 4) {
+      // uncut quad4: the four Gauss points of its bilinear map
+      double x[4][2], u[4][2];
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        const int id = P.conn[(size_t)e * 4 + n];
+#pragma unroll
+        for (int d = 0; d < 2; ++d) { x[n][d] = P.X[(size_t)id * 2 + d]; u[n][d] = U[(size_t)id * 2 + d]; }
+      }
+#pragma unroll
+      for (int qp = 0; qp < 4; ++qp) {
+        double g[4][2], w, eps[3];
+        pgd::quad4_point(x, qp, g, &w);
+#pragma unroll
+        for (int v = 0; v < 3; ++v) eps[v] = P.subscale ? P.eps_macro[v] : 0.0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) pgd::add_strain<2, double>(g[n], u[n], eps);
+        double sig[3];
+        pgd::lei_stress<2, double>(P.Dd + 36 * P.emat[e], eps, sig);
+#pragma unroll
+        for (int v = 0; v < 3; ++v) acc[v] += w * sig[v];
+        acc[NV] += w;
+      }
+    } else if (cc < 0) {
       double x[NPE][DIM], g[NPE][DIM], J, eps[NV];
       int nd[NPE];
 #pragma unroll

@@ -8,6 +8,12 @@ Requests arrive (Poisson, or as a list), each with a seeded geometry.  Two kinds
 * ``cohesive_step`` -- cohesive RVE under prescribed displacement: the tangent K and residual R
   of one load step at a seeded interface state, with the damage state (internal variables) on the
   device; the result is the residual norm and the damage-zone census of the cohesive points.
+  A request may belong to a *session*: the load steps k = 0 .. steps-1 of one RVE, each at the
+  fraction (k+1)/steps of the session's interface state, the converged internal variables
+  committed after each step (the reference's ``InternalVars::copy_data_in`` after a converged
+  load step, src/SolverNonlinear.cpp:96-97, 301).  The session's context -- mesh tables, CSR
+  structure, displacements and committed internal variables -- stays on the device from its
+  first step to its last; its steps run in order.
 
 Pipeline (all stages run at once on different requests):
 
@@ -15,7 +21,11 @@ Pipeline (all stages run at once on different requests):
    (pg_create_host; ctypes releases the GIL, so they run in parallel on the host cores);
 2. the admission controller admits set-up requests in arrival order while the sum of the device
    bytes of the admitted requests stays within the budget and a GPU slot is free -- a request
-   that arrives while others are on the GPU is admitted as soon as slots and memory free up;
+   that arrives while others are on the GPU is admitted as soon as slots and memory free up.  A
+   request's bytes are its size estimate scaled by the largest ratio of measured to estimated
+   bytes seen so far (pg_device_bytes, the peak a finished request held), and once its context is
+   on the device the ledger holds the measured bytes; a resident session keeps its bytes until
+   its last step;
 3. GPU workers upload the admitted request (stream-ordered allocations, no device-wide
    synchronisation), run its work on its own CUDA stream, so the work of all admitted requests
    overlaps on the device, read back the small result and free the context.
@@ -38,6 +48,10 @@ import numpy as np
 
 from . import capi, rve
 
+# Ortiz-Pandolfi interfaces of the load-step sessions (sigma_c, delta_c, beta, unused;
+# src/Material_OPCohesive.cpp): a law with a committed maximum opening, so the steps carry damage
+OP_PARAMS = (50.0, 2e-4, 1.0, 0.0)
+
 
 @dataclass
 class Request:
@@ -46,6 +60,9 @@ class Request:
     desc: capi.ProblemDesc
     arrival: float = 0.0  # seconds after the stream start
     seed: int = 0
+    session: int = -1     # cohesive load-step session (-1: a one-off request)
+    step: int = 0         # load step within the session
+    steps: int = 1        # load steps of the session; the last one frees the resident context
 
 
 @dataclass
@@ -58,7 +75,8 @@ class Result:
     setup_done: float = 0.0
     admitted: float = 0.0
     done: float = 0.0
-    device_bytes: int = 0
+    device_bytes: int = 0        # bytes the admission ledger charged (estimate x calibration)
+    measured_bytes: int = 0      # the most device memory the request's context held
     error: str = ""
 
     @property
@@ -107,16 +125,29 @@ def make_request(rid: int, seed: int = 1, workload: int = 5, scale: float = 1.0)
     return Request(rid, kind, desc, seed=seed)
 
 
-def poisson_stream(n: int, rate: float, seed: int = 1, scale: float = 1.0) -> List[Request]:
-    """n seeded requests with exponential inter-arrival times of mean 1/rate seconds."""
+def poisson_stream(n: int, rate: float, seed: int = 1, scale: float = 1.0, session_steps: int = 1) -> List[Request]:
+    """n seeded requests with exponential inter-arrival times of mean 1/rate seconds.  With
+    session_steps > 1 every cohesive request opens a session of that many load steps (the
+    Ortiz-Pandolfi law, whose committed maximum opening the steps carry), the later steps
+    arriving as further requests of the stream; the stream then holds n first requests."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
-    for rid in range(n):
+    for base in range(n):
         t += rng.exponential(1.0 / rate)
-        r = make_request(rid, seed, scale=scale)
+        r = make_request(base, seed, scale=scale)
         r.arrival = t
+        if session_steps > 1 and r.kind == "cohesive_step":
+            r.desc.coh_law, r.desc.coh = capi.COH_OP, OP_PARAMS
+            r.session, r.steps = base, session_steps
+            ts = t
+            for k in range(1, session_steps):
+                ts += rng.exponential(1.0 / rate)
+                out.append(Request(0, r.kind, r.desc, ts, seed, session=base, step=k, steps=session_steps))
         out.append(r)
+    out.sort(key=lambda q: (q.arrival, q.session, q.step))
+    for rid, q in enumerate(out):
+        q.rid = rid
     return out
 
 
@@ -162,15 +193,23 @@ def run_request(P: capi.Problem, req: Request, stream) -> Dict[str, np.ndarray]:
                 Un = U[idx].contiguous()
                 C[:, k] = P.homogenize(Un.data_ptr(), 1.0)[:nv]
             return {"C": C, "pcg_iterations": it.astype(np.int64)}
-        # cohesive load step: seeded interface openings, damage state on the device
-        U = rve.interface_state(P, seed=req.rid)
+        # cohesive load step: seeded interface openings (step k of a session at (k+1)/steps of
+        # the session's state), damage state on the device; a session commits the step's
+        # internal variables for the next one
+        frac = (req.step + 1) / req.steps
+        U = rve.interface_state(P, seed=req.session if req.session >= 0 else req.rid) * frac
         dU = torch.from_numpy(U).to("cuda", non_blocking=False)
-        if P.n_isv:
+        if req.step == 0 and P.n_isv:
             P.set_isv(np.zeros(P.n_isv))
-        P.assemble_device(dU.data_ptr(), 1.0, capi.FUNC | capi.JAC)
+        P.assemble_device(dU.data_ptr(), frac, capi.FUNC | capi.JAC)
         res = P.residual_norm()
         zones = P.damage_zones() if P.n_isv or P.sizes["n_coh_qp"] else np.zeros(0, np.uint8)
-        return {"residual_norm": np.array([res]), "zones": np.bincount(zones, minlength=4).astype(np.int64)}
+        out = {"residual_norm": np.array([res]), "zones": np.bincount(zones, minlength=4).astype(np.int64)}
+        if req.session >= 0 and P.n_isv:
+            P.commit_isv()
+            # the carried state: the committed internal variables (maximum openings), summed
+            out["committed_isv_sum"] = np.array([float(np.sum(P.get_isv(trial=False)))])
+        return out
 
 
 def homogenization_csv(result: Result) -> str:
@@ -191,6 +230,24 @@ def run_alone(req: Request) -> Result:
     vals = run_request(P, req, stream)
     stream.synchronize()
     out = Result(req.rid, req.kind, P.sizes["n_elem"], vals, 0.0, 0.0, 0.0, time.perf_counter() - t0, device_bytes(P))
+    out.measured_bytes = P.device_bytes()[1]
+    P.close()
+    return out
+
+
+def run_session_alone(reqs: List[Request]) -> List[Result]:
+    """The steps of one session by themselves, in order, on one context."""
+    import torch
+    reqs = sorted(reqs, key=lambda q: q.step)
+    P = capi.Problem(reqs[0].desc)
+    stream = torch.cuda.Stream()
+    out = []
+    for req in reqs:
+        t0 = time.perf_counter()
+        vals = run_request(P, req, stream)
+        stream.synchronize()
+        out.append(Result(req.rid, req.kind, P.sizes["n_elem"], vals, 0.0, 0.0, 0.0, time.perf_counter() - t0,
+                          device_bytes(P)))
     P.close()
     return out
 
@@ -203,6 +260,8 @@ class ServingEngine:
         self.budget = int(memory_budget)
         self.max_inflight = max_inflight
         self.setup_workers = setup_workers
+        self.calibration = 1.0        # largest measured / estimated device bytes seen so far
+        self.peak_charged = 0         # most bytes the ledger held at once
 
     def run(self, requests: List[Request], realtime: bool = True) -> List[Result]:
         import torch
@@ -212,6 +271,10 @@ class ServingEngine:
         ready: "queue.Queue" = queue.Queue()
         lock = threading.Condition()
         state = {"used": 0, "inflight": 0}
+        # resident sessions: id -> {"P", "stream", "bytes", "next" (step), "busy"}; sessions whose
+        # set-up or a step failed (their later steps fail too)
+        sessions: Dict[int, dict] = {}
+        failed: set = set()
         t_start = time.perf_counter()
         now = lambda: time.perf_counter() - t_start
 
@@ -221,11 +284,19 @@ class ServingEngine:
                 if wait > 0:
                     time.sleep(wait)
             r = Result(req.rid, req.kind, 0, {}, arrival=req.arrival if realtime else now())
+            if req.session >= 0 and req.step > 0:
+                # the session's context is (or will be) resident: no set-up of its own
+                r.setup_done = now()
+                ready.put((req, None, r))
+                return
             try:
                 P = capi.Problem(req.desc, device=False)
             except capi.PigfemError as e:
                 r.error = str(e)
                 r.done = now()
+                if req.session >= 0:
+                    with lock:
+                        failed.add(req.session)
                 ready.put((req, None, r))
                 return
             r.elements = P.sizes["n_elem"]
@@ -233,20 +304,62 @@ class ServingEngine:
             r.setup_done = now()
             ready.put((req, P, r))
 
-        def gpu_work(req: Request, P: capi.Problem, r: Result):
+        def charge(delta: int):
+            state["used"] += delta
+            self.peak_charged = max(self.peak_charged, state["used"])
+
+        def gpu_work(req: Request, P: Optional[capi.Problem], r: Result):
             torch.cuda.set_device(dev)
-            stream = torch.cuda.Stream()
+            sess = sessions.get(req.session) if req.session >= 0 else None
+            keep = False
             try:
-                P.upload()
+                if sess is not None and req.step > 0:
+                    P, stream = sess["P"], sess["stream"]
+                    r.elements = P.sizes["n_elem"]
+                else:
+                    stream = torch.cuda.Stream()
+                    P.upload()
+                    # from here on the ledger holds the measured bytes, or the calibrated estimate
+                    # while that is larger (it covers the solver workspace still to come)
+                    with lock:
+                        held = max(r.device_bytes, P.device_bytes()[0])
+                        charge(held - r.device_bytes)
+                        r.device_bytes = held
+                    if req.session >= 0:
+                        with lock:
+                            sessions[req.session] = {"P": P, "stream": stream, "bytes": r.device_bytes,
+                                                     "next": 0, "busy": True}
+                        sess = sessions[req.session]
                 r.values = run_request(P, req, stream)
                 stream.synchronize()
+                keep = sess is not None and req.step < req.steps - 1
             except capi.PigfemError as e:
                 r.error = str(e)
+                if req.session >= 0:
+                    with lock:
+                        failed.add(req.session)
             finally:
-                P.close()
+                measured = P.device_bytes()[1] if P is not None else 0
+                r.measured_bytes = measured
+                est = device_bytes(P) if P is not None else 0
+                if not keep and P is not None:
+                    P.close()
                 r.done = now()
                 with lock:
-                    state["used"] -= r.device_bytes
+                    if est > 0:
+                        self.calibration = max(self.calibration, measured / est)
+                    if sess is not None:
+                        if keep:
+                            # the ledger keeps the session's bytes (now the peak it reached)
+                            charge(measured - sess["bytes"])
+                            sess["bytes"] = measured
+                            sess["next"] = req.step + 1
+                            sess["busy"] = False
+                        else:
+                            charge(-sess["bytes"])
+                            sessions.pop(req.session, None)
+                    else:
+                        charge(-r.device_bytes)
                     state["inflight"] -= 1
                     results[req.rid] = r
                     lock.notify_all()
@@ -255,36 +368,65 @@ class ServingEngine:
         gpu_pool = ThreadPoolExecutor(self.max_inflight)
         for req in sorted(requests, key=lambda q: q.arrival):
             setup_pool.submit(setup, req)
-        # admission in set-up completion order, which follows arrival order up to set-up time
+        # admission in arrival order: a one-off request or a session's first step that does not
+        # fit the budget stops the requests behind it; a later session step needs no new memory
+        # and waits only for its session's previous step
         pending: List = []
         n_left = len(requests)
         while n_left:
             try:
-                item = ready.get(timeout=0.05)
+                item = ready.get(timeout=0.02)
                 pending.append(item)
             except queue.Empty:
                 pass
             pending.sort(key=lambda it: it[0].arrival)
-            while pending:
-                req, P, r = pending[0]
-                if P is None:
+            i = 0
+            while i < len(pending):
+                req, P, r = pending[i]
+                continuing = req.session >= 0 and req.step > 0
+                if P is None and not continuing:
                     with lock:
                         results[req.rid] = r
-                    pending.pop(0)
+                    pending.pop(i)
                     n_left -= 1
                     continue
                 with lock:
-                    fits = state["used"] + r.device_bytes <= self.budget or state["inflight"] == 0
-                    if not (fits and state["inflight"] < self.max_inflight):
+                    if state["inflight"] >= self.max_inflight:
                         break
-                    state["used"] += r.device_bytes
+                    if continuing and req.session in failed:
+                        r.error = "an earlier step of the session failed"
+                        r.done = now()
+                        results[req.rid] = r
+                        pending.pop(i)
+                        n_left -= 1
+                        continue
+                    if continuing:
+                        sess = sessions.get(req.session)
+                        if sess is None or sess["busy"] or sess["next"] != req.step:
+                            i += 1
+                            continue
+                        sess["busy"] = True
+                        r.device_bytes = 0
+                    else:
+                        want = int(r.device_bytes * self.calibration)
+                        if not (state["used"] + want <= self.budget or state["inflight"] == 0):
+                            break
+                        r.device_bytes = want
+                        charge(want)
                     state["inflight"] += 1
                 r.admitted = now()
-                pending.pop(0)
+                pending.pop(i)
                 n_left -= 1
                 gpu_pool.submit(gpu_work, req, P, r)
+            with lock:
+                # a session step waits for its predecessor: sleep until something finishes
+                if pending and state["inflight"] > 0 and ready.empty():
+                    lock.wait(timeout=0.02)
         gpu_pool.shutdown(wait=True)
         setup_pool.shutdown(wait=True)
+        # a session cut short (an error in one of its steps) frees its context here
+        for sess in sessions.values():
+            sess["P"].close()
         return [results[q.rid] for q in requests]
 
 

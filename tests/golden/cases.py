@@ -18,6 +18,9 @@ BL = (50.0, 5e-7, 5e-3, 0.0)
 XN = (50.0, 2e-4, 3e-4, 1.7)
 OP = (50.0, 2e-4, 1.0, 0.0)
 TL = (50.0, 5e-7, 1e-3, 5e-3)
+# transversely isotropic bounding plies (E1, E2, G12, G23, nu12), the glass/epoxy ply of the
+# reference's RVE driver
+PLY = (36.2e3, 7.11e3, 2.32e3, 2.17e3, 0.335)
 
 CASES = {
     # name: dict(elem_type, n, incl, coh_law, coh, subscale, eps_macro, u_scale, isv_scale, seed)
@@ -76,6 +79,48 @@ CASES = {
                              coh_law=0, coh=(0, 0, 0, 0), subscale=0, u_scale=1e-3, isv_scale=0.0, seed=17),
     "coh_bl_polygon": dict(elem_type=0, n=(8, 8), incl=[[0.5533, 0.6147, 0.1452], [0.8061, 0.5055, 0.0803]],
                            coh_law=1, coh=BL, subscale=0, u_scale=1e-6, isv_scale=0.0, seed=18, open=(1e-7, 1.2e-2)),
+    # quad4 background elements: uncut rectangles with hx != hy (Dirichlet and periodic subscale
+    # loading), and quad4 parents cut by fibers (Quad4::detection's polygonal cases: a triangle
+    # and a pentagon, two quads, two fibers on one element with a quad between them), linear,
+    # bilinear and Ortiz-Pandolfi interfaces, periodic with a macroscale strain
+    "lin_quad4_uncut": dict(elem_type=1, n=(7, 5), incl=np.zeros((0, 3)), coh_law=0, coh=(0, 0, 0, 0), subscale=0,
+                            u_scale=1e-3, isv_scale=0.0, seed=36),
+    "lin_quad4_subscale": dict(elem_type=1, n=(9, 6), incl=np.zeros((0, 3)), coh_law=0, coh=(0, 0, 0, 0), subscale=1,
+                               eps_macro=(0.01, -0.004, 0.002), u_scale=1e-3, isv_scale=0.0, seed=37),
+    "lin_quad4_one_fiber": dict(elem_type=1, n=(8, 8), incl=[[0.5, 0.5, 0.23]], coh_law=0, coh=(0, 0, 0, 0),
+                                subscale=0, u_scale=1e-3, isv_scale=0.0, seed=45),
+    "lin_quad4_two_fibers_one_element": dict(elem_type=1, n=(8, 8), incl=[[0.5533, 0.6147, 0.1452], [0.8061, 0.5055, 0.0803]],
+                                             coh_law=0, coh=(0, 0, 0, 0), subscale=0, u_scale=1e-3, isv_scale=0.0, seed=46),
+    "lin_quad4_fiber_subscale": dict(elem_type=1, n=(9, 7), incl=[[0.47, 0.52, 0.21]], coh_law=0, coh=(0, 0, 0, 0),
+                                     subscale=1, eps_macro=(0.01, -0.004, 0.002), u_scale=1e-3, isv_scale=0.0, seed=47),
+    "coh_quad4_bl": dict(elem_type=1, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=1, coh=BL,
+                         subscale=0, u_scale=1e-6, isv_scale=0.0, seed=48, open=(1e-7, 1.2e-2)),
+    "coh_quad4_op": dict(elem_type=1, n=(16, 16), incl=[[0.3, 0.3, 0.12], [0.63, 0.56, 0.13]], coh_law=5, coh=OP,
+                         subscale=0, u_scale=1e-6, isv_scale=1.0, seed=49, open=(1e-6, 1e-3)),
+    "coh_quad4_bl_two_fibers_one_element": dict(elem_type=1, n=(8, 8), incl=[[0.5533, 0.6147, 0.1452], [0.8061, 0.5055, 0.0803]],
+                                                coh_law=1, coh=BL, subscale=0, u_scale=1e-6, isv_scale=0.0, seed=50,
+                                                open=(1e-7, 1.2e-2)),
+    # transversely isotropic bounding plies: the element rows wholly above 0.8 / below 0.2 of the
+    # height take the ply material (fiber axis x), with a fiber / sphere (linear and cohesive)
+    # between them
+    "lin_tri3_plies": dict(elem_type=0, n=(12, 10), incl=[[0.47, 0.52, 0.17]], coh_law=0, coh=(0, 0, 0, 0), subscale=0,
+                           u_scale=1e-3, isv_scale=0.0, seed=38, ply_frac=0.2),
+    "coh_bl_plies": dict(elem_type=0, n=(12, 10), incl=[[0.47, 0.52, 0.17]], coh_law=1, coh=BL, subscale=0,
+                         u_scale=1e-6, isv_scale=0.0, seed=39, open=(1e-7, 1.2e-2), ply_frac=0.2),
+    "lin_tet4_plies": dict(elem_type=2, n=(5, 5, 5), incl=[[0.52, 0.47, 0.49, 0.2]], coh_law=0, coh=(0, 0, 0, 0),
+                           subscale=0, u_scale=1e-3, isv_scale=0.0, seed=40, ply_frac=0.2),
+    # a fiber reaching into a ply: the matrix side of each cut ply element keeps the ply material
+    "lin_tri3_ply_cut": dict(elem_type=0, n=(12, 10), incl=[[0.47, 0.26, 0.17], [0.66, 0.8, 0.11]], coh_law=0,
+                             coh=(0, 0, 0, 0), subscale=0, u_scale=1e-3, isv_scale=0.0, seed=41, ply_frac=0.2,
+                             ply_cut=1),
+    "coh_bl_ply_cut": dict(elem_type=0, n=(12, 10), incl=[[0.47, 0.26, 0.17], [0.66, 0.8, 0.11]], coh_law=1, coh=BL,
+                           subscale=0, u_scale=1e-6, isv_scale=0.0, seed=42, open=(1e-7, 1.2e-2), ply_frac=0.2,
+                           ply_cut=1),
+    "lin_tet4_ply_cut": dict(elem_type=2, n=(5, 5, 5), incl=[[0.52, 0.47, 0.49, 0.31]], coh_law=0, coh=(0, 0, 0, 0),
+                             subscale=0, u_scale=1e-3, isv_scale=0.0, seed=43, ply_frac=0.2, ply_cut=1),
+    "coh_tet4_bl_ply_cut": dict(elem_type=2, n=(5, 5, 5), incl=[[0.52, 0.47, 0.49, 0.31]], coh_law=1, coh=BL,
+                                subscale=0, u_scale=1e-6, isv_scale=0.0, seed=44, open=(1e-7, 1.2e-2), ply_frac=0.2,
+                                ply_cut=1),
     # tet4 (6 tets per hex): uncut, one sphere, periodic subscale with a macroscale strain, and
     # cohesive spheres (one node separated: tet + prism -> 4 tets and a CohTri3; two and two: two
     # prisms -> 6 tets and a CohQuad4)
@@ -150,4 +195,5 @@ def spec_kwargs(c):
     return dict(elem_type=c["elem_type"], n=c["n"], lo=(0.0,) * dim, hi=(1.0,) * dim,
                 inclusions=np.array(c["incl"], dtype=np.float64), E_matrix=E_M, nu_matrix=NU_M, E_fiber=E_F,
                 nu_fiber=NU_F, coh_law=c["coh_law"], coh=c["coh"], plane_strain=True, subscale=bool(c["subscale"]),
-                eps_macro=em, app_strain=app)
+                eps_macro=em, app_strain=app, ply_frac=c.get("ply_frac", 0.0),
+                ply=PLY if c.get("ply_frac", 0.0) > 0 else (0.0,) * 5)

@@ -105,7 +105,7 @@ def test_batch_rejects_mixed_dimensions():
 
 
 def test_batch_3d_autotuned_shape_keeps_results():
-    """3D: the shape the autotuner picks (lanes per general node among 8, 16, 32) leaves every
+    """3D: the shape the autotuner picks (persistent blocks per SM among 2, 4, 8, 16) leaves every
     context's results bitwise those of the single-context call."""
     from pigfem_b200 import capi
     probs, us = _problems(["coh_tet4_opaug_two_spheres", "lin_tet4_one_sphere", "coh_tet4_tl"])

@@ -74,7 +74,7 @@ def test_bilinear_tension_until_the_reference_breaks_down(both):
     after further cut-backs, stops on a zero or non-finite pivot of its direct solver before the
     end of the ramp.  The drop-in run must reproduce every converged record before that first
     failed attempt to the printed digits, and it must not finish the ramp either (in the blown-up
-    attempt 1e-16 differences in K decide how far the run gets).
+    attempt 1e-16 differences in K decide how far the run gets)."""
     c = _case(1, BL, 0.02)
     cpu, _ = _solve(both, c, "cpu")
     gpu, _ = _solve(both, c, "b200")

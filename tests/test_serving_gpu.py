@@ -46,3 +46,43 @@ def test_admission_respects_budget_and_slots():
     spans = sorted((r.admitted, r.done) for r in res)
     for (a0, d0), (a1, d1) in zip(spans, spans[1:]):
         assert a1 >= d0 - 1e-3
+
+
+def test_sessions_stay_resident_and_equal_their_steps_alone():
+    """Cohesive load-step sessions (3 steps each, Ortiz-Pandolfi interfaces) mixed with one-off
+    requests: every step's result is bitwise the same as the session's steps run alone on one
+    context, the carried committed internal variables never decrease from step to step (damage
+    is irreversible), and later steps need no set-up of their own."""
+    from pigfem_b200 import serving
+    reqs = serving.poisson_stream(8, rate=50.0, seed=5, scale=0.2, session_steps=3)
+    sess = {}
+    for q in reqs:
+        if q.session >= 0:
+            sess.setdefault(q.session, []).append(q)
+    assert sess and all(len(v) == 3 for v in sess.values())
+    alone = {}
+    for v in sess.values():
+        for q, a in zip(sorted(v, key=lambda q: q.step), serving.run_session_alone(v)):
+            alone[q.rid] = a
+    for q in reqs:
+        if q.session < 0:
+            alone[q.rid] = serving.run_alone(q)
+    budget = int(2 * max(a.device_bytes for a in alone.values()))
+    eng = serving.ServingEngine(memory_budget=budget, max_inflight=4, setup_workers=4)
+    mixed = {r.rid: r for r in eng.run(reqs, realtime=False)}
+    for q in reqs:
+        m, a = mixed[q.rid], alone[q.rid]
+        assert not m.error, m.error
+        assert sorted(m.values) == sorted(a.values)
+        for k in a.values:
+            assert np.array_equal(m.values[k], a.values[k]), (q.rid, q.session, q.step, k)
+    for v in sess.values():
+        steps = sorted(v, key=lambda q: q.step)
+        sums = [mixed[q.rid].values["committed_isv_sum"][0] for q in steps]
+        assert all(b >= a for a, b in zip(sums, sums[1:])), sums
+        assert sums[-1] > 0
+        for q in steps[1:]:
+            assert mixed[q.rid].admitted >= mixed[steps[steps.index(q) - 1].rid].done - 1e-3
+    # the engine's calibration covers every measured footprint
+    for m in mixed.values():
+        assert m.measured_bytes > 0

@@ -78,7 +78,8 @@ def test_host_setup_matches_golden(name):
 
 @pytest.mark.parametrize("name", ["lin_tri3_three_fibers", "lin_tri3_polygon", "coh_bl_polygon", "coh_bl",
                                   "coh_xn", "coh_bl_two_fibers_one_element", "lin_tet4_one_sphere", "coh_tet4_bl",
-                                  "coh_tet4_opaug_two_spheres"])
+                                  "coh_tet4_opaug_two_spheres", "lin_quad4_one_fiber", "lin_quad4_fiber_subscale",
+                                  "coh_quad4_bl", "coh_quad4_bl_two_fibers_one_element"])
 def test_host_quadrature_matches_live_reference(oracle_lib, name):
     ref = oracle_lib
     R = ref.RefProblem(ref.ProblemSpec(**spec_kwargs(CASES[name])))
@@ -108,7 +109,8 @@ def test_host_quadrature_matches_live_reference(oracle_lib, name):
 
 
 @pytest.mark.parametrize("name", ["lin_tri3_one_fiber", "lin_tri3_subscale", "coh_bl", "coh_opaug", "coh_xn",
-                                  "coh_bl_two_fibers_one_element", "lin_tet4_subscale", "coh_tet4_xn"])
+                                  "coh_bl_two_fibers_one_element", "lin_tet4_subscale", "coh_tet4_xn",
+                                  "coh_quad4_bl_two_fibers_one_element"])
 def test_golden_fixtures_reproduce(oracle_lib, name):
     """The reference, built here from its sources, regenerates the committed fixture bit-exactly."""
     from tests.golden import make_golden
@@ -117,6 +119,36 @@ def test_golden_fixtures_reproduce(oracle_lib, name):
     assert sorted(out) == sorted(g.files)
     for k in g.files:
         assert np.array_equal(out[k], g[k]), k
+
+
+@pytest.mark.parametrize("name", ["lin_tri3_plies", "coh_bl_plies", "lin_tet4_plies", "lin_tri3_ply_cut", "coh_bl_ply_cut",
+                                  "lin_tet4_ply_cut", "coh_tet4_bl_ply_cut", "lin_tri3_three_fibers"])
+def test_element_materials_match_live_reference(oracle_lib, name):
+    """Every uncut element and every sub-element quadrature point carries the reference's material:
+    matrix, fiber, or -- in the bounding plies (every node in the top or bottom fraction of the
+    height) -- the transversely isotropic ply material, which the matrix side of a cut ply element
+    keeps."""
+    ref = oracle_lib
+    R = ref.RefProblem(ref.ProblemSpec(**spec_kwargs(CASES[name])))
+    P = host_problem(name)
+    ecut, qoff, qmat = R.get("elem_cut"), R.get("elem_qp_off"), R.get("qp_mat")
+    mats = R.get("materials").reshape(-1, 3)
+    # reference material index -> 0 matrix, 1 fiber, 2 ply
+    code = np.where(mats[:, 0] == 2, 2, np.where(mats[:, 1] == spec_kwargs(CASES[name])["E_fiber"], 1, 0))
+    uncut = np.nonzero(ecut == 0)[0]
+    ref_mat = code[qmat[qoff[uncut]]]
+    mine = P.debug("elem_mat")[uncut]
+    assert np.array_equal(mine, ref_mat)
+    # the sub-element quadrature points of the cut elements, in the reference's order
+    cut = np.nonzero(ecut)[0]
+    ref_qp = code[np.concatenate([qmat[qoff[e]:qoff[e + 1]] for e in cut])] if len(cut) else np.zeros(0)
+    assert np.array_equal(P.debug("qp_mat"), ref_qp)
+    if CASES[name].get("ply_frac", 0.0) > 0:
+        assert (mine == 2).sum() > 0 and (mine == 1).sum() > 0
+        if CASES[name].get("ply_cut"):
+            assert (ref_qp == 2).sum() > 0 and (ref_qp == 1).sum() > 0
+    P.close()
+    R.close()
 
 
 def test_setup_errors_are_status_codes():
@@ -138,6 +170,15 @@ def test_setup_errors_are_status_codes():
     assert e.value.code == 2
     with pytest.raises(capi.PigfemError) as e:
         capi.Problem(capi.ProblemDesc(n=(8, 8), coh_law=capi.COH_TL, coh=(50.0, 1e-3, 5e-7, 5e-3)), device=False)
+    assert e.value.code == 2
+    # bounding plies: a ply fraction of half the height or more, and a ply material with a
+    # non-positive modulus
+    ply = (36.2e3, 7.11e3, 2.32e3, 2.17e3, 0.335)
+    with pytest.raises(capi.PigfemError) as e:
+        capi.Problem(capi.ProblemDesc(n=(8, 8), ply_frac=0.5, ply=ply), device=False)
+    assert e.value.code == 2
+    with pytest.raises(capi.PigfemError) as e:
+        capi.Problem(capi.ProblemDesc(n=(8, 8), ply_frac=0.25, ply=(36.2e3, 0.0, 2.32e3, 2.17e3, 0.335)), device=False)
     assert e.value.code == 2
 
 

@@ -32,7 +32,8 @@ def _ref(oracle, c):
     return oracle.RefProblem(oracle.ProblemSpec(**spec_kwargs(c)))
 
 
-@pytest.mark.parametrize("name", ["lin_tri3_subscale", "lin_tri3_three_fibers", "lin_tet4_subscale", "coh_opaug"])
+@pytest.mark.parametrize("name", ["lin_tri3_subscale", "lin_tri3_three_fibers", "lin_tet4_subscale", "coh_opaug",
+                                  "lin_quad4_subscale", "lin_quad4_fiber_subscale"])
 def test_homogenize_matches_reference(oracle_lib, name):
     import torch
     c = CASES[name]
