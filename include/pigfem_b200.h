@@ -189,6 +189,22 @@ int pg_pcg_solve(pg_ctx* ctx, const double* d_b, double* d_x, int nrhs, double r
  * sigma from d_U (device, node-major) plus the macroscale strain eps_macro * t_frac. */
 int pg_homogenize(pg_ctx* ctx, const double* d_U, double t_frac, double* out);
 
+/* Material sensitivity of the internal force (SensitivityParameter::assemble_dPdd with a
+ * SensitivityMaterialParameterStructural of a linear elastic isotropic material,
+ * src/SensitivityParameter.cpp:110-153, src/SensitivityMaterialParameter.cpp:41-220): the
+ * derivative of P_int at the node-major device displacements d_U by parameter `param` (0 E,
+ * 1 lambda, 2 mu, 3 K, 4 nu) of `material` (0 matrix, 1 fiber), summed over the elements and
+ * sub-elements of that material, into d_dPf (n_free) and d_dPp (n_const) on the context's stream
+ * (returns once they are written).  The strain is that of d_U alone (no macroscale strain), as in
+ * the reference.  Cohesive problems are PG_ERR_UNSUPPORTED (the cohesive laws' sensitivity
+ * updates are not built). */
+#define PG_SENS_E 0
+#define PG_SENS_LAMBDA 1
+#define PG_SENS_MU 2
+#define PG_SENS_K 3
+#define PG_SENS_NU 4
+int pg_material_sensitivity(pg_ctx* ctx, const double* d_U, int material, int param, double* d_dPf, double* d_dPp);
+
 /* ---- Batches: many contexts assembled by one set of persistent launches replayed from a CUDA
  * graph.  No counterpart in the reference (it assembles one mesh per process).  Each context's
  * results are bitwise those of pg_assemble_device on the same inputs. */

@@ -35,6 +35,7 @@ class _Config(ctypes.Structure):
         ("plane_strain", ctypes.c_int), ("subscale", ctypes.c_int),
         ("eps_macro", ctypes.c_double * 6), ("app_strain", ctypes.c_double),
         ("ply_frac", ctypes.c_double), ("ply", ctypes.c_double * 5),
+        ("sens_mat", ctypes.c_int), ("sens_param", ctypes.c_int),
     ]
 
 
@@ -74,6 +75,8 @@ def lib(variant: str = "cpu"):
         L.pgref_set_macro.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.pgref_destroy.restype = None
         L.pgref_destroy.argtypes = [ctypes.c_void_p]
+        L.pgref_sensitivity.restype = ctypes.c_int
+        L.pgref_sensitivity.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.pgref_bind_gpu.restype = ctypes.c_int
         L.pgref_bind_gpu.argtypes = [ctypes.c_void_p]
         L.pgref_gpu_error.restype = ctypes.c_char_p
@@ -102,6 +105,8 @@ class ProblemSpec:
     app_strain: float = 0.01
     ply_frac: float = 0.0
     ply: Sequence[float] = (0.0,) * 5
+    sens_mat: int = 0          # material sensitivity parameter: 0 none, 1 matrix, 2 fiber
+    sens_param: int = 0        # 0 E, 1 LAMBDA, 2 MU, 3 K, 4 NU
 
 
 class RefProblem:
@@ -134,6 +139,7 @@ class RefProblem:
         c.ply_frac = spec.ply_frac
         for i, v in enumerate(spec.ply):
             c.ply[i] = v
+        c.sens_mat, c.sens_param = spec.sens_mat, spec.sens_param
         self._cfg = c
         self.h = L.pgref_create(ctypes.byref(c))
         nfc = self.get("n_free_const")
@@ -182,6 +188,15 @@ class RefProblem:
             isv_committed = np.ascontiguousarray(isv_committed, dtype=np.float64)
             iv = isv_committed.ctypes.data
         return lib(self.variant).pgref_assemble(self.h, U.ctypes.data, iv, t_frac, int(func), int(jac))
+
+    def sensitivity(self, U: np.ndarray):
+        """The reference's dP_int/dp (free, constrained) of the spec's material parameter at the
+        full DOF vector U."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        rc = lib(self.variant).pgref_sensitivity(self.h, U.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("no material sensitivity parameter in this problem's spec")
+        return self.get("dP_f"), self.get("dP_p")
 
     def homogenize(self) -> np.ndarray:
         lib(self.variant).pgref_homogenize(self.h)

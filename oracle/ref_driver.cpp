@@ -81,6 +81,9 @@ extern "C" const char* pg_dropin_last_error(void) __attribute__((weak));
 #include "CohesiveElem.h"
 #include "pgshim_objects.h"
 #include "WriterHomogenization.h"
+#include "SensitivitySolver.h"
+#include "SensitivityParameter.h"
+#include "SensitivityRightLoad.h"
 #undef protected
 #undef private
 
@@ -121,6 +124,8 @@ typedef struct {
   double app_strain;          /* Dirichlet mode: right x = app_strain*(xmax-xmin), left x = 0, node 0 pinned */
   double ply_frac;            /* bounding plies: top / bottom fraction of the height (0: none) */
   double ply[5];              /* ply material E1, E2, G12, G23, nu12 */
+  int sens_mat;               /* material sensitivity: 0 none, 1 "Matrix", 2 "Fiber" */
+  int sens_param;             /* 0 E, 1 LAMBDA, 2 MU, 3 K, 4 NU */
 } pgref_config;
 
 }  // extern "C"
@@ -446,10 +451,47 @@ void* pgref_create(const pgref_config* cfg) {
     boundary->set_dirichlet_bcs_from_nodeset("left", 0, 0.0);
     for (int d = 0; d < dim; ++d) boundary->set_dirichlet_bc(0, d, 0.0);
   }
+  if (cfg->sens_mat > 0) {
+    // one material sensitivity parameter and the right-edge load function, as Tests/Main.cpp:586-609
+    // registers them before Problem::init (which builds the sensitivity solver)
+    static const char* params[5] = {"E", "LAMBDA", "MU", "K", "NU"};
+    SensitivityRightLoad function;
+    h->prob->addSensitivityFunction(&function);
+    h->prob->addMaterialSensitivityParameter(cfg->sens_mat == 1 ? "Matrix" : "Fiber", params[cfg->sens_param]);
+  }
   h->prob->init();
   h->prob->setup();
   export_mesh(h);
   return h;
+}
+
+/*
+ * The reference's assemble_dPdd of the registered material parameter at the full DOF vector U
+ * (free then constrained): exports dP_f and dP_p.  Returns 0, or -1 without a parameter.
+ */
+int pgref_sensitivity(void* vh, const double* U) {
+  Handle* h = (Handle*)vh;
+  if (h->cfg.sens_mat <= 0 || !h->prob->_sensitivity_solver || h->prob->_sensitivity_solver->_parameters.empty())
+    return -1;
+  writeToScreen = false;
+  logFile = h->log_path;
+  Solver* s = h->prob->get_solver();
+  DofObject* dofs = h->prob->get_dofs();
+  const int nf = (int)dofs->n_global_free_dofs(), np = (int)dofs->n_global_const_dofs();
+  for (int i = 0; i < nf; ++i) s->_U.f->a[i] = U[i];
+  for (int i = 0; i < np; ++i) s->_U.p->a[i] = U[nf + i];
+  s->store_solution(s->_U, h->prob->get_solution());
+  pvector dP;
+  VecDuplicate(s->_U.f, &dP.f);
+  VecDuplicate(s->_U.p, &dP.p);
+  VecSet(dP.f, 0.0);
+  VecSet(dP.p, 0.0);
+  h->prob->_sensitivity_solver->_parameters[0]->assemble_dPdd(dP, h->prob);
+  export_vec(h, "dP_f", dP.f);
+  export_vec(h, "dP_p", dP.p);
+  VecDestroy(&dP.f);
+  VecDestroy(&dP.p);
+  return 0;
 }
 
 /* Solver parameters as Tests/Main.cpp:627-632 sets them. */

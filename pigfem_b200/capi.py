@@ -24,6 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libpigfem_b200.so")
 
 TRI3, QUAD4, TET4 = 0, 1, 2
+SENS_E, SENS_LAMBDA, SENS_MU, SENS_K, SENS_NU = range(5)
 COH_NONE, COH_BL, COH_BLNU, COH_XN, COH_XNNU, COH_OP, COH_OPNU, COH_OPAUG, COH_OPNUAUG = range(9)
 COH_TL, COH_TLNU, COH_STL, COH_STLNU = range(9, 13)   # trilinear and smoothed trilinear
 FUNC, JAC, FP32 = 1, 2, 4
@@ -36,7 +37,7 @@ EXPORTED = [
     "pg_get_sizes", "pg_device_bytes", "pg_get_pattern", "pg_get_nodes", "pg_assemble", "pg_assemble_device", "pg_residual_strains",
     "pg_device_outputs", "pg_set_stream", "pg_set_isv", "pg_get_isv", "pg_commit_isv",
     "pg_get_damage_zones", "pg_residual_norm", "pg_set_timing", "pg_kernel_times", "pg_set_macro_strain",
-    "pg_pcg_solve", "pg_homogenize", "pg_norm2_noalloc",
+    "pg_pcg_solve", "pg_homogenize", "pg_material_sensitivity", "pg_norm2_noalloc",
     "pg_batch_create", "pg_batch_assemble", "pg_batch_wait", "pg_batch_tune", "pg_batch_info",
     "pg_batch_last_error", "pg_batch_destroy",
 ]
@@ -105,6 +106,7 @@ def load_library(path: Optional[str] = None):
         "pg_set_macro_strain": (i32, [vp, p]),
         "pg_pcg_solve": (i32, [vp, vp, vp, i32, dbl, i32, p, p]),
         "pg_homogenize": (i32, [vp, vp, dbl, p]),
+        "pg_material_sensitivity": (i32, [vp, vp, i32, i32, vp, vp]),
         "pg_norm2_noalloc": (i32, [vp, ctypes.c_int64, vp, vp]),
         "pg_batch_create": (i32, [p, i32, ctypes.POINTER(vp)]),
         "pg_batch_assemble": (i32, [vp, p, p, i32]),
@@ -342,6 +344,12 @@ class Problem:
         out = np.zeros(7)
         self._check(load_library().pg_homogenize(self.h, ctypes.c_void_p(d_U), float(t_frac), _ptr(out)))
         return out[: (3 if self.dim == 2 else 6) + 1]
+
+    def material_sensitivity(self, d_U: int, material: int, param: int, d_dPf: int, d_dPp: int):
+        """dP_int/dp of parameter `param` (SENS_E .. SENS_NU) of `material` (0 matrix, 1 fiber)
+        at device displacements d_U, into the device vectors d_dPf (n_free) and d_dPp (n_const)."""
+        self._check(load_library().pg_material_sensitivity(self.h, ctypes.c_void_p(d_U), int(material), int(param),
+                                                           ctypes.c_void_p(d_dPf), ctypes.c_void_p(d_dPp)))
 
     def residual_norm(self) -> float:
         v = ctypes.c_double(0.0)

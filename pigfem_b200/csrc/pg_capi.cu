@@ -469,7 +469,8 @@ int pg_upload(pg_ctx* c) {
         const int st = s.sub_type[sb];
         const int nq = s.sub_qp_off[sb + 1] - s.sub_qp_off[sb];
         if (s.sub_qp_off[sb] != qp) return set_err(c, PG_ERR_STATE, "internal: quadrature offsets out of order");
-        const bool affine = (st == pg::SUB_TRI3 || st == pg::SUB_TET4);
+        // (a quad4 parent's gradients vary from point to point, so its sub-elements never merge)
+        const bool affine = (st == pg::SUB_TRI3 || st == pg::SUB_TET4) && s.etype != pg::QUAD4;
         if (affine) {
           double w = 0.0;
           for (int q = 0; q < nq; ++q) w += s.qp_wgt[qp + q];

@@ -68,6 +68,18 @@ struct pg_ctx {
   // fork, tiles done, (unused), first kernel done, general rows done, join
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   PcgWork pcg;
+  // material sensitivity pass (pg_sens.cu): made on its first call
+  struct SensWork {
+    bool ready = false;
+    double* uncut = nullptr;   // per element: NPE x DIM values
+    double* cut = nullptr;     // per cut-element node: DIM values
+    double* dD = nullptr;      // 2 materials x 5 parameters x 36
+    double* g = nullptr;       // the cut elements' point gradients (unmerged)
+    int* g_off = nullptr;
+    int* pt_off = nullptr;     // a call's point lists
+    double* pt_w = nullptr;
+    int* pt_g = nullptr;
+  } sens;
   double* d_hom = nullptr;  // homogenization partials
   // Device memory comes from the stream-ordered pool on this stream (cudaMallocAsync /
   // cudaFreeAsync): creating and destroying contexts does not synchronise the device, so other

@@ -617,6 +617,48 @@ int build_setup(const ProblemDesc& d, Setup& s) {
     }
   }
 
+  // ---------------- D sensitivities (src/material_lei.cpp:101-227): E, lambda, mu and K scale the
+  // D pattern by coefficients of nu; nu has its own expressions
+  for (int m = 0; m < 2; ++m) {
+    const double E = Es[m], nu = nus[m];
+    for (int p = 0; p < 5; ++p) for (int i = 0; i < 36; ++i) s.dD[m][p][i] = 0.0;
+    double coefs[4];
+    if (dim == 2 && !d.plane_strain) {
+      coefs[0] = 1.0 / (1.0 - nu * nu); coefs[1] = (1.0 - 2.0 * nu) / (nu * (1.0 - nu));
+      coefs[2] = 2.0 / (1.0 - nu); coefs[3] = 3.0 * (1.0 - 2.0 * nu) / (1.0 - nu * nu);
+    } else {
+      coefs[0] = 1.0 / ((1.0 + nu) * (1.0 - 2.0 * nu)); coefs[1] = 1.0 / nu;
+      coefs[2] = 2.0 / (1.0 - 2.0 * nu); coefs[3] = 3.0 / (1.0 + nu);
+    }
+    for (int p = 0; p < 4; ++p) {
+      double* Q = s.dD[m][p];
+      const double c = coefs[p];
+      if (dim == 2) {
+        if (d.plane_strain) { Q[0] = c * (1.0 - nu); Q[1] = c * nu; Q[3] = c * nu; Q[4] = c * (1.0 - nu); Q[8] = c * (1.0 - 2.0 * nu) / 2.0; }
+        else { Q[0] = c; Q[1] = c * nu; Q[3] = c * nu; Q[4] = c; Q[8] = c * (1.0 - nu) / 2.0; }
+      } else {
+        for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) Q[i * 6 + j] = (i == j) ? c * (1.0 - nu) : c * nu;
+        for (int i = 3; i < 6; ++i) Q[i * 6 + i] = c * (1.0 - 2.0 * nu) / 2;
+      }
+    }
+    double* Q = s.dD[m][4];
+    if (dim == 2 && !d.plane_strain) {
+      const double coef = E / (1.0 - nu * nu), dcoef = 2.0 * E * nu / std::pow(1.0 - nu * nu, 2);
+      Q[0] = dcoef; Q[1] = dcoef * nu + coef; Q[3] = dcoef * nu + coef; Q[4] = dcoef;
+      Q[8] = dcoef * (1.0 - nu) / 2.0 - 0.5 * coef;
+    } else {
+      const double coef = E / ((1.0 + nu) * (1.0 - 2.0 * nu));
+      const double dcoef = E * (1.0 + 4.0 * nu) / std::pow(1.0 - nu - 2.0 * nu * nu, 2);
+      if (dim == 2) {
+        Q[0] = dcoef * (1.0 - nu) - coef; Q[1] = dcoef * nu + coef; Q[3] = dcoef * nu + coef; Q[4] = dcoef * (1.0 - nu) - coef;
+        Q[8] = dcoef * (1.0 - 2.0 * nu) / 2.0 - coef;
+      } else {
+        for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) Q[i * 6 + j] = (i == j) ? dcoef * (1.0 - nu) - coef : dcoef * nu + coef;
+        for (int i = 3; i < 6; ++i) Q[i * 6 + i] = dcoef * (1.0 - 2.0 * nu) / 2.0 - coef;
+      }
+    }
+  }
+
   // ---------------- bounding plies: LinearElasticTransverselyIsotropicMaterial::computeLinearDmat
   // (src/material_leti.cpp:52-128): fibers along x, E3 = E2, G13 = G12, nu13 = nu12,
   // nu23 = E2 / (2 G23) - 1; the expressions and their order as the reference writes them

@@ -61,6 +61,9 @@ struct Setup {
   // elastic transversely isotropic); D in Voigt order, row-major
   int nvoigt = 3;
   double D[3][36];
+  // derivatives of D of materials 0 and 1 by E, lambda, mu, K and nu, as
+  // LinearElasticIsotropicMaterial::computeDmatSensitivities forms them (material sensitivities)
+  double dD[2][5][36];
 
   // nodes: standard nodes first, then enrichment nodes (cohesive mirrors after the originals)
   int n_std = 0, n_enr = 0, n_enr_initial = 0;

@@ -49,11 +49,18 @@ __host__ __device__ constexpr int tile2_slot(int cx, int cy, int sub) {
   return ((sub * 2 + (cx & 1)) * kTileCY + cy) * kTileHX + (cx >> 1);
 }
 
+// Stage word a of a 2D tile is stored at a ^ ((a >> 4) & 15): a permutation inside each aligned
+// group of 16 doubles.  The rows of consecutive same-class nodes sit 56 doubles apart, so without
+// it the lanes of a row store would meet in two bank pairs (8-way conflicts); with it the stores
+// are at most 3-way and the warp-wide reads of a segment at most 3-way.
+__host__ __device__ constexpr int tile2_swizzle(int a) { return a ^ ((a >> 4) & 15); }
+
 __host__ __device__ constexpr size_t tile2_smem_bytes() {
   // node data (x, u as two double2 arrays) then the record fields; the stage reuses the record area
   return (size_t)(4 * kTileNodes2 + kTileFields * kTileRecN) * sizeof(double);
 }
 static_assert(kTileFields * kTileRecN >= kTileY * kTileRowStage, "the stage fits the record area");
+static_assert((kTileY * kTileRowStage) % 16 == 0, "the swizzle stays inside the stage");
 
 // Tile descriptor: {first node i, first node j, first segment, segment count}; per own node (class
 // 0 nodes, then class 1) an entry {node id or -1, first free DOF, first CSR slot, stage offset};
@@ -184,27 +191,27 @@ __device__ __forceinline__ void stencil_tile2(const DevProblem& P, const GridInf
   __syncthreads();   // the records are consumed: the stage takes their place
   double* stage = rec;
   if (v.x >= 0) {
-    // the node's two rows, NN neighbour blocks each: [q][slot][d], one run of the CSR
+    // the node's two rows, NN neighbour blocks each: [q][slot][d], one run of the CSR; stage
+    // word a lives at tile2_swizzle(a)
     const int nn = cls0 ? Tri3Stencil0::NN : Tri3Stencil1::NN;
-    double* o = stage + v.w + q * nn * 2;
+    const int o = v.w + q * nn * 2;
 #pragma unroll
     for (int s = 0; s < Tri3Stencil0::NN; ++s)
-      if (s < nn) { o[s * 2] = acc[s][0]; o[s * 2 + 1] = acc[s][1]; }
+      if (s < nn) { stage[tile2_swizzle(o + s * 2)] = acc[s][0]; stage[tile2_swizzle(o + s * 2 + 1)] = acc[s][1]; }
   }
   __syncthreads();
   // D: contiguous segments, a warp per segment
   const int lane = t & 31, warp = t >> 5;
   for (int sg = warp; sg < td.w; sg += kTileThreads / 32) {
     const int4 seg = __ldg(&segs[td.z + sg]);
-    const double* src = stage + seg.x;
     double* dst = P.val[0] + seg.y;
-    for (int k = lane; k < seg.z; k += 32) dst[k] = src[k];
+    for (int k = lane; k < seg.z; k += 32) dst[k] = stage[tile2_swizzle(seg.x + k)];
   }
 }
 
 // One CTA per tile.
 template <typename T, bool JAC = true>
-__global__ void __launch_bounds__(kTileThreads) k_rows_tile2(DevProblem P, GridInfo gi, const int4* __restrict__ tiles,
+__global__ void __launch_bounds__(kTileThreads, 4) k_rows_tile2(DevProblem P, GridInfo gi, const int4* __restrict__ tiles,
                                                             const int4* __restrict__ tnodes, const int4* __restrict__ segs) {
   extern __shared__ double sm[];
   stencil_tile2<T, JAC>(P, gi, __ldg(&tiles[blockIdx.x]), tnodes + (size_t)blockIdx.x * kTileOwn, segs, sm);
