@@ -151,11 +151,18 @@ def general_kernel_bytes(P, fp32: bool) -> float:
     return float(total)
 
 
-def launches_per_step(P) -> int:
-    """Kernels one assembly launches: cohesive points, stencil rows and general rows, each only
-    when it has work (the L2 flush between steps is a torch fill, not counted)."""
+def launches_per_step(P, three_d: bool = False) -> int:
+    """Kernels one step launches (the L2 flush between steps is a torch fill, not counted).  An
+    assembly: k_gen_first (cohesive elements and the general rows' element records), the tiles
+    of the structured rows, k_gen_rows (the general rows), each only when it has work.  The 3D
+    step adds the multi-strain residual pass: its cohesive elements, structured rows and general
+    rows."""
     s = P.sizes
-    return int(s["n_coh_qp"] > 0) + int(len(P.debug("fast_dn")) > 0) + int(len(P.debug("slow_dn")) > 0)
+    fast, slow = len(P.debug("fast_dn")) > 0, len(P.debug("slow_dn")) > 0
+    n = int(s["n_coh_qp"] > 0 or slow) + int(fast) + int(slow)
+    if three_d:
+        n += int(s["n_coh_qp"] > 0) + int(fast) + int(slow)
+    return n
 
 
 class Clocks:
@@ -790,46 +797,58 @@ def main():
         hRf = torch.empty(max(1, dRf.numel()), dtype=torch.float64).pin_memory()
         hRp = torch.empty(max(1, dRp.numel()), dtype=torch.float64).pin_memory()
 
-    def step_host():
+    # keep: the caller's K arrays keep the values of the previous call (PG_KEEP_STATIC), so only
+    # the values that can change come back; the first call of each mode copies everything
+    first = P.changing_values()
+
+    def step_host(keep: bool, full_copy: bool):
         if not three_d:
-            P.assemble(hU_np, 1.0, capi.FUNC | capi.JAC, out=out_np)
+            P.assemble(hU_np, 1.0, capi.FUNC | capi.JAC | (capi.KEEP_STATIC if keep else 0), out=out_np)
             return
-        # U in once; K and R of the first strain, the five other residuals in one pass; K and the
-        # six residuals out
+        # U in once; K and R of the first strain, the five other residuals in one pass; K (or
+        # its changing values) and the six residuals out
         dU.copy_(hU, non_blocking=True)
         P.set_macro_strain(UNIT_STRAINS_3D[0])
         P.assemble_device(dU.data_ptr(), 1.0, capi.FUNC | capi.JAC)
         P.residual_strains(dU.data_ptr(), UNIT_STRAINS_3D[1:], dRf.data_ptr(), dRp.data_ptr() if P.n_const else 0)
         K4, pf, pp = P.device_outputs()
         for i, b in enumerate(("ff", "fp", "pf", "pp")):
-            if P.nnz[i]:
-                outs[f"K_{b}"][:P.nnz[i]].copy_(capi.device_view(K4[i], P.nnz[i]), non_blocking=True)
+            lo = 0 if full_copy else first[i]
+            if P.nnz[i] > lo:
+                outs[f"K_{b}"][lo:P.nnz[i]].copy_(capi.device_view(K4[i], P.nnz[i])[lo:], non_blocking=True)
         outs["P_f"][:P.n_free].copy_(capi.device_view(pf, P.n_free), non_blocking=True)
         if P.n_const:
             outs["P_p"][:P.n_const].copy_(capi.device_view(pp, P.n_const), non_blocking=True)
             hRp[:dRp.numel()].copy_(dRp, non_blocking=True)
         hRf[:dRf.numel()].copy_(dRf, non_blocking=True)
 
-    for _ in range(args.warmup):
-        step_host()
-    torch.cuda.synchronize()
-    replicas.barrier()
-    e2e_ms = 0.0
-    for _ in range(args.e2e_steps or args.steps):
-        flush.zero_()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        step_host()
-        b.record(stream)
-        b.synchronize()
-        e2e_ms += a.elapsed_time(b)
-    e2e_ms = replicas.max_over_ranks([e2e_ms], "cuda")[0]
+    def e2e_run(keep: bool):
+        # warm-up: the first call copies every value (and fills the kept arrays)
+        for w in range(args.warmup):
+            step_host(keep, full_copy=(not keep) or w == 0)
+        torch.cuda.synchronize()
+        replicas.barrier()
+        ms = 0.0
+        for _ in range(args.e2e_steps or args.steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step_host(keep, full_copy=not keep)
+            b.record(stream)
+            b.synchronize()
+            ms += a.elapsed_time(b)
+        return replicas.max_over_ranks([ms], "cuda")[0]
+
+    e2e_full_ms = e2e_run(False)
+    e2e_ms = e2e_run(True)
     clk.__exit__(None, None, None)
     e2e_steps = args.e2e_steps or args.steps
     e2e_value = ws * ne * e2e_steps / (e2e_ms * 1e-3)
+    e2e_full_value = ws * ne * e2e_steps / (e2e_full_ms * 1e-3)
     n_rhs = 6 if three_d else 1
     h2d = U.nbytes
-    d2h = 8 * (sum(P.nnz) + n_rhs * (P.n_free + P.n_const))
+    d2h_full = 8 * (sum(P.nnz) + n_rhs * (P.n_free + P.n_const))
+    d2h = 8 * (sum(max(0, P.nnz[i] - first[i]) for i in range(4)) + n_rhs * (P.n_free + P.n_const))
 
     batched = None
     if args.workload == "cohesive_2d_512" and not args.no_batched:
@@ -879,9 +898,14 @@ def main():
                                  "frac": (g_achieved / peak) if g_achieved else None,
                                  "traffic": profiled_traffic(general_name), "bytes_per_launch": gk_bytes},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": e2e_ms / e2e_steps, "steps": e2e_steps},
+                    "ms_per_step": e2e_ms / e2e_steps, "steps": e2e_steps,
+                    "mode": "PG_KEEP_STATIC: the caller's host K arrays keep the previous call's values; every step "
+                            "copies U in and, out, the K values that can change (rows of DOFs on cohesive elements) "
+                            "and all residuals",
+                    "full_copy": {"value": e2e_full_value, "ms_per_step": e2e_full_ms / e2e_steps,
+                                  "d2h_bytes_per_step": d2h_full}},
             # 3D: the K-and-R assembly and the multi-strain pass launch the same set of kernels
-            "gpu_launches": launches_per_step(P) * (2 if three_d else 1) * args.steps,
+            "gpu_launches": launches_per_step(P, three_d) * args.steps,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "batched": batched,

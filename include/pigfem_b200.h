@@ -34,6 +34,12 @@ extern "C" {
 #define PG_FUNC 1   /* assemble the internal-force vector P_int (assembleFunc) */
 #define PG_JAC 2    /* assemble the stiffness K (assembleJac) */
 #define PG_FP32 4   /* FP32-mixed element integration (FP64 accumulation in the scatter) */
+/* pg_assemble only: the host K arrays still hold what this context's previous PG_JAC |
+ * PG_KEEP_STATIC call with the same arrays and precision wrote there (the caller did not change
+ * them), so only the values that can have changed since are copied back: the suffix of each
+ * block from pg_changing_values on (the rows of the DOFs of nodes on cohesive elements; nothing
+ * for a problem without cohesive elements).  The first such call copies everything. */
+#define PG_KEEP_STATIC 8
 
 /* background element types (Mesh::generate_mesh element types used by the reference drivers) */
 #define PG_TRI3 0
@@ -139,6 +145,11 @@ int pg_assemble_device(pg_ctx* ctx, const double* d_U, double t_frac, int flags)
 int pg_residual_strains(pg_ctx* ctx, const double* d_U, double t_frac, int n_cases, const double* eps,
                         double* d_Rf, double* d_Rp);
 /* Device pointers of the outputs: K values (4 blocks), P_f, P_p. */
+/* The first CSR value of each K block (ff, fp, pf, pp) from which a later assembly of this
+ * context can change values; nnz of the block when none can.  Every bulk law is linear elastic,
+ * so only the entries coupling DOFs of nodes on one cohesive element depend on the state, and
+ * they lie in the rows from the smallest such DOF on. */
+int pg_changing_values(const pg_ctx* ctx, int64_t* first);
 int pg_device_outputs(pg_ctx* ctx, double** K_vals4, double** P_f, double** P_p);
 /* Stream the context launches on (a cudaStream_t, 0 = legacy default). */
 int pg_set_stream(pg_ctx* ctx, void* stream);

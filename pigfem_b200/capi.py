@@ -27,7 +27,7 @@ TRI3, QUAD4, TET4 = 0, 1, 2
 SENS_E, SENS_LAMBDA, SENS_MU, SENS_K, SENS_NU = range(5)
 COH_NONE, COH_BL, COH_BLNU, COH_XN, COH_XNNU, COH_OP, COH_OPNU, COH_OPAUG, COH_OPNUAUG = range(9)
 COH_TL, COH_TLNU, COH_STL, COH_STLNU = range(9, 13)   # trilinear and smoothed trilinear
-FUNC, JAC, FP32 = 1, 2, 4
+FUNC, JAC, FP32, KEEP_STATIC = 1, 2, 4, 8
 ERRORS = {2: "PG_ERR_INPUT", 3: "PG_ERR_GEOMETRY", 4: "PG_ERR_UNSUPPORTED", 7: "PG_ERR_JACOBIAN",
           10: "PG_ERR_DEVICE", 11: "PG_ERR_NONFINITE", 12: "PG_ERR_STATE"}
 
@@ -35,7 +35,7 @@ ERRORS = {2: "PG_ERR_INPUT", 3: "PG_ERR_GEOMETRY", 4: "PG_ERR_UNSUPPORTED", 7: "
 EXPORTED = [
     "pg_create", "pg_create_host", "pg_upload", "pg_debug_array", "pg_destroy", "pg_last_error",
     "pg_get_sizes", "pg_device_bytes", "pg_get_pattern", "pg_get_nodes", "pg_assemble", "pg_assemble_device", "pg_residual_strains",
-    "pg_device_outputs", "pg_set_stream", "pg_set_isv", "pg_get_isv", "pg_commit_isv",
+    "pg_device_outputs", "pg_changing_values", "pg_set_stream", "pg_set_isv", "pg_get_isv", "pg_commit_isv",
     "pg_get_damage_zones", "pg_residual_norm", "pg_set_timing", "pg_kernel_times", "pg_set_macro_strain",
     "pg_pcg_solve", "pg_homogenize", "pg_material_sensitivity", "pg_norm2_noalloc",
     "pg_batch_create", "pg_batch_assemble", "pg_batch_wait", "pg_batch_tune", "pg_batch_info",
@@ -95,6 +95,7 @@ def load_library(path: Optional[str] = None):
         "pg_assemble_device": (i32, [vp, p, dbl, i32]),
         "pg_residual_strains": (i32, [vp, vp, dbl, i32, p, vp, vp]),
         "pg_device_outputs": (i32, [vp, p, p, p]),
+        "pg_changing_values": (i32, [vp, p]),
         "pg_set_stream": (i32, [vp, vp]),
         "pg_set_isv": (i32, [vp, p]),
         "pg_get_isv": (i32, [vp, i32, p]),
@@ -224,6 +225,12 @@ class Problem:
         self.dim = s.dim
         self.n_nodes, self.n_free, self.n_const, self.n_isv = s.n_nodes, s.n_free, s.n_const, s.n_isv
         self.nnz = self.sizes["nnz"]
+
+    def changing_values(self):
+        """First CSR value of each K block from which a later assembly can change values."""
+        v = np.zeros(4, np.int64)
+        self._check(load_library().pg_changing_values(self.h, _ptr(v)))
+        return [int(x) for x in v]
 
     def device_bytes(self):
         """(bytes held now, most bytes held at once) of this context's device allocations."""

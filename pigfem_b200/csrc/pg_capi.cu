@@ -636,6 +636,30 @@ int pg_upload(pg_ctx* c) {
     PG_TRY(upload(c, s.rp[b], &P.rp[b]));
     PG_TRY(dalloc(c, s.ci[b].size(), &P.val[b]));
   }
+  // The values a later assembly can change (PG_KEEP_STATIC, pg_changing_values): every bulk law
+  // is linear elastic, so only the entries coupling DOFs of nodes on one cohesive element depend
+  // on the state; each block's changing values lie in the rows from the smallest such DOF on.
+  {
+    int fmin = s.n_free, pmin = s.n_const;
+    for (int cc = 0; cc < s.ncut; ++cc)
+      for (int ce = s.cut_coh_off[cc]; ce < s.cut_coh_off[cc + 1]; ++ce)
+        for (int q = s.coh_local_off[ce]; q < s.coh_local_off[ce + 1]; ++q) {
+          const int node = s.cut_nodes[s.cut_node_off[cc] + s.coh_local[q]];
+          for (int d = 0; d < dim; ++d) {
+            const int dof = s.node_dof[(size_t)node * dim + d];
+            if (dof < s.n_free) fmin = std::min(fmin, dof);
+            else pmin = std::min(pmin, dof - s.n_free);
+          }
+        }
+    const bool fr = fmin < s.n_free, pr = pmin < s.n_const;
+    long long nnz[4];
+    for (int b = 0; b < 4; ++b) nnz[b] = (long long)s.ci[b].size();
+    c->changing_from[0] = fr ? s.rp[0][fmin] : nnz[0];
+    c->changing_from[1] = (fr && pr) ? s.rp[1][fmin] : nnz[1];
+    c->changing_from[2] = (fr && pr) ? s.rp[2][pmin] : nnz[2];
+    c->changing_from[3] = pr ? s.rp[3][pmin] : nnz[3];
+    c->kept_valid = false;
+  }
   PG_TRY(dalloc(c, (size_t)s.n_free, &P.Pf));
   PG_TRY(dalloc(c, (size_t)s.n_const, &P.Pp));
   PG_TRY(dalloc(c, (size_t)n_nodes * dim, &c->d_U));
@@ -925,10 +949,27 @@ int pg_assemble(pg_ctx* c, const double* U, double t_frac, int flags, double* Kf
   cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
   PG_TRY(launch(c, t_frac, flags));
   double* outs[4] = {Kff, Kfp, Kpf, Kpp};
-  if (flags & PG_JAC)
-    for (int b = 0; b < 4; ++b)
-      if (outs[b] && !s.ci[b].empty())
-        cudaMemcpyAsync(outs[b], c->P.val[b], s.ci[b].size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (flags & PG_JAC) {
+    // PG_KEEP_STATIC with the same host arrays and precision as the last full copy: only the
+    // values that can have changed since (a suffix of each block) go back
+    const bool fp32 = (flags & PG_FP32) != 0;
+    bool keep = (flags & PG_KEEP_STATIC) && c->kept_valid && c->kept_fp32 == fp32;
+    for (int b = 0; b < 4; ++b) keep = keep && outs[b] == c->kept[b];
+    for (int b = 0; b < 4; ++b) {
+      if (!outs[b] || s.ci[b].empty()) continue;
+      const long long from = keep ? c->changing_from[b] : 0, nnz = (long long)s.ci[b].size();
+      if (from < nnz)
+        cudaMemcpyAsync(outs[b] + from, c->P.val[b] + from, (size_t)(nnz - from) * sizeof(double), cudaMemcpyDeviceToHost,
+                        c->stream);
+    }
+    if (flags & PG_KEEP_STATIC) {
+      for (int b = 0; b < 4; ++b) c->kept[b] = outs[b];
+      c->kept_fp32 = fp32;
+      c->kept_valid = true;
+    } else {
+      c->kept_valid = false;
+    }
+  }
   if (flags & PG_FUNC) {
     if (Pf && s.n_free) cudaMemcpyAsync(Pf, c->P.Pf, (size_t)s.n_free * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     if (Pp && s.n_const) cudaMemcpyAsync(Pp, c->P.Pp, (size_t)s.n_const * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
@@ -940,6 +981,12 @@ int pg_assemble(pg_ctx* c, const double* U, double t_frac, int flags, double* Kf
   c->assembled = true;
   if (herr & pgd::ERR_NONFINITE) return set_err(c, PG_ERR_NONFINITE, "non-finite value in a cut-element matrix or vector");
   if (herr) return set_err(c, PG_ERR_DEVICE, "scatter map inconsistency detected on the device");
+  return 0;
+}
+
+int pg_changing_values(const pg_ctx* c, int64_t* first) {
+  if (!c || !first) return PG_ERR_INPUT;
+  for (int b = 0; b < 4; ++b) first[b] = (int64_t)c->changing_from[b];
   return 0;
 }
 

@@ -47,6 +47,12 @@ struct pg_ctx {
   int maxnb_fast = 0;
   int n_coh_qp = 0;
   bool assembled = false;
+  // PG_KEEP_STATIC: the first CSR value of each block from which a later assembly can change
+  // values (the rows of DOFs of nodes on cohesive elements; nnz when no value can change), and
+  // the host arrays (and precision) the last full copy of K went to
+  long long changing_from[4] = {0, 0, 0, 0};
+  double* kept[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool kept_fp32 = false, kept_valid = false;
   std::vector<int> fast_dn, slow_dn;
   int tile_nodes = 128;
   int max_cut_qp = 1, max_cut_nodes = 1;

@@ -259,3 +259,39 @@ def test_residual_strains_need_a_subscale_problem():
     with pytest.raises(capi.PigfemError):
         P.residual_strains(U.data_ptr(), [[0.01, 0.0, 0.0]], R.data_ptr(), R.data_ptr())
     P.close()
+
+
+@pytest.mark.parametrize("name", ["coh_op", "coh_tet4_bl", "coh_quad4_bl", "lin_tri3_three_fibers", "lin_tet4_subscale"])
+def test_keep_static_copies_back_what_changes(name):
+    """PG_KEEP_STATIC: with the host K arrays of the previous call kept, a call copies back only
+    the suffix of each block from pg_changing_values on, and the arrays then hold bitwise the K
+    of a full copy at the new state.  Problems without cohesive elements change no K value."""
+    from pigfem_b200 import capi
+    g = load_case(name)
+    P = build(name)
+    first = P.changing_values()
+    if CASES[name]["coh_law"] == 0:
+        assert first == list(P.nnz)
+    else:
+        assert first[0] < P.nnz[0]
+    if P.n_isv:
+        P.set_isv(g["isv_committed"])
+    U = g["U_dof"][g["node_dofs"]]
+    # a proportionally larger state: every opening grows by 5 % (a random change could push the
+    # bilinear law into its compression branch, whose sinh overflows at these openings)
+    U2 = 1.05 * U
+    keep = {f"K_{b}": np.full(max(P.nnz[i], 1), np.nan) for i, b in enumerate(("ff", "fp", "pf", "pp"))}
+    keep["P_f"] = np.zeros(max(P.n_free, 1))
+    keep["P_p"] = np.zeros(max(P.n_const, 1))
+    flags = capi.FUNC | capi.JAC | capi.KEEP_STATIC
+    P.assemble(U, 1.0, flags, out=keep)          # first call: everything
+    # poison the part a keep call must rewrite, then assemble at the new state
+    for i, b in enumerate(("ff", "fp", "pf", "pp")):
+        keep[f"K_{b}"][first[i]:P.nnz[i]] = np.nan
+    got = P.assemble(U2, 1.0, flags, out=keep)
+    full = P.assemble(U2, 1.0, capi.FUNC | capi.JAC)
+    for k in ("K_ff", "K_fp", "K_pf", "K_pp", "P_f", "P_p"):
+        assert np.array_equal(got[k], full[k]), k
+    if CASES[name]["coh_law"]:
+        # the state does change K inside the copied suffix
+        assert not np.array_equal(full["K_ff"], P.assemble(U, 1.0, capi.FUNC | capi.JAC)["K_ff"])
