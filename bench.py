@@ -260,6 +260,26 @@ def build_problem(args, rank, device=True):
 UNIT_STRAINS_3D = [tuple(1.0 if i == k else 0.0 for i in range(6)) for k in range(6)]
 
 
+def setup_times(R) -> dict:
+    """Wall time of the set-up of R's mesh (host-only context, no upload) with every pass on the
+    host (pg_create_host) and with the per-node / per-element passes on the device
+    (pg_create_prep_device); each the best of two, outside the timed region."""
+    from pigfem_b200 import capi
+    out = {}
+    for key, prep in (("host_s", False), ("device_prep_s", True)):
+        best = None
+        for _ in range(2):
+            t = time.perf_counter()
+            Q = capi.Problem(R.desc, device=False, prep_device=prep)
+            dt = time.perf_counter() - t
+            if prep:
+                out["device_passes_ms"] = Q.prep_device_ms()
+            Q.close()
+            best = dt if best is None else min(best, dt)
+        out[key] = best
+    return out
+
+
 def reference_problem(R, P, U):
     """The reference's own Problem (oracle/_ref) for the same RVE and state as this library's
     problem P; returns it and the DOF vector (free then constrained) of U."""
@@ -771,10 +791,12 @@ def main():
         kt = np.zeros(4)
         if three_d:
             P.set_macro_strain(UNIT_STRAINS_3D[0])
+        P.set_timing(True)
         for _ in range(reps):
             flush.zero_()
             P.assemble_device(dU.data_ptr(), 1.0, flags)
             kt += P.kernel_times()
+        P.set_timing(False)
         return kt / reps
 
     clk = Clocks(local).__enter__()
@@ -875,6 +897,7 @@ def main():
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline(args, R, P, U, out_np)
+        setup = setup_times(R)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms64 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -909,6 +932,7 @@ def main():
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "batched": batched,
+            "setup": setup,
         }
     replicas.finish()
     if line is not None:

@@ -103,6 +103,17 @@ int pg_create(const pg_problem_desc* desc, pg_ctx** out);
  * set-up tables can be read back) and the upload that makes the context assemble-ready. */
 int pg_create_host(const pg_problem_desc* desc, pg_ctx** out);
 int pg_upload(pg_ctx* ctx);
+/* pg_create_host with the set-up's per-node and per-element passes on the current CUDA device:
+ * node detection (Mesh::detect_node, src/Mesh.cpp:2727-2929), the all-equal element test of the
+ * element detection (Tri3/Quad4/Tet4::detection), the enrichment nodes and their intersection
+ * points (Mesh::add_enrichments, src/Mesh.cpp:3103-3252; Inclusion::find_intersection,
+ * src/Inclusion.cpp:32-121) and the standard nodes' DOF numbering (DofObject::
+ * set_local_owned_normal_dofs, src/DofObject.cpp:336-385).  Every table is the one pg_create_host
+ * forms (integers bit-exact, coordinates too); the context is host-only until pg_upload.  Grids
+ * of fewer than 2 cells per direction run every pass on the host. */
+int pg_create_prep_device(const pg_problem_desc* desc, pg_ctx** out);
+/* Device time in ms of the passes pg_create_prep_device ran (-1 when none ran). */
+int pg_prep_device_ms(const pg_ctx* ctx, double* ms);
 /* Read-only view of a set-up table by name (cut-element quadrature, topology); returns 1 for
  * int32, 2 for float64, 0 for an unknown name.  For tests and tools. */
 int pg_debug_array(const pg_ctx* ctx, const char* name, int64_t* n, const void** ptr);
@@ -155,11 +166,12 @@ int pg_device_outputs(pg_ctx* ctx, double** K_vals4, double** P_f, double** P_p)
 int pg_set_stream(pg_ctx* ctx, void* stream);
 
 /* Device timing of the last assembly from CUDA events the context records on its streams:
- * ms[0] cohesive elements, ms[1] stencil rows (2D: side stream, concurrent with ms[0] and ms[2];
- * 3D: after ms[0]), ms[2] general rows (2D: the longer of the rows on cohesive elements, after
- * ms[0], and the other general rows, on their own stream from the start; 3D: after ms[1]),
- * ms[3] the whole assembly (fork to join).  pg_set_timing is kept for callers
- * that toggle it; the events are always recorded. */
+ * ms[0] cohesive elements and element records, ms[1] stencil rows (2D: side stream, concurrent
+ * with ms[0] and ms[2]; 3D: after ms[0]), ms[2] general rows (2D: after ms[0]; 3D: after ms[1]),
+ * ms[3] the whole assembly (fork to join).  The event between ms[0] and ms[2] is recorded only
+ * while timing is on (pg_set_timing(ctx, 1)): without it the general rows start early, while the
+ * kernel before them finishes.  pg_kernel_times returns PG_ERR_STATE when the last assembly ran
+ * with timing off. */
 int pg_set_timing(pg_ctx* ctx, int on);
 int pg_kernel_times(pg_ctx* ctx, float* ms);
 

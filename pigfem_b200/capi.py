@@ -33,7 +33,7 @@ ERRORS = {2: "PG_ERR_INPUT", 3: "PG_ERR_GEOMETRY", 4: "PG_ERR_UNSUPPORTED", 7: "
 
 # Every symbol include/pigfem_b200.h declares.
 EXPORTED = [
-    "pg_create", "pg_create_host", "pg_upload", "pg_debug_array", "pg_destroy", "pg_last_error",
+    "pg_create", "pg_create_host", "pg_create_prep_device", "pg_prep_device_ms", "pg_upload", "pg_debug_array", "pg_destroy", "pg_last_error",
     "pg_get_sizes", "pg_device_bytes", "pg_get_pattern", "pg_get_nodes", "pg_assemble", "pg_assemble_device", "pg_residual_strains",
     "pg_device_outputs", "pg_changing_values", "pg_set_stream", "pg_set_isv", "pg_get_isv", "pg_commit_isv",
     "pg_get_damage_zones", "pg_residual_norm", "pg_set_timing", "pg_kernel_times", "pg_set_macro_strain",
@@ -83,6 +83,8 @@ def load_library(path: Optional[str] = None):
     sig = {
         "pg_create": (i32, [ctypes.POINTER(_Desc), ctypes.POINTER(vp)]),
         "pg_create_host": (i32, [ctypes.POINTER(_Desc), ctypes.POINTER(vp)]),
+        "pg_create_prep_device": (i32, [ctypes.POINTER(_Desc), ctypes.POINTER(vp)]),
+        "pg_prep_device_ms": (i32, [vp, ctypes.POINTER(ctypes.c_double)]),
         "pg_upload": (i32, [vp]),
         "pg_debug_array": (i32, [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(vp)]),
         "pg_destroy": (None, [vp]),
@@ -169,7 +171,9 @@ class ProblemDesc:
 class Problem:
     """One enriched mesh resident on the GPU (a ``pg_ctx``)."""
 
-    def __init__(self, desc: ProblemDesc, device: bool = True):
+    def __init__(self, desc: ProblemDesc, device: bool = True, prep_device: bool = False):
+        """``prep_device``: run the set-up's node detection, element pass, enrichment nodes and
+        standard DOF numbering on the GPU (pg_create_prep_device); the tables are the same."""
         L = load_library()
         self.desc = desc
         dim = desc.dim
@@ -196,7 +200,8 @@ class Problem:
             d.ply[i] = v
         self._d = d
         h = ctypes.c_void_p(0)
-        rc = L.pg_create_host(ctypes.byref(d), ctypes.byref(h))
+        create = L.pg_create_prep_device if prep_device else L.pg_create_host
+        rc = create(ctypes.byref(d), ctypes.byref(h))
         self.h = h
         if rc:
             msg = L.pg_last_error(h).decode() if h.value else "invalid description"
@@ -252,6 +257,12 @@ class Problem:
         dir_ = np.zeros(max(self.n_const, 1))
         self._check(load_library().pg_get_nodes(self.h, _ptr(X), _ptr(dofs), _ptr(dir_)))
         return X.reshape(-1, self.dim), dofs.reshape(-1, self.dim), dir_[: self.n_const]
+
+    def prep_device_ms(self) -> float:
+        """Device time of the preprocessing passes (-1 when the set-up ran on the host alone)."""
+        ms = ctypes.c_double(0.0)
+        self._check(load_library().pg_prep_device_ms(self.h, ctypes.byref(ms)))
+        return float(ms.value)
 
     def debug(self, name: str) -> np.ndarray:
         n = ctypes.c_int64(0)

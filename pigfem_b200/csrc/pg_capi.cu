@@ -110,7 +110,7 @@ int pg_alloc_sync(pg_ctx* c) {
 
 extern "C" {
 
-int pg_create_host(const pg_problem_desc* d, pg_ctx** out) {
+static int create_host(const pg_problem_desc* d, pg_ctx** out, bool device_prep) {
   if (!d || !out) return PG_ERR_INPUT;
   *out = nullptr;
   pg_ctx* c = new pg_ctx;
@@ -128,10 +128,26 @@ int pg_create_host(const pg_problem_desc* d, pg_ctx** out) {
   pd.app_strain = d->app_strain;
   pd.ply_frac = d->ply_frac;
   for (int i = 0; i < 5; ++i) pd.ply[i] = d->ply[i];
-  int rc = pg::build_setup(pd, c->s);
+  pg::PrepResult pr;
+  if (device_prep) {
+    std::string why;
+    if (pg::device_prep(pd, pr, why)) { c->err = why; *out = c; return PG_ERR_DEVICE; }
+    c->prep_ms = pr.valid ? pr.device_ms : -1.0;
+  }
+  int rc = pg::build_setup(pd, c->s, device_prep ? &pr : nullptr);
   if (rc) { c->err = c->s.error; *out = c; return rc == 2 ? PG_ERR_INPUT : (rc == 4 ? PG_ERR_UNSUPPORTED : (rc == 7 ? PG_ERR_JACOBIAN : PG_ERR_GEOMETRY)); }
   c->n_coh_qp = (int)c->s.cqp_wgt.size();
   *out = c;
+  return 0;
+}
+
+int pg_create_host(const pg_problem_desc* d, pg_ctx** out) { return create_host(d, out, false); }
+
+int pg_create_prep_device(const pg_problem_desc* d, pg_ctx** out) { return create_host(d, out, true); }
+
+int pg_prep_device_ms(const pg_ctx* c, double* ms) {
+  if (!c || !ms) return PG_ERR_INPUT;
+  *ms = c->prep_ms;
   return 0;
 }
 
@@ -828,6 +844,7 @@ int pg_set_timing(pg_ctx* c, int on) {
 
 int pg_kernel_times(pg_ctx* c, float* ms) {
   if (!c || !ms || !c->ev[0]) return set_err(c, PG_ERR_STATE, "nothing was launched");
+  if (!c->timed_last) return set_err(c, PG_ERR_STATE, "the last assembly ran with timing off (pg_set_timing)");
   if (cudaEventSynchronize(c->ev[5]) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "event wait failed");
   // [0] cohesive elements and element records, [1] stencil rows (2D: from the start, on their
   // own stream, concurrent with [0] and [2]; 3D: after [0]), [2] general rows (after [0] in 2D,

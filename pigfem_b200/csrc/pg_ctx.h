@@ -47,6 +47,8 @@ struct pg_ctx {
   int maxnb_fast = 0;
   int n_coh_qp = 0;
   bool assembled = false;
+  bool timed_last = false;   // the last assembly recorded every timing event (pg_kernel_times)
+  double prep_ms = -1.0;   // device time of the preprocessing passes (pg_create_prep_device), -1 if none ran
   // PG_KEEP_STATIC: the first CSR value of each block from which a later assembly can change
   // values (the rows of DOFs of nodes on cohesive elements; nnz when no value can change), and
   // the host arrays (and precision) the last full copy of K went to

@@ -38,6 +38,14 @@ struct GenRec {
 template <int DIM>
 __host__ __device__ constexpr int gen_fields() { return GenRec<DIM>::STRIDE; }
 
+// Programmatic dependent launch: k_gen_rows may start while the kernel before it in the stream
+// (k_gen_first in 2D, the tiles in 3D) still runs; griddepcontrol.wait returns once that grid has
+// completed and its writes are visible (at once when the launch had no such dependency), so
+// everything read after it -- the cohesive blocks and the element records -- is complete.
+__device__ __forceinline__ void dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Lets the dependent grid launch now (its blocks then do their independent loads).
+__device__ __forceinline__ void dep_launch() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
 template <int DIM>
 __device__ __forceinline__ void gen_record(const DevProblem& P, int r) {
   constexpr int NPE = DIM + 1;
@@ -84,6 +92,15 @@ __device__ __forceinline__ void gen_block(const DevProblem& P, int b) {
   const int ul1 = __ldg(&P.gblk[b + 1].w);
   const int cl0 = __ldg(&P.gblk_cl[b]), cl1 = __ldg(&P.gblk_cl[b + 1]);
   const int node = bd.x, slot = bd.y;
+  // the destination of the block's values depends on the descriptor alone: its loads are issued
+  // before the sums, so they overlap the loads of the terms
+  const int4 gd = __ldg(&P.gdesc[node]);
+  const int mk = __ldg(&P.dn_nbr_mask[gd.z + slot]);
+  const int pre = __ldg(&P.nbr_pre[gd.z + slot]);
+  const int* rd = P.growd + (size_t)node * 3 * DIM;
+  int rrow[DIM], rF[DIM], rC[DIM];
+#pragma unroll
+  for (int q = 0; q < DIM; ++q) { rrow[q] = __ldg(&rd[q]); rF[q] = __ldg(&rd[DIM + q]); rC[q] = __ldg(&rd[2 * DIM + q]); }
   double acc[D2];
   if (bd.z >= 0) {
     const double* S = P.stat + (size_t)bd.z * D2;
@@ -93,6 +110,7 @@ __device__ __forceinline__ void gen_block(const DevProblem& P, int b) {
 #pragma unroll
     for (int i = 0; i < D2; ++i) acc[i] = 0.0;
   }
+  dep_wait();   // the cohesive blocks and element records below come from k_gen_first
 #pragma unroll 2
   for (int j = cl0; j < cl1; ++j) {
     const int c = __ldg(&P.gcl[j]);
@@ -121,15 +139,11 @@ __device__ __forceinline__ void gen_block(const DevProblem& P, int b) {
   }
   // the block's values: row q of the node, columns of the slot's DOFs (free ones in the row's F
   // block, constrained ones in its C block)
-  const int4 gd = __ldg(&P.gdesc[node]);
-  const int mk = __ldg(&P.dn_nbr_mask[gd.z + slot]);
-  const int pre = __ldg(&P.nbr_pre[gd.z + slot]);
-  const int* rd = P.growd + (size_t)node * 3 * DIM;
 #pragma unroll
   for (int q = 0; q < DIM; ++q) {
-    const bool rf = __ldg(&rd[q]) < P.n_free;
-    double* vF = P.val[rf ? 0 : 2] + __ldg(&rd[DIM + q]) + pre;
-    double* vC = P.val[rf ? 1 : 3] + __ldg(&rd[2 * DIM + q]) + (slot * DIM - pre);
+    const bool rf = rrow[q] < P.n_free;
+    double* vF = P.val[rf ? 0 : 2] + rF[q] + pre;
+    double* vC = P.val[rf ? 1 : 3] + rC[q] + (slot * DIM - pre);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
       if (mk & (1 << d)) *vF++ = acc[q * DIM + d];
@@ -143,12 +157,54 @@ __device__ __forceinline__ void gen_block(const DevProblem& P, int b) {
 // tractions and the uncut elements in adjacency order -- so the result does not depend on L.
 // `valid` is uniform over the group.
 template <int DIM, int L>
+__device__ __forceinline__ void gen_traction(const DevProblem& P, int j, int j1, double* tk) {
+#pragma unroll
+  for (int q = 0; q < DIM; ++q) tk[q] = 0.0;
+  if (j < j1) {
+    const int c = __ldg(&P.gnode_tl[j]);
+    const double sgn = (c & 1) ? -1.0 : 1.0;
+    const double* tp = P.kcoh + (c >> 1);
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) tk[q] = sgn * tp[q];
+  }
+}
+template <int DIM, int L>
+__device__ __forceinline__ void gen_uncut_force(const DevProblem& P, int j, int j1, double* rv) {
+  constexpr int NV = (DIM == 2) ? 3 : 6;
+  using R = GenRec<DIM>;
+#pragma unroll
+  for (int q = 0; q < DIM; ++q) rv[q] = 0.0;
+  if (j < j1) {
+    const int c = __ldg(&P.gnode_ul[j]);
+    const int rec = c >> 2, la = c & 3;
+    const double* o = P.grec + (size_t)rec * R::STRIDE;
+    double ga[DIM], sig[NV];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) ga[d] = o[la * DIM + d];
+    const double w = o[R::W];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) sig[v] = o[R::SIG + v];
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) rv[q] = w * bt_sig<DIM, double>(ga, sig, q);
+  }
+}
+
+// Residual of general node `node` by a group of L lanes (lane g): each part's terms are formed in
+// parallel and summed in a fixed order with shuffles -- the static part in slot order, then the
+// tractions and the uncut elements in adjacency order -- so the result does not depend on L.  The
+// static part reads set-up data and U only, so it is summed before the wait for the kernel that
+// forms the cohesive blocks and element records (a programmatic dependent launch: see
+// k_gen_rows).  `valid` is uniform over the group.
+template <int DIM, int L>
 __device__ __forceinline__ void gen_resid(const DevProblem& P, int node, bool valid) {
   constexpr int NV = (DIM == 2) ? 3 : 6;
-  if (!valid) return;
-  using R = GenRec<DIM>;
+  if (!valid) { dep_wait(); return; }
   const int g = threadIdx.x % L;
   const unsigned gmask = (L >= 32) ? 0xffffffffu : (((1u << L) - 1u) << ((threadIdx.x & 31) / L * L));
+  const int t0 = __ldg(&P.gnode_tl_off[node]), t1 = __ldg(&P.gnode_tl_off[node + 1]);
+  const int u0 = __ldg(&P.gnode_ul_off[node]), u1 = __ldg(&P.gnode_ul_off[node + 1]);
+  const int gdof = (g < DIM) ? __ldg(&P.growd[(size_t)node * 3 * DIM + g]) : 0;
+  double tk[DIM], rv[DIM];
   double r[DIM];
 #pragma unroll
   for (int q = 0; q < DIM; ++q) r[q] = 0.0;
@@ -163,41 +219,16 @@ __device__ __forceinline__ void gen_resid(const DevProblem& P, int node, bool va
         for (int v = 0; v < NV; ++v) r[q] += __ldg(&Gs[q * NV + v]) * P.eps_macro[v];
     }
   }
-  const int t0 = __ldg(&P.gnode_tl_off[node]), t1 = __ldg(&P.gnode_tl_off[node + 1]);
+  dep_wait();
   for (int j0 = t0; j0 < t1; j0 += L) {
-    double tk[DIM];
-#pragma unroll
-    for (int q = 0; q < DIM; ++q) tk[q] = 0.0;
-    if (j0 + g < t1) {
-      const int c = __ldg(&P.gnode_tl[j0 + g]);
-      const double sgn = (c & 1) ? -1.0 : 1.0;
-      const double* tp = P.kcoh + (c >> 1);
-#pragma unroll
-      for (int q = 0; q < DIM; ++q) tk[q] = sgn * tp[q];
-    }
+    gen_traction<DIM, L>(P, j0 + g, t1, tk);
     const int n_here = min(L, t1 - j0);
     for (int jj = 0; jj < n_here; ++jj)
 #pragma unroll
       for (int q = 0; q < DIM; ++q) r[q] += __shfl_sync(gmask, tk[q], jj, L);
   }
-  const int u0 = __ldg(&P.gnode_ul_off[node]), u1 = __ldg(&P.gnode_ul_off[node + 1]);
   for (int j0 = u0; j0 < u1; j0 += L) {
-    double rv[DIM];
-#pragma unroll
-    for (int q = 0; q < DIM; ++q) rv[q] = 0.0;
-    if (j0 + g < u1) {
-      const int c = __ldg(&P.gnode_ul[j0 + g]);
-      const int rec = c >> 2, la = c & 3;
-      const double* o = P.grec + (size_t)rec * R::STRIDE;
-      double ga[DIM], sig[NV];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) ga[d] = o[la * DIM + d];
-      const double w = o[R::W];
-#pragma unroll
-      for (int v = 0; v < NV; ++v) sig[v] = o[R::SIG + v];
-#pragma unroll
-      for (int q = 0; q < DIM; ++q) rv[q] = w * bt_sig<DIM, double>(ga, sig, q);
-    }
+    gen_uncut_force<DIM, L>(P, j0 + g, u1, rv);
     const int n_here = min(L, u1 - j0);
     for (int jj = 0; jj < n_here; ++jj)
 #pragma unroll
@@ -207,7 +238,6 @@ __device__ __forceinline__ void gen_resid(const DevProblem& P, int node, bool va
   double mine = r[0];
 #pragma unroll
   for (int q = 1; q < DIM; ++q) if (g == q) mine = r[q];
-  const int gdof = __ldg(&P.growd[(size_t)node * 3 * DIM + g]);
   if (gdof < P.n_free) P.Pf[gdof] = mine; else P.Pp[gdof - P.n_free] = mine;
 }
 
@@ -234,6 +264,7 @@ __global__ void __launch_bounds__(128) k_gen_resid(DevProblem P, int n0, int n1)
 // the records.
 template <int DIM>
 __global__ void __launch_bounds__(128) k_gen_first(DevProblem P, int coh_blocks) {
+  dep_launch();
   if ((int)blockIdx.x < coh_blocks) {
     constexpr int CQ = CohLanes<DIM>::CQ;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -256,6 +287,7 @@ __global__ void __launch_bounds__(128) k_gen_rows(DevProblem P, int n0, int n1, 
   } else {
     const int b = b0 + (blockIdx.x - res_blocks) * blockDim.x + threadIdx.x;
     if (b < b1) gen_block<DIM>(P, b);
+    else dep_wait();
   }
 }
 

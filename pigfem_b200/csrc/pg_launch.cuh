@@ -47,7 +47,10 @@ void assembly(pg_ctx* c, const pgd::DevProblem& P, bool jac, bool fp32) {
     const int rec_blocks = (simplex_general && P.n_grec > 0) ? blocks_of(P.n_grec) : 0;
     if (coh_blocks + rec_blocks > 0) pgd::k_gen_first<DIM><<<coh_blocks + rec_blocks, 128, 0, gst>>>(P, coh_blocks);
   }
-  cudaEventRecord(c->ev[3], gst);
+  // (the timing event between the cohesive/record kernel and the general rows is recorded only
+  // when timing: an event between them would hold back the general rows' early start)
+  if (c->timing) cudaEventRecord(c->ev[3], gst);
+  c->timed_last = c->timing;
   if (DIM == 2 && c->n_tiles > 0) {
     // 2D: one CTA per 16 x 8 tile of grid nodes, each element formed once (pg_tile.cuh)
     const size_t smem = pgd::tile2_smem_bytes();
@@ -84,8 +87,22 @@ void assembly(pg_ctx* c, const pgd::DevProblem& P, bool jac, bool fp32) {
     // block-parallel general rows (pg_general.cuh): residual lane groups and blocks in one launch
     const int res_blocks = func ? blocks_of((long long)P.n_slow_dn * pgd::kGenResidLanes) : 0;
     const int blk_blocks = jac ? blocks_of(P.n_gblk) : 0;
-    if (res_blocks + blk_blocks > 0)
-      pgd::k_gen_rows<DIM><<<res_blocks + blk_blocks, 128, 0, gst>>>(P, 0, P.n_slow_dn, res_blocks, 0, P.n_gblk);
+    if (res_blocks + blk_blocks > 0) {
+      // programmatic dependent launch: the general rows' blocks start while the kernel before them
+      // in the stream finishes, load their descriptors and static parts, and wait in the kernel
+      // (griddepcontrol.wait) before reading that kernel's output
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)(res_blocks + blk_blocks));
+      cfg.blockDim = dim3(128);
+      cfg.dynamicSmemBytes = 0;
+      cfg.stream = gst;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      at[0].val.programmaticStreamSerializationAllowed = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      cudaLaunchKernelEx(&cfg, pgd::k_gen_rows<DIM>, P, 0, P.n_slow_dn, res_blocks, 0, P.n_gblk);
+    }
   } else if (P.n_slow_dn > 0 && !jac) {
     // quad4 meshes, residual only: entry-parallel groups of L lanes per node
     constexpr int L = 8;

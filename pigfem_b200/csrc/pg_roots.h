@@ -12,14 +12,22 @@
 //     / secant steps inside a sign-change bracket, bisection when they are not safe.
 #pragma once
 
-#include <algorithm>
 #include <cmath>
+
+#ifdef __CUDACC__
+#define PG_HD __host__ __device__
+#else
+#define PG_HD
+#endif
 
 namespace pg {
 
-// f(alpha) and f'(alpha) of the level set along an edge; F provides eval(alpha, &f, &df).
+PG_HD inline double roots_min(double a, double b) { return a < b ? a : b; }
+
+// f(alpha) and f'(alpha) of the level set along an edge; F provides eval(alpha, &f, &df).  The
+// same code runs in the host set-up and in the device preprocessing (pg_prep.cu).
 template <class F>
-double steffensen_then_brent(const F& fn) {
+PG_HD double steffensen_then_brent(const F& fn) {
   // --- Steffensen from alpha = 0.5
   double x = 0.5, f, df;
   fn.eval(x, &f, &df);
@@ -51,7 +59,7 @@ double steffensen_then_brent(const F& fn) {
       alpha = root;
     }
     // converged when |alpha - alpha0| < 1e-7
-    cont = !(alpha == alpha0 || std::fabs(alpha - alpha0) < 1e-7);
+    cont = !(alpha == alpha0 || fabs(alpha - alpha0) < 1e-7);
   }
   if (!(iter == max_iter || alpha < 0.0 || alpha > 1.0)) return alpha;
 
@@ -65,15 +73,15 @@ double steffensen_then_brent(const F& fn) {
   do {
     iter++;
     if ((fb < 0 && fc < 0) || (fb > 0 && fc > 0)) { c = a; fc = fa; d = b - a; e = d; }
-    if (std::fabs(fc) < std::fabs(fb)) { a = b; b = c; c = a; fa = fb; fb = fc; fc = fa; }
-    const double tol = 0.5 * 2.220446049250313e-16 * std::fabs(b);
+    if (fabs(fc) < fabs(fb)) { a = b; b = c; c = a; fa = fb; fb = fc; fc = fa; }
+    const double tol = 0.5 * 2.220446049250313e-16 * fabs(b);
     const double m = 0.5 * (c - b);
     if (fb == 0.0) { alpha = b; xlo = b; xhi = b; }
-    else if (std::fabs(m) <= tol) {
+    else if (fabs(m) <= tol) {
       alpha = b;
       if (b < c) { xlo = b; xhi = c; } else { xlo = c; xhi = b; }
     } else {
-      if (std::fabs(e) < tol || std::fabs(fa) <= std::fabs(fb)) { d = m; e = m; }
+      if (fabs(e) < tol || fabs(fa) <= fabs(fb)) { d = m; e = m; }
       else {
         double p, q, r, ss = fb / fa;
         if (a == c) { p = 2 * m * ss; q = 1 - ss; }
@@ -83,18 +91,18 @@ double steffensen_then_brent(const F& fn) {
           q = (q - 1) * (r - 1) * (ss - 1);
         }
         if (p > 0) q = -q; else p = -p;
-        if (2 * p < std::min(3 * m * q - std::fabs(tol * q), std::fabs(e * q))) { e = d; d = p / q; }
+        if (2 * p < roots_min(3 * m * q - fabs(tol * q), fabs(e * q))) { e = d; d = p / q; }
         else { d = m; e = m; }
       }
       a = b; fa = fb;
-      if (std::fabs(d) > tol) b += d; else b += (m > 0 ? +tol : -tol);
+      if (fabs(d) > tol) b += d; else b += (m > 0 ? +tol : -tol);
       fn.eval(b, &fb, &df);
       alpha = b;
       if ((fb < 0 && fc < 0) || (fb > 0 && fc > 0)) c = a;
       if (b < c) { xlo = b; xhi = c; } else { xlo = c; xhi = b; }
       fc = (c == a) ? fa : fc;
     }
-  } while (!(xlo == xhi || std::fabs(xlo - xhi) < 1e-7) && iter < 100);
+  } while (!(xlo == xhi || fabs(xlo - xhi) < 1e-7) && iter < 100);
   return alpha;
 }
 

@@ -585,8 +585,9 @@ const int kTetEdge[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
 
 }  // namespace
 
-int build_setup(const ProblemDesc& d, Setup& s) {
+int build_setup(const ProblemDesc& d, Setup& s, const PrepResult* pr) {
   s = Setup();
+  if (pr && !pr->valid) pr = nullptr;
   s.desc = d;
   s.etype = d.elem_type;
   s.dim = (d.elem_type == TET4) ? 3 : 2;
@@ -816,7 +817,21 @@ int build_setup(const ProblemDesc& d, Setup& s) {
   }
   const int ninc = (int)incs.size();
   s.node_detect.assign(s.n_std, -1);
-  {
+  if (pr) {
+    // from the device pass; a node on a surface is reported with the inclusion the host loop
+    // meets first for it
+    if ((int)pr->node_detect.size() != s.n_std) { s.error = "internal: device detection size"; return 6; }
+    s.node_detect = pr->node_detect;
+    if (pr->surface_node >= 0) {
+      const int n = pr->surface_node;
+      int j = ninc - 1;
+      for (; j >= 0; --j) if (incs[j].in_box(&X3[(size_t)n * 3]) && incs[j].detect(&X3[(size_t)n * 3]) != 0) break;
+      std::ostringstream os;
+      os << "node " << n << " lies on the surface of inclusion " << j << " (the reference stops here: src/Mesh.cpp:2904-2911)";
+      s.error = os.str();
+      return 3;
+    }
+  } else {
     // nodes in parallel chunks; the first node on a surface (in node order) is the one reported
     const int ntd = setup_threads();
     std::vector<std::pair<int, int>> on_surface(ntd, {-1, -1});
@@ -867,7 +882,12 @@ int build_setup(const ProblemDesc& d, Setup& s) {
   // ---------------- element detection (Tri3::detection / Tet4::detection)
   std::vector<CutCase> cases;
   std::vector<int> cut_elems;
+  if (pr && (int)pr->elem_flag.size() != s.ne) { s.error = "internal: device element pass size"; return 6; }
   for (int e = 0; e < s.ne; ++e) {
+    if (pr && pr->elem_flag[e] != 2) {   // the device's all-equal test
+      if (pr->elem_flag[e] == 1) s.elem_mat[e] = 1;
+      continue;
+    }
     int nd[4];
     for (int q = 0; q < s.npe; ++q) nd[q] = s.node_detect[s.conn[(size_t)e * s.npe + q]];
     bool all_same = true;
@@ -913,7 +933,8 @@ int build_setup(const ProblemDesc& d, Setup& s) {
   // ---------------- enrichment nodes (Mesh::add_enrichments, serial)
   const int (*emap)[2] = (d.elem_type == TRI3) ? kTriEdge : (d.elem_type == QUAD4 ? kQuadEdge : kTetEdge);
   std::set<std::tuple<int, int, int>> cut_edges;  // (min node, max node, inclusion), ordered as std::set<pair<vector,id>>
-  for (int c = 0; c < s.ncut; ++c) {
+  const bool dev_edges = pr && pr->edges_valid;
+  for (int c = 0; c < s.ncut && !dev_edges; ++c) {
     const int e = cut_elems[c];
     const CutCase& cc = cases[c];
     for (size_t i = 0; i < cc.cut_edge.size(); ++i) {
@@ -922,14 +943,30 @@ int build_setup(const ProblemDesc& d, Setup& s) {
       cut_edges.insert(std::make_tuple(a, b, cc.incl[i]));
     }
   }
-  const int n_init = (int)cut_edges.size();
+  const int n_init = dev_edges ? (int)pr->enr_incl.size() : (int)cut_edges.size();
   s.n_enr_initial = n_init;
   s.n_enr = s.cohesive ? 2 * n_init : n_init;
   std::map<std::tuple<int, int, int>, int> edge_index;
   std::vector<double> XE((size_t)s.n_enr * 3);
   s.enr_edge.resize((size_t)s.n_enr * 2);
   s.enr_incl.resize(s.n_enr);
-  {
+  if (dev_edges) {
+    // the device's enrichment nodes, already in the set's order, and their intersection points
+    if (pr->no_sign_change >= 0) {
+      const int k = pr->no_sign_change;
+      std::ostringstream os;
+      os << "no sign change of inclusion " << pr->enr_incl[k] << " on edge " << pr->enr_edge[2 * k] << "-"
+         << pr->enr_edge[2 * k + 1] << " (src/Inclusion.cpp:38-39)";
+      s.error = os.str();
+      return 5;
+    }
+    for (int k = 0; k < n_init; ++k) {
+      for (int q = 0; q < 3; ++q) XE[(size_t)k * 3 + q] = pr->XE[(size_t)k * 3 + q];
+      s.enr_edge[(size_t)k * 2] = pr->enr_edge[2 * k]; s.enr_edge[(size_t)k * 2 + 1] = pr->enr_edge[2 * k + 1];
+      s.enr_incl[k] = pr->enr_incl[k];
+      edge_index[std::make_tuple(pr->enr_edge[2 * k], pr->enr_edge[2 * k + 1], pr->enr_incl[k])] = k;
+    }
+  } else {
     int k = 0;
     for (const auto& t : cut_edges) {
       const int a = std::get<0>(t), b = std::get<1>(t), inc = std::get<2>(t);
@@ -951,6 +988,8 @@ int build_setup(const ProblemDesc& d, Setup& s) {
       edge_index[t] = k;
       ++k;
     }
+  }
+  {
     if (s.cohesive)
       for (int m = 0; m < n_init; ++m) {
         for (int q = 0; q < 3; ++q) XE[(size_t)(m + n_init) * 3 + q] = XE[(size_t)m * 3 + q];
@@ -1225,6 +1264,32 @@ int build_setup(const ProblemDesc& d, Setup& s) {
 
   // ---------------- DOF numbering (DofObject::set_local_owned_normal_dofs / _enrich_dofs)
   // Dirichlet conditions as Tests/Main.cpp:549-581 applies them.
+  if (pr) {
+    // the standard nodes' numbers from the device pass (free index, or -1 - constrained index);
+    // enrichment DOFs follow the standard free ones, constrained DOFs come after all free ones
+    if (pr->std_dof.size() != (size_t)s.n_std * dim) { s.error = "internal: device DOF numbering size"; return 6; }
+    int nfree_std = 0, nconst_ = 0;
+    for (size_t i = 0; i < pr->std_dof.size(); ++i) {
+      const int v = pr->std_dof[i];
+      if (v >= 0) nfree_std = std::max(nfree_std, v + 1);
+      else nconst_ = std::max(nconst_, -v);
+    }
+    const int nfree = nfree_std + s.n_enr * dim;
+    s.n_free = nfree; s.n_const = nconst_;
+    s.node_dof.assign((size_t)n_nodes * dim, -1);
+    for (size_t i = 0; i < pr->std_dof.size(); ++i) {
+      const int v = pr->std_dof[i];
+      s.node_dof[i] = v >= 0 ? v : nfree + (-1 - v);
+    }
+    for (int n = 0; n < s.n_enr; ++n)
+      for (int q = 0; q < dim; ++q) s.node_dof[(size_t)(s.n_std + n) * dim + q] = nfree_std + n * dim + q;
+    s.dirichlet.assign(nconst_, 0.0);
+    if (!d.subscale) {
+      const double app = (d.hi[0] - d.lo[0]) * d.app_strain;
+      for (int k = 0; k <= Nz; ++k)
+        for (int j = 0; j <= Ny; ++j) s.dirichlet[s.node_dof[(size_t)nid(Nx, j, k) * dim] - nfree] = app;
+    }
+  } else {
   std::vector<std::vector<std::pair<bool, double>>> bc(s.n_std, std::vector<std::pair<bool, double>>(dim, {false, 0.0}));
   if (d.subscale) {
     for (int q = 0; q < dim; ++q) bc[0][q] = {true, 0.0};
@@ -1258,6 +1323,7 @@ int build_setup(const ProblemDesc& d, Setup& s) {
     for (int n = 0; n < s.n_std; ++n)
       if (s.dnode[n] != n)
         for (int q = 0; q < dim; ++q) s.node_dof[(size_t)n * dim + q] = s.node_dof[(size_t)s.dnode[n] * dim + q];
+  }
   }
 
   // ---------------- DOF nodes, adjacency and the CSR pattern

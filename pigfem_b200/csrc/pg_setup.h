@@ -120,7 +120,28 @@ struct Setup {
   std::string error;
 };
 
-// Returns 0 on success, a nonzero status with Setup::error filled otherwise.
-int build_setup(const ProblemDesc& d, Setup& s);
+// Results of the device preprocessing passes (pg_prep.cu) for a structured mesh, consumed by
+// build_setup in place of its own loops.  Every table equals what build_setup forms itself.
+struct PrepResult {
+  bool valid = false;
+  std::vector<int> node_detect;         // per standard node: inclusion index or -1
+  int surface_node = -1;                // first node on an inclusion surface, or -1
+  std::vector<unsigned char> elem_flag; // 0 uncut (own material), 1 inside an inclusion, 2 cut candidate
+  bool edges_valid = false;             // the enrichment nodes below are the set-up's (tri3, or one inclusion per element)
+  std::vector<int> enr_edge, enr_incl;  // per enrichment node (mirrors not included): sorted node pair, inclusion
+  std::vector<double> XE;               // per enrichment node: 3 coordinates
+  int no_sign_change = -1;              // first enrichment node whose edge has no sign change, or -1
+  std::vector<int> std_dof;             // standard node * dim: free index >= 0, or -1 - (constrained index)
+  double device_ms = 0.0;               // device time of the passes
+};
+
+// Runs the device passes of pg_prep.cu; 0 on success (pr.valid false when the mesh is outside
+// what they cover), nonzero with err set when a CUDA call fails.
+int device_prep(const ProblemDesc& d, PrepResult& pr, std::string& err);
+
+// Returns 0 on success, a nonzero status with Setup::error filled otherwise.  pr (optional, valid)
+// supplies the node detection, the element pass, the enrichment nodes and the standard nodes' DOF
+// numbering from the device.
+int build_setup(const ProblemDesc& d, Setup& s, const PrepResult* pr = nullptr);
 
 }  // namespace pg

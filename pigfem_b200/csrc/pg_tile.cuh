@@ -7,16 +7,18 @@
 //   B. every element of the 17 x 9 cells touching the tile (306 tri3) is formed once from them --
 //      gradients, weight J W, stress -- into a shared record.  The element's nodes follow the
 //      grid's union-jack split (the set-up checked every stencil node's elements against it);
-//   C. one thread per stencil node and row q (warps 0-3 row 0, warps 4-7 row 1; in each half the
-//      64 nodes of class 0 (8 elements) in two warps and the 64 of class 1 (4 elements) in the
-//      other two) sums its block row and residual entry from the records in adjacency order --
-//      the operations of stencil_rows, with the geometry read instead of recomputed -- keeping the
-//      row in registers and writing the residual entry;
+//   C. one thread per stencil node and row q (lanes 2n and 2n + 1 of a warp hold rows 0 and 1 of
+//      one node, so each record load serves both rows with one shared-memory access; warps 0-3 the
+//      64 nodes of class 0 (8 elements), warps 4-7 the 64 of class 1 (4 elements)) sums its block
+//      row and residual entry from the records in adjacency order -- the operations of
+//      stencil_rows, with the geometry read instead of recomputed -- keeping the row in registers
+//      and writing the residual entry;
 //   D. the rows go to a shared stage laid out like the CSR (a tile row of grid nodes is one run
 //      of the CSR when its nodes' rows are consecutive), and the CTA stores the set-up's
 //      contiguous segments with consecutive threads on consecutive addresses.
 // 3D (stencil_tile3): tiles of 4 x 4 x 4 grid nodes, one CTA of 192 threads (a thread per node
-// and row, rows warp-uniform); the 750 tets of the 5 x 5 x 5 cells touching the tile (six per hex,
+// and row, the three rows of a node on consecutive lanes so a record load serves them with one
+// access); the 750 tets of the 5 x 5 x 5 cells touching the tile (six per hex,
 // the grid's split) are formed once into records; node 0's gradient is not stored but re-formed
 // as the negated sum of the other three, as simplex_geom forms it.
 // Node data and records are structure-of-arrays (2D: of double2 pairs, one 16-byte access each),
@@ -49,18 +51,19 @@ __host__ __device__ constexpr int tile2_slot(int cx, int cy, int sub) {
   return ((sub * 2 + (cx & 1)) * kTileCY + cy) * kTileHX + (cx >> 1);
 }
 
-// Stage word a of a 2D tile is stored at a ^ ((a >> 4) & 15): a permutation inside each aligned
-// group of 16 doubles.  The rows of consecutive same-class nodes sit 56 doubles apart, so without
-// it the lanes of a row store would meet in two bank pairs (8-way conflicts); with it the stores
-// are at most 3-way and the warp-wide reads of a segment at most 3-way.
-__host__ __device__ constexpr int tile2_swizzle(int a) { return a ^ ((a >> 4) & 15); }
+// Stage word a of a 2D tile is stored at a ^ ((a >> 4) & 1): the two doubles of each aligned pair
+// trade places in every other group of 16.  A row store of a warp writes one value of each of 16
+// nodes' two rows (runs 56 doubles apart, rows NN x 2 apart); without the swap those 32 words
+// meet pairwise in 16 banks, with it every store and every warp-wide read of a segment is
+// free of bank conflicts (two wavefronts of 128 bytes).
+__host__ __device__ constexpr int tile2_swizzle(int a) { return a ^ ((a >> 4) & 1); }
 
 __host__ __device__ constexpr size_t tile2_smem_bytes() {
   // node data (x, u as two double2 arrays) then the record fields; the stage reuses the record area
   return (size_t)(4 * kTileNodes2 + kTileFields * kTileRecN) * sizeof(double);
 }
 static_assert(kTileFields * kTileRecN >= kTileY * kTileRowStage, "the stage fits the record area");
-static_assert((kTileY * kTileRowStage) % 16 == 0, "the swizzle stays inside the stage");
+static_assert((kTileY * kTileRowStage) % 2 == 0, "the swizzle stays inside the stage");
 
 // Tile descriptor: {first node i, first node j, first segment, segment count}; per own node (class
 // 0 nodes, then class 1) an entry {node id or -1, first free DOF, first CSR slot, stage offset};
@@ -92,13 +95,13 @@ __device__ __forceinline__ void stencil_tile2(const DevProblem& P, const GridInf
     }
   }
   __syncthreads();
-  // B: elements of the cells touching the tile, slot order
-  for (int k = t; k < RN; k += kTileThreads) {
-    const int h = k % kTileHX, cy = (k / kTileHX) % kTileCY, par = (k / (kTileHX * kTileCY)) & 1;
-    const int sub = k / (2 * kTileHX * kTileCY);
-    const int cx = 2 * h + par;
+  // B: elements of the cells touching the tile, cell order (consecutive lanes read consecutive
+  // nodes), each into its record slot
+  for (int it = t; it < 2 * kTileCX * kTileCY; it += kTileThreads) {
+    const int cx = it % kTileCX, cy = (it / kTileCX) % kTileCY, sub = it / (kTileCX * kTileCY);
+    const int k = tile2_slot(cx, cy, sub);
     const int ci = i0 - 1 + cx, cj = j0 - 1 + cy;
-    if (cx >= kTileCX || ci < 0 || ci >= gi.nx || cj < 0 || cj >= gi.ny) continue;
+    if (ci < 0 || ci >= gi.nx || cj < 0 || cj >= gi.ny) continue;
     // union-jack split of cell (ci, cj): nodes as (di, dj) offsets from its lower-left corner
     int d[3][2];
     if (((ci + cj) & 1) == 0) {
@@ -139,10 +142,10 @@ __device__ __forceinline__ void stencil_tile2(const DevProblem& P, const GridInf
   __syncthreads();
   // C: row q of this thread's node (node entry t % 128: class 0 then class 1); one accumulator
   // serves both classes (class 1 uses its first 5 slots)
-  const int q = t / kTileOwn;
-  const int4 v = __ldg(&tnodes[t % kTileOwn]);
+  const int q = t & 1;
+  const int4 v = __ldg(&tnodes[t >> 1]);
   double acc[JAC ? Tri3Stencil0::NN : 1][2];
-  const bool cls0 = (t % kTileOwn) < kTileOwn / 2;
+  const bool cls0 = (t >> 1) < kTileOwn / 2;
   if (v.x >= 0) {
     const int i = v.x % sx, j = v.x / sx;
     auto rows = [&](auto S) {
@@ -319,8 +322,9 @@ __device__ __forceinline__ void stencil_tile3(const DevProblem& P, const GridInf
     mat[k] = (unsigned char)m;
   }
   __syncthreads();
-  // C: row q of node nl (warps 0-1 row 0, 2-3 row 1, 4-5 row 2)
-  const int nl = t % kT3Nodes, q = t / kT3Nodes;
+  // C: row q of node nl (thread 3 nl + q: a warp's lanes read the records of 11 nodes, the
+  // stage runs of consecutive threads start 45 doubles apart, an odd number of bank pairs)
+  const int nl = t / 3, q = t % 3;
   const int4 v = __ldg(&tnodes[nl]);
   double acc[JAC ? NN : 1][3];
   if (v.x >= 0) {

@@ -17,8 +17,10 @@ Requests arrive (Poisson, or as a list), each with a seeded geometry.  Two kinds
 
 Pipeline (all stages run at once on different requests):
 
-1. set-up workers (host threads) run the C++ IGFEM set-up of each arrived request
-   (pg_create_host; ctypes releases the GIL, so they run in parallel on the host cores);
+1. set-up workers (host threads) run the IGFEM set-up of each arrived request: its per-node and
+   per-element passes (detection, enrichment nodes, standard DOF numbering) on the device, on a
+   stream of their own, and the cut elements' tables and the CSR pattern in C++
+   (pg_create_prep_device; ctypes releases the GIL, so they run in parallel on the host cores);
 2. the admission controller admits set-up requests in arrival order while the sum of the device
    bytes of the admitted requests stays within the budget and a GPU slot is free -- a request
    that arrives while others are on the GPU is admitted as soon as slots and memory free up.  A
@@ -256,10 +258,11 @@ def run_session_alone(reqs: List[Request]) -> List[Result]:
 class ServingEngine:
     """Continuous-batching request loop on one GPU (see the module docstring)."""
 
-    def __init__(self, memory_budget: int, max_inflight: int = 8, setup_workers: int = 8):
+    def __init__(self, memory_budget: int, max_inflight: int = 8, setup_workers: int = 8, prep_device: bool = True):
         self.budget = int(memory_budget)
         self.max_inflight = max_inflight
         self.setup_workers = setup_workers
+        self.prep_device = prep_device   # set-up passes on the device (pg_create_prep_device)
         self.calibration = 1.0        # largest measured / estimated device bytes seen so far
         self.peak_charged = 0         # most bytes the ledger held at once
 
@@ -290,7 +293,7 @@ class ServingEngine:
                 ready.put((req, None, r))
                 return
             try:
-                P = capi.Problem(req.desc, device=False)
+                P = capi.Problem(req.desc, device=False, prep_device=self.prep_device)
             except capi.PigfemError as e:
                 r.error = str(e)
                 r.done = now()
