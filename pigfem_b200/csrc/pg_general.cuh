@@ -22,7 +22,7 @@
 // and the records) and k_gen_rows (residuals and blocks).
 #pragma once
 
-#include "pg_kernels.cuh"
+#include "pg_stencil.cuh"
 
 namespace pgd {
 
@@ -67,9 +67,12 @@ __device__ __forceinline__ void gen_record(const DevProblem& P, int r) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) eps[v] += P.eps_macro[v];
   }
-  double sig[NV];
+  // sigma = D eps over D's nonzero pattern (every bulk material has the isotropic one), D read
+  // from device memory: a per-thread material index into the parameter block would be serialized
+  double sig[NV], dm[(DIM == 2) ? 5 : 12];
   const int m = __ldg(&P.grec_mat[r]);
-  lei_stress<DIM, double>(P.D[m], eps, sig);
+  iso_d<DIM, double>(P, m, dm);
+  lei_stress_iso<DIM, double>(dm, eps, sig);
   double* o = P.grec + (size_t)r * R::STRIDE;
 #pragma unroll
   for (int k = 0; k < NPE; ++k)
@@ -128,11 +131,14 @@ __device__ __forceinline__ void gen_block(const DevProblem& P, int b) {
 #pragma unroll
     for (int d = 0; d < DIM; ++d) { ga[d] = o[la * DIM + d]; gb[d] = o[lb * DIM + d]; }
     const double w = o[R::W];
-    const double* D = P.D[(int)o[R::MAT]];
+    // D's nonzero pattern from device memory (see gen_record); part_iso forms the same values as
+    // bt_d_row over the full D (the terms it leaves out are exact zeros)
+    double dm[(DIM == 2) ? 5 : 12];
+    iso_d<DIM, double>(P, (int)o[R::MAT], dm);
 #pragma unroll
     for (int q = 0; q < DIM; ++q) {
       double part[NV];
-      bt_d_row<DIM, double>(D, ga, q, part);
+      part_iso<DIM, double>(dm, ga, q, part);
 #pragma unroll
       for (int q2 = 0; q2 < DIM; ++q2) acc[q * DIM + q2] += w * part_b<DIM, double>(part, gb, q2);
     }

@@ -678,7 +678,18 @@ __global__ void __launch_bounds__(128) k_rows_general_cases(DevProblem P) {
       const int la = ad.y & 255, mn = ad.y >> 8;
       if (mn == 0) {
         const int nd[4] = {ax.x, ax.y, ax.z, ax.w};
-        const double* D = P.D[ad.w];
+        // the entries of D that lei_stress reads, from device memory (a per-thread material index
+        // into the parameter block would be serialized)
+        double D[36];
+        {
+          constexpr int i2[5] = {0, 1, 3, 4, 8};
+          constexpr int i3[12] = {0, 1, 2, 6, 7, 8, 12, 13, 14, 21, 28, 35};
+#pragma unroll
+          for (int i = 0; i < ((DIM == 2) ? 5 : 12); ++i) {
+            const int o = (DIM == 2) ? i2[i] : i3[i];
+            D[o] = __ldg(&P.Dd[ad.w * 36 + o]);
+          }
+        }
         double x[NPE][DIM], g[NPE][DIM], J;
 #pragma unroll
         for (int n = 0; n < NPE; ++n) load_node<DIM>(P.X, nd[n], x[n]);

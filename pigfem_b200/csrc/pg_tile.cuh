@@ -17,8 +17,7 @@
 //      of the CSR when its nodes' rows are consecutive), and the CTA stores the set-up's
 //      contiguous segments with consecutive threads on consecutive addresses.
 // 3D (stencil_tile3): tiles of 4 x 4 x 4 grid nodes, one CTA of 192 threads (a thread per node
-// and row, the three rows of a node on consecutive lanes so a record load serves them with one
-// access); the 750 tets of the 5 x 5 x 5 cells touching the tile (six per hex,
+// and row, rows warp-uniform); the 750 tets of the 5 x 5 x 5 cells touching the tile (six per hex,
 // the grid's split) are formed once into records; node 0's gradient is not stored but re-formed
 // as the negated sum of the other three, as simplex_geom forms it.
 // Node data and records are structure-of-arrays (2D: of double2 pairs, one 16-byte access each),
@@ -39,7 +38,12 @@ constexpr int kTileNX = kTileX + 2, kTileNY = kTileY + 2;  // nodes with the hal
 constexpr int kTileNodes2 = kTileNX * kTileNY;             // 180
 constexpr int kTileCX = kTileX + 1, kTileCY = kTileY + 1;  // cells touching the tile
 constexpr int kTileHX = (kTileCX + 1) / 2;                 // cell columns per parity (9)
-constexpr int kTileRecN = 2 * 2 * kTileCY * kTileHX;       // record slots (324; 306 used)
+// record slots per (element-in-cell, column parity) plane: the 81 cells of a plane padded to 84,
+// so that within a quarter-warp of the element pass (8 consecutive cells, alternating planes)
+// the two planes' 16-byte record stores fall in different banks
+constexpr int kTilePlane = 84;
+static_assert(kTilePlane >= kTileCY * kTileHX && kTilePlane % 8 == 4, "plane padding");
+constexpr int kTileRecN = 2 * 2 * kTilePlane;              // record slots (336; 306 used)
 constexpr int kTileFields = 12;                            // doubles per record slot (11 used)
 constexpr int kTileRowStage = 8 * 36 + 8 * 20;             // doubles of a tile row's runs (448)
 constexpr int kTileOwn = kTileX * kTileY;                  // the tile's own nodes (128)
@@ -48,22 +52,22 @@ constexpr int kTileThreads = 2 * kTileOwn;                 // a thread per node 
 // Record slot of element `sub` of tile cell (cx, cy): cells of one x parity are consecutive in x,
 // so the class-uniform node warps (nodes two cells apart) read consecutive slots.
 __host__ __device__ constexpr int tile2_slot(int cx, int cy, int sub) {
-  return ((sub * 2 + (cx & 1)) * kTileCY + cy) * kTileHX + (cx >> 1);
+  return (sub * 2 + (cx & 1)) * kTilePlane + cy * kTileHX + (cx >> 1);
 }
 
-// Stage word a of a 2D tile is stored at a ^ ((a >> 4) & 1): the two doubles of each aligned pair
-// trade places in every other group of 16.  A row store of a warp writes one value of each of 16
-// nodes' two rows (runs 56 doubles apart, rows NN x 2 apart); without the swap those 32 words
-// meet pairwise in 16 banks, with it every store and every warp-wide read of a segment is
-// free of bank conflicts (two wavefronts of 128 bytes).
-__host__ __device__ constexpr int tile2_swizzle(int a) { return a ^ ((a >> 4) & 1); }
+// Stage word a of a 2D tile is stored at a ^ ((a >> 4) & 3): a permutation inside each aligned
+// group of 4 doubles, changing with the group of 16 the word falls in.  A half-warp's 8-byte row
+// store writes one value of each of 8 nodes' two rows (runs 56 doubles apart, rows NN x 2 apart),
+// which without it meet in 4 bank pairs (4 wavefronts per half-warp store); with it the stores
+// average 1.6, and the warp-wide reads of a segment stay free of conflicts.
+__host__ __device__ constexpr int tile2_swizzle(int a) { return a ^ ((a >> 4) & 3); }
 
 __host__ __device__ constexpr size_t tile2_smem_bytes() {
   // node data (x, u as two double2 arrays) then the record fields; the stage reuses the record area
   return (size_t)(4 * kTileNodes2 + kTileFields * kTileRecN) * sizeof(double);
 }
 static_assert(kTileFields * kTileRecN >= kTileY * kTileRowStage, "the stage fits the record area");
-static_assert((kTileY * kTileRowStage) % 2 == 0, "the swizzle stays inside the stage");
+static_assert((kTileY * kTileRowStage) % 4 == 0, "the swizzle stays inside the stage");
 
 // Tile descriptor: {first node i, first node j, first segment, segment count}; per own node (class
 // 0 nodes, then class 1) an entry {node id or -1, first free DOF, first CSR slot, stage offset};
@@ -322,9 +326,9 @@ __device__ __forceinline__ void stencil_tile3(const DevProblem& P, const GridInf
     mat[k] = (unsigned char)m;
   }
   __syncthreads();
-  // C: row q of node nl (thread 3 nl + q: a warp's lanes read the records of 11 nodes, the
-  // stage runs of consecutive threads start 45 doubles apart, an odd number of bank pairs)
-  const int nl = t / 3, q = t % 3;
+  // C: row q of node nl (warps 0-1 row 0, 2-3 row 1, 4-5 row 2: the row-dependent operations
+  // stay uniform over a warp)
+  const int nl = t % kT3Nodes, q = t / kT3Nodes;
   const int4 v = __ldg(&tnodes[nl]);
   double acc[JAC ? NN : 1][3];
   if (v.x >= 0) {
