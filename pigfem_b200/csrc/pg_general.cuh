@@ -46,8 +46,9 @@ __device__ __forceinline__ void dep_wait() { asm volatile("griddepcontrol.wait;"
 // Lets the dependent grid launch now (its blocks then do their independent loads).
 __device__ __forceinline__ void dep_launch() { asm volatile("griddepcontrol.launch_dependents;" :::); }
 
+// The record of element record r into o[0 .. STRIDE).
 template <int DIM>
-__device__ __forceinline__ void gen_record(const DevProblem& P, int r) {
+__device__ __forceinline__ void gen_record_values(const DevProblem& P, int r, double* o) {
   constexpr int NPE = DIM + 1;
   constexpr int NV = (DIM == 2) ? 3 : 6;
   using R = GenRec<DIM>;
@@ -73,7 +74,6 @@ __device__ __forceinline__ void gen_record(const DevProblem& P, int r) {
   const int m = __ldg(&P.grec_mat[r]);
   iso_d<DIM, double>(P, m, dm);
   lei_stress_iso<DIM, double>(dm, eps, sig);
-  double* o = P.grec + (size_t)r * R::STRIDE;
 #pragma unroll
   for (int k = 0; k < NPE; ++k)
 #pragma unroll
@@ -84,6 +84,16 @@ __device__ __forceinline__ void gen_record(const DevProblem& P, int r) {
   o[R::MAT] = (double)m;
 #pragma unroll
   for (int f = R::MAT + 1; f < R::STRIDE; ++f) o[f] = 0.0;
+}
+
+template <int DIM>
+__device__ __forceinline__ void gen_record(const DevProblem& P, int r) {
+  constexpr int S = GenRec<DIM>::STRIDE;
+  double o[S];
+  gen_record_values<DIM>(P, r, o);
+  double* dst = P.grec + (size_t)r * S;
+#pragma unroll
+  for (int f = 0; f < S; ++f) dst[f] = o[f];
 }
 
 template <int DIM>
@@ -277,8 +287,23 @@ __global__ void __launch_bounds__(128) k_gen_first(DevProblem P, int coh_blocks)
     const int ce = t / CQ;
     coh_element<DIM>(P, ce, t % CQ, ce < P.n_coh_el);
   } else {
-    const int r = (blockIdx.x - coh_blocks) * blockDim.x + threadIdx.x;
-    if (r < P.n_grec) gen_record<DIM>(P, r);
+    // the block's 128 records are contiguous: staged in shared memory (an odd row pitch, so the
+    // per-thread rows meet no bank twice) and stored by the whole block, consecutive threads on
+    // consecutive addresses
+    constexpr int S = GenRec<DIM>::STRIDE, SP = S + 1;
+    __shared__ double st[128 * SP];
+    const int r0 = (blockIdx.x - coh_blocks) * blockDim.x;
+    const int r = r0 + threadIdx.x;
+    if (r < P.n_grec) {
+      double o[S];
+      gen_record_values<DIM>(P, r, o);
+#pragma unroll
+      for (int f = 0; f < S; ++f) st[threadIdx.x * SP + f] = o[f];
+    }
+    __syncthreads();
+    const int n = min((int)blockDim.x, P.n_grec - r0) * S;
+    double* dst = P.grec + (size_t)r0 * S;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = st[(k / S) * SP + k % S];
   }
 }
 
