@@ -103,14 +103,16 @@ int pg_create(const pg_problem_desc* desc, pg_ctx** out);
  * set-up tables can be read back) and the upload that makes the context assemble-ready. */
 int pg_create_host(const pg_problem_desc* desc, pg_ctx** out);
 int pg_upload(pg_ctx* ctx);
-/* pg_create_host with the set-up's per-node and per-element passes on the current CUDA device:
- * node detection (Mesh::detect_node, src/Mesh.cpp:2727-2929), the all-equal element test of the
- * element detection (Tri3/Quad4/Tet4::detection), the enrichment nodes and their intersection
- * points (Mesh::add_enrichments, src/Mesh.cpp:3103-3252; Inclusion::find_intersection,
- * src/Inclusion.cpp:32-121) and the standard nodes' DOF numbering (DofObject::
- * set_local_owned_normal_dofs, src/DofObject.cpp:336-385).  Every table is the one pg_create_host
- * forms (integers bit-exact, coordinates too); the context is host-only until pg_upload.  Grids
- * of fewer than 2 cells per direction run every pass on the host. */
+/* pg_create_host with the set-up's per-node, per-element and pattern passes on the current CUDA
+ * device: node detection (Mesh::detect_node, src/Mesh.cpp:2727-2929), the all-equal element test
+ * of the element detection (Tri3/Quad4/Tet4::detection), the enrichment nodes and their
+ * intersection points (Mesh::add_enrichments, src/Mesh.cpp:3103-3252; Inclusion::
+ * find_intersection, src/Inclusion.cpp:32-121), the standard nodes' DOF numbering (DofObject::
+ * set_local_owned_normal_dofs, src/DofObject.cpp:336-385), and the DOF nodes' adjacency and the
+ * CSR pattern of the four blocks (Solver::preallocate_matrix, src/Solver.cpp:426-490, 772-896).
+ * The cut elements' case tables and sub-element quadrature stay on the host.  Every table is the
+ * one pg_create_host forms (integers bit-exact, coordinates too); the context is host-only until
+ * pg_upload.  Grids of fewer than 2 cells per direction run every pass on the host. */
 int pg_create_prep_device(const pg_problem_desc* desc, pg_ctx** out);
 /* Device time in ms of the passes pg_create_prep_device ran (-1 when none ran). */
 int pg_prep_device_ms(const pg_ctx* ctx, double* ms);

@@ -32,6 +32,7 @@ struct BatchItem {
   const int4* tiles;    // 2D: the context's stencil tiles (pg_tile.cuh)
   const int4* tnodes;
   const int4* tsegs;
+  const pgd::Tile3Const* t3c;   // 3D: the context's tile shape constants (device copy)
 };
 
 struct BatchCall {
@@ -86,7 +87,7 @@ __global__ void __launch_bounds__(256) k_batch_stencil(const BatchItem* __restri
       __syncthreads();
     } else {
       pgd::stencil_tile3<T, true>(it.P, it.gi, __ldg(&it.tiles[2 * ch.y]), __ldg(&it.tiles[2 * ch.y + 1]),
-                                  it.tnodes + (size_t)ch.y * pgd::kT3Nodes, it.tsegs, stage);
+                                  it.tnodes + (size_t)ch.y * pgd::kT3Nodes, it.tsegs, stage, *it.t3c);
       __syncthreads();
     }
   }
@@ -286,6 +287,7 @@ int pg_batch_create(pg_ctx* const* ctxs, int n, pg_batch** out) {
     items[i].tiles = c->tiles;
     items[i].tnodes = c->tnodes;
     items[i].tsegs = c->tsegs;
+    items[i].t3c = c->d_t3c;
     b->max_mn = std::max(b->max_mn, c->P.max_mn);
     b->n_elem += c->s.ne;
   }

@@ -133,8 +133,17 @@ static int create_host(const pg_problem_desc* d, pg_ctx** out, bool device_prep)
     std::string why;
     if (pg::device_prep(pd, pr, why)) { c->err = why; *out = c; return PG_ERR_DEVICE; }
     c->prep_ms = pr.valid ? pr.device_ms : -1.0;
+    pr.pattern_on_device = pr.valid;
   }
   int rc = pg::build_setup(pd, c->s, device_prep ? &pr : nullptr);
+  if (!rc && pr.pattern_on_device) {
+    // the adjacency and the CSR pattern on the device too
+    std::string why;
+    double ms = 0.0;
+    const int r2 = pg::device_pattern(c->s, why, &ms);
+    if (r2) { c->err = why; *out = c; return r2 == 10 ? PG_ERR_DEVICE : PG_ERR_INPUT; }
+    c->prep_ms += ms;
+  }
   if (rc) { c->err = c->s.error; *out = c; return rc == 2 ? PG_ERR_INPUT : (rc == 4 ? PG_ERR_UNSUPPORTED : (rc == 7 ? PG_ERR_JACOBIAN : PG_ERR_GEOMETRY)); }
   c->n_coh_qp = (int)c->s.cqp_wgt.size();
   *out = c;
@@ -463,6 +472,8 @@ int pg_upload(pg_ctx* c) {
     PG_TRY(upload(c, Dh, &P.Dd));
     PG_TRY(upload(c, Dfh, &P.Dfd));
   }
+  if ((dim == 2 ? pgl::tile_consts<2>(c, P) : pgl::tile_consts<3>(c, P)) != 0)
+    return set_err(c, PG_ERR_DEVICE, "tile shape constants failed");
   std::vector<float> Xf(s.X.begin(), s.X.end());
   PG_TRY(upload(c, s.X, &P.X));
   PG_TRY(upload(c, Xf, &P.Xf));
@@ -872,6 +883,7 @@ void pg_destroy(pg_ctx* c) {
   if (c->side2) cudaStreamDestroy(c->side2);
   for (void* p : c->allocs) cudaFreeAsync(p, c->up);
   if (c->up) cudaStreamDestroy(c->up);   // released once the frees have run
+  delete c->t3c;
   delete c;
 }
 

@@ -12,6 +12,8 @@
 #include <string>
 #include <vector>
 
+namespace pgd { struct Tile3Const; }
+
 // Workspace of the Jacobi-preconditioned CG on K_ff (pg_solver.cu), allocated on first use.
 struct PcgWork {
   int n = 0, cap_rhs = 0, nb = 0;
@@ -47,6 +49,8 @@ struct pg_ctx {
   int maxnb_fast = 0;
   int n_coh_qp = 0;
   bool assembled = false;
+  pgd::Tile3Const* t3c = nullptr;         // 3D tiles' shape constants: host copy (kernel parameter)
+  const pgd::Tile3Const* d_t3c = nullptr; // and device copy (batches)
   bool timed_last = false;   // the last assembly recorded every timing event (pg_kernel_times)
   double prep_ms = -1.0;   // device time of the preprocessing passes (pg_create_prep_device), -1 if none ran
   // PG_KEEP_STATIC: the first CSR value of each block from which a later assembly can change

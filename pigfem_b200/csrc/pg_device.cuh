@@ -40,6 +40,14 @@ struct DevProblem {
   float Df[3][36];
   const double* Dd;   // D of the three bulk materials in device memory (3 x 36), read through the L1
   const float* Dfd;
+  // 2D structured tiles (pg_tile.cuh): every uncut element of the uniform grid is one of four
+  // shapes (2 x cell parity + element in the cell); per shape the gradients of its three nodes, its
+  // weight J W, and its element matrix per bulk material ([(la * 2 + q) * 6 + lb * 2 + q2], FP64
+  // and the FP32-mixed products), formed once at upload by the element code itself
+  double tile_g[4][3][2];
+  double tile_w[4];
+  double tile_ke[4][3][36];
+  float tile_kef[4][3][36];
   CohConst coh;
   // geometry / state
   const double* X;    // n_nodes * dim

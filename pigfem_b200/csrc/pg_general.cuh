@@ -46,8 +46,9 @@ __device__ __forceinline__ void dep_wait() { asm volatile("griddepcontrol.wait;"
 // Lets the dependent grid launch now (its blocks then do their independent loads).
 __device__ __forceinline__ void dep_launch() { asm volatile("griddepcontrol.launch_dependents;" :::); }
 
-// The record of element record r into o[0 .. STRIDE).
-template <int DIM>
+// The record of element record r into o[0 .. STRIDE).  STRAIN: the stress slots hold the strain
+// of U alone (no macroscale part), for the multi-strain pass.
+template <int DIM, bool STRAIN = false>
 __device__ __forceinline__ void gen_record_values(const DevProblem& P, int r, double* o) {
   constexpr int NPE = DIM + 1;
   constexpr int NV = (DIM == 2) ? 3 : 6;
@@ -64,7 +65,7 @@ __device__ __forceinline__ void gen_record_values(const DevProblem& P, int r, do
   for (int v = 0; v < NV; ++v) eps[v] = 0.0;
 #pragma unroll
   for (int k = 0; k < NPE; ++k) add_strain<DIM, double>(g[k], u[k], eps);
-  if (P.subscale) {
+  if (!STRAIN && P.subscale) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) eps[v] += P.eps_macro[v];
   }
@@ -72,8 +73,13 @@ __device__ __forceinline__ void gen_record_values(const DevProblem& P, int r, do
   // from device memory: a per-thread material index into the parameter block would be serialized
   double sig[NV], dm[(DIM == 2) ? 5 : 12];
   const int m = __ldg(&P.grec_mat[r]);
-  iso_d<DIM, double>(P, m, dm);
-  lei_stress_iso<DIM, double>(dm, eps, sig);
+  if (STRAIN) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) sig[v] = eps[v];
+  } else {
+    iso_d<DIM, double>(P, m, dm);
+    lei_stress_iso<DIM, double>(dm, eps, sig);
+  }
 #pragma unroll
   for (int k = 0; k < NPE; ++k)
 #pragma unroll
@@ -275,6 +281,26 @@ __global__ void __launch_bounds__(128) k_gen_resid(DevProblem P, int n0, int n1)
   gen_resid<DIM, kGenResidLanes>(P, node, node < n1);
 }
 
+// Records r0 .. r0 + 127 by a block of 128 threads: the block's records are contiguous, so they are
+// staged in shared memory (an odd row pitch, so the per-thread rows meet no bank twice) and
+// stored by the whole block, consecutive threads on consecutive addresses.
+template <int DIM, bool STRAIN>
+__device__ __forceinline__ void record_block(const DevProblem& P, int r0) {
+  constexpr int S = GenRec<DIM>::STRIDE, SP = S + 1;
+  __shared__ double st[128 * SP];
+  const int r = r0 + threadIdx.x;
+  if (r < P.n_grec) {
+    double o[S];
+    gen_record_values<DIM, STRAIN>(P, r, o);
+#pragma unroll
+    for (int f = 0; f < S; ++f) st[threadIdx.x * SP + f] = o[f];
+  }
+  __syncthreads();
+  const int n = min((int)blockDim.x, P.n_grec - r0) * S;
+  double* dst = P.grec + (size_t)r0 * S;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = st[(k / S) * SP + k % S];
+}
+
 // The cohesive elements and the element records in one launch (both read U and the geometry
 // only): blocks [0, coh_blocks) take the cohesive quadrature lanes (k_coh_elements), the rest
 // the records.
@@ -287,23 +313,7 @@ __global__ void __launch_bounds__(128) k_gen_first(DevProblem P, int coh_blocks)
     const int ce = t / CQ;
     coh_element<DIM>(P, ce, t % CQ, ce < P.n_coh_el);
   } else {
-    // the block's 128 records are contiguous: staged in shared memory (an odd row pitch, so the
-    // per-thread rows meet no bank twice) and stored by the whole block, consecutive threads on
-    // consecutive addresses
-    constexpr int S = GenRec<DIM>::STRIDE, SP = S + 1;
-    __shared__ double st[128 * SP];
-    const int r0 = (blockIdx.x - coh_blocks) * blockDim.x;
-    const int r = r0 + threadIdx.x;
-    if (r < P.n_grec) {
-      double o[S];
-      gen_record_values<DIM>(P, r, o);
-#pragma unroll
-      for (int f = 0; f < S; ++f) st[threadIdx.x * SP + f] = o[f];
-    }
-    __syncthreads();
-    const int n = min((int)blockDim.x, P.n_grec - r0) * S;
-    double* dst = P.grec + (size_t)r0 * S;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = st[(k / S) * SP + k % S];
+    record_block<DIM, false>(P, (blockIdx.x - coh_blocks) * blockDim.x);
   }
 }
 
@@ -320,6 +330,119 @@ __global__ void __launch_bounds__(128) k_gen_rows(DevProblem P, int n0, int n1, 
     if (b < b1) gen_block<DIM>(P, b);
     else dep_wait();
   }
+}
+
+// ---------------------------------------------------------------- multi-strain residuals
+// Records for pg_residual_strains: the stress slots hold the strain of U alone.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_gen_records_strain(DevProblem P) {
+  record_block<DIM, true>(P, blockIdx.x * blockDim.x);
+}
+
+// The residuals of the P.n_cases macroscale strains of general node `node` by a group of L lanes:
+// for each case the operations of gen_resid with that case as the macroscale strain, in the same
+// order -- the static part and its macroscale response, the tractions (the same for every case),
+// then the uncut elements, whose stress is formed from the record's strain of U plus the case's
+// strain -- so each case's values are those of the single-strain assembly.
+template <int DIM, int L>
+__device__ __forceinline__ void gen_resid_cases(const DevProblem& P, int node, bool valid) {
+  constexpr int NV = (DIM == 2) ? 3 : 6;
+  constexpr int MC = 6;
+  using R = GenRec<DIM>;
+  if (!valid) return;
+  const int nc = P.n_cases;
+  const int g = threadIdx.x % L;
+  const unsigned gmask = (L >= 32) ? 0xffffffffu : (((1u << L) - 1u) << ((threadIdx.x & 31) / L * L));
+  const int t0 = __ldg(&P.gnode_tl_off[node]), t1 = __ldg(&P.gnode_tl_off[node + 1]);
+  const int u0 = __ldg(&P.gnode_ul_off[node]), u1 = __ldg(&P.gnode_ul_off[node + 1]);
+  const int gdof = (g < DIM) ? __ldg(&P.growd[(size_t)node * 3 * DIM + g]) : 0;
+  double rs[MC][DIM];
+#pragma unroll
+  for (int c = 0; c < MC; ++c)
+#pragma unroll
+    for (int q = 0; q < DIM; ++q) rs[c][q] = 0.0;
+  if (node < P.n_stat) {
+    const int4 gd = __ldg(&P.gdesc[node]);
+    double su[DIM];
+    static_resid_group<DIM, L>(P, node, gd.w, g, gmask, su);
+    const double* Gs = P.stat_g + (size_t)node * DIM * NV;
+#pragma unroll
+    for (int c = 0; c < MC; ++c) {
+      if (c >= nc) break;
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) {
+        double v = su[q];
+#pragma unroll
+        for (int w = 0; w < NV; ++w) v += __ldg(&Gs[q * NV + w]) * P.eps_cases[c][w];
+        rs[c][q] = v;
+      }
+    }
+  }
+  for (int j0 = t0; j0 < t1; j0 += L) {
+    double tk[DIM];
+    gen_traction<DIM, L>(P, j0 + g, t1, tk);
+    const int n_here = min(L, t1 - j0);
+    for (int jj = 0; jj < n_here; ++jj)
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) {
+        const double t = __shfl_sync(gmask, tk[q], jj, L);
+#pragma unroll
+        for (int c = 0; c < MC; ++c) if (c < nc) rs[c][q] += t;
+      }
+  }
+  for (int j0 = u0; j0 < u1; j0 += L) {
+    double rv[MC][DIM];
+#pragma unroll
+    for (int c = 0; c < MC; ++c)
+#pragma unroll
+      for (int q = 0; q < DIM; ++q) rv[c][q] = 0.0;
+    if (j0 + g < u1) {
+      const int cc = __ldg(&P.gnode_ul[j0 + g]);
+      const int rec = cc >> 2, la = cc & 3;
+      const double* o = P.grec + (size_t)rec * R::STRIDE;
+      double ga[DIM], eps[NV], dm[(DIM == 2) ? 5 : 12];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) ga[d] = o[la * DIM + d];
+      const double w = o[R::W];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) eps[v] = o[R::SIG + v];
+      iso_d<DIM, double>(P, (int)o[R::MAT], dm);
+#pragma unroll
+      for (int c = 0; c < MC; ++c) {
+        if (c >= nc) break;
+        double ek[NV], sig[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) ek[v] = eps[v] + P.eps_cases[c][v];
+        lei_stress_iso<DIM, double>(dm, ek, sig);
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) rv[c][q] = w * bt_sig<DIM, double>(ga, sig, q);
+      }
+    }
+    const int n_here = min(L, u1 - j0);
+    for (int jj = 0; jj < n_here; ++jj)
+#pragma unroll
+      for (int c = 0; c < MC; ++c) {
+        if (c >= nc) break;
+#pragma unroll
+        for (int q = 0; q < DIM; ++q) rs[c][q] += __shfl_sync(gmask, rv[c][q], jj, L);
+      }
+  }
+  if (g >= DIM) return;
+#pragma unroll
+  for (int c = 0; c < MC; ++c) {
+    if (c >= nc) break;
+    double mine = rs[c][0];
+#pragma unroll
+    for (int q = 1; q < DIM; ++q) if (g == q) mine = rs[c][q];
+    if (gdof < P.n_free) P.Pf_cases[(size_t)c * P.n_free + gdof] = mine;
+    else P.Pp_cases[(size_t)c * P.n_const + gdof - P.n_free] = mine;
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(128) k_gen_resid_cases(DevProblem P) {
+  const int node = (blockIdx.x * blockDim.x + threadIdx.x) / kGenResidLanes;
+  gen_resid_cases<DIM, kGenResidLanes>(P, node, node < P.n_slow_dn);
 }
 
 }  // namespace pgd

@@ -625,136 +625,6 @@ __global__ void __launch_bounds__(128) k_rows_general_resid(DevProblem P) {
   if (gdof < P.n_free) P.Pf[gdof] = mine; else P.Pp[gdof - P.n_free] = mine;
 }
 
-// Residuals of the general rows for the P.n_cases macroscale strains of a multi-strain pass,
-// entry-parallel like k_rows_general_resid: the static residual is formed once and each case
-// adds its macroscale-strain response; an uncut element's geometry and strain of U are formed
-// once and each case adds its strain; a cut element adds the cohesive traction (the same for every
-// case).  For each case these are the operations of the single-strain residual with that case as
-// eps_macro, summed in the same order.
-template <int DIM, int L>
-__global__ void __launch_bounds__(128) k_rows_general_cases(DevProblem P) {
-  constexpr int NPE = DIM + 1;
-  constexpr int NV = (DIM == 2) ? 3 : 6;
-  constexpr int MC = 6;
-  const int nc = P.n_cases;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int node = t / L, k = t % L;
-  const bool valid = node < P.n_slow_dn;
-  const unsigned gmask = (L == 32) ? 0xffffffffu : (((1u << L) - 1u) << ((threadIdx.x & 31) / L * L));
-  if (__all_sync(0xffffffffu, !valid)) return;
-  int4 gd = make_int4(0, 0, 0, 0);
-  if (valid) gd = __ldg(&P.gdesc[node]);
-  double rs[MC][DIM];   // per case, every lane of the group
-#pragma unroll
-  for (int c = 0; c < MC; ++c)
-#pragma unroll
-    for (int q = 0; q < DIM; ++q) rs[c][q] = 0.0;
-  if (valid && node < P.n_stat) {
-    double su[DIM];
-    static_resid_group<DIM, L>(P, node, gd.w, k, gmask, su);
-    const double* Gs = P.stat_g + (size_t)node * DIM * NV;
-#pragma unroll
-    for (int c = 0; c < MC; ++c) {
-      if (c >= nc) break;
-#pragma unroll
-      for (int q = 0; q < DIM; ++q) {
-        double v = su[q];
-#pragma unroll
-        for (int w = 0; w < NV; ++w) v += __ldg(&Gs[q * NV + w]) * P.eps_cases[c][w];
-        rs[c][q] = v;
-      }
-    }
-  }
-  for (int e0 = 0; e0 < gd.y; e0 += L) {
-    const int ei = e0 + k;
-    double re[MC][DIM];
-#pragma unroll
-    for (int c = 0; c < MC; ++c)
-#pragma unroll
-      for (int q = 0; q < DIM; ++q) re[c][q] = 0.0;
-    if (ei < gd.y) {
-      const int4 ad = __ldg(&P.adesc[gd.x + ei]);
-      const int4 ax = __ldg(&P.aresd[gd.x + ei]);
-      const int la = ad.y & 255, mn = ad.y >> 8;
-      if (mn == 0) {
-        const int nd[4] = {ax.x, ax.y, ax.z, ax.w};
-        // the entries of D that lei_stress reads, from device memory (a per-thread material index
-        // into the parameter block would be serialized)
-        double D[36];
-        {
-          constexpr int i2[5] = {0, 1, 3, 4, 8};
-          constexpr int i3[12] = {0, 1, 2, 6, 7, 8, 12, 13, 14, 21, 28, 35};
-#pragma unroll
-          for (int i = 0; i < ((DIM == 2) ? 5 : 12); ++i) {
-            const int o = (DIM == 2) ? i2[i] : i3[i];
-            D[o] = __ldg(&P.Dd[ad.w * 36 + o]);
-          }
-        }
-        double x[NPE][DIM], g[NPE][DIM], J;
-#pragma unroll
-        for (int n = 0; n < NPE; ++n) load_node<DIM>(P.X, nd[n], x[n]);
-        simplex_geom<DIM, double>(x, g, &J);
-        const double wgt = J * ((DIM == 2) ? tri4_wsum() : tet5_wsum());
-        double ga[DIM];
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) ga[d] = g[0][d];
-#pragma unroll
-        for (int n = 1; n < NPE; ++n)
-          if (la == n)
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) ga[d] = g[n][d];
-        double eps[NV];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) eps[v] = 0.0;
-#pragma unroll
-        for (int n = 0; n < NPE; ++n) {
-          double u[DIM];
-          load_node<DIM>(P.U, nd[n], u);
-          add_strain<DIM, double>(g[n], u, eps);
-        }
-#pragma unroll
-        for (int c = 0; c < MC; ++c) {
-          if (c >= nc) break;
-          double ek[NV], sig[NV];
-#pragma unroll
-          for (int v = 0; v < NV; ++v) ek[v] = eps[v] + P.eps_cases[c][v];
-          lei_stress<DIM, double>(D, ek, sig);
-#pragma unroll
-          for (int q = 0; q < DIM; ++q) re[c][q] = wgt * bt_sig<DIM, double>(ga, sig, q);
-        }
-      } else if (ax.z >= 0) {
-        double tr[DIM];
-        coh_traction<DIM>(P, ax.z, tr);
-#pragma unroll
-        for (int c = 0; c < MC; ++c) {
-          if (c >= nc) break;
-#pragma unroll
-          for (int q = 0; q < DIM; ++q) re[c][q] = tr[q];
-        }
-      }
-    }
-    const int n_here = min(L, gd.y - e0);
-    for (int jj = 0; jj < n_here; ++jj)
-#pragma unroll
-      for (int c = 0; c < MC; ++c) {
-        if (c >= nc) break;
-#pragma unroll
-        for (int q = 0; q < DIM; ++q) rs[c][q] += __shfl_sync(gmask, re[c][q], jj, L);
-      }
-  }
-  if (!valid || k >= DIM) return;
-  const int gdof = __ldg(&P.growd[(size_t)node * 3 * DIM + k]);
-#pragma unroll
-  for (int c = 0; c < MC; ++c) {
-    if (c >= nc) break;
-    double mine = rs[c][0];
-#pragma unroll
-    for (int q = 1; q < DIM; ++q) if (k == q) mine = rs[c][q];
-    if (gdof < P.n_free) P.Pf_cases[(size_t)c * P.n_free + gdof] = mine;
-    else P.Pp_cases[(size_t)c * P.n_const + gdof - P.n_free] = mine;
-  }
-}
-
 // Set-up: the static part of the general rows next to cut elements (one thread per such node):
 // each cut entry's volumetric block row (K_vol, from k_cut_volumetric) added into the node's
 // neighbour slots and its macroscale-strain response into the node's sum, in entry order.  The

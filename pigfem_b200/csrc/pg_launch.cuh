@@ -25,6 +25,10 @@ void general_static(pg_ctx* c, const pgd::DevProblem& P, double* stat, double* s
 // The residuals of P.n_cases macroscale strains (pg_residual_strains) on the context's stream.
 template <int DIM>
 void residual_cases(pg_ctx* c, const pgd::DevProblem& P);
+// Set-up: the 2D tiles' shape constants (k_tile2_consts) into P, on the allocation stream; a no-op
+// in 3D or without tiles.  0, or 1 when a CUDA call fails.
+template <int DIM>
+int tile_consts(pg_ctx* c, pgd::DevProblem& P);
 
 #ifdef PG_LAUNCH_IMPL
 template <int DIM>
@@ -62,13 +66,13 @@ void assembly(pg_ctx* c, const pgd::DevProblem& P, bool jac, bool fp32) {
     const size_t smem = pgd::tile3_smem_bytes();
     if (!jac) {
       cudaFuncSetAttribute(pgd::k_rows_tile3<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      pgd::k_rows_tile3<double, false><<<c->n_tiles, pgd::kT3Threads, smem, sst>>>(P, c->grid, c->tiles, c->tnodes, c->tsegs);
+      pgd::k_rows_tile3<double, false><<<c->n_tiles, pgd::kT3Threads, smem, sst>>>(P, c->grid, c->tiles, c->tnodes, c->tsegs, *c->t3c);
     } else if (fp32) {
       cudaFuncSetAttribute(pgd::k_rows_tile3<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      pgd::k_rows_tile3<float, true><<<c->n_tiles, pgd::kT3Threads, smem, sst>>>(P, c->grid, c->tiles, c->tnodes, c->tsegs);
+      pgd::k_rows_tile3<float, true><<<c->n_tiles, pgd::kT3Threads, smem, sst>>>(P, c->grid, c->tiles, c->tnodes, c->tsegs, *c->t3c);
     } else {
       cudaFuncSetAttribute(pgd::k_rows_tile3<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      pgd::k_rows_tile3<double, true><<<c->n_tiles, pgd::kT3Threads, smem, sst>>>(P, c->grid, c->tiles, c->tnodes, c->tsegs);
+      pgd::k_rows_tile3<double, true><<<c->n_tiles, pgd::kT3Threads, smem, sst>>>(P, c->grid, c->tiles, c->tnodes, c->tsegs, *c->t3c);
     }
   } else if (c->n_stencil > 0 && !jac) {
     const int tpb = 128;
@@ -154,17 +158,60 @@ void residual_cases(pg_ctx* c, const pgd::DevProblem& P) {
     pgd::k_rows_stencil_cases<DIM><<<grid, 128, 0, c->stream>>>(P, c->grid, c->stencil, c->n_stencil);
   }
   if (P.n_slow_dn > 0) {
-    constexpr int L = 8;
-    const int grid = (int)(((long long)P.n_slow_dn * L + 127) / 128);
-    pgd::k_rows_general_cases<DIM, L><<<grid, 128, 0, c->stream>>>(P);
+    // the general rows' element records with the strain of U (formed once for every case),
+    // then a lane group per general node sums each case's residual as the single-strain
+    // assembly does
+    if (P.n_grec > 0) pgd::k_gen_records_strain<DIM><<<(P.n_grec + 127) / 128, 128, 0, c->stream>>>(P);
+    const int grid = (int)(((long long)P.n_slow_dn * pgd::kGenResidLanes + 127) / 128);
+    pgd::k_gen_resid_cases<DIM><<<grid, 128, 0, c->stream>>>(P);
   }
+}
+
+template <int DIM>
+int tile_consts(pg_ctx* c, pgd::DevProblem& P) {
+  if (c->n_tiles == 0) return 0;
+  const pg::ProblemDesc& d = c->s.desc;
+  if (DIM == 3) {
+    // the 3D shapes into a host copy (the single launches' kernel parameter) and a device copy
+    // (read by the batched launches)
+    const double hx = (d.hi[0] - d.lo[0]) / d.n[0], hy = (d.hi[1] - d.lo[1]) / d.n[1], hz = (d.hi[2] - d.lo[2]) / d.n[2];
+    pgd::Tile3Const* dc = nullptr;
+    if (cudaMallocAsync(&dc, sizeof(pgd::Tile3Const), c->up) != cudaSuccess) return 1;
+    pg_track_alloc(c, dc, sizeof(pgd::Tile3Const));
+    pgd::k_tile3_consts<DIM><<<1, 32, 0, c->up>>>(P, d.lo[0], d.lo[1], d.lo[2], hx, hy, hz, dc);
+    if (!c->t3c) c->t3c = new pgd::Tile3Const;
+    cudaMemcpyAsync(c->t3c, dc, sizeof(pgd::Tile3Const), cudaMemcpyDeviceToHost, c->up);
+    if (cudaStreamSynchronize(c->up) != cudaSuccess) return 1;
+    c->d_t3c = dc;
+    return 0;
+  }
+  const double hx = (d.hi[0] - d.lo[0]) / d.n[0], hy = (d.hi[1] - d.lo[1]) / d.n[1];
+  constexpr int n_out = 24 + 4 + 2 * 432;
+  double* dout = nullptr;
+  if (cudaMallocAsync(&dout, n_out * sizeof(double), c->up) != cudaSuccess) return 1;
+  pgd::k_tile2_consts<DIM><<<1, 32, 0, c->up>>>(P, d.lo[0], d.lo[1], hx, hy, dout);
+  std::vector<double> h(n_out);
+  cudaMemcpyAsync(h.data(), dout, n_out * sizeof(double), cudaMemcpyDeviceToHost, c->up);
+  cudaFreeAsync(dout, c->up);
+  if (cudaStreamSynchronize(c->up) != cudaSuccess) return 1;
+  for (int sh = 0; sh < 4; ++sh) {
+    for (int n = 0; n < 3; ++n) { P.tile_g[sh][n][0] = h[sh * 6 + n * 2]; P.tile_g[sh][n][1] = h[sh * 6 + n * 2 + 1]; }
+    P.tile_w[sh] = h[24 + sh];
+    for (int m = 0; m < 3; ++m)
+      for (int i = 0; i < 36; ++i) {
+        P.tile_ke[sh][m][i] = h[28 + (sh * 3 + m) * 36 + i];
+        P.tile_kef[sh][m][i] = (float)h[28 + 432 + (sh * 3 + m) * 36 + i];
+      }
+  }
+  return 0;
 }
 
 #define PG_INSTANTIATE_LAUNCHES(D)                                                     \
   template void assembly<D>(pg_ctx*, const pgd::DevProblem&, bool, bool);              \
   template void cut_volumetric<D>(pg_ctx*, const pgd::DevProblem&, double*);           \
   template void general_static<D>(pg_ctx*, const pgd::DevProblem&, double*, double*);  \
-  template void residual_cases<D>(pg_ctx*, const pgd::DevProblem&);
+  template void residual_cases<D>(pg_ctx*, const pgd::DevProblem&);                    \
+  template int tile_consts<D>(pg_ctx*, pgd::DevProblem&);
 #endif
 
 }  // namespace pgl

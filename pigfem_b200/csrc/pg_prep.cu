@@ -470,3 +470,281 @@ int device_prep(const ProblemDesc& d, PrepResult& pr, std::string& err) {
 }
 
 }  // namespace pg
+
+// ------------------------------------------------------------------ adjacency and CSR pattern
+// device_pattern forms what build_pattern (pg_setup.cpp) forms, from the same inputs: every
+// element's DOF nodes (structured connectivity, or the cut element's node list), then
+//   dn_adj    (DOF node, element * 32 + local node) keys sorted: each DOF node's entries in
+//             element order;
+//   dn_nbr    (DOF node, DOF node) keys of every node pair of every element, sorted, duplicates
+//             dropped: each DOF node's distinct neighbours in increasing order;
+//   rp / ci   per DOF node the free and constrained columns of its neighbours' DOFs, its rows'
+//             lengths scanned into the four blocks' row pointers, then the columns written.
+#include <cub/cub.cuh>
+
+namespace pgp {
+
+struct PatIn {
+  Grid g;
+  int npe, ne, n_dn, n_free, n_const;
+  const int* cut_of;
+  const int* cut_node_off;
+  const int* cut_nodes;
+  const int* node_dn;
+  const int* dn_node;
+  const int* node_dof;
+};
+
+__device__ __forceinline__ int pat_nodes(const PatIn& in, int e, int* nd) {
+  const int c = in.cut_of[e];
+  if (c < 0) return elem_nodes(in.g, e, nd);
+  const int o = in.cut_node_off[c], m = in.cut_node_off[c + 1] - o;
+  for (int a = 0; a < m; ++a) nd[a] = in.cut_nodes[o + a];
+  return m;
+}
+
+__global__ void k_pat_count(PatIn in, int* m_of, int* m2_of) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= in.ne) return;
+  const int c = in.cut_of[e];
+  const int m = (c < 0) ? in.npe : in.cut_node_off[c + 1] - in.cut_node_off[c];
+  m_of[e] = m;
+  m2_of[e] = m * m;
+}
+
+__global__ void k_pat_fill(PatIn in, const int* adj_off, const int* pair_off, unsigned long long* adj_key,
+                           unsigned long long* pair_key) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= in.ne) return;
+  int nd[32], dn[32];
+  const int m = pat_nodes(in, e, nd);
+  for (int a = 0; a < m; ++a) dn[a] = in.node_dn[nd[a]];
+  unsigned long long* ak = adj_key + adj_off[e];
+  unsigned long long* pk = pair_key + pair_off[e];
+  for (int a = 0; a < m; ++a) {
+    const unsigned long long hi = (unsigned long long)(unsigned)dn[a] << 32;
+    ak[a] = hi | (unsigned)(e * 32 + a);
+    for (int b = 0; b < m; ++b) pk[a * m + b] = hi | (unsigned)dn[b];
+  }
+}
+
+// off[d] = first position of DOF node d in the sorted keys (keys of every d in [0, n_dn) present
+// or not), off[n_dn] = n; low[i] = the key's low word.
+__global__ void k_pat_bounds(const unsigned long long* key, int n, int n_dn, int* off, int* low) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > n) return;
+  const int d = (i < n) ? (int)(key[i] >> 32) : n_dn;
+  const int dp = (i > 0) ? (int)(key[i - 1] >> 32) : -1;
+  for (int x = dp + 1; x <= d; ++x) off[x] = i;
+  if (i < n) low[i] = (int)(unsigned)(key[i] & 0xffffffffull);
+}
+
+// Row lengths: DOF node a's rows get, per block, the count of its neighbours' free / constrained
+// DOFs.  rp[b] holds lengths at [row + 1] (the scan follows).
+__global__ void k_pat_rowlen(PatIn in, const int* nbr_off, const int* nbr, int* rp0, int* rp1, int* rp2, int* rp3) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= in.n_dn) return;
+  const int dim = in.g.dim;
+  int cf = 0, cp = 0;
+  for (int k = nbr_off[a]; k < nbr_off[a + 1]; ++k) {
+    const int nbn = in.dn_node[nbr[k]];
+    for (int q = 0; q < dim; ++q) { if (in.node_dof[nbn * dim + q] < in.n_free) cf++; else cp++; }
+  }
+  const int na = in.dn_node[a];
+  for (int q = 0; q < dim; ++q) {
+    const int gq = in.node_dof[na * dim + q];
+    if (gq < in.n_free) { rp0[gq + 1] = cf; rp1[gq + 1] = cp; }
+    else { rp2[gq - in.n_free + 1] = cf; rp3[gq - in.n_free + 1] = cp; }
+  }
+}
+
+__global__ void k_pat_cols(PatIn in, const int* nbr_off, const int* nbr, const int* rp0, const int* rp1,
+                           const int* rp2, const int* rp3, int* ci0, int* ci1, int* ci2, int* ci3) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= in.n_dn) return;
+  const int dim = in.g.dim;
+  const int na = in.dn_node[a];
+  for (int q = 0; q < dim; ++q) {
+    const int gq = in.node_dof[na * dim + q];
+    const bool rf = gq < in.n_free;
+    int pf = rf ? rp0[gq] : rp2[gq - in.n_free];
+    int pp = rf ? rp1[gq] : rp3[gq - in.n_free];
+    int* cif = rf ? ci0 : ci2;
+    int* cip = rf ? ci1 : ci3;
+    for (int k = nbr_off[a]; k < nbr_off[a + 1]; ++k) {
+      const int nbn = in.dn_node[nbr[k]];
+      for (int q2 = 0; q2 < dim; ++q2) {
+        const int g2 = in.node_dof[nbn * dim + q2];
+        if (g2 < in.n_free) cif[pf++] = g2; else cip[pp++] = g2 - in.n_free;
+      }
+    }
+  }
+}
+
+}  // namespace pgp
+
+namespace pg {
+
+namespace {
+// Stream-ordered allocations freed together when the scope ends.
+struct DevAllocs {
+  cudaStream_t st;
+  std::vector<void*> p;
+  bool failed = false;
+  explicit DevAllocs(cudaStream_t s) : st(s) {}
+  template <class T>
+  T* get(size_t n) {
+    void* q = nullptr;
+    if (cudaMallocAsync(&q, std::max<size_t>(1, n) * sizeof(T), st) != cudaSuccess) { failed = true; return nullptr; }
+    p.push_back(q);
+    return static_cast<T*>(q);
+  }
+  ~DevAllocs() { for (void* q : p) cudaFreeAsync(q, st); }
+};
+template <class T>
+T* upload_vec(DevAllocs& A, const std::vector<T>& v) {
+  T* d = A.get<T>(v.size());
+  if (d && !v.empty()) cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, A.st);
+  return d;
+}
+}  // namespace
+
+int device_pattern(Setup& s, std::string& err, double* device_ms) {
+  const int dim = s.dim;
+  pgp::PatIn in{};
+  in.g.dim = dim;
+  in.g.etype = s.etype;
+  in.g.nx = s.desc.n[0]; in.g.ny = s.desc.n[1]; in.g.nz = (dim == 3) ? s.desc.n[2] : 0;
+  in.npe = s.npe; in.ne = s.ne; in.n_dn = s.n_dn; in.n_free = s.n_free; in.n_const = s.n_const;
+  // element sizes and their totals (64-bit on the host: a pattern beyond int32 stops here)
+  long long n_adj = 0, n_pair = 0;
+  {
+    std::vector<int> cm(s.ncut);
+    for (int c = 0; c < s.ncut; ++c) {
+      cm[c] = s.cut_node_off[c + 1] - s.cut_node_off[c];
+      if (cm[c] > 32) { err = "element with more than 32 nodes"; return 8; }
+      n_adj += cm[c]; n_pair += (long long)cm[c] * cm[c];
+    }
+    n_adj += (long long)(s.ne - s.ncut) * s.npe;
+    n_pair += (long long)(s.ne - s.ncut) * s.npe * s.npe;
+  }
+  if (n_adj > 2147483647LL || n_pair > 2147483647LL) { err = "mesh too large"; return 2; }
+  cudaStream_t st;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) { err = "cudaStreamCreate failed"; return 10; }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  int rc = 0;
+  {
+    DevAllocs A(st);
+    in.cut_of = upload_vec(A, s.cut_of);
+    in.cut_node_off = upload_vec(A, s.cut_node_off);
+    in.cut_nodes = upload_vec(A, s.cut_nodes);
+    in.node_dn = upload_vec(A, s.node_dn);
+    in.dn_node = upload_vec(A, s.dn_node);
+    in.node_dof = upload_vec(A, s.node_dof);
+    const int ne = s.ne, na = (int)n_adj, np = (int)n_pair, ndn = s.n_dn;
+    int* m_of = A.get<int>(ne);
+    int* m2_of = A.get<int>(ne);
+    int* adj_off = A.get<int>(ne);
+    int* pair_off = A.get<int>(ne);
+    unsigned long long* ak = A.get<unsigned long long>(na);
+    unsigned long long* ak2 = A.get<unsigned long long>(na);
+    unsigned long long* pk = A.get<unsigned long long>(np);
+    unsigned long long* pk2 = A.get<unsigned long long>(np);
+    int* adj_o = A.get<int>(ndn + 1);
+    int* adj_v = A.get<int>(na);
+    int* nbr_o = A.get<int>(ndn + 1);
+    int* n_sel = A.get<int>(1);
+    int *rp[4], *ci[4];
+    const int nrows[4] = {s.n_free, s.n_free, s.n_const, s.n_const};
+    for (int b = 0; b < 4; ++b) rp[b] = A.get<int>(nrows[b] + 1);
+    // CUB temporary storage: the largest of the scans, sorts and the unique selection
+    int dn_bits = 1;
+    while ((1LL << dn_bits) <= ndn) ++dn_bits;
+    size_t t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, t1, m_of, adj_off, ne, st);
+    cub::DeviceRadixSort::SortKeys(nullptr, t2, ak, ak2, na, 0, 32 + dn_bits, st);
+    cub::DeviceRadixSort::SortKeys(nullptr, t3, pk, pk2, np, 0, 32 + dn_bits, st);
+    cub::DeviceSelect::Unique(nullptr, t4, pk2, pk, n_sel, np, st);
+    cub::DeviceScan::InclusiveSum(nullptr, t5, rp[0] + 1, rp[0] + 1, std::max(s.n_free, s.n_const), st);
+    const size_t tb = std::max(std::max(std::max(t1, t2), std::max(t3, t4)), t5);
+    void* tmp = A.get<char>(tb);
+    if (A.failed) { err = "device memory for the pattern"; rc = 10; }
+    if (!rc) {
+      pgp::k_pat_count<<<(ne + 255) / 256, 256, 0, st>>>(in, m_of, m2_of);
+      size_t tbb = tb;
+      cub::DeviceScan::ExclusiveSum(tmp, tbb, m_of, adj_off, ne, st);
+      tbb = tb;
+      cub::DeviceScan::ExclusiveSum(tmp, tbb, m2_of, pair_off, ne, st);
+      pgp::k_pat_fill<<<(ne + 127) / 128, 128, 0, st>>>(in, adj_off, pair_off, ak, pk);
+      tbb = tb;
+      cub::DeviceRadixSort::SortKeys(tmp, tbb, ak, ak2, na, 0, 32 + dn_bits, st);
+      pgp::k_pat_bounds<<<(na + 256) / 256, 256, 0, st>>>(ak2, na, ndn, adj_o, adj_v);
+      tbb = tb;
+      cub::DeviceRadixSort::SortKeys(tmp, tbb, pk, pk2, np, 0, 32 + dn_bits, st);
+      tbb = tb;
+      cub::DeviceSelect::Unique(tmp, tbb, pk2, pk, n_sel, np, st);
+      int nnb = 0;
+      cudaMemcpyAsync(&nnb, n_sel, sizeof(int), cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess) { err = "device pattern failed"; rc = 10; }
+      int* nbr_v = rc ? nullptr : A.get<int>(nnb);
+      if (!rc && A.failed) { err = "device memory for the pattern"; rc = 10; }
+      if (!rc) {
+        pgp::k_pat_bounds<<<(nnb + 256) / 256, 256, 0, st>>>(pk, nnb, ndn, nbr_o, nbr_v);
+        for (int b = 0; b < 4; ++b) cudaMemsetAsync(rp[b], 0, (nrows[b] + 1) * sizeof(int), st);
+        pgp::k_pat_rowlen<<<(ndn + 127) / 128, 128, 0, st>>>(in, nbr_o, nbr_v, rp[0], rp[1], rp[2], rp[3]);
+        for (int b = 0; b < 4; ++b)
+          if (nrows[b] > 0) {
+            tbb = tb;
+            cub::DeviceScan::InclusiveSum(tmp, tbb, rp[b] + 1, rp[b] + 1, nrows[b], st);
+          }
+        int tot[4] = {0, 0, 0, 0};
+        for (int b = 0; b < 4; ++b) cudaMemcpyAsync(&tot[b], rp[b] + nrows[b], sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) { err = "device pattern failed"; rc = 10; }
+        if (!rc) {
+          for (int b = 0; b < 4; ++b) ci[b] = A.get<int>(tot[b]);
+          if (A.failed) { err = "device memory for the pattern"; rc = 10; }
+        }
+        if (!rc) {
+          pgp::k_pat_cols<<<(ndn + 127) / 128, 128, 0, st>>>(in, nbr_o, nbr_v, rp[0], rp[1], rp[2], rp[3], ci[0], ci[1],
+                                                              ci[2], ci[3]);
+          // results
+          s.dn_adj_off.resize(ndn + 1);
+          s.dn_adj.resize(na);
+          s.dn_nbr_off.resize(ndn + 1);
+          s.dn_nbr.resize(nnb);
+          cudaMemcpyAsync(s.dn_adj_off.data(), adj_o, (ndn + 1) * sizeof(int), cudaMemcpyDeviceToHost, st);
+          cudaMemcpyAsync(s.dn_adj.data(), adj_v, (size_t)na * sizeof(int), cudaMemcpyDeviceToHost, st);
+          cudaMemcpyAsync(s.dn_nbr_off.data(), nbr_o, (ndn + 1) * sizeof(int), cudaMemcpyDeviceToHost, st);
+          cudaMemcpyAsync(s.dn_nbr.data(), nbr_v, (size_t)nnb * sizeof(int), cudaMemcpyDeviceToHost, st);
+          s.nrows[0] = s.n_free; s.ncols[0] = s.n_free;
+          s.nrows[1] = s.n_free; s.ncols[1] = s.n_const;
+          s.nrows[2] = s.n_const; s.ncols[2] = s.n_free;
+          s.nrows[3] = s.n_const; s.ncols[3] = s.n_const;
+          for (int b = 0; b < 4; ++b) {
+            s.rp[b].resize(nrows[b] + 1);
+            s.ci[b].resize(tot[b]);
+            cudaMemcpyAsync(s.rp[b].data(), rp[b], (nrows[b] + 1) * sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (tot[b] > 0) cudaMemcpyAsync(s.ci[b].data(), ci[b], (size_t)tot[b] * sizeof(int), cudaMemcpyDeviceToHost, st);
+          }
+          if (cudaStreamSynchronize(st) != cudaSuccess) { err = "device pattern failed"; rc = 10; }
+        }
+      }
+    }
+    cudaEventRecord(e1, st);
+  }
+  if (!rc && cudaStreamSynchronize(st) != cudaSuccess) { err = "device pattern failed"; rc = 10; }
+  if (!rc && device_ms) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    *device_ms = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(st);
+  return rc;
+}
+
+}  // namespace pg

@@ -585,6 +585,126 @@ const int kTetEdge[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
 
 }  // namespace
 
+// The DOF nodes' adjacency (element, local node) in element order, their sorted distinct
+// neighbours and the CSR pattern of the four blocks (Solver::preallocate_matrix with
+// populate_local_neighbors, src/Solver.cpp:426-490, 772-896: every DOF pair of every element).
+int build_pattern(Setup& s) {
+  const int dim = s.dim;
+  auto elem_n = [&](int e) {
+    const int c = s.cut_of[e];
+    return c < 0 ? s.npe : s.cut_node_off[c + 1] - s.cut_node_off[c];
+  };
+  auto elem_node = [&](int e, int a) {
+    const int c = s.cut_of[e];
+    return c < 0 ? s.conn[(size_t)e * s.npe + a] : s.cut_nodes[s.cut_node_off[c] + a];
+  };
+  // Adjacency of every DOF node in element order (element, local node) and its sorted distinct
+  // neighbours.  Elements are split into contiguous chunks; each chunk counts its entries per DOF
+  // node, the counts place every chunk's entries after the earlier chunks' (so each node's list
+  // stays in element order), and the chunks fill their places in parallel.
+  for (int e = 0; e < s.ne; ++e)
+    if (elem_n(e) > 32) { s.error = "element with more than 32 nodes"; return 8; }
+  const int nt = setup_threads();
+  std::vector<std::vector<long long>> cadj(nt, std::vector<long long>(s.n_dn, 0)), cnb(nt, std::vector<long long>(s.n_dn, 0));
+  chunked(s.ne, nt, [&](int k, int e0, int e1) {
+    for (int e = e0; e < e1; ++e) {
+      const int m = elem_n(e);
+      for (int a = 0; a < m; ++a) {
+        const int da = s.node_dn[elem_node(e, a)];
+        cadj[k][da] += 1;
+        cnb[k][da] += m;
+      }
+    }
+  });
+  std::vector<long long> adj_off(s.n_dn + 1, 0), nb_off(s.n_dn + 1, 0);
+  for (int a = 0; a < s.n_dn; ++a) {
+    long long ta = adj_off[a], tb = nb_off[a];
+    for (int k = 0; k < nt; ++k) {
+      const long long ca = cadj[k][a], cb = cnb[k][a];
+      cadj[k][a] = ta; cnb[k][a] = tb;   // the chunk's first place for this node
+      ta += ca; tb += cb;
+    }
+    adj_off[a + 1] = ta; nb_off[a + 1] = tb;
+  }
+  if (adj_off[s.n_dn] > 2147483647LL || nb_off[s.n_dn] > 2147483647LL) { s.error = "mesh too large"; return 2; }
+  s.dn_adj.assign((size_t)adj_off[s.n_dn], 0);
+  std::vector<int> nb_all((size_t)nb_off[s.n_dn]);
+  chunked(s.ne, nt, [&](int k, int e0, int e1) {
+    for (int e = e0; e < e1; ++e) {
+      const int m = elem_n(e);
+      for (int a = 0; a < m; ++a) {
+        const int da = s.node_dn[elem_node(e, a)];
+        s.dn_adj[(size_t)cadj[k][da]++] = e * 32 + a;
+        long long& p = cnb[k][da];
+        for (int b = 0; b < m; ++b) nb_all[(size_t)p++] = s.node_dn[elem_node(e, b)];
+      }
+    }
+  });
+  s.dn_adj_off.resize(s.n_dn + 1);
+  for (int a = 0; a <= s.n_dn; ++a) s.dn_adj_off[a] = (int)adj_off[a];
+  std::vector<int> nb_cnt(s.n_dn);
+  chunked(s.n_dn, nt, [&](int, int a0, int a1) {
+    for (int a = a0; a < a1; ++a) {
+      int* b = nb_all.data() + nb_off[a];
+      int* e = nb_all.data() + nb_off[a + 1];
+      std::sort(b, e);
+      nb_cnt[a] = (int)(std::unique(b, e) - b);
+    }
+  });
+  s.dn_nbr_off.assign(s.n_dn + 1, 0);
+  for (int a = 0; a < s.n_dn; ++a) s.dn_nbr_off[a + 1] = s.dn_nbr_off[a] + nb_cnt[a];
+  s.dn_nbr.resize(s.dn_nbr_off[s.n_dn]);
+  chunked(s.n_dn, nt, [&](int, int a0, int a1) {
+    for (int a = a0; a < a1; ++a)
+      std::copy(nb_all.begin() + nb_off[a], nb_all.begin() + nb_off[a] + nb_cnt[a], s.dn_nbr.begin() + s.dn_nbr_off[a]);
+  });
+  // CSR of the four blocks; rows in DOF order follow DOF-node order.
+  s.nrows[0] = s.n_free; s.ncols[0] = s.n_free;
+  s.nrows[1] = s.n_free; s.ncols[1] = s.n_const;
+  s.nrows[2] = s.n_const; s.ncols[2] = s.n_free;
+  s.nrows[3] = s.n_const; s.ncols[3] = s.n_const;
+  for (int b = 0; b < 4; ++b) { s.rp[b].assign(s.nrows[b] + 1, 0); s.ci[b].clear(); }
+  // row lengths (each DOF node writes only its own rows' entries)
+  chunked(s.n_dn, nt, [&](int, int a0, int a1) {
+  for (int a = a0; a < a1; ++a) {
+    const int na = s.dn_node[a];
+    int cf = 0, cp = 0;
+    for (int k = s.dn_nbr_off[a]; k < s.dn_nbr_off[a + 1]; ++k) {
+      const int nbn = s.dn_node[s.dn_nbr[k]];
+      for (int q = 0; q < dim; ++q) { if (s.node_dof[(size_t)nbn * dim + q] < s.n_free) cf++; else cp++; }
+    }
+    for (int q = 0; q < dim; ++q) {
+      const int g = s.node_dof[(size_t)na * dim + q];
+      if (g < s.n_free) { s.rp[0][g + 1] = cf; s.rp[1][g + 1] = cp; }
+      else { s.rp[2][g - s.n_free + 1] = cf; s.rp[3][g - s.n_free + 1] = cp; }
+    }
+  }
+  });
+  for (int b = 0; b < 4; ++b) for (int r = 0; r < s.nrows[b]; ++r) s.rp[b][r + 1] += s.rp[b][r];
+  for (int b = 0; b < 4; ++b) s.ci[b].assign(s.rp[b][s.nrows[b]], -1);
+  chunked(s.n_dn, nt, [&](int, int a0, int a1) {
+  for (int a = a0; a < a1; ++a) {
+    const int na = s.dn_node[a];
+    for (int q = 0; q < dim; ++q) {
+      const int g = s.node_dof[(size_t)na * dim + q];
+      const bool rf = g < s.n_free;
+      int pf = rf ? s.rp[0][g] : s.rp[2][g - s.n_free];
+      int pp = rf ? s.rp[1][g] : s.rp[3][g - s.n_free];
+      int* cif = rf ? s.ci[0].data() : s.ci[2].data();
+      int* cip = rf ? s.ci[1].data() : s.ci[3].data();
+      for (int k = s.dn_nbr_off[a]; k < s.dn_nbr_off[a + 1]; ++k) {
+        const int nbn = s.dn_node[s.dn_nbr[k]];
+        for (int q2 = 0; q2 < dim; ++q2) {
+          const int g2 = s.node_dof[(size_t)nbn * dim + q2];
+          if (g2 < s.n_free) cif[pf++] = g2; else cip[pp++] = g2 - s.n_free;
+        }
+      }
+    }
+  }
+  });
+  return 0;
+}
+
 int build_setup(const ProblemDesc& d, Setup& s, const PrepResult* pr) {
   s = Setup();
   if (pr && !pr->valid) pr = nullptr;
@@ -1331,119 +1451,9 @@ int build_setup(const ProblemDesc& d, Setup& s, const PrepResult* pr) {
   for (int n = 0; n < n_nodes; ++n)
     if (s.dnode[n] == n) { s.node_dn[n] = s.n_dn++; s.dn_node.push_back(n); }
   for (int n = 0; n < n_nodes; ++n) s.node_dn[n] = s.node_dn[s.dnode[n]];
-  // Adjacency of every DOF node in element order (element, local node) and its sorted distinct
-  // neighbours.  Elements are split into contiguous chunks; each chunk counts its entries per DOF
-  // node, the counts place every chunk's entries after the earlier chunks' (so each node's list
-  // stays in element order), and the chunks fill their places in parallel.
-  auto elem_n = [&](int e) {
-    const int c = s.cut_of[e];
-    return c < 0 ? s.npe : s.cut_node_off[c + 1] - s.cut_node_off[c];
-  };
-  auto elem_node = [&](int e, int a) {
-    const int c = s.cut_of[e];
-    return c < 0 ? s.conn[(size_t)e * s.npe + a] : s.cut_nodes[s.cut_node_off[c] + a];
-  };
-  for (int e = 0; e < s.ne; ++e)
-    if (elem_n(e) > 32) { s.error = "element with more than 32 nodes"; return 8; }
-  const int nt = setup_threads();
-  std::vector<std::vector<long long>> cadj(nt, std::vector<long long>(s.n_dn, 0)), cnb(nt, std::vector<long long>(s.n_dn, 0));
-  chunked(s.ne, nt, [&](int k, int e0, int e1) {
-    for (int e = e0; e < e1; ++e) {
-      const int m = elem_n(e);
-      for (int a = 0; a < m; ++a) {
-        const int da = s.node_dn[elem_node(e, a)];
-        cadj[k][da] += 1;
-        cnb[k][da] += m;
-      }
-    }
-  });
-  std::vector<long long> adj_off(s.n_dn + 1, 0), nb_off(s.n_dn + 1, 0);
-  for (int a = 0; a < s.n_dn; ++a) {
-    long long ta = adj_off[a], tb = nb_off[a];
-    for (int k = 0; k < nt; ++k) {
-      const long long ca = cadj[k][a], cb = cnb[k][a];
-      cadj[k][a] = ta; cnb[k][a] = tb;   // the chunk's first place for this node
-      ta += ca; tb += cb;
-    }
-    adj_off[a + 1] = ta; nb_off[a + 1] = tb;
-  }
-  if (adj_off[s.n_dn] > 2147483647LL || nb_off[s.n_dn] > 2147483647LL) { s.error = "mesh too large"; return 2; }
-  s.dn_adj.assign((size_t)adj_off[s.n_dn], 0);
-  std::vector<int> nb_all((size_t)nb_off[s.n_dn]);
-  chunked(s.ne, nt, [&](int k, int e0, int e1) {
-    for (int e = e0; e < e1; ++e) {
-      const int m = elem_n(e);
-      for (int a = 0; a < m; ++a) {
-        const int da = s.node_dn[elem_node(e, a)];
-        s.dn_adj[(size_t)cadj[k][da]++] = e * 32 + a;
-        long long& p = cnb[k][da];
-        for (int b = 0; b < m; ++b) nb_all[(size_t)p++] = s.node_dn[elem_node(e, b)];
-      }
-    }
-  });
-  s.dn_adj_off.resize(s.n_dn + 1);
-  for (int a = 0; a <= s.n_dn; ++a) s.dn_adj_off[a] = (int)adj_off[a];
-  std::vector<int> nb_cnt(s.n_dn);
-  chunked(s.n_dn, nt, [&](int, int a0, int a1) {
-    for (int a = a0; a < a1; ++a) {
-      int* b = nb_all.data() + nb_off[a];
-      int* e = nb_all.data() + nb_off[a + 1];
-      std::sort(b, e);
-      nb_cnt[a] = (int)(std::unique(b, e) - b);
-    }
-  });
-  s.dn_nbr_off.assign(s.n_dn + 1, 0);
-  for (int a = 0; a < s.n_dn; ++a) s.dn_nbr_off[a + 1] = s.dn_nbr_off[a] + nb_cnt[a];
-  s.dn_nbr.resize(s.dn_nbr_off[s.n_dn]);
-  chunked(s.n_dn, nt, [&](int, int a0, int a1) {
-    for (int a = a0; a < a1; ++a)
-      std::copy(nb_all.begin() + nb_off[a], nb_all.begin() + nb_off[a] + nb_cnt[a], s.dn_nbr.begin() + s.dn_nbr_off[a]);
-  });
-  // CSR of the four blocks; rows in DOF order follow DOF-node order.
-  s.nrows[0] = s.n_free; s.ncols[0] = s.n_free;
-  s.nrows[1] = s.n_free; s.ncols[1] = s.n_const;
-  s.nrows[2] = s.n_const; s.ncols[2] = s.n_free;
-  s.nrows[3] = s.n_const; s.ncols[3] = s.n_const;
-  for (int b = 0; b < 4; ++b) { s.rp[b].assign(s.nrows[b] + 1, 0); s.ci[b].clear(); }
-  // row lengths (each DOF node writes only its own rows' entries)
-  chunked(s.n_dn, nt, [&](int, int a0, int a1) {
-  for (int a = a0; a < a1; ++a) {
-    const int na = s.dn_node[a];
-    int cf = 0, cp = 0;
-    for (int k = s.dn_nbr_off[a]; k < s.dn_nbr_off[a + 1]; ++k) {
-      const int nbn = s.dn_node[s.dn_nbr[k]];
-      for (int q = 0; q < dim; ++q) { if (s.node_dof[(size_t)nbn * dim + q] < s.n_free) cf++; else cp++; }
-    }
-    for (int q = 0; q < dim; ++q) {
-      const int g = s.node_dof[(size_t)na * dim + q];
-      if (g < s.n_free) { s.rp[0][g + 1] = cf; s.rp[1][g + 1] = cp; }
-      else { s.rp[2][g - s.n_free + 1] = cf; s.rp[3][g - s.n_free + 1] = cp; }
-    }
-  }
-  });
-  for (int b = 0; b < 4; ++b) for (int r = 0; r < s.nrows[b]; ++r) s.rp[b][r + 1] += s.rp[b][r];
-  for (int b = 0; b < 4; ++b) s.ci[b].assign(s.rp[b][s.nrows[b]], -1);
-  chunked(s.n_dn, nt, [&](int, int a0, int a1) {
-  for (int a = a0; a < a1; ++a) {
-    const int na = s.dn_node[a];
-    for (int q = 0; q < dim; ++q) {
-      const int g = s.node_dof[(size_t)na * dim + q];
-      const bool rf = g < s.n_free;
-      int pf = rf ? s.rp[0][g] : s.rp[2][g - s.n_free];
-      int pp = rf ? s.rp[1][g] : s.rp[3][g - s.n_free];
-      int* cif = rf ? s.ci[0].data() : s.ci[2].data();
-      int* cip = rf ? s.ci[1].data() : s.ci[3].data();
-      for (int k = s.dn_nbr_off[a]; k < s.dn_nbr_off[a + 1]; ++k) {
-        const int nbn = s.dn_node[s.dn_nbr[k]];
-        for (int q2 = 0; q2 < dim; ++q2) {
-          const int g2 = s.node_dof[(size_t)nbn * dim + q2];
-          if (g2 < s.n_free) cif[pf++] = g2; else cip[pp++] = g2 - s.n_free;
-        }
-      }
-    }
-  }
-  });
-  return 0;
+  if (pr && pr->pattern_on_device) return 0;   // the caller forms the adjacency and the pattern
+  return build_pattern(s);
+
 }
 
 }  // namespace pg

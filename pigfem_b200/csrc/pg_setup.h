@@ -132,12 +132,20 @@ struct PrepResult {
   std::vector<double> XE;               // per enrichment node: 3 coordinates
   int no_sign_change = -1;              // first enrichment node whose edge has no sign change, or -1
   std::vector<int> std_dof;             // standard node * dim: free index >= 0, or -1 - (constrained index)
+  bool pattern_on_device = false;       // build_setup leaves the adjacency and the pattern to device_pattern
   double device_ms = 0.0;               // device time of the passes
 };
 
 // Runs the device passes of pg_prep.cu; 0 on success (pr.valid false when the mesh is outside
 // what they cover), nonzero with err set when a CUDA call fails.
 int device_prep(const ProblemDesc& d, PrepResult& pr, std::string& err);
+
+// The DOF nodes' adjacency and neighbour lists and the CSR pattern of the four blocks, from the
+// rest of the set-up: on the host (build_pattern) or on the device (device_pattern, pg_prep.cu;
+// the same tables bit for bit).  0 on success; device_pattern returns nonzero with err set when a
+// CUDA call fails, build_pattern with Setup::error set when the mesh is too large.
+int build_pattern(Setup& s);
+int device_pattern(Setup& s, std::string& err, double* device_ms);
 
 // Returns 0 on success, a nonzero status with Setup::error filled otherwise.  pr (optional, valid)
 // supplies the node detection, the element pass, the enrichment nodes and the standard nodes' DOF
