@@ -262,17 +262,18 @@ UNIT_STRAINS_3D = [tuple(1.0 if i == k else 0.0 for i in range(6)) for k in rang
 
 def setup_times(R) -> dict:
     """Wall time of the set-up of R's mesh (host-only context, no upload) with every pass on the
-    host (pg_create_host) and with the per-node / per-element passes on the device
-    (pg_create_prep_device); each the best of two, outside the timed region."""
+    host (pg_create_host), with the per-node / per-element passes on the device, and with the
+    pattern on the device too (pg_create_prep_device); each the best of two, outside the timed
+    region."""
     from pigfem_b200 import capi
     out = {}
-    for key, prep in (("host_s", False), ("device_prep_s", True)):
+    for key, prep, pat in (("host_s", False, False), ("device_nodes_s", True, False), ("device_prep_s", True, True)):
         best = None
         for _ in range(2):
             t = time.perf_counter()
-            Q = capi.Problem(R.desc, device=False, prep_device=prep)
+            Q = capi.Problem(R.desc, device=False, prep_device=prep, prep_pattern=pat)
             dt = time.perf_counter() - t
-            if prep:
+            if prep and pat:
                 out["device_passes_ms"] = Q.prep_device_ms()
             Q.close()
             best = dt if best is None else min(best, dt)

@@ -103,8 +103,8 @@ int pg_create(const pg_problem_desc* desc, pg_ctx** out);
  * set-up tables can be read back) and the upload that makes the context assemble-ready. */
 int pg_create_host(const pg_problem_desc* desc, pg_ctx** out);
 int pg_upload(pg_ctx* ctx);
-/* pg_create_host with the set-up's per-node, per-element and pattern passes on the current CUDA
- * device: node detection (Mesh::detect_node, src/Mesh.cpp:2727-2929), the all-equal element test
+/* pg_create_host with the set-up's per-node, per-element and (PG_PREP_PATTERN) pattern passes on
+ * the current CUDA device: node detection (Mesh::detect_node, src/Mesh.cpp:2727-2929), the all-equal element test
  * of the element detection (Tri3/Quad4/Tet4::detection), the enrichment nodes and their
  * intersection points (Mesh::add_enrichments, src/Mesh.cpp:3103-3252; Inclusion::
  * find_intersection, src/Inclusion.cpp:32-121), the standard nodes' DOF numbering (DofObject::
@@ -113,7 +113,12 @@ int pg_upload(pg_ctx* ctx);
  * The cut elements' case tables and sub-element quadrature stay on the host.  Every table is the
  * one pg_create_host forms (integers bit-exact, coordinates too); the context is host-only until
  * pg_upload.  Grids of fewer than 2 cells per direction run every pass on the host. */
-int pg_create_prep_device(const pg_problem_desc* desc, pg_ctx** out);
+int pg_create_prep_device(const pg_problem_desc* desc, int passes, pg_ctx** out);
+/* passes of pg_create_prep_device: the per-node and per-element passes, and the adjacency and
+ * pattern (the latter sorts every element's node pairs; a caller whose GPU is busy with other
+ * work may keep it on the host threads) */
+#define PG_PREP_NODES 1
+#define PG_PREP_PATTERN 2
 /* Device time in ms of the passes pg_create_prep_device ran (-1 when none ran). */
 int pg_prep_device_ms(const pg_ctx* ctx, double* ms);
 /* Read-only view of a set-up table by name (cut-element quadrature, topology); returns 1 for

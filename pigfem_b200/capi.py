@@ -28,6 +28,7 @@ SENS_E, SENS_LAMBDA, SENS_MU, SENS_K, SENS_NU = range(5)
 COH_NONE, COH_BL, COH_BLNU, COH_XN, COH_XNNU, COH_OP, COH_OPNU, COH_OPAUG, COH_OPNUAUG = range(9)
 COH_TL, COH_TLNU, COH_STL, COH_STLNU = range(9, 13)   # trilinear and smoothed trilinear
 FUNC, JAC, FP32, KEEP_STATIC = 1, 2, 4, 8
+PREP_NODES, PREP_PATTERN = 1, 2
 ERRORS = {2: "PG_ERR_INPUT", 3: "PG_ERR_GEOMETRY", 4: "PG_ERR_UNSUPPORTED", 7: "PG_ERR_JACOBIAN",
           10: "PG_ERR_DEVICE", 11: "PG_ERR_NONFINITE", 12: "PG_ERR_STATE"}
 
@@ -83,7 +84,7 @@ def load_library(path: Optional[str] = None):
     sig = {
         "pg_create": (i32, [ctypes.POINTER(_Desc), ctypes.POINTER(vp)]),
         "pg_create_host": (i32, [ctypes.POINTER(_Desc), ctypes.POINTER(vp)]),
-        "pg_create_prep_device": (i32, [ctypes.POINTER(_Desc), ctypes.POINTER(vp)]),
+        "pg_create_prep_device": (i32, [ctypes.POINTER(_Desc), i32, ctypes.POINTER(vp)]),
         "pg_prep_device_ms": (i32, [vp, ctypes.POINTER(ctypes.c_double)]),
         "pg_upload": (i32, [vp]),
         "pg_debug_array": (i32, [vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(vp)]),
@@ -171,9 +172,10 @@ class ProblemDesc:
 class Problem:
     """One enriched mesh resident on the GPU (a ``pg_ctx``)."""
 
-    def __init__(self, desc: ProblemDesc, device: bool = True, prep_device: bool = False):
+    def __init__(self, desc: ProblemDesc, device: bool = True, prep_device: bool = False, prep_pattern: bool = True):
         """``prep_device``: run the set-up's node detection, element pass, enrichment nodes and
-        standard DOF numbering on the GPU (pg_create_prep_device); the tables are the same."""
+        standard DOF numbering on the GPU (pg_create_prep_device), and with ``prep_pattern`` the
+        adjacency and CSR pattern too; the tables are the same."""
         L = load_library()
         self.desc = desc
         dim = desc.dim
@@ -200,8 +202,10 @@ class Problem:
             d.ply[i] = v
         self._d = d
         h = ctypes.c_void_p(0)
-        create = L.pg_create_prep_device if prep_device else L.pg_create_host
-        rc = create(ctypes.byref(d), ctypes.byref(h))
+        if prep_device:
+            rc = L.pg_create_prep_device(ctypes.byref(d), PREP_NODES | (PREP_PATTERN if prep_pattern else 0), ctypes.byref(h))
+        else:
+            rc = L.pg_create_host(ctypes.byref(d), ctypes.byref(h))
         self.h = h
         if rc:
             msg = L.pg_last_error(h).decode() if h.value else "invalid description"

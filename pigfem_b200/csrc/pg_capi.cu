@@ -110,7 +110,7 @@ int pg_alloc_sync(pg_ctx* c) {
 
 extern "C" {
 
-static int create_host(const pg_problem_desc* d, pg_ctx** out, bool device_prep) {
+static int create_host(const pg_problem_desc* d, pg_ctx** out, bool device_prep, bool device_pattern) {
   if (!d || !out) return PG_ERR_INPUT;
   *out = nullptr;
   pg_ctx* c = new pg_ctx;
@@ -133,7 +133,7 @@ static int create_host(const pg_problem_desc* d, pg_ctx** out, bool device_prep)
     std::string why;
     if (pg::device_prep(pd, pr, why)) { c->err = why; *out = c; return PG_ERR_DEVICE; }
     c->prep_ms = pr.valid ? pr.device_ms : -1.0;
-    pr.pattern_on_device = pr.valid;
+    pr.pattern_on_device = pr.valid && device_pattern;
   }
   int rc = pg::build_setup(pd, c->s, device_prep ? &pr : nullptr);
   if (!rc && pr.pattern_on_device) {
@@ -150,9 +150,12 @@ static int create_host(const pg_problem_desc* d, pg_ctx** out, bool device_prep)
   return 0;
 }
 
-int pg_create_host(const pg_problem_desc* d, pg_ctx** out) { return create_host(d, out, false); }
+int pg_create_host(const pg_problem_desc* d, pg_ctx** out) { return create_host(d, out, false, false); }
 
-int pg_create_prep_device(const pg_problem_desc* d, pg_ctx** out) { return create_host(d, out, true); }
+int pg_create_prep_device(const pg_problem_desc* d, int passes, pg_ctx** out) {
+  if (!(passes & PG_PREP_NODES)) return create_host(d, out, false, false);
+  return create_host(d, out, true, (passes & PG_PREP_PATTERN) != 0);
+}
 
 int pg_prep_device_ms(const pg_ctx* c, double* ms) {
   if (!c || !ms) return PG_ERR_INPUT;
@@ -693,11 +696,15 @@ int pg_upload(pg_ctx* c) {
   PG_TRY(dalloc(c, 1, &c->d_err));
   P.err = c->d_err;
   PG_TRY(dalloc(c, 1024, &c->d_red));
-  // Static part of the general rows next to cut elements: the general nodes are sorted with the
-  // ones that have cut adjacent elements first, so those form the prefix [0, n_stat).  Each gets
-  // its neighbour slots' blocks (slab layout), the slot node ids and a macroscale-strain response.
+  // Static part of the general rows.  tri3 / tet4: every general node gets one, holding its cut
+  // and uncut elements' volumetric blocks (every bulk law is linear elastic, so these do not
+  // depend on the state; k_general_static forms them once), and an assembly adds only the
+  // cohesive blocks.  quad4: only the general nodes with cut adjacent elements, sorted first, so
+  // they form the prefix [0, n_stat).  Each gets its neighbour slots' blocks (slab layout), the
+  // slot node ids and a macroscale-strain response.
   {
     const int nv = (dim == 2) ? 3 : 6;
+    const bool full_static = s.etype != pg::QUAD4;
     int n_stat = 0;
     for (size_t i = 0; i < slow.size(); ++i) {
       const int4 gd = gdesc[i];
@@ -705,6 +712,7 @@ int pg_upload(pg_ctx* c) {
       if (has_cut && (int)i != n_stat) return set_err(c, PG_ERR_STATE, "internal: general nodes next to cut elements are not a prefix");
       if (has_cut) ++n_stat;
     }
+    if (full_static) n_stat = (int)slow.size();
     std::vector<int> stat_off(n_stat + 1, 0), stat_node;
     for (int i = 0; i < n_stat; ++i) {
       const int4 gd = gdesc[i];
@@ -720,10 +728,10 @@ int pg_upload(pg_ctx* c) {
     PG_TRY(dalloc(c, (size_t)n_stat * dim * nv, &dsg));
     P.stat = dst;
     P.stat_g = dsg;
-    // Block-parallel general rows (pg_general.cuh; tri3 / tet4): the records of the uncut
-    // elements adjacent to general nodes, one block per (general node, neighbour slot) with its
-    // static index and its cohesive and uncut contributions in adjacency order, and per node the
-    // residual lists
+    // Block-parallel general rows (pg_general.cuh; tri3 / tet4): one block per (general node,
+    // neighbour slot) with its static index and its cohesive contributions in adjacency order,
+    // and per node the traction list; the uncut elements are in the static image, so the record
+    // and uncut lists stay empty
     if (s.etype != pg::QUAD4) {
       const int D2 = dim * dim;
       std::vector<int> rec_of(s.ne, -1);
@@ -753,7 +761,7 @@ int pg_upload(pg_ctx* c) {
             }
             const int toff = kc_off_h[ce] + nh * nh * D2 + (n1 % nh) * dim;
             tl.push_back(toff * 2 + ((n1 >= nh) ? 0 : 1));
-          } else {
+          } else if (!full_static) {
             const int e = ad.x;
             if (rec_of[e] < 0) {
               rec_of[e] = (int)grec_nodes.size();
@@ -808,6 +816,14 @@ int pg_upload(pg_ctx* c) {
       for (double* p : {dke, dg}) pg_untrack_free(c, p);
       P.ke = nullptr;
       P.gmac = nullptr;
+    } else if (full_static && n_stat > 0) {
+      // no cut elements: the image holds the uncut elements alone
+      if (dim == 2) pgl::general_static<2>(c, P, dst, dsg);
+      else pgl::general_static<3>(c, P, dst, dsg);
+      int herr = 0;
+      cudaMemcpyAsync(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->up);
+      if (cudaStreamSynchronize(c->up) != cudaSuccess) return set_err(c, PG_ERR_DEVICE, "general-row set-up kernel failed");
+      if (herr) return set_err(c, PG_ERR_NONFINITE, "non-finite general-row stiffness at set-up");
     }
   }
   return pg_alloc_sync(c);

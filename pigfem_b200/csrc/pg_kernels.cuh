@@ -625,10 +625,12 @@ __global__ void __launch_bounds__(128) k_rows_general_resid(DevProblem P) {
   if (gdof < P.n_free) P.Pf[gdof] = mine; else P.Pp[gdof - P.n_free] = mine;
 }
 
-// Set-up: the static part of the general rows next to cut elements (one thread per such node):
-// each cut entry's volumetric block row (K_vol, from k_cut_volumetric) added into the node's
-// neighbour slots and its macroscale-strain response into the node's sum, in entry order.  The
-// entries are cut-first, so the walk stops at the first uncut one.  stat and stat_g start at zero.
+// Set-up: the static part of the general rows (one thread per node of the image): each cut
+// entry's volumetric block row (K_vol, from k_cut_volumetric) added into the node's neighbour
+// slots and its macroscale-strain response into the node's sum, in entry order; in tri3 / tet4
+// meshes the uncut elements' block rows and responses follow (every bulk law is linear elastic,
+// so they do not depend on the state either), while quad4 meshes stop at the first uncut entry
+// (the entries are cut-first).  stat and stat_g start at zero.
 template <int DIM>
 __global__ void __launch_bounds__(128) k_general_static(DevProblem P, double* stat, double* stat_g) {
   constexpr int NV = (DIM == 2) ? 3 : 6;
@@ -643,7 +645,29 @@ __global__ void __launch_bounds__(128) k_general_static(DevProblem P, double* st
     const int4 ad = __ldg(&P.adesc[gd.x + e]);
     const int4 ax = __ldg(&P.aresd[gd.x + e]);
     const int la = ad.y & 255, mn = ad.y >> 8;
-    if (mn == 0) break;
+    if (mn == 0) {
+      // uncut simplex (tri3 / tet4 meshes: every general node's image holds its uncut elements
+      // too): the block row la, w B_la^T D B_b for each element node b, and the macroscale
+      // response w B_la^T D -- the products of simplex_block, once per mesh
+      if (P.npe != DIM + 1) break;
+      constexpr int NPE = DIM + 1;
+      const int nd[4] = {ax.x, ax.y, ax.z, ax.w};
+      double x[NPE][DIM], g[NPE][DIM], J;
+      for (int n = 0; n < NPE; ++n) load_node<DIM>(P.X, nd[n], x[n]);
+      simplex_geom<DIM, double>(x, g, &J);
+      const double wgt = J * ((DIM == 2) ? tri4_wsum() : tet5_wsum());
+      const double* D = P.Dd + ad.w * 36;
+      for (int q = 0; q < DIM; ++q) {
+        double part[NV];
+        bt_d_row<DIM, double>(D, g[la], q, part);
+        for (int b = 0; b < NPE; ++b) {
+          double* o = S + (size_t)((ad.z >> (8 * b)) & 255) * D2;
+          for (int q2 = 0; q2 < DIM; ++q2) o[q * DIM + q2] += wgt * part_b<DIM, double>(part, g[b], q2);
+        }
+        for (int v = 0; v < NV; ++v) Gs[q * NV + v] += wgt * part[v];
+      }
+      continue;
+    }
     const int cc = ax.x;
     const double* kr = P.ke + __ldg(&P.ke_off[cc]) + (size_t)la * mn * D2;   // block row la of K_vol
     for (int b = 0; b < mn; ++b) {

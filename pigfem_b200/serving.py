@@ -20,7 +20,9 @@ Pipeline (all stages run at once on different requests):
 1. set-up workers (host threads) run the IGFEM set-up of each arrived request: its per-node and
    per-element passes (detection, enrichment nodes, standard DOF numbering) on the device, on a
    stream of their own, and the cut elements' tables and the CSR pattern in C++
-   (pg_create_prep_device; ctypes releases the GIL, so they run in parallel on the host cores);
+   (pg_create_prep_device with PG_PREP_NODES: the device pattern's sorts would compete with the
+   admitted requests' work; ctypes releases the GIL, so the workers run in parallel on the host
+   cores);
 2. the admission controller admits set-up requests in arrival order while the sum of the device
    bytes of the admitted requests stays within the budget and a GPU slot is free -- a request
    that arrives while others are on the GPU is admitted as soon as slots and memory free up.  A
@@ -293,7 +295,7 @@ class ServingEngine:
                 ready.put((req, None, r))
                 return
             try:
-                P = capi.Problem(req.desc, device=False, prep_device=self.prep_device)
+                P = capi.Problem(req.desc, device=False, prep_device=self.prep_device, prep_pattern=False)
             except capi.PigfemError as e:
                 r.error = str(e)
                 r.done = now()

@@ -1,8 +1,9 @@
 """Device IGFEM preprocessing (pg_create_prep_device) against the host set-up (pg_create_host).
 
 The device passes -- node detection, the element pass of the cut detection, the enrichment nodes
-with their intersection points, and the standard nodes' DOF numbering -- feed the rest of the
-set-up, so every table of the two set-ups must agree: integer tables (detection values, element
+with their intersection points, the standard nodes' DOF numbering, and (PG_PREP_PATTERN) the DOF
+nodes' adjacency and the CSR pattern -- replace the host's own loops, so every table of the two
+set-ups must agree: integer tables (detection values, element
 materials, cut elements, enrichment edges, sub-element and cohesive topology, DOF numbers, the
 four CSR patterns) bit-exact, and the coordinates and quadrature data too (the device passes are
 compiled without floating-point contraction and form every value with the host's operations).
@@ -22,10 +23,10 @@ TABLES = ("node_detect", "elem_mat", "cut_of", "cut_elem", "enr_edge", "enr_incl
           "cqp_wgt", "cqp_isv", "dn_node", "dn_nbr_off", "dn_nbr", "dn_adj_off", "dn_adj")
 
 
-def both(desc):
+def both(desc, pattern=True):
     from pigfem_b200 import capi
     H = capi.Problem(desc, device=False)
-    D = capi.Problem(desc, device=False, prep_device=True)
+    D = capi.Problem(desc, device=False, prep_device=True, prep_pattern=pattern)
     return H, D
 
 
@@ -53,6 +54,9 @@ def test_device_prep_matches_host_setup(name):
     from pigfem_b200 import capi
     H, D = both(capi.ProblemDesc(**spec_kwargs(CASES[name])))
     assert_same_setup(H, D)
+    # the per-node passes alone (PG_PREP_NODES, the pattern on the host threads)
+    _, D1 = both(capi.ProblemDesc(**spec_kwargs(CASES[name])), pattern=False)
+    assert_same_setup(H, D1)
     n = CASES[name]["n"]
     if min(n) >= 2:
         assert D.prep_device_ms() >= 0.0
