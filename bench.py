@@ -153,13 +153,12 @@ def general_kernel_bytes(P, fp32: bool) -> float:
 
 def launches_per_step(P, three_d: bool = False) -> int:
     """Kernels one step launches (the L2 flush between steps is a torch fill, not counted).  An
-    assembly: k_gen_first (cohesive elements and the general rows' element records), the tiles
-    of the structured rows, k_gen_rows (the general rows), each only when it has work.  The 3D
-    step adds the multi-strain residual pass: its cohesive elements, structured rows and general
-    rows."""
+    assembly: k_gen_first (the cohesive elements), the tiles of the structured rows, k_gen_rows
+    (the general rows), each only when it has work.  The 3D step adds the multi-strain residual
+    pass: its cohesive elements, structured rows and general rows."""
     s = P.sizes
     fast, slow = len(P.debug("fast_dn")) > 0, len(P.debug("slow_dn")) > 0
-    n = int(s["n_coh_qp"] > 0 or slow) + int(fast) + int(slow)
+    n = int(s["n_coh_qp"] > 0) + int(fast) + int(slow)
     if three_d:
         n += int(s["n_coh_qp"] > 0) + int(fast) + int(slow)
     return n

@@ -94,8 +94,8 @@ __global__ void __launch_bounds__(256) k_batch_stencil(const BatchItem* __restri
 }
 
 // The block-parallel general rows (pg_general.cuh) of every context: chunk = {context, first
-// item, count <= 128, pass} with pass 0 records, 1 blocks, 2 residuals; the passes are three
-// launches in that order.
+// item, count <= 128, pass} with pass 1 blocks, 2 residuals (pass 0, element records, has no
+// chunks: the general rows read their static image); the passes are launches in that order.
 template <int DIM>
 __global__ void __launch_bounds__(128) k_batch_gen(const BatchItem* __restrict__ items, const int4* __restrict__ chunks,
                                                   int n_chunks) {
@@ -109,8 +109,7 @@ __global__ void __launch_bounds__(128) k_batch_gen(const BatchItem* __restrict__
     }
     if ((int)threadIdx.x >= ch.z) continue;
     const int k = ch.y + threadIdx.x;
-    if (ch.w == 0) pgd::gen_record<DIM>(P, k);
-    else if (P.flags & pgd::FLAG_JAC) pgd::gen_block<DIM>(P, k);
+    if (ch.w == 1 && (P.flags & pgd::FLAG_JAC)) pgd::gen_block<DIM>(P, k);
   }
 }
 
@@ -184,7 +183,7 @@ int build_chunks(pg_batch* b) {
     for (int f = 0; f < c->P.n_coh_el; f += coh_chunk)
       coh.push_back(make_int4(i, f, std::min(coh_chunk, c->P.n_coh_el - f), 0));
     for (int tl = 0; tl < c->n_tiles; ++tl) sten.push_back(make_int4(i, tl, 1, 0));
-    const int ng[3] = {c->P.n_grec, c->P.n_gblk, c->P.n_slow_dn};
+    const int ng[3] = {0, c->P.n_gblk, c->P.n_slow_dn};
     for (int pass = 0; pass < 3; ++pass)
       for (int f = 0, per = (pass == 2) ? 128 / pgd::kGenResidLanes : 128; f < ng[pass]; f += per)
         gen[pass].push_back(make_int4(i, f, std::min(per, ng[pass] - f), pass));

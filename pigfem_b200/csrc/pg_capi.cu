@@ -730,76 +730,46 @@ int pg_upload(pg_ctx* c) {
     P.stat_g = dsg;
     // Block-parallel general rows (pg_general.cuh; tri3 / tet4): one block per (general node,
     // neighbour slot) with its static index and its cohesive contributions in adjacency order,
-    // and per node the traction list; the uncut elements are in the static image, so the record
-    // and uncut lists stay empty
+    // and per node the traction list (the uncut elements are in the static image)
     if (s.etype != pg::QUAD4) {
       const int D2 = dim * dim;
-      std::vector<int> rec_of(s.ne, -1);
-      std::vector<int4> grec_nodes;
-      std::vector<int> grec_mat;
       std::vector<int4> gblk;
-      std::vector<int> gblk_cl(1, 0), gcl, gul, tl_off(1, 0), tl, ul_off(1, 0), ulist;
-      std::vector<std::vector<int>> bcl, bul;
+      std::vector<int> gblk_cl(1, 0), gcl, tl_off(1, 0), tl;
+      std::vector<std::vector<int>> bcl;
       for (size_t i = 0; i < slow.size(); ++i) {
         const int4 gd = gdesc[i];
         bcl.assign(gd.w, std::vector<int>());
-        bul.assign(gd.w, std::vector<int>());
         for (int k = gd.x; k < gd.x + gd.y; ++k) {
           const int4 ad = adesc[k], ax = aresd[k];
-          const int la = ad.y & 255, mn = ad.y >> 8;
-          if (mn > 0) {
-            const int cpa = ax.z;
-            if (cpa < 0) continue;
-            const int ce = cpa >> 5, n1 = cpa & 31, nh = s.coh_nh[ce];
-            for (int b = 0; b < mn; ++b) {
-              const int cpb = cohpos_h[ax.y + b];
-              if (cpb < 0 || (cpb >> 5) != ce) continue;
-              const int n2 = cpb & 31;
-              const int off = kc_off_h[ce] + ((n1 % nh) * nh + (n2 % nh)) * D2;
-              const int neg = ((n1 >= nh) == (n2 >= nh)) ? 0 : 1;
-              bcl[slots[ad.z + b]].push_back(off * 2 + neg);
-            }
-            const int toff = kc_off_h[ce] + nh * nh * D2 + (n1 % nh) * dim;
-            tl.push_back(toff * 2 + ((n1 >= nh) ? 0 : 1));
-          } else if (!full_static) {
-            const int e = ad.x;
-            if (rec_of[e] < 0) {
-              rec_of[e] = (int)grec_nodes.size();
-              grec_nodes.push_back(ax);
-              grec_mat.push_back(ad.w);
-            }
-            const int r = rec_of[e];
-            if (r >= (1 << 26)) return set_err(c, PG_ERR_UNSUPPORTED, "too many general-row elements");
-            for (int b = 0; b < s.npe; ++b) bul[(ad.z >> (8 * b)) & 255].push_back(r * 16 + la * 4 + b);
-            ulist.push_back(r * 4 + la);
+          const int mn = ad.y >> 8;
+          if (mn == 0) continue;   // uncut: in the static image
+          const int cpa = ax.z;
+          if (cpa < 0) continue;
+          const int ce = cpa >> 5, n1 = cpa & 31, nh = s.coh_nh[ce];
+          for (int b = 0; b < mn; ++b) {
+            const int cpb = cohpos_h[ax.y + b];
+            if (cpb < 0 || (cpb >> 5) != ce) continue;
+            const int n2 = cpb & 31;
+            const int off = kc_off_h[ce] + ((n1 % nh) * nh + (n2 % nh)) * D2;
+            const int neg = ((n1 >= nh) == (n2 >= nh)) ? 0 : 1;
+            bcl[slots[ad.z + b]].push_back(off * 2 + neg);
           }
+          const int toff = kc_off_h[ce] + nh * nh * D2 + (n1 % nh) * dim;
+          tl.push_back(toff * 2 + ((n1 >= nh) ? 0 : 1));
         }
         for (int k = 0; k < gd.w; ++k) {
-          const int stat_idx = (int)i < n_stat ? stat_off[i] + k : -1;
-          gblk.push_back(make_int4((int)i, k, stat_idx, (int)gul.size()));
+          gblk.push_back(make_int4((int)i, k, stat_off[i] + k, 0));
           gcl.insert(gcl.end(), bcl[k].begin(), bcl[k].end());
-          gul.insert(gul.end(), bul[k].begin(), bul[k].end());
           gblk_cl.push_back((int)gcl.size());
         }
         tl_off.push_back((int)tl.size());
-        ul_off.push_back((int)ulist.size());
       }
-      gblk.push_back(make_int4(-1, 0, -1, (int)gul.size()));   // sentinel: the end of the last block's list
-      P.n_grec = (int)grec_nodes.size();
-      P.n_gblk = (int)gblk.size() - 1;
-      PG_TRY(upload(c, grec_nodes, &P.grec_nodes));
-      PG_TRY(upload(c, grec_mat, &P.grec_mat));
-      double* dgr = nullptr;
-      PG_TRY(dalloc(c, (size_t)P.n_grec * (size_t)(dim == 2 ? pgd::gen_fields<2>() : pgd::gen_fields<3>()), &dgr));
-      P.grec = dgr;
+      P.n_gblk = (int)gblk.size();
       PG_TRY(upload(c, gblk, &P.gblk));
       PG_TRY(upload(c, gblk_cl, &P.gblk_cl));
       PG_TRY(upload(c, gcl, &P.gcl));
-      PG_TRY(upload(c, gul, &P.gul));
       PG_TRY(upload(c, tl_off, &P.gnode_tl_off));
       PG_TRY(upload(c, tl, &P.gnode_tl));
-      PG_TRY(upload(c, ul_off, &P.gnode_ul_off));
-      PG_TRY(upload(c, ulist, &P.gnode_ul));
     }
     c->stat_doubles = (long long)stat_off[n_stat] * dim * dim + (long long)n_stat * dim * nv;
     if (s.ncut > 0) {

@@ -90,18 +90,13 @@ struct DevProblem {
   const int* tile_elem_off; const int* tile_elems; int tile_max_elems;  // elements each tile of fast nodes touches
   const uint16_t* adj_local;                     // tile-local index of each adjacency entry's element
   const int* slow_dn; int n_slow_dn;             // the remaining DOF nodes
-  // Block-parallel general rows (pg_general.cuh; tri3 / tet4 meshes).  Records: the uncut elements
-  // adjacent to general nodes, formed once per assembly (record r at grec[r * GenRec::STRIDE]:
-  // the NPE x DIM gradients, J W, the NV stresses, the material).  Blocks: one per (general node,
-  // neighbour slot), node-major: {node, slot, static index or -1, first uncut contribution}; its
-  // cohesive contributions [gblk_cl[b], gblk_cl[b + 1]) as (kcoh offset << 1 | negative), its
-  // uncut contributions [gblk[b].w, gblk[b + 1].w) as (record << 4 | la << 2 | lb), both in
-  // adjacency order.  Per general node the residual lists: tractions (kcoh offset << 1 | negative)
-  // and uncut entries (record << 2 | la), in adjacency order.
-  int n_grec, n_gblk;
-  const int4* grec_nodes; const int* grec_mat; double* grec;
-  const int4* gblk; const int* gblk_cl; const int* gcl; const int* gul;
-  const int* gnode_tl_off; const int* gnode_tl; const int* gnode_ul_off; const int* gnode_ul;
+  // Block-parallel general rows (pg_general.cuh; tri3 / tet4 meshes): one block per (general
+  // node, neighbour slot), node-major: {node, slot, static index, -}; its cohesive contributions
+  // [gblk_cl[b], gblk_cl[b + 1]) as (kcoh offset << 1 | negative) in adjacency order; per general
+  // node the residual's traction list (kcoh offset << 1 | negative), in adjacency order.
+  int n_gblk;
+  const int4* gblk; const int* gblk_cl; const int* gcl;
+  const int* gnode_tl_off; const int* gnode_tl;
   int maxnb_general;                             // slab slots per node in k_rows_general
   const int4* gdesc; const int* growd; const int4* adesc; const int4* aresd;  // k_rows_general descriptors
   // cohesive points

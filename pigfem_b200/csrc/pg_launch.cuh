@@ -48,8 +48,7 @@ void assembly(pg_ctx* c, const pgd::DevProblem& P, bool jac, bool fp32) {
   cudaStream_t sst = (DIM == 2) ? c->side : c->stream;
   {
     const int coh_blocks = (P.n_coh_el > 0) ? blocks_of((long long)P.n_coh_el * pgd::CohLanes<DIM>::CQ) : 0;
-    const int rec_blocks = (simplex_general && P.n_grec > 0) ? blocks_of(P.n_grec) : 0;
-    if (coh_blocks + rec_blocks > 0) pgd::k_gen_first<DIM><<<coh_blocks + rec_blocks, 128, 0, gst>>>(P, coh_blocks);
+    if (coh_blocks > 0) pgd::k_gen_first<DIM><<<coh_blocks, 128, 0, gst>>>(P);
   }
   // (the timing event between the cohesive/record kernel and the general rows is recorded only
   // when timing: an event between them would hold back the general rows' early start)
@@ -158,10 +157,7 @@ void residual_cases(pg_ctx* c, const pgd::DevProblem& P) {
     pgd::k_rows_stencil_cases<DIM><<<grid, 128, 0, c->stream>>>(P, c->grid, c->stencil, c->n_stencil);
   }
   if (P.n_slow_dn > 0) {
-    // the general rows' element records with the strain of U (formed once for every case),
-    // then a lane group per general node sums each case's residual as the single-strain
-    // assembly does
-    if (P.n_grec > 0) pgd::k_gen_records_strain<DIM><<<(P.n_grec + 127) / 128, 128, 0, c->stream>>>(P);
+    // a lane group per general node sums each case's residual as the single-strain assembly does
     const int grid = (int)(((long long)P.n_slow_dn * pgd::kGenResidLanes + 127) / 128);
     pgd::k_gen_resid_cases<DIM><<<grid, 128, 0, c->stream>>>(P);
   }
