@@ -17,7 +17,10 @@
 //   DOF numbering       DofObject::set_local_owned_normal_dofs (src/DofObject.cpp:336-385) for the
 //                       standard nodes of the structured grid: free DOFs in node order, the
 //                       constrained ones numbered apart, both in closed form from the node's grid
-//                       position (the Dirichlet or periodic conditions of Tests/Main.cpp:549-581).
+//                       position (the Dirichlet or periodic conditions of Tests/Main.cpp:549-581);
+//   pattern             (device_pattern, at the end of this file) the DOF nodes' adjacency, their
+//                       sorted neighbours and the four CSR patterns (Solver::preallocate_matrix,
+//                       src/Solver.cpp:426-490, 772-896), from sorted 64-bit keys.
 //
 // This file is compiled without floating-point contraction (-fmad=false), so every coordinate,
 // level-set value and root iterate is formed with the same IEEE operations, in the same order, as
